@@ -1,0 +1,153 @@
+"""ctypes binding of libfysics_b200.so (include/fysics_b200.h).
+
+The shared library is the product: every call below runs hand-written sm_100a kernels.
+There is no Python or CPU fallback -- if the library is missing, import fails loudly, and
+without a CUDA device every entry point returns FY_ENODEV.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libfysics_b200.so"
+
+FY_OK, FY_EINVAL, FY_ENOMEM, FY_ECUDA, FY_ENODEV = 0, 1, 2, 3, 4
+FY_EUNSUPPORTED, FY_ETIMEDOUT, FY_EBUSY, FY_EDEGENERATE = 5, 6, 7, 8
+
+
+class Physics(C.Structure):
+    """fy_physics (fysics.h:23-35): 8 doubles."""
+    _fields_ = [("delta_beta", C.c_double), ("energy_kev", C.c_double),
+                ("distance_mm", C.c_double), ("pixel_um", C.c_double),
+                ("unsharp_sigma", C.c_double), ("unsharp_coeff", C.c_double),
+                ("psf_sigma_vox", C.c_double), ("psf_sigma_z_vox", C.c_double)]
+
+
+class NoiseModel(C.Structure):
+    """fy_noise_model (fysics.h:191-197)."""
+    _fields_ = [("g", C.c_double), ("b", C.c_double), ("noise_ref", C.c_double),
+                ("ref_intensity", C.c_double), ("n_bins_used", C.c_int)]
+
+
+class Dering(C.Structure):
+    """fy_dering (fysics.h:406-415)."""
+    _fields_ = [("Z", C.c_long), ("Y", C.c_long), ("X", C.c_long),
+                ("cy", C.c_double), ("cx", C.c_double),
+                ("slab_z", C.c_int), ("nslab", C.c_int), ("ns", C.c_int), ("nr", C.c_int),
+                ("sum", C.POINTER(C.c_float)), ("cnt", C.POINTER(C.c_uint)),
+                ("ring", C.POINTER(C.c_float)), ("have_rings", C.c_int)]
+
+
+_P = C.c_void_p
+_i, _l, _d, _f, _sz = C.c_int, C.c_long, C.c_double, C.c_float, C.c_size_t
+_PP = C.POINTER(Physics)
+_PN = C.POINTER(NoiseModel)
+_PD = C.POINTER(Dering)
+_PDBL = C.POINTER(C.c_double)
+
+# name -> (restype, argtypes): every symbol declared in include/fysics_b200.h
+SIGNATURES = {
+    "fy_is_pow2": (_i, [_i]),
+    "fy_next_pow2": (_i, [_i]),
+    "fy_next_fft_size": (_i, [_i]),
+    "fy_fft1d": (None, [_P, _P, _i, _i]),
+    "fy_fft3d": (None, [_P, _P, _i, _i, _i, _i]),
+    "fy_fft3d_normalize": (None, [_P, _P, _i, _i, _i]),
+    "fy_u8_to_float": (None, [_P, _P, _sz]),
+    "fy_float_to_u8": (None, [_P, _P, _sz]),
+    "fy_u8_to_phys": (None, [_P, _P, _sz, _d, _d]),
+    "fy_phys_to_u8": (None, [_P, _P, _sz, _d, _d]),
+    "fy_phys_to_u8_level": (_f, [_d, _d, _d]),
+    "fy_paganin_transfer": (_d, [_d, _PP]),
+    "fy_unsharp_transfer": (_d, [_d, _PP]),
+    "fy_recon_transfer": (_d, [_d, _PP]),
+    "fy_auto_reg": (_d, [_PP, _d]),
+    "fy_auto_deltabeta_scale": (_d, [_PP]),
+    "fy_kernel_halo": (_i, [_PP]),
+    "fy_deconvolve": (_i, [_P, _P, _i, _i, _i, _PP, _d]),
+    "fy_deconvolve_matched": (_i, [_P, _P, _i, _i, _i, _PP, _d]),
+    "fy_guided_denoise": (_i, [_P, _P, _i, _i, _i, _i, _d]),
+    "fy_guided_denoise_ws": (_i, [_P, _P, _i, _i, _i, _i, _d, _P]),
+    "fy_guided_ws_floats": (_sz, [_i, _i, _i]),
+    "fy_guided_denoise_fast_ws": (_i, [_P, _P, _i, _i, _i, _i, _d, _i, _P]),
+    "fy_box_smooth": (None, [_P, _P, _P, _i, _i, _i, _i]),
+    "fy_guided_eps_for_noise": (_d, [_d]),
+    "fy_estimate_noise": (_i, [_P, _i, _i, _i, _i, _d, _d, _PN]),
+    "fy_dering_init": (_i, [_PD, _l, _l, _l, _d, _d, _i, _i]),
+    "fy_dering_free": (None, [_PD]),
+    "fy_dering_tile_init": (_i, [_PD, _PD]),
+    "fy_dering_tile_reset": (None, [_PD]),
+    "fy_dering_accumulate_u8": (None, [_PD, _P, _l, _l, _l, _l, _l, _i]),
+    "fy_dering_merge_tile": (None, [_PD, _i, _PD]),
+    "fy_dering_finalize": (_l, [_PD, _i, C.c_uint, _d, _d]),
+    "fy_dering_apply": (None, [_PD, _P, _l, _l, _l, _l, _l, _l, _d]),
+    "fy_phase_correlate": (_i, [_P, _P, _i, _i, _i, _PDBL, _PDBL, _i]),
+    # ---- fy_gpu_* extension
+    "fy_gpu_init": (_i, [_i]),
+    "fy_gpu_last_status": (_i, []),
+    "fy_gpu_last_error": (C.c_char_p, []),
+    "fy_gpu_release": (None, []),
+    "fy_gpu_kernel_launches": (C.c_ulonglong, []),
+    "fy_gpu_u8_to_phys": (_i, [_P, _P, _sz, _d, _d, _P]),
+    "fy_gpu_phys_to_u8": (_i, [_P, _P, _sz, _d, _d, _P]),
+    "fy_gpu_deconvolve_ex": (_i, [_P, _i, _d, _d, _P, _i, _i, _i, _PP, _d, _i, _d, _P]),
+    "fy_gpu_guided": (_i, [_P, _P, _i, _i, _i, _i, _d, _i, _P]),
+    "fy_gpu_guided_scratch_bytes": (_sz, [_i, _i, _i, _i, _i]),
+    "fy_gpu_noise_scratch_bytes": (_sz, [_i, _i, _i]),
+    "fy_gpu_estimate_noise": (_i, [_P, _i, _i, _i, _i, _d, _d, _P, _P]),
+    "fy_gpu_noise_model": (_i, [_P, _i, _i, _i, _PN, _P]),
+    "fy_gpu_noise_eps": (_P, [_P, _i, _i, _i]),
+    "fy_gpu_dering_create": (_i, [C.POINTER(_P), _l, _l, _l, _d, _d, _i, _i]),
+    "fy_gpu_dering_destroy": (None, [_P]),
+    "fy_gpu_dering_reset": (_i, [_P, _P]),
+    "fy_gpu_dering_accumulate_u8": (_i, [_P, _P, _l, _l, _l, _l, _l, _l, _i, _P]),
+    "fy_gpu_dering_finalize": (_i, [_P, _i, C.c_uint, _d, _d, _P]),
+    "fy_gpu_dering_apply": (_i, [_P, _P, _l, _l, _l, _l, _l, _l, _d, _P]),
+    "fy_gpu_dering_download": (_i, [_P, _PD, C.POINTER(_l), _P]),
+}
+
+_lib = None
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Load the CUDA library (once). Raises if it was not built: no fallback exists."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise ImportError(f"{p} is missing: build it with `python -m fysics_b200.build` "
+                          "(fysics_b200 has no CPU fallback)")
+    lib = C.CDLL(str(p), mode=C.RTLD_LOCAL)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class FysicsError(RuntimeError):
+    def __init__(self, rc: int, where: str):
+        msg = load().fy_gpu_last_error()
+        super().__init__(f"{where} failed with status {rc}: {msg.decode() if msg else ''}")
+        self.rc = rc
+
+
+def check(rc: int, where: str) -> int:
+    if rc != 0:
+        raise FysicsError(rc, where)
+    return rc
+
+
+def check_void(where: str) -> None:
+    """For void entry points: raise if the call recorded a failure."""
+    lib = load()
+    st = lib.fy_gpu_last_status()
+    if st != 0:
+        raise FysicsError(st, where)

@@ -1,0 +1,148 @@
+// fy_context.cu -- per-thread CUDA state, error reporting and shared twiddle tables.
+#include "fy_context.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <map>
+#include <mutex>
+#include <vector>
+
+namespace fy {
+
+cudaError_t DevBuf::ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    if (p) { cudaFree(p); p = nullptr; cap = 0; }
+    if (!bytes) return cudaSuccess;
+    size_t want = bytes + (bytes >> 4);        // 6% slack for slowly growing sizes
+    want = (want + 255) & ~(size_t)255;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) { p = nullptr; cap = 0; cudaGetLastError(); return e; }
+    cap = want;
+    return cudaSuccess;
+}
+void DevBuf::release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+
+cudaError_t HostBuf::ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    if (p) { cudaFreeHost(p); p = nullptr; cap = 0; }
+    if (!bytes) return cudaSuccess;
+    cudaError_t e = cudaMallocHost(&p, bytes);
+    if (e != cudaSuccess) { p = nullptr; cap = 0; cudaGetLastError(); return e; }
+    cap = bytes;
+    return cudaSuccess;
+}
+void HostBuf::release() { if (p) cudaFreeHost(p); p = nullptr; cap = 0; }
+
+static thread_local ThreadCtx t_ctx;
+ThreadCtx& ctx() { return t_ctx; }
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_ctx.status = code;
+    t_ctx.err = buf;
+    return code;
+}
+
+int fail_cuda(cudaError_t e, const char* what) {
+    const int code = (e == cudaErrorMemoryAllocation) ? FY_ENOMEM : FY_ECUDA;
+    return fail(code, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+static int init_device(int device) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        return fail(FY_ENODEV, "no CUDA device available (%s); fysics_b200 has no CPU fallback",
+                    e != cudaSuccess ? cudaGetErrorString(e) : "device count 0");
+    }
+    if (device < 0 || device >= n) return fail(FY_EINVAL, "device %d out of range [0,%d)", device, n);
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return fail_cuda(e, "cudaSetDevice");
+    ThreadCtx& c = t_ctx;
+    if (c.st && c.dev != device) {          // switching devices: drop the old state
+        cudaStreamDestroy(c.st); c.st = nullptr;
+        if (c.ws_done) { cudaEventDestroy(c.ws_done); c.ws_done = nullptr; }
+    }
+    c.dev = device;
+    cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, device);
+    if (!c.st && (e = cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail_cuda(e, "cudaStreamCreate");
+    if (!c.ws_done && (e = cudaEventCreateWithFlags(&c.ws_done, cudaEventDisableTiming)) != cudaSuccess)
+        return fail_cuda(e, "cudaEventCreate");
+    return FY_OK;
+}
+
+int ensure_ctx() {
+    ThreadCtx& c = t_ctx;
+    if (c.dev >= 0 && c.st) {
+        int cur = -1;
+        if (cudaGetDevice(&cur) == cudaSuccess && cur == c.dev) return FY_OK;
+        cudaError_t e = cudaSetDevice(c.dev);
+        return e == cudaSuccess ? FY_OK : fail_cuda(e, "cudaSetDevice");
+    }
+    int dev = 0;
+    if (const char* s = getenv("FY_DEVICE")) dev = atoi(s);
+    return init_device(dev);
+}
+
+void ws_acquire(cudaStream_t s) {
+    ThreadCtx& c = t_ctx;
+    if (c.ws_pending) cudaStreamWaitEvent(s, c.ws_done, 0);
+}
+void ws_release(cudaStream_t s) {
+    ThreadCtx& c = t_ctx;
+    if (cudaEventRecord(c.ws_done, s) == cudaSuccess) c.ws_pending = true;
+}
+
+bool is_pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Twiddles are generated in FP64 and rounded once (fft.c:47-61 does the same).
+const float2* twiddles(int n) {
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, float2*> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find({dev, n});
+    if (it != cache.end()) return it->second;
+    std::vector<float2> h((size_t)n);
+    const double step = 2.0 * 3.14159265358979323846 / (double)n;
+    for (int m = 0; m < n; ++m) h[(size_t)m] = make_float2((float)cos(step * m), (float)sin(step * m));
+    float2* d = nullptr;
+    if (cudaMalloc(&d, sizeof(float2) * (size_t)n) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    if (cudaMemcpy(d, h.data(), sizeof(float2) * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d); cudaGetLastError(); return nullptr;
+    }
+    cache[{dev, n}] = d;
+    return d;
+}
+
+}  // namespace fy
+
+extern "C" {
+int fy_gpu_init(int device) {
+    fy::ThreadCtx& c = fy::ctx();
+    c.status = 0; c.err.clear();
+    return fy::init_device(device);
+}
+int fy_gpu_last_status(void) { return fy::ctx().status; }
+const char* fy_gpu_last_error(void) { return fy::ctx().err.c_str(); }
+unsigned long long fy_gpu_kernel_launches(void) { return fy::ctx().launches; }
+void fy_gpu_release(void) {
+    fy::ThreadCtx& c = fy::ctx();
+    if (c.st) cudaStreamSynchronize(c.st);
+    c.vin.release(); c.vout.release(); c.spec.release(); c.spec2.release();
+    c.aux.release(); c.aux2.release(); c.small.release();
+    c.pin.release(); c.pin2.release();
+    c.tab.buf.release(); c.tab.valid = false;
+}
+}

@@ -1,0 +1,312 @@
+// fy_deconv.cu -- fused half-spectrum Wiener deconvolution (fy_deconvolve /
+// fy_deconvolve_matched, paganin.c:152-342) as five HBM passes:
+//
+//   P1 X  : gather rows (u8 dewindow or f32) with reflect padding in x, two rows per
+//           complex FFT, untangle -> half-spectrum rows         (paganin.c:165-194)
+//   P2 Y  : forward over py for each stored z plane, reflect/zero rows gathered on load
+//   P3 Z  : forward over pz (reflected planes gathered on load), radial weight from the
+//           4096-entry LUT over u = f^2 with linear interpolation (paganin.c:212-244),
+//           inverse over pz, store only the z < nz planes that survive the crop
+//   P4 Y  : inverse for z < nz, store only rows y < ny          (paganin.c:254-260)
+//   P5 X  : two-for-one C2R of surviving rows, x 1/(pz*py*px), crop (paganin.c:262-289)
+//
+// Algorithmic traffic at p = n (no padding): P1 4+4 (1+4 from u8), P2 8, P3 8, P4 8,
+// P5 4+4 bytes per voxel.
+#include "fy_internal.h"
+
+namespace {
+constexpr int MAXNT = FY_FFT_MAXNT;
+// Threads per CTA never exceed W*n/E: 512 for 2^k lines (E=16), 256 for 3*2^k (E=24).
+template <int E> struct KB { static constexpr int nt = (E % 3 == 0) ? 256 : 512; };
+
+struct SrcF32 {
+    const float* p;
+    FY_D float at(size_t row, int x, int nx, float, float) const { return __ldg(p + row * nx + x); }
+};
+struct SrcU8 {
+    const uint8_t* p;
+    FY_D float at(size_t row, int x, int nx, float lo, float scale) const {
+        return __fmaf_rn((float)__ldg(p + row * nx + x), scale, lo);
+    }
+};
+
+// Thread -> (line l, thread-in-line tl) with the line index fastest.
+struct Lane {
+    int l, tl;
+    FY_D Lane(int wlog) : l(threadIdx.x & ((1 << wlog) - 1)), tl(threadIdx.x >> wlog) {}
+};
+
+// ---------------------------------------------------------------- P1
+// Rows q = z*ny + y (z < nz, y < ny) paired (2m, 2m+1) into one complex line; a CTA owns
+// W lines. Rows are staged through shared memory with x the fastest thread index, so
+// global reads are row-contiguous and every thread has E independent loads in flight.
+template <int E, class Src>
+__global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(Src src, float lo, float scale, float2* __restrict__ spec,
+                                                    SpecGeom g, const __grid_constant__ FftPlan pl,
+                                                    const float2* __restrict__ tw, int wlog, FastDiv dpx,
+                                                    FastDiv dhx) {
+    extern __shared__ float4 smem4[];
+    const int W = 1 << wlog, LP = W + 1;
+    float2* s = reinterpret_cast<float2*>(smem4);
+    float2* stw = s + pl.n * LP;
+    const long Q = (long)g.nz * g.ny;
+    const long q0 = (long)blockIdx.x * 2 * W;
+    load_twiddles(stw, tw, pl.n);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {                       // W*px = E*blockDim.x elements
+        const int idx = threadIdx.x + e * blockDim.x;
+        const int l = dpx.div(idx), x = idx - l * g.px;
+        const long qa = q0 + 2 * l, qb = qa + 1;
+        const int sx = x < g.nx ? x : (g.zero_pad ? -1 : reflect_idx(x, g.nx));
+        float a = 0.f, b = 0.f;
+        if (sx >= 0) {
+            if (qa < Q) a = src.at((size_t)qa, sx, g.nx, lo, scale);
+            if (qb < Q) b = src.at((size_t)qb, sx, g.nx, lo, scale);
+        }
+        s[x * LP + l] = make_float2(a, b);
+    }
+    __syncthreads();
+    const Lane ln(wlog);
+    line_fft<E>(s, LP, ln.l, ln.tl, pl, stw, -1.f,
+                [&](int i) { return s[i * LP + ln.l]; },
+                [&](int i, float2 v) { s[i * LP + ln.l] = v; });
+    __syncthreads();
+    const int tot = W * g.hx;
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+        const int l = dhx.div(idx), k = idx - l * g.hx;
+        const long qa = q0 + 2 * l, qb = qa + 1;
+        if (qa >= Q) continue;
+        const int mk = k == 0 ? 0 : g.px - k;
+        float2 A, B;
+        untangle(s[k * LP + l], s[mk * LP + l], A, B);
+        spec[((size_t)(qa / g.ny) * g.py + (qa % g.ny)) * g.hxp + k] = A;
+        if (qb < Q) spec[((size_t)(qb / g.ny) * g.py + (qb % g.ny)) * g.hxp + k] = B;
+    }
+}
+
+// ---------------------------------------------------------------- P2
+// CTA = (column tile of W half-spectrum columns, stored plane z). Pass-0 inputs come
+// straight from global memory (W consecutive columns = one 8W-byte run per point);
+// rows >= ny are the reflected (or zero) rows.
+template <int E>
+__global__ void __launch_bounds__(KB<E>::nt, 2) k_y_fwd(float2* __restrict__ spec, SpecGeom g, const __grid_constant__ FftPlan pl,
+                                                 const float2* __restrict__ tw, int wlog) {
+    extern __shared__ float4 smem4[];
+    const int W = 1 << wlog;
+    float2* s = reinterpret_cast<float2*>(smem4);
+    float2* stw = s + pl.n * W;
+    const Lane ln(wlog);
+    float2* col = spec + (size_t)blockIdx.y * g.py * g.hxp + blockIdx.x * W + ln.l;
+    load_twiddles(stw, tw, pl.n);
+    __syncthreads();
+    line_fft<E>(s, W, ln.l, ln.tl, pl, stw, -1.f,
+                [&](int i) {
+                    const int ys = i < g.ny ? i : (g.zero_pad ? -1 : reflect_idx(i, g.ny));
+                    return ys < 0 ? make_float2(0.f, 0.f) : col[(size_t)ys * g.hxp];
+                },
+                [&](int i, float2 v) { col[(size_t)i * g.hxp] = v; });
+}
+
+// ---------------------------------------------------------------- P3
+// CTA = (column tile, row y). Forward over z (reflected planes gathered on load), radial
+// LUT weight over the tile in shared memory, inverse over z, store z < nz.
+template <int E>
+__global__ void __launch_bounds__(KB<E>::nt, 2) k_z_weight(float2* __restrict__ spec, SpecGeom g,
+                                                       const __grid_constant__ FftPlan pl,
+                                                       const float2* __restrict__ tw,
+                                                       const float* __restrict__ lut,
+                                                       const double* __restrict__ fz2,
+                                                       const double* __restrict__ fy2,
+                                                       const double* __restrict__ fx2, double us, int wlog) {
+    extern __shared__ float4 smem4[];
+    const int W = 1 << wlog;
+    float2* s = reinterpret_cast<float2*>(smem4);
+    float2* stw = s + pl.n * W;
+    double* sfz = reinterpret_cast<double*>(stw + pl.n);
+    float* slut = reinterpret_cast<float*>(sfz + pl.n);
+    const Lane ln(wlog);
+    const int c0 = blockIdx.x * W;
+    const size_t zstride = (size_t)g.py * g.hxp;
+    float2* col = spec + (size_t)blockIdx.y * g.hxp + c0 + ln.l;
+    load_twiddles(stw, tw, pl.n);
+    for (int i = threadIdx.x; i < pl.n; i += blockDim.x) sfz[i] = fz2[i];
+    for (int i = threadIdx.x; i <= FY_LUT_N; i += blockDim.x) slut[i] = lut[i];
+    __syncthreads();
+    line_fft<E>(s, W, ln.l, ln.tl, pl, stw, -1.f,
+                [&](int i) {
+                    const int zs = i < g.nz ? i : (g.zero_pad ? -1 : reflect_idx(i, g.nz));
+                    return zs < 0 ? make_float2(0.f, 0.f) : col[(size_t)zs * zstride];
+                },
+                [&](int z, float2 v) { s[z * W + ln.l] = v; });
+    __syncthreads();
+    {   // weight: the same W-column slot for every element this thread touches
+        const int k = c0 + ln.l;
+        const double fyx = k < g.hx ? fy2[blockIdx.y] : 0.0;
+        const double fxx = k < g.hx ? __ldg(fx2 + k) : 0.0;
+        for (int z = ln.tl; z < pl.n; z += blockDim.x >> wlog) {
+            const double t = ((sfz[z] + fyx) + fxx) * us;    // paganin.c:234-236
+            int ti = (int)t;
+            if (ti >= FY_LUT_N) ti = FY_LUT_N - 1;
+            const float w = slut[ti] + (slut[ti + 1] - slut[ti]) * (float)(t - ti);
+            const float2 v = s[z * W + ln.l];
+            s[z * W + ln.l] = make_float2(v.x * w, v.y * w);
+        }
+    }
+    __syncthreads();
+    line_fft<E>(s, W, ln.l, ln.tl, pl, stw, +1.f,
+                [&](int i) { return s[i * W + ln.l]; },
+                [&](int z, float2 v) { if (z < g.nz) col[(size_t)z * zstride] = v; });
+}
+
+// ---------------------------------------------------------------- P4
+template <int E>
+__global__ void __launch_bounds__(KB<E>::nt, 2) k_y_inv(float2* __restrict__ spec, SpecGeom g, const __grid_constant__ FftPlan pl,
+                                                 const float2* __restrict__ tw, int keep_rows, int wlog) {
+    extern __shared__ float4 smem4[];
+    const int W = 1 << wlog;
+    float2* s = reinterpret_cast<float2*>(smem4);
+    float2* stw = s + pl.n * W;
+    const Lane ln(wlog);
+    float2* col = spec + (size_t)blockIdx.y * g.py * g.hxp + blockIdx.x * W + ln.l;
+    load_twiddles(stw, tw, pl.n);
+    __syncthreads();
+    line_fft<E>(s, W, ln.l, ln.tl, pl, stw, +1.f,
+                [&](int i) { return col[(size_t)i * g.hxp]; },
+                [&](int i, float2 v) { if (i < keep_rows) col[(size_t)i * g.hxp] = v; });
+}
+
+// ---------------------------------------------------------------- P5
+template <int E>
+__global__ void __launch_bounds__(KB<E>::nt, 2) k_x_inv(const float2* __restrict__ spec, float* __restrict__ dst,
+                                                    SpecGeom g, const __grid_constant__ FftPlan pl,
+                                                    const float2* __restrict__ tw, float invN, int wlog,
+                                                    FastDiv dnx, FastDiv dhx) {
+    extern __shared__ float4 smem4[];
+    const int W = 1 << wlog, LP = W + 1;
+    float2* s = reinterpret_cast<float2*>(smem4);
+    float2* stw = s + pl.n * LP;
+    const long Q = (long)g.nz * g.ny;
+    const long q0 = (long)blockIdx.x * 2 * W;
+    load_twiddles(stw, tw, pl.n);
+    const int hi_max = g.px - g.hx;                 // m in [1, px-hx] mirrors to px-m
+    const int tot = W * g.hx;
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+        const int l = dhx.div(idx), k = idx - l * g.hx;
+        const long qa = q0 + 2 * l, qb = qa + 1;
+        const float2 A = qa < Q ? spec[((size_t)(qa / g.ny) * g.py + (qa % g.ny)) * g.hxp + k] : make_float2(0.f, 0.f);
+        const float2 B = qb < Q ? spec[((size_t)(qb / g.ny) * g.py + (qb % g.ny)) * g.hxp + k] : make_float2(0.f, 0.f);
+        s[k * LP + l] = pack_lo(A, B);
+        if (k >= 1 && k <= hi_max) s[(g.px - k) * LP + l] = pack_hi(A, B);
+    }
+    __syncthreads();
+    const Lane ln(wlog);
+    line_fft<E>(s, LP, ln.l, ln.tl, pl, stw, +1.f,
+                [&](int i) { return s[i * LP + ln.l]; },
+                [&](int i, float2 v) { s[i * LP + ln.l] = v; });
+    __syncthreads();
+    const int totx = W * g.nx;
+    for (int idx = threadIdx.x; idx < totx; idx += blockDim.x) {
+        const int l = dnx.div(idx), x = idx - l * g.nx;
+        const long qa = q0 + 2 * l, qb = qa + 1;
+        if (qa >= Q) continue;
+        const float2 v = s[x * LP + l];
+        dst[(size_t)qa * g.nx + x] = v.x * invN;
+        if (qb < Q) dst[(size_t)qb * g.nx + x] = v.y * invN;
+    }
+}
+
+}  // namespace
+
+size_t fy_deconv_spec_elems(const SpecGeom& g) { return (size_t)g.nz * g.py * g.hxp; }
+
+cudaError_t fy_launch_deconv(const DeconvLaunch& d, cudaStream_t st) {
+    const SpecGeom& g = d.g;
+    cudaError_t e = cudaSuccess;
+    const long Q = (long)g.nz * g.ny;
+    // P1: X forward, rows paired two per line
+    {
+        const TileShape t = fy_tile_shape(g.px);
+        const size_t smem = (size_t)g.px * (t.W + 1) * sizeof(float2) + (size_t)g.px * sizeof(float2);
+        const unsigned grid = (unsigned)((Q + 2 * t.W - 1) / (2 * t.W));
+        e = fy_with_e(t.E, [&](auto ec) -> cudaError_t {
+            constexpr int E = decltype(ec)::value;
+            if (d.src_u8) {
+                auto k = k_x_fwd<E, SrcU8>;
+                cudaError_t e2 = fy_smem_optin(k, smem);
+                if (e2 != cudaSuccess) return e2;
+                k<<<grid, t.NT, smem, st>>>(SrcU8{(const uint8_t*)d.src}, d.lo, d.scale, d.spec, g, d.plx, d.twx, t.wlog, FastDiv(g.px), FastDiv(g.hx));
+            } else {
+                auto k = k_x_fwd<E, SrcF32>;
+                cudaError_t e2 = fy_smem_optin(k, smem);
+                if (e2 != cudaSuccess) return e2;
+                k<<<grid, t.NT, smem, st>>>(SrcF32{(const float*)d.src}, 0.f, 0.f, d.spec, g, d.plx, d.twx, t.wlog, FastDiv(g.px), FastDiv(g.hx));
+            }
+            return cudaGetLastError();
+        });
+        if (e != cudaSuccess) return e;
+    }
+    // P2: Y forward over the stored planes
+    {
+        const TileShape t = fy_tile_shape(g.py);
+        const size_t smem = (size_t)g.py * t.W * sizeof(float2) + (size_t)g.py * sizeof(float2);
+        dim3 grid(ceil_div_i(g.hx, t.W), g.nz);
+        e = fy_with_e(t.E, [&](auto ec) -> cudaError_t {
+            constexpr int E = decltype(ec)::value;
+            auto k = k_y_fwd<E>;
+            cudaError_t e2 = fy_smem_optin(k, smem);
+            if (e2 != cudaSuccess) return e2;
+            k<<<grid, t.NT, smem, st>>>(d.spec, g, d.ply, d.twy, t.wlog);
+            return cudaGetLastError();
+        });
+        if (e != cudaSuccess) return e;
+    }
+    // P3: Z forward, weight, Z inverse
+    {
+        const TileShape t = fy_tile_shape(g.pz);
+        const size_t smem = (size_t)g.pz * t.W * sizeof(float2) + (size_t)g.pz * sizeof(float2) +
+                            (size_t)g.pz * sizeof(double) + (FY_LUT_N + 1) * sizeof(float);
+        dim3 grid(ceil_div_i(g.hx, t.W), g.py);
+        e = fy_with_e(t.E, [&](auto ec) -> cudaError_t {
+            constexpr int E = decltype(ec)::value;
+            auto k = k_z_weight<E>;
+            cudaError_t e2 = fy_smem_optin(k, smem);
+            if (e2 != cudaSuccess) return e2;
+            k<<<grid, t.NT, smem, st>>>(d.spec, g, d.plz, d.twz, d.lut, d.fz2, d.fy2, d.fx2, d.us, t.wlog);
+            return cudaGetLastError();
+        });
+        if (e != cudaSuccess) return e;
+    }
+    // P4: Y inverse, keep rows < ny
+    {
+        const TileShape t = fy_tile_shape(g.py);
+        const size_t smem = (size_t)g.py * t.W * sizeof(float2) + (size_t)g.py * sizeof(float2);
+        dim3 grid(ceil_div_i(g.hx, t.W), g.nz);
+        e = fy_with_e(t.E, [&](auto ec) -> cudaError_t {
+            constexpr int E = decltype(ec)::value;
+            auto k = k_y_inv<E>;
+            cudaError_t e2 = fy_smem_optin(k, smem);
+            if (e2 != cudaSuccess) return e2;
+            k<<<grid, t.NT, smem, st>>>(d.spec, g, d.ply, d.twy, g.ny, t.wlog);
+            return cudaGetLastError();
+        });
+        if (e != cudaSuccess) return e;
+    }
+    // P5: X C2R, crop, 1/N
+    {
+        const TileShape t = fy_tile_shape(g.px);
+        const size_t smem = (size_t)g.px * (t.W + 1) * sizeof(float2) + (size_t)g.px * sizeof(float2);
+        const unsigned grid = (unsigned)((Q + 2 * t.W - 1) / (2 * t.W));
+        const float invN = 1.0f / ((float)g.pz * (float)g.py * (float)g.px);   // paganin.c:263
+        e = fy_with_e(t.E, [&](auto ec) -> cudaError_t {
+            constexpr int E = decltype(ec)::value;
+            auto k = k_x_inv<E>;
+            cudaError_t e2 = fy_smem_optin(k, smem);
+            if (e2 != cudaSuccess) return e2;
+            k<<<grid, t.NT, smem, st>>>(d.spec, d.dst, g, d.plx, d.twx, invN, t.wlog, FastDiv(g.nx), FastDiv(g.hx));
+            return cudaGetLastError();
+        });
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}

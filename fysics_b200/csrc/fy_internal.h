@@ -1,0 +1,103 @@
+// fy_internal.h -- host-side declarations shared between the kernel files and the C-ABI
+// layer (fy_api.cu). Not part of the public interface.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <type_traits>
+#include "fy_spectral.cuh"
+
+#define FY_LUT_N 4096   // paganin.c:138, radial weight LUT over u = f^2
+
+// Everything the five deconvolution passes need, all device pointers.
+struct DeconvLaunch {
+    const void* src;          // f32 or u8 volume (nz,ny,nx)
+    int src_u8;               // 1: u8 source dewindowed as lo + u8*scale (stream.c:41-46)
+    float lo, scale;
+    float* dst;               // f32 (nz,ny,nx); may alias src when src is f32
+    float2* spec;             // nz * py * hxp complex workspace
+    SpecGeom g;
+    FftPlan plx, ply, plz;
+    const float2 *twx, *twy, *twz;
+    const float* lut;         // FY_LUT_N+1 floats
+    const double *fz2, *fy2, *fx2;
+    double us;                // LUT index scale FY_LUT_N / umax
+};
+cudaError_t fy_launch_deconv(const DeconvLaunch& d, cudaStream_t st);
+size_t fy_deconv_spec_elems(const SpecGeom& g);
+
+// Elementwise stream ops (stream.c)
+cudaError_t fy_launch_u8_to_phys(const uint8_t* in, float* out, size_t n, float lo, float scale,
+                                 cudaStream_t st);
+cudaError_t fy_launch_phys_to_u8(const float* in, uint8_t* out, size_t n, float lo, float inv,
+                                 cudaStream_t st);
+cudaError_t fy_launch_float_to_u8(const float* in, uint8_t* out, size_t n, cudaStream_t st);
+cudaError_t fy_launch_u8_to_float(const uint8_t* in, float* out, size_t n, cudaStream_t st);
+
+// Guided filter / box mean (fy_guided.cu)
+size_t fy_guided_fused_smem(int r);
+cudaError_t fy_launch_guided_fused(const float* in, float* out, float* out_b, int nz, int ny, int nx, int r,
+                                   float eps, int mode, int sms, cudaStream_t st);
+cudaError_t fy_launch_guided_generic(const float* in, float* out, float* ws, int nz, int ny, int nx, int r,
+                                     float eps, cudaStream_t st, int& launches);
+cudaError_t fy_launch_guided_fast(const float* in, float* out, float* ws, int nz, int ny, int nx, int r,
+                                  float eps, int s, int sms, cudaStream_t st, int& launches);
+cudaError_t fy_launch_box_mean(const float* in, float* out, float* tmp, int nz, int ny, int nx, int r,
+                               cudaStream_t st, int& launches);
+
+// Noise model (fy_noise.cu)
+size_t fy_noise_ctl_bytes();
+cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, int win, double flat_pct,
+                                     double ref_intensity, float* scratch, void* ctl_mem, int sms,
+                                     cudaStream_t st, int& launches);
+cudaError_t fy_noise_read(const void* ctl_mem, double* g, double* b, double* noise_ref, double* ref_intensity,
+                          int* used, cudaStream_t st);
+const float* fy_noise_eps_ptr(const void* ctl_mem);
+
+// Ring removal (fy_dering.cu)
+cudaError_t fy_launch_dering_accum(const uint8_t* buf, const int* map, unsigned long long* sum, unsigned int* cnt,
+                                   int nbins, long dz, long dy, long dx, int ss, int sms, cudaStream_t st);
+cudaError_t fy_launch_dering_finalize(const float* sum_f, const unsigned int* cnt, float* ring, void* scratch,
+                                      unsigned long long* detected, int* have_rings, int nslab, int ns, int nr,
+                                      int hp_win, unsigned min_cnt, double min_amp, double max_amp,
+                                      cudaStream_t st);
+size_t fy_dering_finalize_scratch(int nslab, int ns, int nr);
+cudaError_t fy_launch_dering_apply(float* f, const float* ring, const int* have_rings, int nslab, int nr,
+                                   int slab_z, double cy, double cx, long z0, long y0, long x0, long dz, long dy,
+                                   long dx, double scale, cudaStream_t st);
+
+// Opt a kernel into > 48 KB of dynamic shared memory (idempotent).
+template <class K>
+inline cudaError_t fy_smem_optin(K kernel, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// Runtime elements-per-thread (fy_fft_e) -> compile-time E for kernel instantiation.
+template <class F>
+inline cudaError_t fy_with_e(int e, F&& f) {
+    switch (e) {
+        case 24: return f(std::integral_constant<int, 24>{});
+        case 16: return f(std::integral_constant<int, 16>{});
+        case 12: return f(std::integral_constant<int, 12>{});
+        case 8: return f(std::integral_constant<int, 8>{});
+        case 6: return f(std::integral_constant<int, 6>{});
+        case 4: return f(std::integral_constant<int, 4>{});
+        case 3: return f(std::integral_constant<int, 3>{});
+        case 2: return f(std::integral_constant<int, 2>{});
+        default: return f(std::integral_constant<int, 1>{});
+    }
+}
+
+// Launch shape of a tile of lines of length n: W lines, NT = W*n/E threads.
+struct TileShape {
+    int W, wlog, E, NT;
+};
+inline TileShape fy_tile_shape(int n) {
+    TileShape t;
+    t.W = fy_tile_lines(n);
+    t.wlog = fy_log2i(t.W);
+    t.E = fy_fft_e(n);
+    t.NT = t.W * n / t.E;
+    return t;
+}

@@ -1,0 +1,203 @@
+/* fysics_b200.h -- B200 (sm_100a) drop-in for the fysics per-cube restoration hot path.
+ *
+ * Part 1 declares the SAME C symbols, signatures and struct layouts as the reference's
+ * public header (fysics.h), for exactly the functions on the restoration path. A C caller
+ * of fysics links libfysics_b200.so ahead of libfysics and gets these entry points on the
+ * GPU with unchanged semantics: caller-owned HOST buffers, synchronous calls, outputs
+ * valid on return, int 0 = success. Each declaration cites the fysics.h line it replaces.
+ * Every call runs on the GPU; there is no CPU fallback. Without a usable CUDA device an
+ * int entry point returns FY_ENODEV (4) and a void entry point leaves its outputs
+ * untouched and records the error, readable through fy_gpu_last_error().
+ *
+ * Part 2 is the fy_gpu_* extension: device pointers, CUDA streams (passed as void*),
+ * fused chains, batches and the serving loop. Nothing in it has a reference counterpart
+ * except where stated.
+ */
+#ifndef FYSICS_B200_H
+#define FYSICS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ====================================================================== part 1: drop-in */
+
+/* fysics.h:23-35 -- 8 doubles, layout-identical */
+typedef struct {
+    double delta_beta;
+    double energy_kev;
+    double distance_mm;
+    double pixel_um;
+    double unsharp_sigma;
+    double unsharp_coeff;
+    double psf_sigma_vox;
+    double psf_sigma_z_vox;
+} fy_physics;
+
+/* fysics.h:191-197 */
+typedef struct {
+    double g;
+    double b;
+    double noise_ref;
+    double ref_intensity;
+    int    n_bins_used;
+} fy_noise_model;
+
+/* fysics.h:406-415 -- callers read ring[] and have_rings directly; fwrite-serialisable */
+typedef struct {
+    long Z, Y, X;
+    double cy, cx;
+    int slab_z, nslab;
+    int ns, nr;
+    float *sum;
+    unsigned int *cnt;
+    float *ring;
+    int have_rings;
+} fy_dering;
+
+/* FFT sizes, fysics.h:38-40 */
+int  fy_is_pow2(int n);
+int  fy_next_pow2(int n);
+int  fy_next_fft_size(int n);
+/* fysics.h:41-43: in-place split re/im transforms (sizes 2^k, 3*2^k up to 4096 per axis) */
+void fy_fft1d(float *re, float *im, int n, int sign);
+void fy_fft3d(float *re, float *im, int nz, int ny, int nx, int sign);
+void fy_fft3d_normalize(float *re, float *im, int nz, int ny, int nx);
+
+/* u8 <-> float windowing, fysics.h:56-57, 70-76 */
+void  fy_u8_to_float(const unsigned char *in, float *out, size_t n);
+void  fy_float_to_u8(const float *in, unsigned char *out, size_t n);
+void  fy_u8_to_phys(const unsigned char *in, float *out, size_t n, double f32_min, double f32_max);
+void  fy_phys_to_u8(const float *in, unsigned char *out, size_t n, double f32_min, double f32_max);
+float fy_phys_to_u8_level(double phys, double f32_min, double f32_max);
+
+/* transfer functions and plan-time helpers, fysics.h:98-117, 146 */
+double fy_paganin_transfer(double f_cyc_per_voxel, const fy_physics *p);
+double fy_unsharp_transfer(double f_cyc_per_voxel, const fy_physics *p);
+double fy_recon_transfer(double f_cyc_per_voxel, const fy_physics *p);
+double fy_auto_reg(const fy_physics *p, double base);
+double fy_auto_deltabeta_scale(const fy_physics *p);
+int    fy_kernel_halo(const fy_physics *p);
+
+/* Wiener deconvolution, fysics.h:131-142 (in/out may alias) */
+int fy_deconvolve(const float *in, float *out, int nz, int ny, int nx,
+                  const fy_physics *p, double reg);
+int fy_deconvolve_matched(const float *in, float *out, int nz, int ny, int nx,
+                          const fy_physics *p, double tikhonov);
+
+/* guided filter, fysics.h:152-167 */
+int    fy_guided_denoise(const float *in, float *out, int nz, int ny, int nx,
+                         int radius, double eps);
+int    fy_guided_denoise_ws(const float *in, float *out, int nz, int ny, int nx,
+                            int radius, double eps, float *ws);
+size_t fy_guided_ws_floats(int nz, int ny, int nx);
+int    fy_guided_denoise_fast_ws(const float *in, float *out, int nz, int ny, int nx,
+                                 int radius, double eps, int s, float *ws);
+void   fy_box_smooth(const float *in, float *out, float *tmp, int nz, int ny, int nx, int r);
+double fy_guided_eps_for_noise(double noise_ref);
+
+/* noise model, fysics.h:203-205 */
+int fy_estimate_noise(const float *in, int nz, int ny, int nx, int win, double flat_pct,
+                      double ref_intensity, fy_noise_model *out);
+
+/* ring removal, fysics.h:417-433 */
+int  fy_dering_init(fy_dering *d, long Z, long Y, long X, double cy, double cx,
+                    int slab_z, int ns);
+void fy_dering_free(fy_dering *d);
+int  fy_dering_tile_init(fy_dering *t, const fy_dering *d);
+void fy_dering_tile_reset(fy_dering *t);
+void fy_dering_accumulate_u8(fy_dering *t, const unsigned char *buf, long y0, long x0,
+                             long dz, long dy, long dx, int ss);
+void fy_dering_merge_tile(fy_dering *d, int slab, const fy_dering *t);
+long fy_dering_finalize(fy_dering *d, int hp_win, unsigned int min_cnt, double min_amp,
+                        double max_amp);
+void fy_dering_apply(const fy_dering *d, float *f, long z0, long y0, long x0, long dz,
+                     long dy, long dx, double scale);
+
+/* phase correlation, fysics.h:311-313 */
+int fy_phase_correlate(const float *fixed, const float *moving, int nz, int ny, int nx,
+                       double *shift, double *peak, int window);
+
+/* ================================================================== part 2: fy_gpu_* */
+
+/* status codes (0 = success; 1 is the reference's generic failure) */
+#define FY_OK 0
+#define FY_EINVAL 1
+#define FY_ENOMEM 2
+#define FY_ECUDA 3
+#define FY_ENODEV 4
+#define FY_EUNSUPPORTED 5
+#define FY_ETIMEDOUT 6
+#define FY_EBUSY 7
+#define FY_EDEGENERATE 8
+
+/* Select the CUDA device for the calling thread (default 0). No reference counterpart. */
+int         fy_gpu_init(int device);
+/* Status and message of the calling thread's last failed call. */
+int         fy_gpu_last_status(void);
+const char *fy_gpu_last_error(void);
+/* Release the calling thread's stream and cached device/pinned buffers. */
+void        fy_gpu_release(void);
+/* Launch counter: number of kernels this thread has launched (for measurement). */
+unsigned long long fy_gpu_kernel_launches(void);
+
+/* Device-pointer forms of the drop-in calls, enqueued on `stream` (a cudaStream_t, NULL =
+ * legacy default stream) and NOT synchronised: results are valid once the stream reaches
+ * them. Same argument meaning as part 1 (fysics.h lines cited there). */
+int fy_gpu_u8_to_phys(const unsigned char *d_in, float *d_out, size_t n,
+                      double f32_min, double f32_max, void *stream);
+int fy_gpu_phys_to_u8(const float *d_in, unsigned char *d_out, size_t n,
+                      double f32_min, double f32_max, void *stream);
+
+/* kind: 0 = fy_deconvolve (Wiener of Paganin x unsharp, gain cap 8, param = reg),
+ *       1 = fy_deconvolve_matched (PSF x unsharp, param = tikhonov),
+ *       2 = Paganin x unsharp Wiener with anisotropic z: fz^2 scaled by fz2_scale
+ *           (= (sigma_z/sigma_xy)^2), cap 8, param = reg -- deconv_radial's fz2_scale
+ *           (paganin.c:140-154), which fysics reaches only through the matched weight.
+ * src_u8 != 0: d_in is u8 and is dewindowed on load as fy_u8_to_phys(f32_min, f32_max). */
+int fy_gpu_deconvolve_ex(const void *d_in, int src_u8, double f32_min, double f32_max,
+                         float *d_out, int nz, int ny, int nx, const fy_physics *p,
+                         double param, int kind, double fz2_scale, void *stream);
+
+/* Guided filter on device buffers: s <= 1 exact (fy_guided_denoise_ws), s >= 2 the
+ * s-decimated fast variant (fy_guided_denoise_fast_ws). d_in may equal d_out. */
+int    fy_gpu_guided(const float *d_in, float *d_out, int nz, int ny, int nx, int radius,
+                     double eps, int s, void *stream);
+size_t fy_gpu_guided_scratch_bytes(int nz, int ny, int nx, int radius, int s);
+
+/* Noise model on a device volume (fy_estimate_noise, fysics.h:203-205). d_scratch holds
+ * fy_gpu_noise_scratch_bytes(): local mean/variance fields plus a control block in which
+ * the model stays on the device. fy_gpu_noise_model copies it to the host (synchronises
+ * `stream`); fy_gpu_noise_eps returns the device address of the float guided eps
+ * fy_guided_eps_for_noise(noise_ref) for chaining without a host round trip. */
+size_t fy_gpu_noise_scratch_bytes(int nz, int ny, int nx);
+int    fy_gpu_estimate_noise(const float *d_in, int nz, int ny, int nx, int win, double flat_pct,
+                             double ref_intensity, void *d_scratch, void *stream);
+int    fy_gpu_noise_model(const void *d_scratch, int nz, int ny, int nx, fy_noise_model *out,
+                          void *stream);
+const float *fy_gpu_noise_eps(const void *d_scratch, int nz, int ny, int nx);
+
+/* Device-resident ring state for chains (fy_dering's arrays live on the GPU). accumulate
+ * adds a device u8 region at global (z0,y0,x0) into slab z0/slab_z (accumulate + merge);
+ * finalize runs the sector vote on the device; apply subtracts on a device f32 region and
+ * is a no-op when fewer than 2 radii were detected; download copies the state into a host
+ * fy_dering created with fy_dering_init on the same geometry. */
+typedef struct fy_gpu_dering fy_gpu_dering;
+int  fy_gpu_dering_create(fy_gpu_dering **out, long Z, long Y, long X, double cy, double cx,
+                          int slab_z, int ns);
+void fy_gpu_dering_destroy(fy_gpu_dering *h);
+int  fy_gpu_dering_reset(fy_gpu_dering *h, void *stream);
+int  fy_gpu_dering_accumulate_u8(fy_gpu_dering *h, const unsigned char *d_buf, long z0, long y0,
+                                 long x0, long dz, long dy, long dx, int ss, void *stream);
+int  fy_gpu_dering_finalize(fy_gpu_dering *h, int hp_win, unsigned int min_cnt, double min_amp,
+                            double max_amp, void *stream);
+int  fy_gpu_dering_apply(const fy_gpu_dering *h, float *d_f, long z0, long y0, long x0, long dz,
+                         long dy, long dx, double scale, void *stream);
+int  fy_gpu_dering_download(const fy_gpu_dering *h, fy_dering *d, long *detected, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FYSICS_B200_H */
