@@ -1,0 +1,414 @@
+#!/usr/bin/env python
+"""Benchmark of the fysics restoration path on B200 (one JSON line on stdout, rank 0).
+
+Workload: the production-size drop-in configuration -- one 512^3 u8 cube of the seeded
+scroll phantom (pixel 2.4 um, delta_beta x fy_auto_deltabeta_scale, anisotropic PSF
+sigma_z/sigma_xy = 1.17, 40 synthetic rings), restored by the full chain
+  fy_u8_to_phys -> fy_deconvolve_matched (psf 1.0 / 1.17) -> fy_estimate_noise (win 5,
+  10th pct, ref 0.4) -> guided filter (r 2, eps = (3*noise_ref)^2) -> ring subtraction
+  (accumulate ss=2 on the u8 input, vote(15, 100, 0.5, 6.0), apply),
+through fy_gpu_restore_u8. A step is one cube.
+
+  value   Mvox/s with the cube resident in HBM (device-timed with CUDA events, max over ranks)
+  e2e     Mvox/s through host buffers: pinned u8 in -> H2D -> chain -> D2H -> pinned f32 out
+  --impl reference  the reference's CPU implementation (oracle/_ref, compiled from its own
+          sources) on the host cores, same metric, bounded sample
+
+Multi-GPU (torchrun): cubes are independent -- each rank restores its own cube (weak
+scaling, no collective on the data path); the barrier and the max of the per-rank times
+use torch.distributed.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mvoxel/s deconv+denoise and p50/p99 cube latency, served vs plain, same B200"
+SHAPE = (512, 512, 512)
+WORKLOAD = "512^3 u8 scroll phantom, dewindow->deconv_matched(aniso 1.17)->noise->guided(r2)->dering"
+
+
+def physics_for(fb):
+    import fysics_b200.phantom as ph
+    p = fb.physics(delta_beta=500.0, energy_kev=110.0, distance_mm=1200.0, pixel_um=2.4, unsharp_sigma=0.8,
+                   unsharp_coeff=0.5, psf_sigma_vox=1.0, psf_sigma_z_vox=1.17)
+    scale = fb.load().fy_auto_deltabeta_scale(C.byref(p))
+    p.delta_beta *= scale
+    del ph
+    return p, scale
+
+
+def restore_cfg(fb, dering_handle):
+    cfg = fb.RestoreCfg()
+    fb.load().fy_restore_cfg_default(C.byref(cfg))
+    cfg.deconv_kind = 1
+    cfg.deconv_param = 0.05
+    cfg.noise_win = 5
+    cfg.noise_flat_pct = 10.0
+    cfg.noise_ref_intensity = 0.4
+    cfg.guided_radius = 2
+    cfg.guided_s = 1
+    cfg.dering = dering_handle
+    cfg.dering_accumulate = 1
+    cfg.dering_ss = 2
+    cfg.dering_hp_win = 15
+    cfg.dering_min_cnt = 100
+    cfg.dering_min_amp = 0.5
+    cfg.dering_max_amp = 6.0
+    cfg.dering_scale = 1.0 / 255.0
+    return cfg
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------ roofline
+def algorithmic_bytes(name: str, n: int, geo: dict) -> float | None:
+    """Bytes a kernel must move per launch (read once + written once), 512^3 u8 chain."""
+    nz, ny, nx = geo["shape"]
+    px = geo["px"]
+    hx = px // 2 + 1
+    half = nz * ny * hx * 8            # one stored half-spectrum (nz planes)
+    table = {
+        "deconv.x_fwd": n * 1 + half,
+        "deconv.y_fwd": half + nz * geo["py"] * hx * 8,
+        "deconv.z_weight": 2 * nz * geo["py"] * hx * 8,
+        "deconv.y_inv": nz * geo["py"] * hx * 8 + half,
+        "deconv.x_inv": half + n * 4,
+        "guided": n * 8,
+        "dering.apply": n * 8,
+    }
+    return table.get(name)
+
+
+def read_profile(lib):
+    cnt = lib.fy_gpu_profile_stop()
+    per = {}
+    for i in range(1, cnt):
+        nm = C.c_char_p()
+        ms = C.c_float()
+        if lib.fy_gpu_profile_read(i, C.byref(nm), C.byref(ms)) == 0:
+            per.setdefault(nm.value.decode(), []).append(ms.value)
+    return per
+
+
+# ------------------------------------------------------------------------------ CPU legs
+def cpu_reference_sample(u8_host: np.ndarray, steps: int = 1, crop: int = 128, budget_s: float = 20.0):
+    """The reference CPU chain on crops of the benchmark cube, one crop per host thread
+    (the reference's own tile parallelism, pipeline.c:1008-1020); returns Mvox/s."""
+    import oracle
+    from concurrent.futures import ThreadPoolExecutor
+    L = oracle.ref()
+    cores = os.cpu_count() or 1
+    phys = oracle.ref_physics(delta_beta=500.0 * 0.35, energy_kev=110.0, distance_mm=1200.0, pixel_um=2.4,
+                              unsharp_sigma=0.8, unsharp_coeff=0.5, psf_sigma_vox=1.0, psf_sigma_z_vox=1.17)
+    nz = u8_host.shape[0] // crop
+    crops = [(z, y, x) for z in range(nz) for y in range(u8_host.shape[1] // crop) for x in range(u8_host.shape[2] // crop)]
+
+    def one(i):
+        z, y, x = crops[i % len(crops)]
+        sub = np.ascontiguousarray(u8_host[z * crop:(z + 1) * crop, y * crop:(y + 1) * crop, x * crop:(x + 1) * crop])
+        n = sub.size
+        f = np.empty(sub.shape, np.float32)
+        L.fy_u8_to_phys(oracle.p(sub), oracle.p(f), n, 0.0, 1.0)
+        d = np.empty_like(f)
+        L.fy_deconvolve_matched(oracle.p(f), oracle.p(d), crop, crop, crop, C.byref(phys), 0.05)
+        nm = oracle.RefNoise()
+        L.fy_estimate_noise(oracle.p(d), crop, crop, crop, 5, 10.0, 0.4, C.byref(nm))
+        eps = L.fy_guided_eps_for_noise(nm.noise_ref)
+        ws = np.empty(4 * n, np.float32)
+        out = np.empty_like(f)
+        L.fy_guided_denoise_ws(oracle.p(d), oracle.p(out), crop, crop, crop, 2, eps, oracle.p(ws))
+        dr, dt = oracle.RefDering(), oracle.RefDering()
+        L.fy_dering_init(C.byref(dr), crop, crop, crop, -1, -1, 512, 8)
+        L.fy_dering_tile_init(C.byref(dt), C.byref(dr))
+        L.fy_dering_accumulate_u8(C.byref(dt), oracle.p(sub), 0, 0, crop, crop, crop, 2)
+        L.fy_dering_merge_tile(C.byref(dr), 0, C.byref(dt))
+        L.fy_dering_finalize(C.byref(dr), 15, 100, 0.5, 6.0)
+        L.fy_dering_apply(C.byref(dr), oracle.p(out), 0, 0, 0, crop, crop, crop, 1.0 / 255.0)
+        L.fy_dering_free(C.byref(dt)); L.fy_dering_free(C.byref(dr))
+        return n
+
+    t0 = time.perf_counter()
+    one(0)                                                  # calibrate one crop, 1 thread
+    t_one = time.perf_counter() - t0
+    per_thread = max(1, int(budget_s / max(t_one, 1e-3)))
+    jobs = cores * max(1, min(per_thread, 4)) * steps
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        vox = sum(ex.map(one, range(jobs)))
+    dt = time.perf_counter() - t0
+    return {"value": vox / dt / 1e6, "unit": "Mvoxel/s", "cores": cores, "kind": "reference",
+            "sample": f"{jobs} crops of {crop}^3 from the benchmark cube, one per host thread "
+                      f"({cores} threads), reference compiled from its sources; {dt:.1f} s wall; "
+                      f"single-thread latency {t_one * 1e3:.0f} ms per {crop}^3 crop"}
+
+
+# ------------------------------------------------------------------------------ main
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world <= 1:
+        return 0, 1, 0, None
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    import datetime
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, world, local, dist
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import fysics_b200.phantom as ph
+    import oracle
+    if not oracle.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfysics_ref.so not built"}))
+        return
+    u8 = ph.phantom(SHAPE, seed=args.seed, delta_beta=500.0 * 0.35, pixel_um=2.4, fz2_scale=1.17 ** 2,
+                    rings=40, device="cpu") if args.cpu_phantom else None
+    if u8 is None:
+        import torch
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+        u8 = ph.phantom(SHAPE, seed=args.seed, delta_beta=500.0 * 0.35, pixel_um=2.4, fz2_scale=1.17 ** 2,
+                        rings=40, device=dev).cpu().numpy()
+    res = cpu_reference_sample(u8, steps=1, budget_s=args.cpu_budget)
+    n = int(np.prod(SHAPE))
+    line = {"metric": METRIC, "value": res["value"], "unit": "Mvoxel/s", "impl": "reference",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": n / (res["value"] * 1e6) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cube": "512^3", "l2": "working set > L2"},
+            "cpu_baseline": res,
+            "e2e": {"value": res["value"], "unit": "Mvoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cpu-phantom", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local, dist = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    import torch
+    import fysics_b200 as fb
+    import fysics_b200.phantom as ph
+    lib = fb.load()
+    dev = local
+    fb.check(lib.fy_gpu_init(dev), "fy_gpu_init")
+    torch.cuda.set_device(dev)
+    p, db_scale = physics_for(fb)
+    u8 = ph.phantom(SHAPE, seed=args.seed + rank, delta_beta=p.delta_beta, energy_kev=p.energy_kev,
+                    distance_mm=p.distance_mm, pixel_um=p.pixel_um, unsharp_sigma=p.unsharp_sigma,
+                    unsharp_coeff=p.unsharp_coeff, fz2_scale=1.17 ** 2, rings=40, device=f"cuda:{dev}")
+    nz, ny, nx = SHAPE
+    n = nz * ny * nx
+    out = torch.empty(SHAPE, dtype=torch.float32, device=f"cuda:{dev}")
+    stream = torch.cuda.Stream(device=dev)
+    sp = C.c_void_p(stream.cuda_stream)
+    h = C.c_void_p()
+    fb.check(lib.fy_gpu_dering_create(C.byref(h), nz, ny, nx, -1.0, -1.0, 512, 8), "fy_gpu_dering_create")
+    cfg = restore_cfg(fb, h)
+
+    def step(src_ptr, dst_ptr):
+        fb.check(lib.fy_gpu_dering_reset(h, sp), "fy_gpu_dering_reset")
+        fb.check(lib.fy_gpu_restore_u8(src_ptr, dst_ptr, nz, ny, nx, 0.0, 1.0, C.byref(p), C.byref(cfg), sp),
+                 "fy_gpu_restore_u8")
+
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step(C.c_void_p(u8.data_ptr()), C.c_void_p(out.data_ptr()))
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident timed region (per-step events -> latency; profile marks)
+    clocks = ClockSampler(dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    launches0 = lib.fy_gpu_kernel_launches()
+    barrier()
+    clocks.start()
+    lib.fy_gpu_profile_start(64 * args.steps + 8, sp)
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for k in range(args.steps):
+            step(C.c_void_p(u8.data_ptr()), C.c_void_p(out.data_ptr()))
+            ev[k + 1].record(stream)
+    stream.synchronize()
+    barrier()
+    clock = clocks.stop()
+    launches = lib.fy_gpu_kernel_launches() - launches0
+    prof = read_profile(lib)
+    per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[args.steps])
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / args.steps
+    value = world * n * args.steps / (total_ms * 1e-3) / 1e6
+
+    # ---- end to end through pinned host buffers
+    h_in = torch.empty(SHAPE, dtype=torch.uint8, pin_memory=True)
+    h_in.copy_(u8.cpu())
+    h_out = torch.empty(SHAPE, dtype=torch.float32, pin_memory=True)
+    d_in = torch.empty_like(u8)
+    e2e_steps = max(3, min(args.steps, 10))
+    ee = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps + 1)]
+    barrier()
+    with torch.cuda.stream(stream):
+        ee[0].record(stream)
+        for k in range(e2e_steps):
+            d_in.copy_(h_in, non_blocking=True)
+            step(C.c_void_p(d_in.data_ptr()), C.c_void_p(out.data_ptr()))
+            h_out.copy_(out, non_blocking=True)
+            ee[k + 1].record(stream)
+    stream.synchronize()
+    barrier()
+    e2e_steps_ms = [ee[k].elapsed_time(ee[k + 1]) for k in range(e2e_steps)]
+    e2e_ms = ee[0].elapsed_time(ee[e2e_steps])
+    if dist:
+        t = torch.tensor([e2e_ms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * n * e2e_steps / (e2e_ms * 1e-3) / 1e6
+
+    # ---- roofline of the dominant kernel (live event timings above)
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    geo = {"shape": SHAPE, "px": fb.load().fy_next_fft_size(nx), "py": fb.load().fy_next_fft_size(ny)}
+    kernels = {}
+    for name, v in prof.items():
+        avg = sum(v) / len(v)
+        ab = algorithmic_bytes(name, n, geo)
+        kernels[name] = {"avg_ms": avg, "launches": len(v), "share": sum(v) / max(sum(map(sum, prof.values())), 1e-9),
+                         "gbs": (ab / (avg * 1e-3) / 1e9) if ab else None}
+    dom = max((k for k in kernels if kernels[k]["gbs"] is not None), key=lambda k: kernels[k]["avg_ms"], default=None)
+    roof = None
+    if dom:
+        ach = kernels[dom]["gbs"]
+        roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                "frac": ach / hbm_peak, "traffic": None, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": algorithmic_bytes(dom, n, geo)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            import oracle
+            if oracle.have_ref():
+                cpu = cpu_reference_sample(u8.cpu().numpy(), budget_s=args.cpu_budget)
+        except Exception as exc:       # the baseline is reported, never required
+            cpu = {"value": None, "error": str(exc)[:200]}
+
+    lat = sorted(per_step)
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mvoxel/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cube": "512^3 u8", "deltabeta_scale": db_scale,
+                   "l2": "inputs and working set (~3 GB) larger than the 126 MB L2",
+                   "parallelism": f"replicas x{world} (one cube per GPU, no collective)"},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "e2e_p50": float(np.percentile(e2e_steps_ms, 50)),
+                       "e2e_p99": float(np.percentile(e2e_steps_ms, 99))},
+        "e2e": {"value": e2e_value, "unit": "Mvoxel/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": 4 * n},
+        "gpu_launches": int(launches),
+        "roofline": roof,
+        "kernels": kernels,
+        "clocks": clock,
+        "cpu_baseline": cpu,
+    }
+    lib.fy_gpu_dering_destroy(h)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

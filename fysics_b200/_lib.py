@@ -31,6 +31,17 @@ class NoiseModel(C.Structure):
                 ("ref_intensity", C.c_double), ("n_bins_used", C.c_int)]
 
 
+class RestoreCfg(C.Structure):
+    """fy_restore_cfg (include/fysics_b200.h)."""
+    _fields_ = [("deconv_kind", C.c_int), ("deconv_param", C.c_double), ("fz2_scale", C.c_double),
+                ("noise_win", C.c_int), ("noise_flat_pct", C.c_double), ("noise_ref_intensity", C.c_double),
+                ("guided_eps", C.c_double), ("guided_radius", C.c_int), ("guided_s", C.c_int),
+                ("dering", C.c_void_p), ("dering_accumulate", C.c_int), ("dering_ss", C.c_int),
+                ("dering_hp_win", C.c_int), ("dering_min_cnt", C.c_uint), ("dering_min_amp", C.c_double),
+                ("dering_max_amp", C.c_double), ("dering_scale", C.c_double),
+                ("z0", C.c_long), ("y0", C.c_long), ("x0", C.c_long)]
+
+
 class Dering(C.Structure):
     """fy_dering (fysics.h:406-415)."""
     _fields_ = [("Z", C.c_long), ("Y", C.c_long), ("X", C.c_long),
@@ -106,6 +117,14 @@ SIGNATURES = {
     "fy_gpu_dering_finalize": (_i, [_P, _i, C.c_uint, _d, _d, _P]),
     "fy_gpu_dering_apply": (_i, [_P, _P, _l, _l, _l, _l, _l, _l, _d, _P]),
     "fy_gpu_dering_download": (_i, [_P, _PD, C.POINTER(_l), _P]),
+    "fy_gpu_phase_correlate_scratch_bytes": (_sz, [_i, _i, _i]),
+    "fy_restore_cfg_default": (None, [C.c_void_p]),
+    "fy_gpu_restore_u8": (_i, [_P, _P, _i, _i, _i, _d, _d, _PP, C.c_void_p, _P]),
+    "fy_gpu_profile_start": (_i, [_i, _P]),
+    "fy_gpu_profile_stop": (_i, []),
+    "fy_gpu_profile_read": (_i, [_i, C.POINTER(C.c_char_p), C.POINTER(C.c_float)]),
+    "fy_gpu_phase_correlate_batch": (_i, [_P, _P, _i, _i, _i, _i, _i, _P, _PDBL, _PDBL,
+                                          C.POINTER(C.c_longlong), C.POINTER(_i), _P]),
 }
 
 _lib = None

@@ -126,9 +126,71 @@ const float2* twiddles(int n) {
     return d;
 }
 
+// ---------------------------------------------------------------- smem opt-in cache
 }  // namespace fy
 
+cudaError_t fy_smem_optin_raw(const void* kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& have = done[{kernel, dev}];
+    if (have >= bytes) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) have = bytes;
+    return e;
+}
+
+namespace fy {
+// ---------------------------------------------------------------- profiling marks
+struct Prof {
+    bool on = false;
+    int n = 0;
+    std::vector<cudaEvent_t> ev;
+    std::vector<const char*> names;
+};
+static thread_local Prof t_prof;
+
+}  // namespace fy
+
+void fy_prof_mark(cudaStream_t st, const char* name) {
+    fy::Prof& P = fy::t_prof;
+    if (!P.on || P.n >= (int)P.ev.size()) return;
+    if (cudaEventRecord(P.ev[(size_t)P.n], st) == cudaSuccess) P.names[(size_t)P.n++] = name;
+}
+
 extern "C" {
+// Per-kernel timing with CUDA events recorded on the launching stream after every
+// instrumented launch. start(capacity) arms it and records the origin mark; read(i)
+// returns the name of mark i and the milliseconds since mark i-1 (after the stream has
+// been synchronised).
+int fy_gpu_profile_start(int capacity, void* stream) {
+    fy::Prof& P = fy::t_prof;
+    if (capacity < 2) capacity = 2;
+    while ((int)P.ev.size() < capacity) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return fy::fail(FY_ECUDA, "fy_gpu_profile_start: event");
+        P.ev.push_back(e);
+        P.names.push_back(nullptr);
+    }
+    P.n = 0;
+    P.on = true;
+    fy_prof_mark((cudaStream_t)stream, "start");
+    return FY_OK;
+}
+int fy_gpu_profile_stop(void) {
+    fy::t_prof.on = false;
+    return fy::t_prof.n;
+}
+int fy_gpu_profile_read(int i, const char** name, float* ms) {
+    fy::Prof& P = fy::t_prof;
+    if (i <= 0 || i >= P.n) return FY_EINVAL;
+    if (name) *name = P.names[(size_t)i];
+    if (ms && cudaEventElapsedTime(ms, P.ev[(size_t)i - 1], P.ev[(size_t)i]) != cudaSuccess) return FY_ECUDA;
+    return FY_OK;
+}
+
 int fy_gpu_init(int device) {
     fy::ThreadCtx& c = fy::ctx();
     c.status = 0; c.err.clear();

@@ -246,6 +246,7 @@ cudaError_t fy_launch_deconv(const DeconvLaunch& d, cudaStream_t st) {
         });
         if (e != cudaSuccess) return e;
     }
+    fy_prof_mark(st, "deconv.x_fwd");
     // P2: Y forward over the stored planes
     {
         const TileShape t = fy_tile_shape(g.py);
@@ -261,6 +262,7 @@ cudaError_t fy_launch_deconv(const DeconvLaunch& d, cudaStream_t st) {
         });
         if (e != cudaSuccess) return e;
     }
+    fy_prof_mark(st, "deconv.y_fwd");
     // P3: Z forward, weight, Z inverse
     {
         const TileShape t = fy_tile_shape(g.pz);
@@ -277,6 +279,7 @@ cudaError_t fy_launch_deconv(const DeconvLaunch& d, cudaStream_t st) {
         });
         if (e != cudaSuccess) return e;
     }
+    fy_prof_mark(st, "deconv.z_weight");
     // P4: Y inverse, keep rows < ny
     {
         const TileShape t = fy_tile_shape(g.py);
@@ -292,6 +295,7 @@ cudaError_t fy_launch_deconv(const DeconvLaunch& d, cudaStream_t st) {
         });
         if (e != cudaSuccess) return e;
     }
+    fy_prof_mark(st, "deconv.y_inv");
     // P5: X C2R, crop, 1/N
     {
         const TileShape t = fy_tile_shape(g.px);
@@ -308,5 +312,31 @@ cudaError_t fy_launch_deconv(const DeconvLaunch& d, cudaStream_t st) {
         });
         if (e != cudaSuccess) return e;
     }
+    fy_prof_mark(st, "deconv.x_inv");
     return cudaSuccess;
+}
+
+// Y pass over `nplanes` stored planes of a half spectrum (shared with phase correlation):
+// sign -1 forward (rows >= ny gathered by reflection or zero), +1 inverse keeping rows
+// < keep_rows.
+cudaError_t fy_launch_spec_y(float2* spec, const SpecGeom& g, const FftPlan& ply, const float2* twy, int nplanes,
+                             int sign, int keep_rows, cudaStream_t st) {
+    const TileShape t = fy_tile_shape(g.py);
+    const size_t smem = (size_t)g.py * t.W * sizeof(float2) + (size_t)g.py * sizeof(float2);
+    dim3 grid(ceil_div_i(g.hx, t.W), nplanes);
+    return fy_with_e(t.E, [&](auto ec) -> cudaError_t {
+        constexpr int E = decltype(ec)::value;
+        if (sign < 0) {
+            auto k = k_y_fwd<E>;
+            cudaError_t e2 = fy_smem_optin(k, smem);
+            if (e2 != cudaSuccess) return e2;
+            k<<<grid, t.NT, smem, st>>>(spec, g, ply, twy, t.wlog);
+        } else {
+            auto k = k_y_inv<E>;
+            cudaError_t e2 = fy_smem_optin(k, smem);
+            if (e2 != cudaSuccess) return e2;
+            k<<<grid, t.NT, smem, st>>>(spec, g, ply, twy, keep_rows, t.wlog);
+        }
+        return cudaGetLastError();
+    });
 }

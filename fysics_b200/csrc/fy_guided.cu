@@ -112,8 +112,10 @@ struct GuidedSmem {
 template <int R, int MODE>
 __global__ void __launch_bounds__(GNT) k_guided_fused(const float* __restrict__ in, float* __restrict__ out,
                                                       float* __restrict__ out_b,
-                                                      int nz, int ny, int nx, float eps, int zchunk) {
+                                                      int nz, int ny, int nx, float eps,
+                                                      const float* __restrict__ eps_ptr, int zchunk) {
     using S = GuidedSmem<R>;
+    if (eps_ptr) eps = *eps_ptr;                     // chained: eps from the device noise model
     extern __shared__ float4 smem4[];
     S& sm = *reinterpret_cast<S*>(smem4);
     const int x0 = blockIdx.x * GTX, y0 = blockIdx.y * GTY;
@@ -269,7 +271,7 @@ size_t fy_guided_fused_smem(int r) {
 // while neighbouring tiles still read their input halos). mode 1 writes box(a) to out and
 // box(b) to out_b instead of the filtered volume.
 cudaError_t fy_launch_guided_fused(const float* in, float* out, float* out_b, int nz, int ny, int nx, int r,
-                                   float eps, int mode, int sms, cudaStream_t st) {
+                                   float eps, int mode, int sms, cudaStream_t st, const float* eps_ptr) {
     const dim3 tiles(ceil_div_i(nx, GTX), ceil_div_i(ny, GTY), 1);
     // z chunks: enough CTAs for ~4 waves, but chunks of >= 8r planes so the 4r-plane
     // warm-up stays a small fraction
@@ -284,7 +286,7 @@ cudaError_t fy_launch_guided_fused(const float* in, float* out, float* out_b, in
     cudaError_t e = cudaSuccess;
 #define FY_GF(RR, MM)                                                                    \
     if ((e = fy_smem_optin(k_guided_fused<RR, MM>, smem)) != cudaSuccess) return e;       \
-    k_guided_fused<RR, MM><<<grid, GNT, smem, st>>>(in, out, out_b, nz, ny, nx, eps, zchunk);
+    k_guided_fused<RR, MM><<<grid, GNT, smem, st>>>(in, out, out_b, nz, ny, nx, eps, eps_ptr, zchunk);
     if (mode == 0) {
         switch (r) {
             case 1: FY_GF(1, 0) break;
@@ -360,14 +362,14 @@ __global__ void __launch_bounds__(256) k_upsample_apply(const float* __restrict_
 
 // Fast guided filter (s >= 2, all low dims >= 2, rl = max(1, r/s) <= 4). ws: >= 3*nl floats.
 cudaError_t fy_launch_guided_fast(const float* in, float* out, float* ws, int nz, int ny, int nx, int r,
-                                  float eps, int s, int sms, cudaStream_t st, int& launches) {
+                                  float eps, int s, int sms, cudaStream_t st, int& launches, const float* eps_ptr) {
     const int lz = (nz + s - 1) / s, ly = (ny + s - 1) / s, lx = (nx + s - 1) / s;
     const size_t nl = (size_t)lz * ly * lx;
     float *il = ws, *ma = ws + nl, *mb = ws + 2 * nl;
     int rl = r / s;
     if (rl < 1) rl = 1;
     k_decimate<<<grid_1d(nl), 256, 0, st>>>(in, il, ny, nx, lz, ly, lx, s);
-    cudaError_t e = fy_launch_guided_fused(il, ma, mb, lz, ly, lx, rl, eps, 1, sms, st);
+    cudaError_t e = fy_launch_guided_fused(il, ma, mb, lz, ly, lx, rl, eps, 1, sms, st, eps_ptr);
     if (e != cudaSuccess) return e;
     dim3 grid(ceil_div_i(nx, 128), ny, nz);
     k_upsample_apply<<<grid, 128, 0, st>>>(in, out, ma, mb, nz, ny, nx, lz, ly, lx, s);

@@ -25,6 +25,9 @@ struct DeconvLaunch {
 };
 cudaError_t fy_launch_deconv(const DeconvLaunch& d, cudaStream_t st);
 size_t fy_deconv_spec_elems(const SpecGeom& g);
+cudaError_t fy_launch_spec_y(float2* spec, const SpecGeom& g, const FftPlan& ply, const float2* twy, int nplanes,
+                             int sign, int keep_rows, cudaStream_t st);
+cudaError_t fy_launch_cfft3d(float2* c, int nz, int ny, int nx, int nxp, int sign, cudaStream_t st);
 
 // Elementwise stream ops (stream.c)
 cudaError_t fy_launch_u8_to_phys(const uint8_t* in, float* out, size_t n, float lo, float scale,
@@ -37,11 +40,12 @@ cudaError_t fy_launch_u8_to_float(const uint8_t* in, float* out, size_t n, cudaS
 // Guided filter / box mean (fy_guided.cu)
 size_t fy_guided_fused_smem(int r);
 cudaError_t fy_launch_guided_fused(const float* in, float* out, float* out_b, int nz, int ny, int nx, int r,
-                                   float eps, int mode, int sms, cudaStream_t st);
+                                   float eps, int mode, int sms, cudaStream_t st, const float* eps_ptr = nullptr);
 cudaError_t fy_launch_guided_generic(const float* in, float* out, float* ws, int nz, int ny, int nx, int r,
                                      float eps, cudaStream_t st, int& launches);
 cudaError_t fy_launch_guided_fast(const float* in, float* out, float* ws, int nz, int ny, int nx, int r,
-                                  float eps, int s, int sms, cudaStream_t st, int& launches);
+                                  float eps, int s, int sms, cudaStream_t st, int& launches,
+                                  const float* eps_ptr = nullptr);
 cudaError_t fy_launch_box_mean(const float* in, float* out, float* tmp, int nz, int ny, int nx, int r,
                                cudaStream_t st, int& launches);
 
@@ -66,11 +70,18 @@ cudaError_t fy_launch_dering_apply(float* f, const float* ring, const int* have_
                                    int slab_z, double cy, double cx, long z0, long y0, long x0, long dz, long dy,
                                    long dx, double scale, cudaStream_t st);
 
-// Opt a kernel into > 48 KB of dynamic shared memory (idempotent).
+// Per-kernel profiling marks (fy_context.cu): records a CUDA event on st after a launch
+// when profiling is enabled on the calling thread; no-op otherwise.
+void fy_prof_mark(cudaStream_t st, const char* name);
+
+// Opt a kernel into a large dynamic shared-memory carve-out. Above 32 KB of dynamic smem
+// (the default limit is 48 KB including static smem), raise the kernel's limit once per
+// device and size; cached so launches pay the driver call only when the size grows.
+cudaError_t fy_smem_optin_raw(const void* kernel, size_t bytes);
 template <class K>
 inline cudaError_t fy_smem_optin(K kernel, size_t bytes) {
-    if (bytes <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (bytes <= 32 * 1024) return cudaSuccess;
+    return fy_smem_optin_raw((const void*)kernel, bytes);
 }
 
 // Runtime elements-per-thread (fy_fft_e) -> compile-time E for kernel instantiation.

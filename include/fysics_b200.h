@@ -197,6 +197,53 @@ int  fy_gpu_dering_apply(const fy_gpu_dering *h, float *d_f, long z0, long y0, l
                          long dy, long dx, double scale, void *stream);
 int  fy_gpu_dering_download(const fy_gpu_dering *h, fy_dering *d, long *detected, void *stream);
 
+/* Phase correlation of `npairs` device volume pairs (fixed[i], moving[i] at a stride of
+ * nz*ny*nx floats) with fy_phase_correlate's semantics (fysics.h:311-313). d_scratch holds
+ * fy_gpu_phase_correlate_scratch_bytes(). Results go to host arrays: shift[3*npairs],
+ * peak[npairs] and peak_index[npairs] (nullable; flat index of the integer peak in the
+ * power-of-two padded surface), status[npairs] (0 ok, 1 degenerate input). Synchronises
+ * `stream` before returning. */
+size_t fy_gpu_phase_correlate_scratch_bytes(int nz, int ny, int nx);
+int    fy_gpu_phase_correlate_batch(const float *d_fixed, const float *d_moving, int npairs,
+                                    int nz, int ny, int nx, int window, void *d_scratch,
+                                    double *shift, double *peak, long long *peak_index,
+                                    int *status, void *stream);
+
+/* The per-cube restoration chain on device buffers: dewindow (fused into the
+ * deconvolution) -> Wiener deconvolution -> noise model -> guided filter with
+ * eps = fy_guided_eps_for_noise(noise_ref) taken on the device -> ring subtraction.
+ * No host round trip inside. Workspaces are the calling thread's. */
+typedef struct {
+    int    deconv_kind;          /* 0 fy_deconvolve, 1 fy_deconvolve_matched, 2 anisotropic Paganin */
+    double deconv_param;         /* reg / tikhonov; <= 0 takes the entry point's default */
+    double fz2_scale;            /* kind 2: (sigma_z/sigma_xy)^2 */
+    int    noise_win;            /* fy_estimate_noise arguments */
+    double noise_flat_pct;
+    double noise_ref_intensity;
+    double guided_eps;           /* > 0: fixed eps instead of the noise model */
+    int    guided_radius;
+    int    guided_s;             /* <= 1 exact, >= 2 decimated fast variant */
+    fy_gpu_dering *dering;       /* NULL: no ring removal */
+    int    dering_accumulate;    /* 1: accumulate this cube's u8 input and vote before applying */
+    int    dering_ss;
+    int    dering_hp_win;
+    unsigned int dering_min_cnt;
+    double dering_min_amp, dering_max_amp;
+    double dering_scale;         /* ring u8 units -> output units */
+    long   z0, y0, x0;           /* global offset of the cube (ring geometry) */
+} fy_restore_cfg;
+void fy_restore_cfg_default(fy_restore_cfg *cfg);
+int  fy_gpu_restore_u8(const unsigned char *d_u8, float *d_out, int nz, int ny, int nx,
+                       double f32_min, double f32_max, const fy_physics *p,
+                       const fy_restore_cfg *cfg, void *stream);
+
+/* Per-kernel timing: CUDA events recorded on the launching stream after every launch of
+ * the instrumented kernels. read(i) gives mark i's name and the ms since mark i-1, once
+ * the stream has been synchronised. */
+int fy_gpu_profile_start(int capacity, void *stream);
+int fy_gpu_profile_stop(void);
+int fy_gpu_profile_read(int i, const char **name, float *ms);
+
 #ifdef __cplusplus
 }
 #endif
