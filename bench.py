@@ -257,7 +257,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--cpu-phantom", action="store_true")
+    ap.add_argument("--size", type=int, default=512, help="cube edge (512 = the benchmark workload)")
     args = ap.parse_args()
+    global SHAPE, WORKLOAD
+    if args.size != 512:
+        SHAPE = (args.size,) * 3
+        WORKLOAD = WORKLOAD.replace("512^3", f"{args.size}^3")
     args.warmup = max(args.warmup, 3)
     rank, world, local, dist = dist_setup(args.gpus)
     if args.impl == "reference":
@@ -390,7 +395,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "Mvoxel/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "cube": "512^3 u8", "deltabeta_scale": db_scale,
+        "config": {"workload": WORKLOAD, "cube": f"{SHAPE[0]}^3 u8", "deltabeta_scale": db_scale,
                    "l2": "inputs and working set (~3 GB) larger than the 126 MB L2",
                    "parallelism": f"replicas x{world} (one cube per GPU, no collective)"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),

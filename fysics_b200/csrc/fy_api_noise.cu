@@ -33,7 +33,7 @@ extern "C" int fy_estimate_noise(const float* in, int nz, int ny, int nx, int wi
     fy::ws_acquire(st);
     cudaError_t e;
     if ((e = c.vin.ensure(n * sizeof(float))) != cudaSuccess) return fail_cuda(e, what);
-    if ((e = c.aux.ensure(2 * n * sizeof(float))) != cudaSuccess) return fail_cuda(e, what);
+    if ((e = c.aux.ensure(fy_noise_scratch_floats(n) * sizeof(float))) != cudaSuccess) return fail_cuda(e, what);
     if ((e = c.small.ensure(fy_noise_ctl_bytes())) != cudaSuccess) return fail_cuda(e, what);
     if ((e = c.pin.ensure(sizeof(ModelHost))) != cudaSuccess) return fail_cuda(e, what);
     if ((e = cudaMemcpyAsync(c.vin.p, in, n * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess)
@@ -61,7 +61,7 @@ extern "C" int fy_estimate_noise(const float* in, int nz, int ny, int nx, int wi
 // (d_ctl); fy_gpu_noise_model() copies it out, fy_gpu_noise_eps() gives the device address
 // of the guided eps float so a chained filter needs no host round trip.
 extern "C" size_t fy_gpu_noise_scratch_bytes(int nz, int ny, int nx) {
-    return 2 * (size_t)nz * ny * nx * sizeof(float) + fy_noise_ctl_bytes();
+    return fy_noise_scratch_floats((size_t)nz * ny * nx) * sizeof(float) + fy_noise_ctl_bytes();
 }
 extern "C" int fy_gpu_estimate_noise(const float* d_in, int nz, int ny, int nx, int win, double flat_pct,
                                      double ref_intensity, void* d_scratch, void* stream) {
@@ -73,7 +73,7 @@ extern "C" int fy_gpu_estimate_noise(const float* d_in, int nz, int ny, int nx, 
     if ((rc = fy::ensure_ctx())) return rc;
     const size_t n = (size_t)nz * ny * nx;
     float* stats = (float*)d_scratch;
-    void* ctl = (char*)d_scratch + 2 * n * sizeof(float);
+    void* ctl = (char*)d_scratch + fy_noise_scratch_floats(n) * sizeof(float);
     int launches = 0;
     cudaError_t e = fy_launch_estimate_noise(d_in, nz, ny, nx, win, flat_pct, ref_intensity, stats, ctl,
                                              ctx().sms, (cudaStream_t)stream, launches);
@@ -90,7 +90,7 @@ extern "C" int fy_gpu_noise_model(const void* d_scratch, int nz, int ny, int nx,
     fy::ThreadCtx& c = ctx();
     cudaError_t e = c.pin.ensure(sizeof(ModelHost));
     if (e != cudaSuccess) return fail_cuda(e, "fy_gpu_noise_model");
-    const void* ctl = (const char*)d_scratch + 2 * (size_t)nz * ny * nx * sizeof(float);
+    const void* ctl = (const char*)d_scratch + fy_noise_scratch_floats((size_t)nz * ny * nx) * sizeof(float);
     ModelHost* mh = (ModelHost*)c.pin.p;
     cudaStream_t st = (cudaStream_t)stream;
     if ((e = fy_noise_read(ctl, &mh->g, &mh->b, &mh->noise_ref, &mh->ref_intensity, &mh->used, st)) != cudaSuccess)
@@ -101,5 +101,5 @@ extern "C" int fy_gpu_noise_model(const void* d_scratch, int nz, int ny, int nx,
     return FY_OK;
 }
 extern "C" const float* fy_gpu_noise_eps(const void* d_scratch, int nz, int ny, int nx) {
-    return fy_noise_eps_ptr((const char*)d_scratch + 2 * (size_t)nz * ny * nx * sizeof(float));
+    return fy_noise_eps_ptr((const char*)d_scratch + fy_noise_scratch_floats((size_t)nz * ny * nx) * sizeof(float));
 }

@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(KBc<E>::nt, 2) k_crow(float2* __restrict__ c, 
     }
     __syncthreads();
     const Lane ln(wlog);
-    line_fft<E>(s, LP, ln.l, ln.tl, pl, stw, sign,
+    line_fft<E>(s + ln.l, LP, ln.tl, pl, stw, sign,
                 [&](int i) { return s[i * LP + ln.l]; },
                 [&](int i, float2 v) { s[i * LP + ln.l] = v; });
     __syncthreads();
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(KBc<E>::nt, 2) k_ccol(float2* __restrict__ c, 
     float2* col = c + (size_t)blockIdx.y * bstride + (size_t)blockIdx.x * W + ln.l;
     load_twiddles(stw, tw, pl.n);
     __syncthreads();
-    line_fft<E>(s, W, ln.l, ln.tl, pl, stw, sign,
+    line_fft<E>(s + ln.l, W, ln.tl, pl, stw, sign,
                 [&](int i) { return col[(size_t)i * pstride]; },
                 [&](int i, float2 v) { col[(size_t)i * pstride] = v; });
 }

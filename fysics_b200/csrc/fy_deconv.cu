@@ -19,16 +19,6 @@ constexpr int MAXNT = FY_FFT_MAXNT;
 // Threads per CTA never exceed W*n/E: 512 for 2^k lines (E=16), 256 for 3*2^k (E=24).
 template <int E> struct KB { static constexpr int nt = (E % 3 == 0) ? 256 : 512; };
 
-struct SrcF32 {
-    const float* p;
-    FY_D float at(size_t row, int x, int nx, float, float) const { return __ldg(p + row * nx + x); }
-};
-struct SrcU8 {
-    const uint8_t* p;
-    FY_D float at(size_t row, int x, int nx, float lo, float scale) const {
-        return __fmaf_rn((float)__ldg(p + row * nx + x), scale, lo);
-    }
-};
 
 // Thread -> (line l, thread-in-line tl) with the line index fastest.
 struct Lane {
@@ -37,48 +27,83 @@ struct Lane {
 };
 
 // ---------------------------------------------------------------- P1
-// Rows q = z*ny + y (z < nz, y < ny) paired (2m, 2m+1) into one complex line; a CTA owns
-// W lines. Rows are staged through shared memory with x the fastest thread index, so
-// global reads are row-contiguous and every thread has E independent loads in flight.
-template <int E, class Src>
-__global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(Src src, float lo, float scale, float2* __restrict__ spec,
-                                                    SpecGeom g, const __grid_constant__ FftPlan pl,
-                                                    const float2* __restrict__ tw, int wlog, FastDiv dpx,
-                                                    FastDiv dhx) {
+// Rows q = z*ny + y (z < nz, y < ny) paired (2m, 2m+1) into one complex line; a CTA owns W
+// lines, staged line-major in shared memory (pitch px+1, odd: conflict-free for the FFT's
+// line-strided accesses). Each thread loads the same VEC-wide chunk of both rows of a line
+// pair, so it writes VEC consecutive complex values; reflect padding is filled from the
+// staged line afterwards.
+template <class T, int VEC> struct VecLoad;
+template <> struct VecLoad<float, 4> {
+    static FY_D void run(const float* p, float* v) {
+        const float4 x = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    }
+};
+template <> struct VecLoad<uint8_t, 4> {
+    static FY_D void run(const uint8_t* p, float* v) {
+        const uchar4 x = __ldg(reinterpret_cast<const uchar4*>(p));
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    }
+};
+template <class T> struct VecLoad<T, 1> {
+    static FY_D void run(const T* p, float* v) { v[0] = (float)__ldg(p); }
+};
+
+template <int E, class T, int VEC>
+__global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(const T* __restrict__ src, float lo, float scale, int is_u8,
+                                                        float2* __restrict__ spec, SpecGeom g,
+                                                        const __grid_constant__ FftPlan pl,
+                                                        const float2* __restrict__ tw, int wlog, FastDiv dchunk,
+                                                        FastDiv dhx, FastDiv dpad) {
     extern __shared__ float4 smem4[];
-    const int W = 1 << wlog, LP = W + 1;
+    const int W = 1 << wlog, LPX = g.px + 1;
     float2* s = reinterpret_cast<float2*>(smem4);
-    float2* stw = s + pl.n * LP;
+    float2* stw = s + W * LPX;
     const long Q = (long)g.nz * g.ny;
     const long q0 = (long)blockIdx.x * 2 * W;
     load_twiddles(stw, tw, pl.n);
-#pragma unroll
-    for (int e = 0; e < E; ++e) {                       // W*px = E*blockDim.x elements
-        const int idx = threadIdx.x + e * blockDim.x;
-        const int l = dpx.div(idx), x = idx - l * g.px;
+    const int nch = g.nx / VEC;
+    for (int it = threadIdx.x; it < W * nch; it += blockDim.x) {
+        const int l = dchunk.div(it), x = (it - l * nch) * VEC;
         const long qa = q0 + 2 * l, qb = qa + 1;
-        const int sx = x < g.nx ? x : (g.zero_pad ? -1 : reflect_idx(x, g.nx));
-        float a = 0.f, b = 0.f;
-        if (sx >= 0) {
-            if (qa < Q) a = src.at((size_t)qa, sx, g.nx, lo, scale);
-            if (qb < Q) b = src.at((size_t)qb, sx, g.nx, lo, scale);
+        float va[VEC], vb[VEC];
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) va[j] = vb[j] = 0.f;
+        if (qa < Q) VecLoad<T, VEC>::run(src + qa * g.nx + x, va);
+        if (qb < Q) VecLoad<T, VEC>::run(src + qb * g.nx + x, vb);
+        float2* dst = s + l * LPX + x;
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            float a = va[j], b = vb[j];
+            if (is_u8) {                                   // fy_u8_to_phys, FMA as the reference build
+                a = qa < Q ? __fmaf_rn(a, scale, lo) : 0.f;
+                b = qb < Q ? __fmaf_rn(b, scale, lo) : 0.f;
+            }
+            dst[j] = make_float2(a, b);
         }
-        s[x * LP + l] = make_float2(a, b);
+    }
+    const int npad = g.px - g.nx;
+    if (npad > 0) {
+        __syncthreads();
+        for (int it = threadIdx.x; it < W * npad; it += blockDim.x) {
+            const int l = dpad.div(it), x = g.nx + (it - l * npad);
+            s[l * LPX + x] = g.zero_pad ? make_float2(0.f, 0.f) : s[l * LPX + reflect_idx(x, g.nx)];
+        }
     }
     __syncthreads();
     const Lane ln(wlog);
-    line_fft<E>(s, LP, ln.l, ln.tl, pl, stw, -1.f,
-                [&](int i) { return s[i * LP + ln.l]; },
-                [&](int i, float2 v) { s[i * LP + ln.l] = v; });
+    float2* line = s + ln.l * LPX;
+    line_fft<E>(line, 1, ln.tl, pl, stw, -1.f,
+                [&](int i) { return line[i]; },
+                [&](int i, float2 v) { line[i] = v; });
     __syncthreads();
-    const int tot = W * g.hx;
-    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < W * g.hx; idx += blockDim.x) {
         const int l = dhx.div(idx), k = idx - l * g.hx;
         const long qa = q0 + 2 * l, qb = qa + 1;
         if (qa >= Q) continue;
         const int mk = k == 0 ? 0 : g.px - k;
         float2 A, B;
-        untangle(s[k * LP + l], s[mk * LP + l], A, B);
+        untangle(s[l * LPX + k], s[l * LPX + mk], A, B);
         spec[((size_t)(qa / g.ny) * g.py + (qa % g.ny)) * g.hxp + k] = A;
         if (qb < Q) spec[((size_t)(qb / g.ny) * g.py + (qb % g.ny)) * g.hxp + k] = B;
     }
@@ -99,7 +124,7 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_y_fwd(float2* __restrict__ spe
     float2* col = spec + (size_t)blockIdx.y * g.py * g.hxp + blockIdx.x * W + ln.l;
     load_twiddles(stw, tw, pl.n);
     __syncthreads();
-    line_fft<E>(s, W, ln.l, ln.tl, pl, stw, -1.f,
+    line_fft<E>(s + ln.l, W, ln.tl, pl, stw, -1.f,
                 [&](int i) {
                     const int ys = i < g.ny ? i : (g.zero_pad ? -1 : reflect_idx(i, g.ny));
                     return ys < 0 ? make_float2(0.f, 0.f) : col[(size_t)ys * g.hxp];
@@ -132,7 +157,7 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_z_weight(float2* __restrict__ 
     for (int i = threadIdx.x; i < pl.n; i += blockDim.x) sfz[i] = fz2[i];
     for (int i = threadIdx.x; i <= FY_LUT_N; i += blockDim.x) slut[i] = lut[i];
     __syncthreads();
-    line_fft<E>(s, W, ln.l, ln.tl, pl, stw, -1.f,
+    line_fft<E>(s + ln.l, W, ln.tl, pl, stw, -1.f,
                 [&](int i) {
                     const int zs = i < g.nz ? i : (g.zero_pad ? -1 : reflect_idx(i, g.nz));
                     return zs < 0 ? make_float2(0.f, 0.f) : col[(size_t)zs * zstride];
@@ -153,7 +178,7 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_z_weight(float2* __restrict__ 
         }
     }
     __syncthreads();
-    line_fft<E>(s, W, ln.l, ln.tl, pl, stw, +1.f,
+    line_fft<E>(s + ln.l, W, ln.tl, pl, stw, +1.f,
                 [&](int i) { return s[i * W + ln.l]; },
                 [&](int z, float2 v) { if (z < g.nz) col[(size_t)z * zstride] = v; });
 }
@@ -170,49 +195,57 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_y_inv(float2* __restrict__ spe
     float2* col = spec + (size_t)blockIdx.y * g.py * g.hxp + blockIdx.x * W + ln.l;
     load_twiddles(stw, tw, pl.n);
     __syncthreads();
-    line_fft<E>(s, W, ln.l, ln.tl, pl, stw, +1.f,
+    line_fft<E>(s + ln.l, W, ln.tl, pl, stw, +1.f,
                 [&](int i) { return col[(size_t)i * g.hxp]; },
                 [&](int i, float2 v) { if (i < keep_rows) col[(size_t)i * g.hxp] = v; });
 }
 
 // ---------------------------------------------------------------- P5
-template <int E>
+// Line-major like P1; the two output rows of a line are written VEC floats at a time.
+template <int E, int VEC>
 __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_inv(const float2* __restrict__ spec, float* __restrict__ dst,
-                                                    SpecGeom g, const __grid_constant__ FftPlan pl,
-                                                    const float2* __restrict__ tw, float invN, int wlog,
-                                                    FastDiv dnx, FastDiv dhx) {
+                                                        SpecGeom g, const __grid_constant__ FftPlan pl,
+                                                        const float2* __restrict__ tw, float invN, int wlog,
+                                                        FastDiv dchunk, FastDiv dhx) {
     extern __shared__ float4 smem4[];
-    const int W = 1 << wlog, LP = W + 1;
+    const int W = 1 << wlog, LPX = g.px + 1;
     float2* s = reinterpret_cast<float2*>(smem4);
-    float2* stw = s + pl.n * LP;
+    float2* stw = s + W * LPX;
     const long Q = (long)g.nz * g.ny;
     const long q0 = (long)blockIdx.x * 2 * W;
     load_twiddles(stw, tw, pl.n);
     const int hi_max = g.px - g.hx;                 // m in [1, px-hx] mirrors to px-m
-    const int tot = W * g.hx;
-#pragma unroll 4
-    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < W * g.hx; idx += blockDim.x) {
         const int l = dhx.div(idx), k = idx - l * g.hx;
         const long qa = q0 + 2 * l, qb = qa + 1;
         const float2 A = qa < Q ? spec[((size_t)(qa / g.ny) * g.py + (qa % g.ny)) * g.hxp + k] : make_float2(0.f, 0.f);
         const float2 B = qb < Q ? spec[((size_t)(qb / g.ny) * g.py + (qb % g.ny)) * g.hxp + k] : make_float2(0.f, 0.f);
-        s[k * LP + l] = pack_lo(A, B);
-        if (k >= 1 && k <= hi_max) s[(g.px - k) * LP + l] = pack_hi(A, B);
+        s[l * LPX + k] = pack_lo(A, B);
+        if (k >= 1 && k <= hi_max) s[l * LPX + g.px - k] = pack_hi(A, B);
     }
     __syncthreads();
     const Lane ln(wlog);
-    line_fft<E>(s, LP, ln.l, ln.tl, pl, stw, +1.f,
-                [&](int i) { return s[i * LP + ln.l]; },
-                [&](int i, float2 v) { s[i * LP + ln.l] = v; });
+    float2* line = s + ln.l * LPX;
+    line_fft<E>(line, 1, ln.tl, pl, stw, +1.f,
+                [&](int i) { return line[i]; },
+                [&](int i, float2 v) { line[i] = v; });
     __syncthreads();
-    const int totx = W * g.nx;
-    for (int idx = threadIdx.x; idx < totx; idx += blockDim.x) {
-        const int l = dnx.div(idx), x = idx - l * g.nx;
+    const int nch = g.nx / VEC;
+    for (int it = threadIdx.x; it < W * nch; it += blockDim.x) {
+        const int l = dchunk.div(it), x = (it - l * nch) * VEC;
         const long qa = q0 + 2 * l, qb = qa + 1;
         if (qa >= Q) continue;
-        const float2 v = s[x * LP + l];
-        dst[(size_t)qa * g.nx + x] = v.x * invN;
-        if (qb < Q) dst[(size_t)qb * g.nx + x] = v.y * invN;
+        const float2* v = s + l * LPX + x;
+        if (VEC == 4) {
+            *reinterpret_cast<float4*>(dst + qa * g.nx + x) =
+                make_float4(v[0].x * invN, v[1].x * invN, v[2].x * invN, v[3].x * invN);
+            if (qb < Q)
+                *reinterpret_cast<float4*>(dst + qb * g.nx + x) =
+                    make_float4(v[0].y * invN, v[1].y * invN, v[2].y * invN, v[3].y * invN);
+        } else {
+            dst[qa * g.nx + x] = v[0].x * invN;
+            if (qb < Q) dst[qb * g.nx + x] = v[0].y * invN;
+        }
     }
 }
 
@@ -224,24 +257,26 @@ cudaError_t fy_launch_deconv(const DeconvLaunch& d, cudaStream_t st) {
     const SpecGeom& g = d.g;
     cudaError_t e = cudaSuccess;
     const long Q = (long)g.nz * g.ny;
-    // P1: X forward, rows paired two per line
+    // P1: X forward, rows paired two per line (line-major staging)
     {
         const TileShape t = fy_tile_shape(g.px);
-        const size_t smem = (size_t)g.px * (t.W + 1) * sizeof(float2) + (size_t)g.px * sizeof(float2);
+        const size_t smem = (size_t)t.W * (g.px + 1) * sizeof(float2) + (size_t)g.px * sizeof(float2);
         const unsigned grid = (unsigned)((Q + 2 * t.W - 1) / (2 * t.W));
+        const int esz = d.src_u8 ? 1 : 4;
+        const bool vec = g.nx % 4 == 0 && ((uintptr_t)d.src % (4 * esz)) == 0;
+        const int pad = g.px - g.nx > 0 ? g.px - g.nx : 1;
         e = fy_with_e(t.E, [&](auto ec) -> cudaError_t {
             constexpr int E = decltype(ec)::value;
-            if (d.src_u8) {
-                auto k = k_x_fwd<E, SrcU8>;
-                cudaError_t e2 = fy_smem_optin(k, smem);
-                if (e2 != cudaSuccess) return e2;
-                k<<<grid, t.NT, smem, st>>>(SrcU8{(const uint8_t*)d.src}, d.lo, d.scale, d.spec, g, d.plx, d.twx, t.wlog, FastDiv(g.px), FastDiv(g.hx));
-            } else {
-                auto k = k_x_fwd<E, SrcF32>;
-                cudaError_t e2 = fy_smem_optin(k, smem);
-                if (e2 != cudaSuccess) return e2;
-                k<<<grid, t.NT, smem, st>>>(SrcF32{(const float*)d.src}, 0.f, 0.f, d.spec, g, d.plx, d.twx, t.wlog, FastDiv(g.px), FastDiv(g.hx));
-            }
+            cudaError_t e2 = cudaSuccess;
+            const FastDiv dch(vec ? g.nx / 4 : g.nx), dhx(g.hx), dpad(pad);
+#define FY_P1(T, V)                                                                                   \
+            { auto k = k_x_fwd<E, T, V>;                                                              \
+              if ((e2 = fy_smem_optin(k, smem)) != cudaSuccess) return e2;                            \
+              k<<<grid, t.NT, smem, st>>>((const T*)d.src, d.lo, d.scale, d.src_u8, d.spec, g, d.plx, d.twx, \
+                                          t.wlog, dch, dhx, dpad); }
+            if (d.src_u8) { if (vec) FY_P1(uint8_t, 4) else FY_P1(uint8_t, 1) }
+            else { if (vec) FY_P1(float, 4) else FY_P1(float, 1) }
+#undef FY_P1
             return cudaGetLastError();
         });
         if (e != cudaSuccess) return e;
@@ -296,18 +331,26 @@ cudaError_t fy_launch_deconv(const DeconvLaunch& d, cudaStream_t st) {
         if (e != cudaSuccess) return e;
     }
     fy_prof_mark(st, "deconv.y_inv");
-    // P5: X C2R, crop, 1/N
+    // P5: X C2R, crop, 1/N (line-major staging, vector stores when rows are 16-byte aligned)
     {
         const TileShape t = fy_tile_shape(g.px);
-        const size_t smem = (size_t)g.px * (t.W + 1) * sizeof(float2) + (size_t)g.px * sizeof(float2);
+        const size_t smem = (size_t)t.W * (g.px + 1) * sizeof(float2) + (size_t)g.px * sizeof(float2);
         const unsigned grid = (unsigned)((Q + 2 * t.W - 1) / (2 * t.W));
         const float invN = 1.0f / ((float)g.pz * (float)g.py * (float)g.px);   // paganin.c:263
+        const bool vec = g.nx % 4 == 0 && ((uintptr_t)d.dst % 16) == 0;
         e = fy_with_e(t.E, [&](auto ec) -> cudaError_t {
             constexpr int E = decltype(ec)::value;
-            auto k = k_x_inv<E>;
-            cudaError_t e2 = fy_smem_optin(k, smem);
-            if (e2 != cudaSuccess) return e2;
-            k<<<grid, t.NT, smem, st>>>(d.spec, d.dst, g, d.plx, d.twx, invN, t.wlog, FastDiv(g.nx), FastDiv(g.hx));
+            cudaError_t e2 = cudaSuccess;
+            const FastDiv dch(vec ? g.nx / 4 : g.nx), dhx(g.hx);
+            if (vec) {
+                auto k = k_x_inv<E, 4>;
+                if ((e2 = fy_smem_optin(k, smem)) != cudaSuccess) return e2;
+                k<<<grid, t.NT, smem, st>>>(d.spec, d.dst, g, d.plx, d.twx, invN, t.wlog, dch, dhx);
+            } else {
+                auto k = k_x_inv<E, 1>;
+                if ((e2 = fy_smem_optin(k, smem)) != cudaSuccess) return e2;
+                k<<<grid, t.NT, smem, st>>>(d.spec, d.dst, g, d.plx, d.twx, invN, t.wlog, dch, dhx);
+            }
             return cudaGetLastError();
         });
         if (e != cudaSuccess) return e;

@@ -62,19 +62,29 @@ __global__ void __launch_bounds__(256) k_dering_accum(const uint8_t* __restrict_
 // ---------------------------------------------------------------- finalize
 // sum_f/cnt: float sums and counts exactly as the reference stores them (fy_dering.sum is
 // float), so p = sum/cnt is the same IEEE float division.
-__global__ void k_dering_smooth(const float* __restrict__ sum_f, const unsigned int* __restrict__ cnt,
-                                float* __restrict__ p, float* __restrict__ hp, unsigned char* __restrict__ vd,
-                                int nslab, int ns, int nr, int hw, unsigned min_cnt) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;     // (slab, sector)
-    if (id >= nslab * ns) return;
-    const size_t off = (size_t)id * nr;
-    for (int r = 0; r < nr; ++r) {
+//
+// The reference sweeps radii in order and invalidates bin r when fewer than hw valid bins
+// lie within +-hw, which later bins then see (dering.c:161-169). One block per (slab,
+// sector): all radii are evaluated in parallel against the original validity; if no bin
+// would be invalidated, that IS the sequential result (the first invalidation in the sweep
+// would have been seen with unmodified validity). Otherwise one thread resumes the sweep
+// sequentially from the first invalidated radius, which reproduces it exactly.
+__global__ void __launch_bounds__(256) k_dering_smooth(const float* __restrict__ sum_f,
+                                                       const unsigned int* __restrict__ cnt,
+                                                       float* __restrict__ p, float* __restrict__ hp,
+                                                       unsigned char* __restrict__ vd, int ns, int nr, int hw,
+                                                       unsigned min_cnt) {
+    __shared__ int s_first;
+    const size_t off = (size_t)blockIdx.x * nr;       // (slab, sector) row
+    if (threadIdx.x == 0) s_first = nr;
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
         const unsigned c = cnt[off + r];
         const unsigned char v = c >= min_cnt;
         vd[off + r] = v;
         p[off + r] = v ? sum_f[off + r] / (float)c : 0.0f;
     }
-    for (int r = 0; r < nr; ++r) {
+    __syncthreads();
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
         if (!vd[off + r]) { hp[off + r] = 0.0f; continue; }
         double acc = 0;
         int c = 0;
@@ -82,7 +92,20 @@ __global__ void k_dering_smooth(const float* __restrict__ sum_f, const unsigned 
         for (int j = lo; j <= hi; ++j)
             if (vd[off + j]) { acc += p[off + j]; ++c; }
         if (c >= hw) hp[off + r] = p[off + r] - (float)(acc / c);
-        else { hp[off + r] = 0.0f; vd[off + r] = 0; }
+        else atomicMin(&s_first, r);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_first < nr) {           // rare: sequential from the first change
+        for (int r = s_first; r < nr; ++r) {
+            if (!vd[off + r]) { hp[off + r] = 0.0f; continue; }
+            double acc = 0;
+            int c = 0;
+            const int lo = r - hw < 0 ? 0 : r - hw, hi = r + hw >= nr ? nr - 1 : r + hw;
+            for (int j = lo; j <= hi; ++j)
+                if (vd[off + j]) { acc += p[off + j]; ++c; }
+            if (c >= hw) hp[off + r] = p[off + r] - (float)(acc / c);
+            else { hp[off + r] = 0.0f; vd[off + r] = 0; }
+        }
     }
 }
 
@@ -137,15 +160,21 @@ __global__ void __launch_bounds__(256) k_dering_apply(float* __restrict__ f, con
     const double gy = (double)(y0 + y) - cy, gx = (double)(x0 + x) - cx;
     const int ri = (int)(sqrt(gy * gy + gx * gx) + 0.5);
     if (ri >= nr) return;
-    for (long z = 0; z < dz; ++z) {
-        long s = (z0 + z) / slab_z;
-        if (s < 0) s = 0;
-        if (s >= nslab) s = nslab - 1;
-        float* p = f + ((size_t)z * dy + y) * dx + x;
-        const float v0 = *p;
-        if (v0 <= 0.0f) continue;
-        const float v = v0 - sc * __ldg(ring + (size_t)s * nr + ri);
-        *p = v > 0.0f ? v : 0.0f;
+    const size_t zs = (size_t)dy * dx;
+    float* col = f + (size_t)y * dx + x;
+    for (long z = 0; z < dz; z += 4) {
+        float v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = (z + k < dz) ? col[(size_t)(z + k) * zs] : 0.0f;   // 4 loads in flight
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (z + k >= dz || v[k] <= 0.0f) continue;     // masked voxels untouched
+            long s = (z0 + z + k) / slab_z;
+            if (s < 0) s = 0;
+            if (s >= nslab) s = nslab - 1;
+            const float w = v[k] - sc * __ldg(ring + (size_t)s * nr + ri);
+            col[(size_t)(z + k) * zs] = w > 0.0f ? w : 0.0f;
+        }
     }
 }
 
@@ -185,7 +214,7 @@ cudaError_t fy_launch_dering_finalize(const float* sum_f, const unsigned int* cn
     cudaError_t e = cudaMemsetAsync(detected, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     const int hw = hp_win / 2;
-    k_dering_smooth<<<(nslab * ns + 63) / 64, 64, 0, st>>>(sum_f, cnt, p, hp, vd, nslab, ns, nr, hw, min_cnt);
+    k_dering_smooth<<<nslab * ns, 256, 0, st>>>(sum_f, cnt, p, hp, vd, ns, nr, hw, min_cnt);
     const long nv = (long)nslab * nr;
     k_dering_vote<<<(unsigned)((nv + 127) / 128), 128, 0, st>>>(hp, vd, ring, nslab, ns, nr, (float)min_amp,
                                                                 (float)max_amp, detected);

@@ -176,10 +176,11 @@ FY_D void with_radix(int R, F&& f) {
 
 // Full line transform. `ld(i)` supplies input point i (called once per owned point,
 // before any shared-memory write); `st(i, v)` receives output point i. Pass boundaries
-// exchange through `s` (point-major, pitch LP, this thread's line l). All threads of
-// the CTA must call this together (it contains __syncthreads()).
+// exchange through shared memory at sline[i*ps] (sline = this thread's line: s + l for a
+// point-major tile of pitch ps, or s + l*pitch with ps = 1 for a line-major tile). All
+// threads of the CTA must call this together (it contains __syncthreads()).
 template <int E, class LD, class ST>
-FY_D void line_fft(float2* __restrict__ s, int LP, int l, int tl, const FftPlan& pl,
+FY_D void line_fft(float2* __restrict__ sline, int ps, int tl, const FftPlan& pl,
                    const float2* __restrict__ tw, float sign, LD ld, ST st) {
     constexpr int C = (E % 3 == 0) ? 3 : 1;
     const int n = pl.n, tpl = n / E;
@@ -192,8 +193,8 @@ FY_D void line_fft(float2* __restrict__ s, int LP, int l, int tl, const FftPlan&
     }
     with_radix<E>(pl.radix[0], [&](auto Rc) { pass_load<E, decltype(Rc)::value>(v, n, tl, tpl, ld); });
     __syncthreads();
-    auto sld = [&](int i) { return s[i * LP + l]; };
-    auto sst = [&](int i, float2 x) { s[i * LP + l] = x; };
+    auto sld = [&](int i) { return sline[i * ps]; };
+    auto sst = [&](int i, float2 x) { sline[i * ps] = x; };
     for (int p = 0; p < pl.npass; ++p) {
         const int R = pl.radix[p];
         const int nslog = pl.nslog[p];

@@ -91,165 +91,200 @@ cudaError_t box3(const float* in, float* out, float* tmp, int nz, int ny, int nx
 }
 
 // ---------------------------------------------------------------- fused z-sliding path
+// CTA = 32 x 16 output columns sliding along z, 256 threads. Per input plane zi:
+//   1. stage u = I - c over the tile + 2R halo (zeros outside the volume)
+//   2. X means of u, u^2 over the a/b support columns (4 columns per thread)
+//   3. Y means (4 rows per thread) pushed into a (2R+1)-plane z ring held in registers;
+//      the ring gives mean/corr of plane zc = zi - R -> a, b over the support
+//   4. X means of a, b over the output columns
+//   5. Y means into a second register ring -> box(a), box(b) of plane zo = zi - 2R ->
+//      out = box(a)*I + box(b)
+// Widths are padded to multiples of 4 so every 4-wide segment stays inside its array.
 constexpr int GTY = 16, GTX = 32, GNT = 256;
 
 template <int R>
+struct GuidedGeo {
+    static constexpr int NR = 2 * R + 1;
+    static constexpr int AY = GTY + 2 * R, AX = GTX + 2 * R;     // a/b support
+    static constexpr int AYP = (AY + 3) & ~3, AXP = (AX + 3) & ~3;
+    static constexpr int IYP = AYP + 2 * R, IXP = AXP + 2 * R;   // staged u region (padded)
+};
+
+template <int R>
 struct GuidedSmem {
-    static constexpr int H2 = 2 * R;
-    static constexpr int IY = GTY + 2 * H2, IX = GTX + 2 * H2;   // staged I region
-    static constexpr int AY = GTY + 2 * R, AX = GTX + 2 * R;     // a/b support region
-    static constexpr int NR = 2 * R + 1;                          // ring depth
-    float I[NR][IY][IX];
-    float xs1[IY][AX], xs2[IY][AX];       // X means of (I-c), (I-c)^2 for the newest plane
-    float m1[NR][AY][AX], m2[NR][AY][AX]; // XY means
-    float pa[AY][AX], pb[AY][AX];         // a, b of the centre plane
-    float xa[AY][GTX], xb[AY][GTX];       // X means of a, b
-    float A[NR][GTY][GTX], B[NR][GTY][GTX];
+    using G = GuidedGeo<R>;
+    float I[G::IYP][G::IXP];
+    float xs1[G::IYP][G::AXP], xs2[G::IYP][G::AXP];
+    float pa[G::AYP][G::AXP], pb[G::AYP][G::AXP];
+    float xa[G::AYP][GTX], xb[G::AYP][GTX];
+    float rx_s[G::AXP], ry_s[G::AYP];     // reciprocals of the support columns / rows
 };
 
 // MODE 0: out = box(a)*I + box(b). MODE 1: out = box(a), out_b = box(b) (the fast
 // variant's low-resolution coefficient fields, guided.c:181-182).
 template <int R, int MODE>
-__global__ void __launch_bounds__(GNT) k_guided_fused(const float* __restrict__ in, float* __restrict__ out,
-                                                      float* __restrict__ out_b,
-                                                      int nz, int ny, int nx, float eps,
-                                                      const float* __restrict__ eps_ptr, int zchunk) {
-    using S = GuidedSmem<R>;
+__global__ void __launch_bounds__(GNT, 2) k_guided_fused(const float* __restrict__ in, float* __restrict__ out,
+                                                         float* __restrict__ out_b,
+                                                         int nz, int ny, int nx, float eps,
+                                                         const float* __restrict__ eps_ptr, int zchunk) {
+    using G = GuidedGeo<R>;
+    constexpr int NR = G::NR;
+    __shared__ GuidedSmem<R> sm;
     if (eps_ptr) eps = *eps_ptr;                     // chained: eps from the device noise model
-    extern __shared__ float4 smem4[];
-    S& sm = *reinterpret_cast<S*>(smem4);
     const int x0 = blockIdx.x * GTX, y0 = blockIdx.y * GTY;
     const int zs = blockIdx.z * zchunk;
     const int ze = min(nz, zs + zchunk);
     const int t = threadIdx.x;
     const size_t plane = (size_t)ny * nx;
-    // per-tile shift: first in-volume sample of the tile (same c for every voxel the
-    // CTA touches, so every box window sees one constant shift)
+    // per-tile shift: one constant for every window this CTA forms
     const float c = __ldg(in + (size_t)zs * plane + (size_t)y0 * nx + x0);
+    for (int i = t; i < G::AXP; i += GNT) {
+        const int gx = x0 - R + i;
+        sm.rx_s[i] = (gx >= 0 && gx < nx) ? box_recip(gx, nx, R) : 0.f;
+    }
+    for (int i = t; i < G::AYP; i += GNT) {
+        const int gy = y0 - R + i;
+        sm.ry_s[i] = (gy >= 0 && gy < ny) ? box_recip(gy, ny, R) : 0.f;
+    }
+    // step-3 role: support column xa3, support rows 4*rb3 .. +3
+    constexpr int N3 = (G::AYP / 4) * G::AXP;
+    const bool role3 = t < N3;
+    const int xa3 = t % G::AXP, rb3 = t / G::AXP;
+    // step-5 role: output column t % 32, output rows 4*(t/32) .. +3
+    const bool role5 = t < 4 * GTX;
+    const int xc5 = t % GTX, rb5 = t / GTX;
+    float r1[NR][4], r2[NR][4], ra[NR][4], rb[NR][4];
+#pragma unroll
+    for (int q = 0; q < NR; ++q)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) r1[q][k] = r2[q][k] = ra[q][k] = rb[q][k] = 0.f;
+    __syncthreads();
 
     for (int zi = zs - 2 * R; zi < ze + 2 * R; ++zi) {
-        const int slot = ((zi % S::NR) + S::NR) % S::NR;
         const bool zin = zi >= 0 && zi < nz;
-        // 1. stage I plane zi (zeros outside the volume)
-        for (int k = t; k < S::IY * S::IX; k += GNT) {
-            const int yy = k / S::IX, xx = k - yy * S::IX;
-            const int gy = y0 - S::H2 + yy, gx = x0 - S::H2 + xx;
+        // 1. stage u
+        for (int k = t; k < G::IYP * G::IXP; k += GNT) {
+            const int yy = k / G::IXP, xx = k - yy * G::IXP;
+            const int gy = y0 - 2 * R + yy, gx = x0 - 2 * R + xx;
             float v = 0.f;
-            if (zin && gy >= 0 && gy < ny && gx >= 0 && gx < nx) v = __ldg(in + (size_t)zi * plane + (size_t)gy * nx + gx);
-            sm.I[slot][yy][xx] = v;
+            if (zin && gy >= 0 && gy < ny && gx >= 0 && gx < nx) v = __ldg(in + (size_t)zi * plane + (size_t)gy * nx + gx) - c;
+            sm.I[yy][xx] = v;
         }
         __syncthreads();
-        // 2. X means of (I-c) and (I-c)^2 over columns of the a/b support
-        for (int k = t; k < S::IY * S::AX; k += GNT) {
-            const int yy = k / S::AX, xa = k - yy * S::AX;
-            const int gx = x0 - R + xa, gy = y0 - S::H2 + yy;
-            float s1 = 0.f, s2 = 0.f;
-            if (zin && gy >= 0 && gy < ny && gx >= 0 && gx < nx) {
+        // 2. X means of u, u^2 (4 support columns per thread)
+        for (int sgi = t; sgi < G::IYP * (G::AXP / 4); sgi += GNT) {
+            const int yy = sgi / (G::AXP / 4), x4 = 4 * (sgi % (G::AXP / 4));
+            float u[4 + 2 * R];
 #pragma unroll
-                for (int d = -R; d <= R; ++d) {
-                    const int xx = xa + R + d, g = gx + d;
-                    if (g >= 0 && g < nx) {
-                        const float u = sm.I[slot][yy][xx] - c;
-                        s1 += u; s2 += u * u;
-                    }
-                }
-                const float rx = box_recip(gx, nx, R);
-                s1 *= rx; s2 *= rx;
-            }
-            sm.xs1[yy][xa] = s1; sm.xs2[yy][xa] = s2;
-        }
-        __syncthreads();
-        // 3. Y means -> XY means of the newest plane into the ring
-        for (int k = t; k < S::AY * S::AX; k += GNT) {
-            const int ya = k / S::AX, xa = k - ya * S::AX;
-            const int gy = y0 - R + ya;
-            float s1 = 0.f, s2 = 0.f;
-            if (gy >= 0 && gy < ny) {
+            for (int j = 0; j < 4 + 2 * R; ++j) u[j] = sm.I[yy][x4 + j];
 #pragma unroll
-                for (int d = -R; d <= R; ++d) { s1 += sm.xs1[ya + R + d][xa]; s2 += sm.xs2[ya + R + d][xa]; }
-                const float ry = box_recip(gy, ny, R);
-                s1 *= ry; s2 *= ry;
-            }
-            sm.m1[slot][ya][xa] = s1; sm.m2[slot][ya][xa] = s2;
-        }
-        __syncthreads();
-        // 4. centre plane zc = zi - R: mean/corr -> a, b over the support
-        const int zc = zi - R;
-        const bool zc_in = zc >= 0 && zc < nz && zc >= zs - R && zc < ze + R;
-        for (int k = t; k < S::AY * S::AX; k += GNT) {
-            const int ya = k / S::AX, xa = k - ya * S::AX;
-            const int gy = y0 - R + ya, gx = x0 - R + xa;
-            float a = 0.f, b = 0.f;
-            if (zc_in && gy >= 0 && gy < ny && gx >= 0 && gx < nx) {
+            for (int k = 0; k < 4; ++k) {
                 float s1 = 0.f, s2 = 0.f;
 #pragma unroll
-                for (int q = 0; q < S::NR; ++q) { s1 += sm.m1[q][ya][xa]; s2 += sm.m2[q][ya][xa]; }
-                const float rz = box_recip(zc, nz, R);
-                const float e1 = s1 * rz, e2 = s2 * rz;          // E[I-c], E[(I-c)^2]
-                float var = e2 - e1 * e1;
-                if (var < 0.f) var = 0.f;
-                const float mean = e1 + c;
-                a = var / (var + eps);
-                b = mean * (1.0f - a);
+                for (int j = 0; j <= 2 * R; ++j) { s1 += u[k + j]; s2 += u[k + j] * u[k + j]; }
+                const float rx = sm.rx_s[x4 + k];
+                sm.xs1[yy][x4 + k] = s1 * rx;
+                sm.xs2[yy][x4 + k] = s2 * rx;
             }
-            sm.pa[ya][xa] = a; sm.pb[ya][xa] = b;
         }
         __syncthreads();
-        // 5. X means of a, b over the output columns
-        for (int k = t; k < S::AY * GTX; k += GNT) {
-            const int ya = k / GTX, xt = k - ya * GTX;
-            const int gx = x0 + xt;
-            float s1 = 0.f, s2 = 0.f;
-            if (gx < nx) {
+        // 3. Y means -> z ring -> a, b of plane zc over the support
+        const int zc = zi - R;
+        if (role3) {
 #pragma unroll
-                for (int d = -R; d <= R; ++d) { s1 += sm.pa[ya][xt + R + d]; s2 += sm.pb[ya][xt + R + d]; }
-                const float rx = box_recip(gx, nx, R);
-                s1 *= rx; s2 *= rx;
+            for (int q = 0; q < NR - 1; ++q)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) { r1[q][k] = r1[q + 1][k]; r2[q][k] = r2[q + 1][k]; }
+            float a1[4 + 2 * R], a2[4 + 2 * R];
+#pragma unroll
+            for (int j = 0; j < 4 + 2 * R; ++j) { a1[j] = sm.xs1[4 * rb3 + j][xa3]; a2[j] = sm.xs2[4 * rb3 + j][xa3]; }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                float s1 = 0.f, s2 = 0.f;
+#pragma unroll
+                for (int j = 0; j <= 2 * R; ++j) { s1 += a1[k + j]; s2 += a2[k + j]; }
+                const float ry = sm.ry_s[4 * rb3 + k];
+                r1[NR - 1][k] = s1 * ry;
+                r2[NR - 1][k] = s2 * ry;
             }
-            sm.xa[ya][xt] = s1; sm.xb[ya][xt] = s2;
+            const bool zc_ok = zc >= 0 && zc < nz && zc >= zs - R && zc < ze + R;
+            const float rz = zc_ok ? box_recip(zc, nz, R) : 0.f;
+            const int gx = x0 - R + xa3;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int gy = y0 - R + 4 * rb3 + k;
+                float a = 0.f, b = 0.f;
+                if (zc_ok && gx >= 0 && gx < nx && gy >= 0 && gy < ny && 4 * rb3 + k < G::AY && xa3 < G::AX) {
+                    float s1 = 0.f, s2 = 0.f;
+#pragma unroll
+                    for (int q = 0; q < NR; ++q) { s1 += r1[q][k]; s2 += r2[q][k]; }
+                    const float e1 = s1 * rz, e2 = s2 * rz;      // E[I-c], E[(I-c)^2]
+                    float var = e2 - e1 * e1;
+                    if (var < 0.f) var = 0.f;
+                    const float mean = e1 + c;
+                    a = var / (var + eps);                        // guided.c:129
+                    b = mean * (1.0f - a);                        // guided.c:131
+                }
+                sm.pa[4 * rb3 + k][xa3] = a;
+                sm.pb[4 * rb3 + k][xa3] = b;
+            }
         }
         __syncthreads();
-        // 6. Y means of a, b into the a/b ring (slot of zc)
-        const int cslot = ((zc % S::NR) + S::NR) % S::NR;
-        for (int k = t; k < GTY * GTX; k += GNT) {
-            const int yt = k / GTX, xt = k - yt * GTX;
-            const int gy = y0 + yt;
-            float s1 = 0.f, s2 = 0.f;
-            if (gy < ny) {
+        // 4. X means of a, b over the output columns
+        for (int sgi = t; sgi < G::AYP * (GTX / 4); sgi += GNT) {
+            const int ya = sgi / (GTX / 4), x4 = 4 * (sgi % (GTX / 4));
+            float pa[4 + 2 * R], pb[4 + 2 * R];
 #pragma unroll
-                for (int d = -R; d <= R; ++d) { s1 += sm.xa[yt + R + d][xt]; s2 += sm.xb[yt + R + d][xt]; }
-                const float ry = box_recip(gy, ny, R);
-                s1 *= ry; s2 *= ry;
+            for (int j = 0; j < 4 + 2 * R; ++j) { pa[j] = sm.pa[ya][x4 + j]; pb[j] = sm.pb[ya][x4 + j]; }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                float s1 = 0.f, s2 = 0.f;
+#pragma unroll
+                for (int j = 0; j <= 2 * R; ++j) { s1 += pa[k + j]; s2 += pb[k + j]; }
+                const float rx = sm.rx_s[R + x4 + k];
+                sm.xa[ya][x4 + k] = s1 * rx;
+                sm.xb[ya][x4 + k] = s2 * rx;
             }
-            sm.A[cslot][yt][xt] = s1; sm.B[cslot][yt][xt] = s2;
         }
         __syncthreads();
-        // 7. output plane zo = zi - 2R
-        const int zo = zi - 2 * R;
-        if (zo >= zs && zo < ze) {
-            const int oslot = ((zo % S::NR) + S::NR) % S::NR;
-            const float rz = box_recip(zo, nz, R);
-            for (int k = t; k < GTY * GTX; k += GNT) {
-                const int yt = k / GTX, xt = k - yt * GTX;
-                const int gy = y0 + yt, gx = x0 + xt;
-                if (gy < ny && gx < nx) {
-                    float sa = 0.f, sb = 0.f;
+        // 5. Y means -> z ring -> output plane zo
+        if (role5) {
 #pragma unroll
-                    for (int q = 0; q < S::NR; ++q) { sa += sm.A[q][yt][xt]; sb += sm.B[q][yt][xt]; }
+            for (int q = 0; q < NR - 1; ++q)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) { ra[q][k] = ra[q + 1][k]; rb[q][k] = rb[q + 1][k]; }
+            float sa[4 + 2 * R], sb[4 + 2 * R];
+#pragma unroll
+            for (int j = 0; j < 4 + 2 * R; ++j) { sa[j] = sm.xa[4 * rb5 + j][xc5]; sb[j] = sm.xb[4 * rb5 + j][xc5]; }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                float s1 = 0.f, s2 = 0.f;
+#pragma unroll
+                for (int j = 0; j <= 2 * R; ++j) { s1 += sa[k + j]; s2 += sb[k + j]; }
+                const float ry = sm.ry_s[R + 4 * rb5 + k];
+                ra[NR - 1][k] = s1 * ry;
+                rb[NR - 1][k] = s2 * ry;
+            }
+            const int zo = zi - 2 * R;
+            if (zo >= zs && zo < ze) {
+                const float rz = box_recip(zo, nz, R);
+                const int gx = x0 + xc5;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int gy = y0 + 4 * rb5 + k;
+                    if (gy >= ny || gx >= nx) continue;
+                    float s1 = 0.f, s2 = 0.f;
+#pragma unroll
+                    for (int q = 0; q < NR; ++q) { s1 += ra[q][k]; s2 += rb[q][k]; }
                     const size_t o = (size_t)zo * plane + (size_t)gy * nx + gx;
-                    if (MODE == 0) {
-                        const float iv = sm.I[oslot][yt + S::H2][xt + S::H2];
-                        out[o] = (sa * rz) * iv + sb * rz;
-                    } else {
-                        out[o] = sa * rz;
-                        out_b[o] = sb * rz;
-                    }
+                    if (MODE == 0) out[o] = (s1 * rz) * __ldg(in + o) + s2 * rz;
+                    else { out[o] = s1 * rz; out_b[o] = s2 * rz; }
                 }
             }
         }
-        // the next iteration's stage-1 writes slot (zi+1) % NR, last read in step 7 of the
-        // iteration 2R earlier; step 2/3 of this iteration already passed barriers.
-        __syncthreads();
+        // next plane: step 1 writes I (last read in step 2), step 2 writes xs (read in step 3),
+        // step 3 writes pa/pb (read in step 4) and step 4 writes xa/xb (read in step 5): each
+        // is separated from its reader by at least one barrier above.
     }
 }
 
@@ -257,15 +292,7 @@ __global__ void __launch_bounds__(GNT) k_guided_fused(const float* __restrict__ 
 
 int fy_guided_fused_max_radius() { return 4; }
 
-size_t fy_guided_fused_smem(int r) {
-    switch (r) {
-        case 1: return sizeof(GuidedSmem<1>);
-        case 2: return sizeof(GuidedSmem<2>);
-        case 3: return sizeof(GuidedSmem<3>);
-        case 4: return sizeof(GuidedSmem<4>);
-        default: return 0;
-    }
-}
+size_t fy_guided_fused_smem(int r) { return r >= 1 && r <= 4 ? 0 : 0; }   // static shared memory
 
 // Fused exact guided filter, r in [1,4]. in != out required (out planes are written
 // while neighbouring tiles still read their input halos). mode 1 writes box(a) to out and
@@ -276,17 +303,13 @@ cudaError_t fy_launch_guided_fused(const float* in, float* out, float* out_b, in
     // z chunks: enough CTAs for ~4 waves, but chunks of >= 8r planes so the 4r-plane
     // warm-up stays a small fraction
     const long tiles_xy = (long)tiles.x * tiles.y;
-    int nchunk = (int)((4L * sms + tiles_xy - 1) / tiles_xy);
+    int nchunk = (int)((6L * sms + tiles_xy - 1) / tiles_xy);
     const int min_chunk = 8 * r;
     if (nchunk > nz / min_chunk) nchunk = nz / min_chunk;
     if (nchunk < 1) nchunk = 1;
     const int zchunk = ceil_div_i(nz, nchunk);
     dim3 grid(tiles.x, tiles.y, ceil_div_i(nz, zchunk));
-    const size_t smem = fy_guided_fused_smem(r);
-    cudaError_t e = cudaSuccess;
-#define FY_GF(RR, MM)                                                                    \
-    if ((e = fy_smem_optin(k_guided_fused<RR, MM>, smem)) != cudaSuccess) return e;       \
-    k_guided_fused<RR, MM><<<grid, GNT, smem, st>>>(in, out, out_b, nz, ny, nx, eps, eps_ptr, zchunk);
+#define FY_GF(RR, MM) k_guided_fused<RR, MM><<<grid, GNT, 0, st>>>(in, out, out_b, nz, ny, nx, eps, eps_ptr, zchunk);
     if (mode == 0) {
         switch (r) {
             case 1: FY_GF(1, 0) break;

@@ -51,6 +51,7 @@ cudaError_t fy_launch_box_mean(const float* in, float* out, float* tmp, int nz, 
 
 // Noise model (fy_noise.cu)
 size_t fy_noise_ctl_bytes();
+size_t fy_noise_scratch_floats(size_t n);
 cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, int win, double flat_pct,
                                      double ref_intensity, float* scratch, void* ctl_mem, int sms,
                                      cudaStream_t st, int& launches);

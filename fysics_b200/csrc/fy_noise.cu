@@ -20,8 +20,6 @@ namespace {
 
 constexpr int NB = 24;                 // intensity bins, noise.c:111
 constexpr int NT_MAX = 64;             // selection targets: 2 per bin + spare
-constexpr int DB_ALL = 11;             // digit bits for whole-volume selections (11/11/10)
-constexpr int DB_BIN = 8;              // digit bits for per-bin selections (4 x 8)
 
 FY_D uint32_t fkey(float f) {
     const uint32_t u = __float_as_uint(f);
@@ -42,27 +40,33 @@ FY_HD float funkey(uint32_t k) {
 }  // namespace
 
 // Device-resident control block of one estimate (lives in the caller's scratch).
+// Selection targets: target t selects the order statistic k_t (0-based) of the keys of
+// group g_t. Bins: t = bin id. Whole volume: t = 0, 1 (1st/99th percentile) or t = 0
+// (variance fallback). After the digit passes, prefix_t is the k-th key, eq_t the number of
+// keys equal to it and rank_t its rank among them; the (k+1)-th key is the same key when
+// rank_t + 1 < eq_t, else the smallest key greater than it (k_sel_next).
 struct NoiseCtl {
-    // inputs
     long long n;
     double flat_pct, ref_intensity;
-    // selection targets
-    int ntarget;
-    int tgroup[NT_MAX];                // group id: -1 = whole volume, 0..23 = bin
-    long long trank[NT_MAX];           // remaining rank within the current prefix
-    uint32_t tprefix[NT_MAX];          // decided high bits
+    int ntarget, mode;                 // mode 0 means lo/hi, 1 bins, 2 variance fallback, 3 done
+    long long tk[NT_MAX];              // requested rank k
+    long long trank[NT_MAX];           // remaining rank inside the decided prefix
+    long long tgroup_n[NT_MAX];        // group size
+    unsigned long long teq[NT_MAX];    // keys equal to the selected key
+    uint32_t tprefix[NT_MAX];
+    uint32_t tnext[NT_MAX];            // min key > selected key (when needed)
     int tactive[NT_MAX];
-    // results
+    int tneed_next[NT_MAX];
     double lo, hi;
     double edge[NB + 1];
-    long long bcount[NB];
+    float fedge[NB + 1];               // smallest float >= edge[k]: exact float membership test
+    float fscale;                      // NB/(hi-lo) for the bin guess
+    unsigned long long bcount[NB];
     double bfloor[NB];
-    int pct_k_lo, mode;                // mode: 0 means lo/hi, 1 bins, 2 whole-volume var fallback
-    double pct_f_lo, pct_f_hi;
     double out_g, out_b, out_noise_ref, out_ref_intensity;
     int out_used;
     float eps;                         // fy_guided_eps_for_noise(noise_ref), for a chained guided filter
-    unsigned int hist[NT_MAX * 256];   // per-target histogram (bins: 256; whole: up to 2048 over 4 targets)
+    unsigned int hist[NT_MAX * 256];   // per-target histogram (bins: 24 x 256; whole: 2 x 2048)
 };
 
 namespace {
@@ -70,139 +74,227 @@ namespace {
 constexpr int SNT = 256, STY = 16, STX = 32;
 
 // ---------------------------------------------------------------- 1. local stats
+// CTA = 32 x 16 output columns sliding along z. Per input plane: stage (I - c) with zeros
+// outside the volume (so window sums need no bounds checks); 4-column X sums of u and u^2
+// by 8*(16+2R) threads; 4-row Y sums by 128 threads, which keep a (2R+1)-plane z ring of
+// their XY sums in registers and emit mean/variance for the plane R behind.
 template <int R>
 struct StatSmem {
     static constexpr int IY = STY + 2 * R, IX = STX + 2 * R, NR = 2 * R + 1;
-    float I[NR][IY][IX];
+    float I[IY][IX];
     float xs1[IY][STX], xs2[IY][STX];
-    float m1[NR][STY][STX], m2[NR][STY][STX];
 };
 
 template <int R>
-__global__ void __launch_bounds__(SNT) k_noise_stats(const float* __restrict__ in, float* __restrict__ mean,
-                                                     float* __restrict__ var, int nz, int ny, int nx,
-                                                     float inv_wc, int wci, int zchunk) {
+__global__ void __launch_bounds__(SNT, 2) k_noise_stats(const float* __restrict__ in, float* __restrict__ mean,
+                                                        float* __restrict__ var, int nz, int ny, int nx,
+                                                        float inv_wc, int wci, int zchunk) {
     using S = StatSmem<R>;
-    extern __shared__ float4 smem4[];
-    S& sm = *reinterpret_cast<S*>(smem4);
+    constexpr int NR = S::NR;
+    __shared__ S sm;
     const int x0 = blockIdx.x * STX, y0 = blockIdx.y * STY;
     const int zs = blockIdx.z * zchunk, ze = min(nz, zs + zchunk);
     const int t = threadIdx.x;
     const size_t plane = (size_t)ny * nx;
     const float c = __ldg(in + (size_t)zs * plane + (size_t)y0 * nx + x0);
+    // Y-stage role: column xc, rows 4*rb .. 4*rb+3 (threads 0..127)
+    const bool yrole = t < 4 * STX;
+    const int xc = t % STX, rb = t / STX;
+    float r1[NR][4], r2[NR][4];
+#pragma unroll
+    for (int q = 0; q < NR; ++q)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) r1[q][k] = r2[q][k] = 0.f;
+    int cyx[4];
+    if (yrole) {
+        const int gx = x0 + xc, cx = min(gx + R, nx - 1) - max(gx - R, 0) + 1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int gy = y0 + 4 * rb + k;
+            cyx[k] = (min(gy + R, ny - 1) - max(gy - R, 0) + 1) * cx;
+        }
+    }
     for (int zi = zs - R; zi < ze + R; ++zi) {
-        const int slot = ((zi % S::NR) + S::NR) % S::NR;
         const bool zin = zi >= 0 && zi < nz;
         for (int k = t; k < S::IY * S::IX; k += SNT) {
             const int yy = k / S::IX, xx = k - yy * S::IX;
             const int gy = y0 - R + yy, gx = x0 - R + xx;
             float v = 0.f;
             if (zin && gy >= 0 && gy < ny && gx >= 0 && gx < nx) v = __ldg(in + (size_t)zi * plane + (size_t)gy * nx + gx) - c;
-            sm.I[slot][yy][xx] = v;
+            sm.I[yy][xx] = v;
         }
         __syncthreads();
-        // X sums (shifted values, zero outside)
-        for (int k = t; k < S::IY * STX; k += SNT) {
-            const int yy = k / STX, xt = k - yy * STX;
-            const int gx0 = x0 + xt;
-            float s1 = 0.f, s2 = 0.f;
+        if (t < (STX / 4) * S::IY) {                        // X sums, 4 columns per thread
+            const int yy = t / (STX / 4), x4 = 4 * (t % (STX / 4));
+            float u[4 + 2 * R];
 #pragma unroll
-            for (int d = -R; d <= R; ++d) {
-                const int g = gx0 + d;
-                if (g >= 0 && g < nx) { const float u = sm.I[slot][yy][xt + R + d]; s1 += u; s2 += u * u; }
-            }
-            sm.xs1[yy][xt] = s1; sm.xs2[yy][xt] = s2;
-        }
-        __syncthreads();
-        for (int k = t; k < STY * STX; k += SNT) {
-            const int yt = k / STX, xt = k - yt * STX;
-            float s1 = 0.f, s2 = 0.f;
+            for (int j = 0; j < 4 + 2 * R; ++j) u[j] = sm.I[yy][x4 + j];
 #pragma unroll
-            for (int d = -R; d <= R; ++d) { s1 += sm.xs1[yt + R + d][xt]; s2 += sm.xs2[yt + R + d][xt]; }
-            sm.m1[slot][yt][xt] = s1; sm.m2[slot][yt][xt] = s2;
-        }
-        __syncthreads();
-        const int zo = zi - R;
-        if (zo >= zs && zo < ze) {
-            const int cz = min(zo + R, nz - 1) - max(zo - R, 0) + 1;
-            for (int k = t; k < STY * STX; k += SNT) {
-                const int yt = k / STX, xt = k - yt * STX;
-                const int gy = y0 + yt, gx = x0 + xt;
-                if (gy >= ny || gx >= nx) continue;
+            for (int k = 0; k < 4; ++k) {
                 float s1 = 0.f, s2 = 0.f;
 #pragma unroll
-                for (int q = 0; q < S::NR; ++q) { s1 += sm.m1[q][yt][xt]; s2 += sm.m2[q][yt][xt]; }
-                const int cy = min(gy + R, ny - 1) - max(gy - R, 0) + 1;
-                const int cx = min(gx + R, nx - 1) - max(gx - R, 0) + 1;
-                const int nini = cz * cy * cx;
-                const float nin = (float)nini;
-                // raw sums: S1 = S1' + nin*c, S2 = S2' + 2c*S1' + nin*c^2
-                const float m = (s1 + nin * c) * inv_wc;
-                float v;
-                if (nini == wci) {                        // interior: shifted, cancellation-free
-                    const float e1 = s1 * inv_wc;
-                    v = s2 * inv_wc - e1 * e1;
-                } else {
-                    v = (s2 + 2.0f * c * s1 + nin * c * c) * inv_wc - m * m;
-                }
-                if (v < 0.f) v = 0.f;
-                const size_t o = (size_t)zo * plane + (size_t)gy * nx + gx;
-                mean[o] = m;
-                var[o] = v;
+                for (int j = 0; j <= 2 * R; ++j) { s1 += u[k + j]; s2 += u[k + j] * u[k + j]; }
+                sm.xs1[yy][x4 + k] = s1; sm.xs2[yy][x4 + k] = s2;
             }
         }
         __syncthreads();
+        if (yrole) {                                        // Y sums + z ring
+#pragma unroll
+            for (int q = 0; q < NR - 1; ++q)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) { r1[q][k] = r1[q + 1][k]; r2[q][k] = r2[q + 1][k]; }
+            float a1[4 + 2 * R], a2[4 + 2 * R];
+#pragma unroll
+            for (int j = 0; j < 4 + 2 * R; ++j) { a1[j] = sm.xs1[4 * rb + j][xc]; a2[j] = sm.xs2[4 * rb + j][xc]; }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                float s1 = 0.f, s2 = 0.f;
+#pragma unroll
+                for (int j = 0; j <= 2 * R; ++j) { s1 += a1[k + j]; s2 += a2[k + j]; }
+                r1[NR - 1][k] = s1; r2[NR - 1][k] = s2;
+            }
+            const int zo = zi - R;
+            if (zo >= zs && zo < ze) {
+                const int cz = min(zo + R, nz - 1) - max(zo - R, 0) + 1;
+                const int gx = x0 + xc;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int gy = y0 + 4 * rb + k;
+                    if (gy >= ny || gx >= nx) continue;
+                    float s1 = 0.f, s2 = 0.f;
+#pragma unroll
+                    for (int q = 0; q < NR; ++q) { s1 += r1[q][k]; s2 += r2[q][k]; }
+                    const int nini = cz * cyx[k];
+                    const float nin = (float)nini;
+                    // raw sums: S1 = S1' + nin*c, S2 = S2' + 2c*S1' + nin*c^2
+                    const float m = (s1 + nin * c) * inv_wc;
+                    float v;
+                    if (nini == wci) {                      // interior: shifted, cancellation-free
+                        const float e1 = s1 * inv_wc;
+                        v = s2 * inv_wc - e1 * e1;
+                    } else {
+                        v = (s2 + 2.0f * c * s1 + nin * c * c) * inv_wc - m * m;
+                    }
+                    if (v < 0.f) v = 0.f;
+                    const size_t o = (size_t)zo * plane + (size_t)gy * nx + gx;
+                    mean[o] = m;
+                    var[o] = v;
+                }
+            }
+        }
     }
 }
 
 // ---------------------------------------------------------------- 2. radix select
-// Group of element i: -1 (whole volume) for modes 0/2; bin id (or -2 = no bin) for mode 1.
-FY_D int bin_of(float mv, const NoiseCtl* __restrict__ ctl) {
-    const double m = (double)mv;
-    if (!(m >= ctl->edge[0] && m < ctl->edge[NB])) return -2;
-    int b = (int)((m - ctl->lo) / (ctl->hi - ctl->lo) * NB);
-    if (b < 0) b = 0;
-    if (b > NB - 1) b = NB - 1;
-    while (b > 0 && m < ctl->edge[b]) --b;               // exact edges (noise.c:118-122)
-    while (b < NB - 1 && m >= ctl->edge[b + 1]) ++b;
+// Exact bin of a float mean: m >= edge[k] <=> m >= fedge[k] with fedge[k] the smallest float
+// >= edge[k] (noise.c:118-122 in double), so membership needs only float compares.
+FY_D int bin_of(float m, const float* __restrict__ fe, float lo_f, float scale) {
+    if (!(m >= fe[0] && m < fe[NB])) return -1;
+    int b = (int)((m - lo_f) * scale);
+    b = b < 0 ? 0 : (b > NB - 1 ? NB - 1 : b);
+    while (b > 0 && m < fe[b]) --b;
+    while (b < NB - 1 && m >= fe[b + 1]) ++b;
     return b;
 }
 
-// Histogram one digit (bits [shift, shift+db)) of every active target's prefix group.
+// warp-aggregated shared-memory increment of h[code] (code < 0: nothing)
+FY_D void agg_inc(unsigned int* h, int code) {
+    const unsigned peers = __match_any_sync(0xffffffffu, code);
+    if (code >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[code], (unsigned)__popc(peers));
+}
+
+// u8 bin id per voxel (255 = no bin) and per-bin counts
+__global__ void __launch_bounds__(256) k_bin_assign(const float* __restrict__ mean, uint8_t* __restrict__ bin,
+                                                    NoiseCtl* __restrict__ ctl) {
+    __shared__ unsigned int cnt[NB];
+    __shared__ float fe[NB + 1];
+    if (threadIdx.x < NB) cnt[threadIdx.x] = 0;
+    if (threadIdx.x <= NB) fe[threadIdx.x] = ctl->fedge[threadIdx.x];
+    __syncthreads();
+    const float lo_f = ctl->fedge[0], scale = ctl->fscale;
+    const long long n = ctl->n, n4 = (n + 3) / 4;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n4; base += stride) {
+        const long long q = base + threadIdx.x;
+        int b4[4] = {-1, -1, -1, -1};
+        if (q < n4) {
+            if (4 * q + 3 < n) {
+                const float4 m = __ldg(reinterpret_cast<const float4*>(mean) + q);
+                b4[0] = bin_of(m.x, fe, lo_f, scale); b4[1] = bin_of(m.y, fe, lo_f, scale);
+                b4[2] = bin_of(m.z, fe, lo_f, scale); b4[3] = bin_of(m.w, fe, lo_f, scale);
+                *reinterpret_cast<uchar4*>(bin + 4 * q) =
+                    make_uchar4(b4[0] < 0 ? 255 : b4[0], b4[1] < 0 ? 255 : b4[1], b4[2] < 0 ? 255 : b4[2],
+                                b4[3] < 0 ? 255 : b4[3]);
+            } else {
+                for (int j = 0; j < 4 && 4 * q + j < n; ++j) {
+                    b4[j] = bin_of(mean[4 * q + j], fe, lo_f, scale);
+                    bin[4 * q + j] = b4[j] < 0 ? 255 : (uint8_t)b4[j];
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) agg_inc(cnt, b4[j]);
+    }
+    __syncthreads();
+    if (threadIdx.x < NB && cnt[threadIdx.x]) atomicAdd(&ctl->bcount[threadIdx.x], (unsigned long long)cnt[threadIdx.x]);
+}
+
+// One digit pass (bits [shift, shift + DB)) for every active target whose prefix matches.
+// mode 0: keys of mean, targets 0 and 1 over all voxels; mode 1: keys of var, target = bin;
+// mode 2: keys of var, target 0 over all voxels.
 template <int DB>
 __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean, const float* __restrict__ var,
-                                                  NoiseCtl* __restrict__ ctl, int shift, int want_mode) {
-    extern __shared__ unsigned int h[];                  // ntarget << DB counters
-    __shared__ int s_act;
+                                                  const uint8_t* __restrict__ bin, NoiseCtl* __restrict__ ctl,
+                                                  int shift, int want_mode) {
+    extern __shared__ unsigned int h[];
+    __shared__ uint32_t sp[NT_MAX];
+    __shared__ int sa[NT_MAX];
     if (ctl->mode != want_mode) return;
     constexpr int NBK = 1 << DB;
     const int nt = ctl->ntarget;
-    if (threadIdx.x == 0) {
-        int a = 0;
-        for (int t = 0; t < nt; ++t) a |= ctl->tactive[t];
-        s_act = a;
-    }
     for (int i = threadIdx.x; i < nt * NBK; i += blockDim.x) h[i] = 0;
+    for (int i = threadIdx.x; i < nt; i += blockDim.x) { sp[i] = ctl->tprefix[i]; sa[i] = ctl->tactive[i]; }
     __syncthreads();
-    if (!s_act) return;
-    const long long n = ctl->n;
-    const int mode = ctl->mode;
     const int top = shift + DB;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const float mv = __ldg(mean + i);
-        uint32_t key;
-        int grp;
-        if (mode == 0) { key = fkey(mv); grp = -1; }
-        else if (mode == 1) { grp = bin_of(mv, ctl); if (grp < 0) continue; key = fkey(__ldg(var + i)); }
-        else { key = fkey(__ldg(var + i)); grp = -1; }
-        const uint32_t hi_bits = top >= 32 ? 0u : (key >> top);
-        const int dig = (key >> shift) & (NBK - 1);
-        if (mode == 1) {
-            for (int t = 2 * grp; t < 2 * grp + 2; ++t)
-                if (ctl->tactive[t] && ctl->tprefix[t] == hi_bits) atomicAdd(&h[t * NBK + dig], 1u);
-        } else {
-            for (int t = 0; t < nt; ++t)
-                if (ctl->tactive[t] && ctl->tprefix[t] == hi_bits) atomicAdd(&h[t * NBK + dig], 1u);
+    const long long n = ctl->n, n4 = (n + 3) / 4;
+    const float* src = want_mode == 0 ? mean : var;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n4; base += stride) {
+        const long long q = base + threadIdx.x;
+        float v[4] = {0.f, 0.f, 0.f, 0.f};
+        int g[4] = {-1, -1, -1, -1};
+        if (q < n4) {
+            if (4 * q + 3 < n) {
+                const float4 x = __ldg(reinterpret_cast<const float4*>(src) + q);
+                v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+                if (want_mode == 1) {
+                    const uchar4 bb = __ldg(reinterpret_cast<const uchar4*>(bin) + q);
+                    g[0] = bb.x; g[1] = bb.y; g[2] = bb.z; g[3] = bb.w;
+                } else {
+                    g[0] = g[1] = g[2] = g[3] = 0;
+                }
+            } else {
+                for (int j = 0; j < 4 && 4 * q + j < n; ++j) {
+                    v[j] = src[4 * q + j];
+                    g[j] = want_mode == 1 ? bin[4 * q + j] : 0;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t key = fkey(v[j]);
+            const uint32_t hb = top >= 32 ? 0u : (key >> top);
+            const int dig = (key >> shift) & (NBK - 1);
+            if (want_mode == 1) {
+                const int t = g[j];
+                const bool hit = t >= 0 && t < NB && sa[t] && sp[t] == hb;
+                agg_inc(h, hit ? t * NBK + dig : -1);
+            } else {
+                for (int t = 0; t < nt; ++t) {
+                    const bool hit = g[j] == 0 && sa[t] && sp[t] == hb;
+                    agg_inc(h, hit ? t * NBK + dig : -1);
+                }
+            }
         }
     }
     __syncthreads();
@@ -210,34 +302,112 @@ __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean
         if (h[i]) atomicAdd(&ctl->hist[i], h[i]);
 }
 
-// After a digit pass: every target picks the bucket holding its rank (one warp per target).
-__global__ void k_sel_scan(NoiseCtl* __restrict__ ctl, int db, int want_mode) {
+// After a digit pass: target t (one block) finds the bucket holding its rank by a block
+// scan of the histogram, extends its prefix, records how many keys share the final key.
+__global__ void __launch_bounds__(256) k_sel_scan(NoiseCtl* __restrict__ ctl, int db, int want_mode, int last) {
+    __shared__ unsigned long long part[256];
     if (ctl->mode != want_mode) return;
     const int t = blockIdx.x;
     if (t >= ctl->ntarget || !ctl->tactive[t]) return;
-    const int nbk = 1 << db;
+    const int nbk = 1 << db, per = nbk / 256 > 0 ? nbk / 256 : 1;
     unsigned int* h = ctl->hist + (size_t)t * nbk;
-    if (threadIdx.x == 0) {
-        long long r = ctl->trank[t], acc = 0;
-        int b = 0;
-        for (; b < nbk; ++b) {
-            if (acc + (long long)h[b] > r) break;
+    const int b0 = threadIdx.x * per;
+    unsigned long long mine = 0;
+    for (int b = b0; b < b0 + per && b < nbk; ++b) mine += h[b];
+    part[threadIdx.x] = mine;
+    __syncthreads();
+    for (int off = 1; off < 256; off <<= 1) {                // inclusive scan
+        const unsigned long long add = threadIdx.x >= off ? part[threadIdx.x - off] : 0ull;
+        __syncthreads();
+        part[threadIdx.x] += add;
+        __syncthreads();
+    }
+    const long long r = ctl->trank[t];
+    const unsigned long long before = threadIdx.x ? part[threadIdx.x - 1] : 0ull;
+    if ((unsigned long long)r >= before && (unsigned long long)r < part[threadIdx.x]) {
+        unsigned long long acc = before;
+        for (int b = b0; b < b0 + per && b < nbk; ++b) {
+            if (acc + h[b] > (unsigned long long)r) {
+                ctl->trank[t] = r - (long long)acc;
+                ctl->tprefix[t] = (ctl->tprefix[t] << db) | (uint32_t)b;
+                if (last) ctl->teq[t] = h[b];
+                break;
+            }
             acc += h[b];
         }
-        if (b == nbk) b = nbk - 1;                       // cannot happen for a valid rank
-        ctl->trank[t] = r - acc;
-        ctl->tprefix[t] = (ctl->tprefix[t] << db) | (uint32_t)b;
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nbk; i += blockDim.x) h[i] = 0;
+    if (last && threadIdx.x == 0) {
+        ctl->tneed_next[t] = (ctl->trank[t] + 1 >= (long long)ctl->teq[t]) && (ctl->tk[t] + 1 < ctl->tgroup_n[t]);
+        ctl->tnext[t] = 0xffffffffu;
+    }
 }
 
-// percentile() interpolation (noise.c:69-72) from the two selected order statistics
-FY_D double interp(const NoiseCtl* ctl, int t0, double f, bool has_next) {
-    const double v0 = (double)funkey(ctl->tprefix[t0]);
+// Smallest key greater than the selected key, for targets whose k+1 lies past it.
+__global__ void __launch_bounds__(256) k_sel_next(const float* __restrict__ mean, const float* __restrict__ var,
+                                                  const uint8_t* __restrict__ bin, NoiseCtl* __restrict__ ctl,
+                                                  int want_mode) {
+    __shared__ uint32_t sp[NT_MAX];
+    __shared__ int sn[NT_MAX];
+    __shared__ unsigned int smin[NT_MAX];
+    __shared__ int s_any;
+    if (ctl->mode != want_mode) return;
+    const int nt = ctl->ntarget;
+    if (threadIdx.x == 0) s_any = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+        sp[i] = ctl->tprefix[i];
+        sn[i] = ctl->tactive[i] && ctl->tneed_next[i];
+        smin[i] = 0xffffffffu;
+        if (sn[i]) s_any = 1;
+    }
+    __syncthreads();
+    if (!s_any) return;
+    const long long n = ctl->n;
+    const float* src = want_mode == 0 ? mean : var;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const long long i = base + threadIdx.x;
+        uint32_t key = 0xffffffffu;
+        int g = -1;
+        if (i < n) {
+            key = fkey(__ldg(src + i));
+            g = want_mode == 1 ? (int)__ldg(bin + i) : 0;
+        }
+        for (int t = 0; t < nt; ++t) {
+            const bool mine = want_mode == 1 ? (g == t) : (g == 0);
+            const uint32_t cand = (mine && sn[t] && key > sp[t]) ? key : 0xffffffffu;
+            const uint32_t m = __reduce_min_sync(0xffffffffu, cand);
+            if ((threadIdx.x & 31) == 0 && m != 0xffffffffu) atomicMin(&smin[t], m);
+            if (want_mode == 1) {}   // every lane loops over all targets (warp-uniform)
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nt; i += blockDim.x)
+        if (sn[i] && smin[i] != 0xffffffffu) atomicMin(&ctl->tnext[i], smin[i]);
+}
+
+// value of order statistic k+1 of target t
+FY_D double next_value(const NoiseCtl* ctl, int t) {
+    return ctl->tneed_next[t] ? (double)funkey(ctl->tnext[t]) : (double)funkey(ctl->tprefix[t]);
+}
+// percentile() interpolation (noise.c:69-72)
+FY_D double interp(const NoiseCtl* ctl, int t, double f, bool has_next) {
+    const double v0 = (double)funkey(ctl->tprefix[t]);
     if (!has_next) return v0;
-    const double v1 = (double)funkey(ctl->tprefix[t0 + 1]);
-    return v0 * (1 - f) + v1 * f;
+    return v0 * (1 - f) + next_value(ctl, t) * f;
+}
+
+FY_D void target_init(NoiseCtl* ctl, int t, long long k, long long group_n, bool on) {
+    ctl->tk[t] = k;
+    ctl->trank[t] = k;
+    ctl->tgroup_n[t] = group_n;
+    ctl->tprefix[t] = 0;
+    ctl->teq[t] = 0;
+    ctl->tactive[t] = on;
+    ctl->tneed_next[t] = 0;
+    ctl->tnext[t] = 0xffffffffu;
 }
 
 __global__ void k_noise_setup(NoiseCtl* ctl, long long n, double flat_pct, double ref_intensity) {
@@ -245,58 +415,42 @@ __global__ void k_noise_setup(NoiseCtl* ctl, long long n, double flat_pct, doubl
     ctl->flat_pct = flat_pct;
     ctl->ref_intensity = ref_intensity;
     ctl->mode = 0;
-    // targets: 1st percentile (k, k+1) and 99th (k, k+1) of the means
-    for (int t = 0; t < NT_MAX; ++t) { ctl->tactive[t] = 0; ctl->tprefix[t] = 0; ctl->trank[t] = 0; ctl->tgroup[t] = -1; }
+    for (int t = 0; t < NT_MAX; ++t) target_init(ctl, t, 0, 0, false);
     const double i1 = 1.0 / 100.0 * (double)(n - 1), i99 = 99.0 / 100.0 * (double)(n - 1);
-    const long long k1 = (long long)i1, k99 = (long long)i99;
-    ctl->pct_f_lo = i1 - (double)k1;
-    ctl->pct_f_hi = i99 - (double)k99;
-    ctl->trank[0] = k1;  ctl->tactive[0] = 1;
-    ctl->trank[1] = k1 + 1; ctl->tactive[1] = (k1 + 1 < n);
-    ctl->trank[2] = k99; ctl->tactive[2] = 1;
-    ctl->trank[3] = k99 + 1; ctl->tactive[3] = (k99 + 1 < n);
-    ctl->ntarget = 4;
+    target_init(ctl, 0, (long long)i1, n, true);              // 1st percentile of the means
+    target_init(ctl, 1, (long long)i99, n, true);             // 99th
+    ctl->ntarget = 2;
+    for (int b = 0; b < NB; ++b) ctl->bcount[b] = 0;
 }
 
-// lo/hi from the selected means; bin edges; bin counts are filled by k_bin_count next.
+// lo/hi from the selected means; bin edges (noise.c:106-119)
 __global__ void k_noise_bins_setup(NoiseCtl* ctl) {
     const long long n = ctl->n;
     const double i1 = 1.0 / 100.0 * (double)(n - 1), i99 = 99.0 / 100.0 * (double)(n - 1);
     const long long k1 = (long long)i1, k99 = (long long)i99;
-    double lo = interp(ctl, 0, ctl->pct_f_lo, k1 + 1 < n);
-    double hi = interp(ctl, 2, ctl->pct_f_hi, k99 + 1 < n);
+    double lo = interp(ctl, 0, i1 - (double)k1, k1 + 1 < n);
+    double hi = interp(ctl, 1, i99 - (double)k99, k99 + 1 < n);
     if (hi <= lo) hi = lo + 1e-6;                       // noise.c:109
     ctl->lo = lo; ctl->hi = hi;
-    for (int k = 0; k <= NB; ++k) ctl->edge[k] = lo + (hi - lo) * k / NB;   // noise.c:118-119
-    for (int b = 0; b < NB; ++b) ctl->bcount[b] = 0;
+    for (int k = 0; k <= NB; ++k) {
+        const double e = lo + (hi - lo) * k / NB;      // noise.c:118-119
+        ctl->edge[k] = e;
+        float f = (float)e;
+        if ((double)f < e) f = nextafterf(f, INFINITY);
+        ctl->fedge[k] = f;
+    }
+    ctl->fscale = (float)(NB / (hi - lo));
     ctl->mode = 1;
 }
 
-__global__ void __launch_bounds__(256) k_bin_count(const float* __restrict__ mean, NoiseCtl* __restrict__ ctl) {
-    __shared__ unsigned long long cnt[NB];
-    if (threadIdx.x < NB) cnt[threadIdx.x] = 0;
-    __syncthreads();
-    const long long n = ctl->n;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int b = bin_of(__ldg(mean + i), ctl);
-        if (b >= 0) atomicAdd(&cnt[b], 1ull);
-    }
-    __syncthreads();
-    if (threadIdx.x < NB && cnt[threadIdx.x]) atomicAdd((unsigned long long*)&ctl->bcount[threadIdx.x], cnt[threadIdx.x]);
-}
-
-// per-bin targets (k, k+1) of the flat_pct percentile, bins with >= 200 voxels (noise.c:123)
+// per-bin targets of the flat_pct percentile, bins with >= 200 voxels (noise.c:123)
 __global__ void k_bin_targets(NoiseCtl* ctl) {
-    ctl->ntarget = 2 * NB;
+    ctl->ntarget = NB;
     for (int b = 0; b < NB; ++b) {
-        const long long c = ctl->bcount[b];
+        const long long c = (long long)ctl->bcount[b];
         const bool on = c >= 200;
         const double idx = ctl->flat_pct / 100.0 * (double)(c - 1);
-        const long long k = on ? (long long)idx : 0;
-        ctl->tgroup[2 * b] = ctl->tgroup[2 * b + 1] = b;
-        ctl->tprefix[2 * b] = ctl->tprefix[2 * b + 1] = 0;
-        ctl->trank[2 * b] = k; ctl->tactive[2 * b] = on;
-        ctl->trank[2 * b + 1] = k + 1; ctl->tactive[2 * b + 1] = on && (k + 1 < c);
+        target_init(ctl, b, on ? (long long)idx : 0, c, on);
     }
 }
 
@@ -318,35 +472,32 @@ FY_D double pct_small(double* v, int n, double pct) {       // percentile() on <
     return v[lo];
 }
 
-// Collect bin floors, then either fit (>= 1 bin) or arm the whole-volume var fallback.
+// stage 0: bin floors; arm the whole-volume fallback when no bin qualifies (mode 2).
+// stage 1: IRLS fit (FP64) and outputs.
 __global__ void k_noise_fit(NoiseCtl* ctl, int stage) {
     if (stage == 0) {
         int used = 0;
         for (int b = 0; b < NB; ++b) {
-            const long long c = ctl->bcount[b];
+            const long long c = (long long)ctl->bcount[b];
             if (c < 200) continue;
             const double idx = ctl->flat_pct / 100.0 * (double)(c - 1);
             const long long k = (long long)idx;
-            ctl->bfloor[b] = interp(ctl, 2 * b, idx - (double)k, k + 1 < c);
+            ctl->bfloor[b] = interp(ctl, b, idx - (double)k, k + 1 < c);
             ++used;
         }
         ctl->out_used = used;
-        if (used == 0) {                                  // noise.c:166-171 fallback
+        if (used == 0) {                                  // noise.c:166-171
             const long long n = ctl->n;
             const double idx = ctl->flat_pct / 100.0 * (double)(n - 1);
-            const long long k = (long long)idx;
-            ctl->pct_f_lo = idx - (double)k;
-            for (int t = 0; t < NT_MAX; ++t) { ctl->tactive[t] = 0; ctl->tprefix[t] = 0; }
-            ctl->ntarget = 2;
-            ctl->trank[0] = k; ctl->tactive[0] = 1;
-            ctl->trank[1] = k + 1; ctl->tactive[1] = k + 1 < n;
+            for (int t = 0; t < NT_MAX; ++t) target_init(ctl, t, 0, 0, false);
+            target_init(ctl, 0, (long long)idx, n, true);
+            ctl->ntarget = 1;
             ctl->mode = 2;
         } else {
             ctl->mode = 3;
         }
         return;
     }
-    // stage 1: the fit itself (FP64)
     double bin_i[NB], bin_f[NB], wv[NB];
     long long bin_c[NB];
     int used = 0;
@@ -354,15 +505,15 @@ __global__ void k_noise_fit(NoiseCtl* ctl, int stage) {
         if (ctl->bcount[b] < 200) continue;
         bin_i[used] = 0.5 * (ctl->edge[b] + ctl->edge[b + 1]);
         bin_f[used] = ctl->bfloor[b];
-        bin_c[used] = ctl->bcount[b];
+        bin_c[used] = (long long)ctl->bcount[b];
         ++used;
     }
     double g = 0, bb = 0;
     if (ctl->mode == 2) {
         const long long n = ctl->n;
         const double idx = ctl->flat_pct / 100.0 * (double)(n - 1);
-        bb = interp(ctl, 0, ctl->pct_f_lo, (long long)idx + 1 < n);
-        g = 0;
+        const long long k = (long long)idx;
+        bb = interp(ctl, 0, idx - (double)k, k + 1 < n);
     } else if (used >= 3) {                               // IRLS, noise.c:139-161
         for (int i = 0; i < used; i++) wv[i] = sqrt((double)bin_c[i]);
         for (int it = 0; it < 4; it++) {
@@ -384,111 +535,104 @@ __global__ void k_noise_fit(NoiseCtl* ctl, int stage) {
             }
         }
     } else if (used > 0) {                                // noise.c:162-165
-        double s = 0;
-        for (int i = 0; i < used; i++) s += bin_f[i];
-        bb = s / used; g = 0;
+        double sum = 0;
+        for (int i = 0; i < used; i++) sum += bin_f[i];
+        bb = sum / used;
     }
     if (!isfinite(g)) g = 0;
     if (!isfinite(bb)) bb = 0;
     double var_ref = g * ctl->ref_intensity + bb;
     if (var_ref < 0) var_ref = bb > 0 ? bb : 0;
-    const double noise_ref = sqrt(var_ref) * 1.15;
+    const double noise_ref = sqrt(var_ref) * 1.15;      // noise.c:181-187
     ctl->out_g = g; ctl->out_b = bb;
     ctl->out_noise_ref = noise_ref;
     ctl->out_ref_intensity = ctl->ref_intensity;
-    double eps = (3.0 * noise_ref) * (3.0 * noise_ref);
+    double eps = (3.0 * noise_ref) * (3.0 * noise_ref);  // noise.c:197-202
     if (!(eps > 1e-8)) eps = 1e-8;
     ctl->eps = (float)eps;
 }
 
 unsigned grid_sel(long long n, int sms) {
-    long long g = (n + 255) / 256;
-    const long long cap = (long long)sms * 4;
+    long long g = (n / 4 + 255) / 256;
+    const long long cap = (long long)sms * 8;
     return (unsigned)(g < cap ? (g ? g : 1) : cap);
 }
 
 }  // namespace
 
 size_t fy_noise_ctl_bytes() { return (sizeof(NoiseCtl) + 255) & ~(size_t)255; }
+// Scratch layout (floats): mean [0, nr), var [nr, 2nr), bin ids (bytes) from 2nr, with
+// nr = n rounded up to 64 floats so every sub-array (and the control block after the
+// scratch) starts 256-byte aligned for the vector loads.
+static size_t round64(size_t v) { return (v + 63) & ~(size_t)63; }
+size_t fy_noise_scratch_floats(size_t n) { return 2 * round64(n) + round64((n + 3) / 4); }
 
-size_t fy_noise_stats_smem(int r) {
-    switch (r) {
-        case 1: return sizeof(StatSmem<1>);
-        case 2: return sizeof(StatSmem<2>);
-        case 3: return sizeof(StatSmem<3>);
-        case 4: return sizeof(StatSmem<4>);
-        default: return 0;
-    }
-}
-
-// Enqueue the whole estimate. scratch: 2n floats (mean, var); ctl: fy_noise_ctl_bytes().
-// Supports win in {3..9} (r = win/2 <= 4).
+// Enqueue the whole estimate. scratch: 2n floats (mean, var) + n bytes (bin ids);
+// ctl: fy_noise_ctl_bytes(). Supports win in {3..9} (r = win/2 <= 4).
 cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, int win, double flat_pct,
                                      double ref_intensity, float* scratch, void* ctl_mem, int sms,
                                      cudaStream_t st, int& launches) {
     NoiseCtl* ctl = (NoiseCtl*)ctl_mem;
     const long long n = (long long)nz * ny * nx;
+    const size_t nr = ((size_t)n + 63) & ~(size_t)63;
     float* mean = scratch;
-    float* var = scratch + n;
+    float* var = scratch + nr;
+    uint8_t* bin = (uint8_t*)(scratch + 2 * nr);
     const int r = win / 2;
     const float inv_wc = (float)(1.0 / ((double)win * win * win));
-    // 1. stats
-    {
+    {   // 1. stats
         const dim3 tiles(ceil_div_i(nx, STX), ceil_div_i(ny, STY), 1);
         const long txy = (long)tiles.x * tiles.y;
-        int nchunk = (int)((4L * sms + txy - 1) / txy);
+        int nchunk = (int)((6L * sms + txy - 1) / txy);
         if (nchunk > nz / (8 * r)) nchunk = nz / (8 * r);
         if (nchunk < 1) nchunk = 1;
         const int zchunk = ceil_div_i(nz, nchunk);
         dim3 grid(tiles.x, tiles.y, ceil_div_i(nz, zchunk));
-        const size_t smem = fy_noise_stats_smem(r);
-        cudaError_t e0;
-#define FY_NS(RR)                                                                            \
-        if ((e0 = fy_smem_optin(k_noise_stats<RR>, smem)) != cudaSuccess) return e0;         \
-        k_noise_stats<RR><<<grid, SNT, smem, st>>>(in, mean, var, nz, ny, nx, inv_wc, win * win * win, zchunk);
         switch (r) {
-            case 1: FY_NS(1) break;
-            case 2: FY_NS(2) break;
-            case 3: FY_NS(3) break;
-            case 4: FY_NS(4) break;
+            case 1: k_noise_stats<1><<<grid, SNT, 0, st>>>(in, mean, var, nz, ny, nx, inv_wc, win * win * win, zchunk); break;
+            case 2: k_noise_stats<2><<<grid, SNT, 0, st>>>(in, mean, var, nz, ny, nx, inv_wc, win * win * win, zchunk); break;
+            case 3: k_noise_stats<3><<<grid, SNT, 0, st>>>(in, mean, var, nz, ny, nx, inv_wc, win * win * win, zchunk); break;
+            case 4: k_noise_stats<4><<<grid, SNT, 0, st>>>(in, mean, var, nz, ny, nx, inv_wc, win * win * win, zchunk); break;
             default: return cudaErrorInvalidValue;
         }
-#undef FY_NS
-        launches += 1;
+        fy_prof_mark(st, "noise.stats");
     }
     const unsigned g = grid_sel(n, sms);
     unsigned int* hist = ctl->hist;
     const size_t hist_bytes = sizeof(ctl->hist);
-    const size_t smem_all = 4 * 2048 * sizeof(unsigned int), smem_bin = 2 * NB * 256 * sizeof(unsigned int);
+    const size_t smem_all = 2 * 2048 * sizeof(unsigned int), smem_bin = NB * 256 * sizeof(unsigned int);
     cudaError_t e;
-    if ((e = fy_smem_optin(k_sel_hist<DB_ALL>, smem_all)) != cudaSuccess) return e;
-    if ((e = fy_smem_optin(k_sel_hist<DB_BIN>, smem_bin)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(hist, 0, hist_bytes, st)) != cudaSuccess) return e;
     k_noise_setup<<<1, 1, 0, st>>>(ctl, n, flat_pct, ref_intensity);
-    // 2a. 1st/99th percentile of the means: 11 + 11 + 10 bits
+    // 2a. 1st/99th percentile of the means: 11 + 11 + 10 bits, then the k+1 neighbours
     const int all_digits[3][2] = {{21, 11}, {10, 11}, {0, 10}};
-    for (auto& dg : all_digits) {
-        k_sel_hist<DB_ALL><<<g, 256, smem_all, st>>>(mean, var, ctl, dg[0], 0);
-        k_sel_scan<<<4, 256, 0, st>>>(ctl, dg[1], 0);
+    for (int i = 0; i < 3; ++i) {
+        if (all_digits[i][1] == 11) k_sel_hist<11><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0], 0);
+        else k_sel_hist<10><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0], 0);
+        k_sel_scan<<<2, 256, 0, st>>>(ctl, all_digits[i][1], 0, i == 2);
     }
+    k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 0);
     k_noise_bins_setup<<<1, 1, 0, st>>>(ctl);
-    k_bin_count<<<g, 256, 0, st>>>(mean, ctl);
+    k_bin_assign<<<g, 256, 0, st>>>(mean, bin, ctl);
     k_bin_targets<<<1, 1, 0, st>>>(ctl);
-    if ((e = cudaMemsetAsync(hist, 0, hist_bytes, st)) != cudaSuccess) return e;
-    // 2b. per-bin flat_pct percentile of the variance: 4 x 8 bits
+    fy_prof_mark(st, "noise.lohi+bins");
+    // 2b. per-bin flat_pct percentile of the variance: 4 x 8 bits, then the k+1 neighbours
     for (int sh = 24; sh >= 0; sh -= 8) {
-        k_sel_hist<DB_BIN><<<g, 256, smem_bin, st>>>(mean, var, ctl, sh, 1);
-        k_sel_scan<<<2 * NB, 256, 0, st>>>(ctl, 8, 1);
+        k_sel_hist<8><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, sh, 1);
+        k_sel_scan<<<NB, 256, 0, st>>>(ctl, 8, 1, sh == 0);
     }
+    k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 1);
     k_noise_fit<<<1, 1, 0, st>>>(ctl, 0);
-    if ((e = cudaMemsetAsync(hist, 0, hist_bytes, st)) != cudaSuccess) return e;
+    fy_prof_mark(st, "noise.bin_select");
     // 2c. fallback (mode 2 only): flat_pct percentile over all voxels' variance
-    for (auto& dg : all_digits) {
-        k_sel_hist<DB_ALL><<<g, 256, smem_all, st>>>(mean, var, ctl, dg[0], 2);
-        k_sel_scan<<<2, 256, 0, st>>>(ctl, dg[1], 2);
+    for (int i = 0; i < 3; ++i) {
+        if (all_digits[i][1] == 11) k_sel_hist<11><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0], 2);
+        else k_sel_hist<10><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0], 2);
+        k_sel_scan<<<1, 256, 0, st>>>(ctl, all_digits[i][1], 2, i == 2);
     }
+    k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 2);
     k_noise_fit<<<1, 1, 0, st>>>(ctl, 1);
-    launches += 1 + 6 + 3 + 8 + 1 + 6 + 1;
+    launches += 1 + 1 + 6 + 1 + 1 + 1 + 1 + 8 + 1 + 1 + 6 + 1 + 1;
     return cudaGetLastError();
 }
 

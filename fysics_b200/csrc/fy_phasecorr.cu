@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(KBp<E>::nt, 2) k_pc_x(const float* __restrict_
     }
     __syncthreads();
     const Lane ln(wlog);
-    line_fft<E>(s, LP, ln.l, ln.tl, pl, stw, -1.f,
+    line_fft<E>(s + ln.l, LP, ln.tl, pl, stw, -1.f,
                 [&](int i) { return s[i * LP + ln.l]; },
                 [&](int i, float2 v) { s[i * LP + ln.l] = v; });
     __syncthreads();
@@ -165,11 +165,11 @@ __global__ void __launch_bounds__(KBp<E>::nt, 1) k_pc_z(float2* __restrict__ spe
     if (threadIdx.x == 0) s_max = 0.f;
     load_twiddles(stw, tw, n);
     __syncthreads();
-    line_fft<E>(sf, W, ln.l, ln.tl, pl, stw, -1.f,
+    line_fft<E>(sf + ln.l, W, ln.tl, pl, stw, -1.f,
                 [&](int i) { return i < g.nz ? specF[coff + (size_t)i * zstride] : make_float2(0.f, 0.f); },
                 [&](int i, float2 v) { sf[i * W + ln.l] = v; });
     __syncthreads();
-    line_fft<E>(sm, W, ln.l, ln.tl, pl, stw, -1.f,
+    line_fft<E>(sm + ln.l, W, ln.tl, pl, stw, -1.f,
                 [&](int i) { return i < g.nz ? specM[coff + (size_t)i * zstride] : make_float2(0.f, 0.f); },
                 [&](int i, float2 v) { sm[i * W + ln.l] = v; });
     __syncthreads();
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(KBp<E>::nt, 1) k_pc_z(float2* __restrict__ spe
     atomicMax((unsigned int*)&s_max, __float_as_uint(lmax));   // non-negative floats order as uints
     __syncthreads();
     if (threadIdx.x == 0) atomicMax(&ctl->maxmag_bits, __float_as_uint(s_max));
-    line_fft<E>(sf, W, ln.l, ln.tl, pl, stw, +1.f,
+    line_fft<E>(sf + ln.l, W, ln.tl, pl, stw, +1.f,
                 [&](int i) { return sf[i * W + ln.l]; },
                 [&](int i, float2 v) { specF[coff + (size_t)i * zstride] = v; });
 }
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(KBp<E>::nt, 2) k_pc_c2r(const float2* __restri
     }
     __syncthreads();
     const Lane ln(wlog);
-    line_fft<E>(s, LP, ln.l, ln.tl, pl, stw, +1.f,
+    line_fft<E>(s + ln.l, LP, ln.tl, pl, stw, +1.f,
                 [&](int i) { return s[i * LP + ln.l]; },
                 [&](int i, float2 v) { s[i * LP + ln.l] = v; });
     __syncthreads();

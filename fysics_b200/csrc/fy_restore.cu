@@ -80,7 +80,7 @@ extern "C" int fy_gpu_restore_u8(const unsigned char* d_u8, float* d_out, int nz
     const float* eps_ptr = nullptr;
     int launches = 0;
     if (!(cfg->guided_eps > 0)) {
-        if ((e = c.aux.ensure(2 * n * sizeof(float))) != cudaSuccess) return fail_cuda(e, what);
+        if ((e = c.aux.ensure(fy_noise_scratch_floats(n) * sizeof(float))) != cudaSuccess) return fail_cuda(e, what);
         if ((e = c.small.ensure(fy_noise_ctl_bytes())) != cudaSuccess) return fail_cuda(e, what);
         double pct = cfg->noise_flat_pct <= 0 ? 10.0 : cfg->noise_flat_pct;
         if ((e = fy_launch_estimate_noise(dec, nz, ny, nx, win, pct, cfg->noise_ref_intensity, c.aux.as<float>(),
