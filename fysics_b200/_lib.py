@@ -110,6 +110,7 @@ SIGNATURES = {
     "fy_gpu_estimate_noise": (_i, [_P, _i, _i, _i, _i, _d, _d, _P, _P]),
     "fy_gpu_noise_model": (_i, [_P, _i, _i, _i, _PN, _P]),
     "fy_gpu_noise_eps": (_P, [_P, _i, _i, _i]),
+    "fy_gpu_estimate_noise_noalloc": (_i, [_P, _i, _i, _i, _i, _d, _d, _P, _P, _P]),
     "fy_gpu_dering_create": (_i, [C.POINTER(_P), _l, _l, _l, _d, _d, _i, _i]),
     "fy_gpu_dering_destroy": (None, [_P]),
     "fy_gpu_dering_reset": (_i, [_P, _P]),

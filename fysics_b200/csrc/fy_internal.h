@@ -58,6 +58,8 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
 cudaError_t fy_noise_read(const void* ctl_mem, double* g, double* b, double* noise_ref, double* ref_intensity,
                           int* used, cudaStream_t st);
 const float* fy_noise_eps_ptr(const void* ctl_mem);
+// Copy a finished model into caller device memory (an fy_noise_model; d_eps may be null).
+cudaError_t fy_noise_store(const void* ctl_mem, void* d_model, float* d_eps, cudaStream_t st);
 
 // Ring removal (fy_dering.cu)
 cudaError_t fy_launch_dering_accum(const uint8_t* buf, const int* map, unsigned long long* sum, unsigned int* cnt,

@@ -15,6 +15,7 @@
 //      (3*noise_ref)^2 floored at 1e-8 (noise.c:197-202).
 // The launch sequence is fixed (no host decisions), so a chain can keep it on one stream.
 #include "fy_internal.h"
+#include "fysics_b200.h"
 
 namespace {
 
@@ -650,3 +651,21 @@ cudaError_t fy_noise_read(const void* ctl_mem, double* g, double* b, double* noi
 }
 
 const float* fy_noise_eps_ptr(const void* ctl_mem) { return &((const NoiseCtl*)ctl_mem)->eps; }
+
+namespace {
+// One thread copies a finished model into caller device memory laid out as fy_noise_model.
+__global__ void k_noise_store(const NoiseCtl* __restrict__ ctl, fy_noise_model* __restrict__ m,
+                              float* __restrict__ eps) {
+    m->g = ctl->out_g;
+    m->b = ctl->out_b;
+    m->noise_ref = ctl->out_noise_ref;
+    m->ref_intensity = ctl->out_ref_intensity;
+    m->n_bins_used = ctl->out_used;
+    if (eps) *eps = ctl->eps;
+}
+}  // namespace
+
+cudaError_t fy_noise_store(const void* ctl_mem, void* d_model, float* d_eps, cudaStream_t st) {
+    k_noise_store<<<1, 1, 0, st>>>((const NoiseCtl*)ctl_mem, (fy_noise_model*)d_model, d_eps);
+    return cudaGetLastError();
+}

@@ -179,6 +179,24 @@ int    fy_gpu_noise_model(const void *d_scratch, int nz, int ny, int nx, fy_nois
                           void *stream);
 const float *fy_gpu_noise_eps(const void *d_scratch, int nz, int ny, int nx);
 
+/* Noise model without any allocation; it has no counterpart in the reference. It is for
+ * callers that may not allocate device memory while they run, e.g. a serving loop whose
+ * HBM is already committed to its own pool, where a cudaMalloc can fail or stall the
+ * device. Scratch is one static device array inside the library, sized for
+ * FY_NOISE_NOALLOC_MAX_VOXELS voxels (128^3, about 18 MB). Every GPU that loads the
+ * library holds it until the process exits. Larger volumes return FY_EUNSUPPORTED.
+ * Runs on the calling thread's current device and enqueues on `stream`. The model goes to
+ * d_model, caller device memory laid out as fy_noise_model. d_eps, which may be NULL,
+ * receives the float fy_guided_eps_for_noise(noise_ref).
+ * The first call on each device resolves the array's device address. Make that first
+ * call before any stream capture. All calls on a device share the array, which keeps
+ * the previous call's contents. Calls whose GPU work can overlap race on it, e.g. calls
+ * on unordered streams or from several host threads, so serialise them. */
+#define FY_NOISE_NOALLOC_MAX_VOXELS 2097152
+int    fy_gpu_estimate_noise_noalloc(const float *d_in, int nz, int ny, int nx, int win,
+                                     double flat_pct, double ref_intensity,
+                                     fy_noise_model *d_model, float *d_eps, void *stream);
+
 /* Device-resident ring state for chains (fy_dering's arrays live on the GPU). accumulate
  * adds a device u8 region at global (z0,y0,x0) into slab z0/slab_z (accumulate + merge);
  * finalize runs the sector vote on the device; apply subtracts on a device f32 region and
