@@ -9,7 +9,7 @@ using fy::fail_cuda;
 namespace {
 
 // Enqueue an exact (s <= 1) or fast (s >= 2) guided filter on device buffers. `scratch`
-// must hold fy_guided_scratch_floats(); in == out is allowed (handled by a copy).
+// must hold guided_scratch_floats(); in == out is allowed.
 size_t guided_scratch_floats(int nz, int ny, int nx, int radius, int s) {
     const size_t n = (size_t)nz * ny * nx;
     if (radius < 1) radius = 2;
@@ -17,11 +17,11 @@ size_t guided_scratch_floats(int nz, int ny, int nx, int radius, int s) {
         const int lz = (nz + s - 1) / s, ly = (ny + s - 1) / s, lx = (nx + s - 1) / s;
         if (lz >= 2 && ly >= 2 && lx >= 2) {
             int rl = radius / s; if (rl < 1) rl = 1;
-            if (rl <= 4) return 3 * (size_t)lz * ly * lx;
+            if (rl <= 4) return fy_guided_fast_scratch_floats(lz, ly, lx);
             return 3 * (size_t)lz * ly * lx + 4 * (size_t)lz * ly * lx;
         }
     }
-    return radius <= 4 ? n : 4 * n;        // fused: a copy for aliasing; generic: 4n
+    return radius <= 4 ? fy_guided_fused_scratch_floats(n) : 4 * n;   // exact: a, b fields; generic: 4n
 }
 
 int enqueue_guided(const float* in, float* out, float* scratch, int nz, int ny, int nx, int radius,
@@ -29,7 +29,6 @@ int enqueue_guided(const float* in, float* out, float* scratch, int nz, int ny, 
     fy::ThreadCtx& c = ctx();
     if (radius < 1) radius = 2;                                    // guided.c:115
     const float epsf = (float)eps;
-    const size_t n = (size_t)nz * ny * nx;
     int launches = 0;
     cudaError_t e = cudaSuccess;
     bool fast = false;
@@ -46,14 +45,8 @@ int enqueue_guided(const float* in, float* out, float* scratch, int nz, int ny, 
             return fail(FY_EUNSUPPORTED, "%s: fast path low-grid radius %d > 4", what, rl);
         }
     } else if (radius <= 4) {
-        const float* src = in;
-        if (in == out) {                                           // fused path cannot alias
-            e = cudaMemcpyAsync(scratch, in, n * sizeof(float), cudaMemcpyDeviceToDevice, st);
-            if (e != cudaSuccess) return fail_cuda(e, what);
-            src = scratch;
-        }
-        e = fy_launch_guided_fused(src, out, nullptr, nz, ny, nx, radius, epsf, 0, c.sms, st);
-        launches = 1;
+        e = fy_launch_guided_fused(in, out, nullptr, scratch, nz, ny, nx, radius, epsf, 0, c.sms, st);
+        launches = 2;
     } else {
         e = fy_launch_guided_generic(in, out, scratch, nz, ny, nx, radius, epsf, st, launches);
     }

@@ -38,9 +38,12 @@ cudaError_t fy_launch_float_to_u8(const float* in, uint8_t* out, size_t n, cudaS
 cudaError_t fy_launch_u8_to_float(const uint8_t* in, float* out, size_t n, cudaStream_t st);
 
 // Guided filter / box mean (fy_guided.cu)
-size_t fy_guided_fused_smem(int r);
-cudaError_t fy_launch_guided_fused(const float* in, float* out, float* out_b, int nz, int ny, int nx, int r,
-                                   float eps, int mode, int sms, cudaStream_t st, const float* eps_ptr = nullptr);
+// exact r <= 4: ab_ws holds fy_guided_fused_scratch_floats(n); out may alias in
+size_t fy_guided_fused_scratch_floats(size_t n);
+size_t fy_guided_fast_scratch_floats(int lz, int ly, int lx);
+cudaError_t fy_launch_guided_fused(const float* in, float* out, float* out_b, float* ab_ws, int nz, int ny, int nx,
+                                   int r, float eps, int mode, int sms, cudaStream_t st,
+                                   const float* eps_ptr = nullptr);
 cudaError_t fy_launch_guided_generic(const float* in, float* out, float* ws, int nz, int ny, int nx, int r,
                                      float eps, cudaStream_t st, int& launches);
 cudaError_t fy_launch_guided_fast(const float* in, float* out, float* ws, int nz, int ny, int nx, int r,

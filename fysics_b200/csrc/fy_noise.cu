@@ -1,8 +1,8 @@
 // fy_noise.cu -- per-volume noise model fy_estimate_noise (noise.c:75-192) on the GPU.
 //
-//   1. k_noise_stats: local box sums over (2r+1)^3 windows with zero outside the volume and
-//      the FIXED divisor win^3 (noise.c:20-59, 92-101): mean m and variance
-//      v = max(S2/wc - m^2, 0). z-sliding like the guided kernel; sums are direct
+//   1. Local stats, a z-sliding box pass (fy_zbox.cuh): box sums over (2r+1)^3 windows with
+//      zero outside the volume and the FIXED divisor win^3 (noise.c:20-59, 92-101): mean m
+//      and variance v = max(S2/wc - m^2, 0). Sums are direct
 //      (2r+1)-tap float sums of (I - c) and (I - c)^2 with a per-tile shift c, and interior
 //      voxels use v = S2'/wc - (S1'/wc)^2, which equals the reference's S2/wc - (S1/wc)^2
 //      without its cancellation.
@@ -16,6 +16,7 @@
 // The launch sequence is fixed (no host decisions), so a chain can keep it on one stream.
 #include "fy_internal.h"
 #include "fysics_b200.h"
+#include "fy_zbox.cuh"
 
 namespace {
 
@@ -72,119 +73,9 @@ struct NoiseCtl {
 
 namespace {
 
-constexpr int SNT = 256, STY = 16, STX = 32;
 
 // ---------------------------------------------------------------- 1. local stats
-// CTA = 32 x 16 output columns sliding along z. Per input plane: stage (I - c) with zeros
-// outside the volume (so window sums need no bounds checks); 4-column X sums of u and u^2
-// by 8*(16+2R) threads; 4-row Y sums by 128 threads, which keep a (2R+1)-plane z ring of
-// their XY sums in registers and emit mean/variance for the plane R behind.
-template <int R>
-struct StatSmem {
-    static constexpr int IY = STY + 2 * R, IX = STX + 2 * R, NR = 2 * R + 1;
-    float I[IY][IX];
-    float xs1[IY][STX], xs2[IY][STX];
-};
-
-template <int R>
-__global__ void __launch_bounds__(SNT, 2) k_noise_stats(const float* __restrict__ in, float* __restrict__ mean,
-                                                        float* __restrict__ var, int nz, int ny, int nx,
-                                                        float inv_wc, int wci, int zchunk) {
-    using S = StatSmem<R>;
-    constexpr int NR = S::NR;
-    __shared__ S sm;
-    const int x0 = blockIdx.x * STX, y0 = blockIdx.y * STY;
-    const int zs = blockIdx.z * zchunk, ze = min(nz, zs + zchunk);
-    const int t = threadIdx.x;
-    const size_t plane = (size_t)ny * nx;
-    const float c = __ldg(in + (size_t)zs * plane + (size_t)y0 * nx + x0);
-    // Y-stage role: column xc, rows 4*rb .. 4*rb+3 (threads 0..127)
-    const bool yrole = t < 4 * STX;
-    const int xc = t % STX, rb = t / STX;
-    float r1[NR][4], r2[NR][4];
-#pragma unroll
-    for (int q = 0; q < NR; ++q)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) r1[q][k] = r2[q][k] = 0.f;
-    int cyx[4];
-    if (yrole) {
-        const int gx = x0 + xc, cx = min(gx + R, nx - 1) - max(gx - R, 0) + 1;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int gy = y0 + 4 * rb + k;
-            cyx[k] = (min(gy + R, ny - 1) - max(gy - R, 0) + 1) * cx;
-        }
-    }
-    for (int zi = zs - R; zi < ze + R; ++zi) {
-        const bool zin = zi >= 0 && zi < nz;
-        for (int k = t; k < S::IY * S::IX; k += SNT) {
-            const int yy = k / S::IX, xx = k - yy * S::IX;
-            const int gy = y0 - R + yy, gx = x0 - R + xx;
-            float v = 0.f;
-            if (zin && gy >= 0 && gy < ny && gx >= 0 && gx < nx) v = __ldg(in + (size_t)zi * plane + (size_t)gy * nx + gx) - c;
-            sm.I[yy][xx] = v;
-        }
-        __syncthreads();
-        if (t < (STX / 4) * S::IY) {                        // X sums, 4 columns per thread
-            const int yy = t / (STX / 4), x4 = 4 * (t % (STX / 4));
-            float u[4 + 2 * R];
-#pragma unroll
-            for (int j = 0; j < 4 + 2 * R; ++j) u[j] = sm.I[yy][x4 + j];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                float s1 = 0.f, s2 = 0.f;
-#pragma unroll
-                for (int j = 0; j <= 2 * R; ++j) { s1 += u[k + j]; s2 += u[k + j] * u[k + j]; }
-                sm.xs1[yy][x4 + k] = s1; sm.xs2[yy][x4 + k] = s2;
-            }
-        }
-        __syncthreads();
-        if (yrole) {                                        // Y sums + z ring
-#pragma unroll
-            for (int q = 0; q < NR - 1; ++q)
-#pragma unroll
-                for (int k = 0; k < 4; ++k) { r1[q][k] = r1[q + 1][k]; r2[q][k] = r2[q + 1][k]; }
-            float a1[4 + 2 * R], a2[4 + 2 * R];
-#pragma unroll
-            for (int j = 0; j < 4 + 2 * R; ++j) { a1[j] = sm.xs1[4 * rb + j][xc]; a2[j] = sm.xs2[4 * rb + j][xc]; }
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                float s1 = 0.f, s2 = 0.f;
-#pragma unroll
-                for (int j = 0; j <= 2 * R; ++j) { s1 += a1[k + j]; s2 += a2[k + j]; }
-                r1[NR - 1][k] = s1; r2[NR - 1][k] = s2;
-            }
-            const int zo = zi - R;
-            if (zo >= zs && zo < ze) {
-                const int cz = min(zo + R, nz - 1) - max(zo - R, 0) + 1;
-                const int gx = x0 + xc;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int gy = y0 + 4 * rb + k;
-                    if (gy >= ny || gx >= nx) continue;
-                    float s1 = 0.f, s2 = 0.f;
-#pragma unroll
-                    for (int q = 0; q < NR; ++q) { s1 += r1[q][k]; s2 += r2[q][k]; }
-                    const int nini = cz * cyx[k];
-                    const float nin = (float)nini;
-                    // raw sums: S1 = S1' + nin*c, S2 = S2' + 2c*S1' + nin*c^2
-                    const float m = (s1 + nin * c) * inv_wc;
-                    float v;
-                    if (nini == wci) {                      // interior: shifted, cancellation-free
-                        const float e1 = s1 * inv_wc;
-                        v = s2 * inv_wc - e1 * e1;
-                    } else {
-                        v = (s2 + 2.0f * c * s1 + nin * c * c) * inv_wc - m * m;
-                    }
-                    if (v < 0.f) v = 0.f;
-                    const size_t o = (size_t)zo * plane + (size_t)gy * nx + gx;
-                    mean[o] = m;
-                    var[o] = v;
-                }
-            }
-        }
-    }
-}
+// z-sliding box pass (fy_zbox.cuh, ZB_NOISE): 4 B read + 8 B written per voxel.
 
 // ---------------------------------------------------------------- 2. radix select
 // Exact bin of a float mean: m >= edge[k] <=> m >= fedge[k] with fedge[k] the smallest float
@@ -582,20 +473,12 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     const int r = win / 2;
     const float inv_wc = (float)(1.0 / ((double)win * win * win));
     {   // 1. stats
-        const dim3 tiles(ceil_div_i(nx, STX), ceil_div_i(ny, STY), 1);
-        const long txy = (long)tiles.x * tiles.y;
-        int nchunk = (int)((6L * sms + txy - 1) / txy);
-        if (nchunk > nz / (8 * r)) nchunk = nz / (8 * r);
-        if (nchunk < 1) nchunk = 1;
-        const int zchunk = ceil_div_i(nz, nchunk);
-        dim3 grid(tiles.x, tiles.y, ceil_div_i(nz, zchunk));
-        switch (r) {
-            case 1: k_noise_stats<1><<<grid, SNT, 0, st>>>(in, mean, var, nz, ny, nx, inv_wc, win * win * win, zchunk); break;
-            case 2: k_noise_stats<2><<<grid, SNT, 0, st>>>(in, mean, var, nz, ny, nx, inv_wc, win * win * win, zchunk); break;
-            case 3: k_noise_stats<3><<<grid, SNT, 0, st>>>(in, mean, var, nz, ny, nx, inv_wc, win * win * win, zchunk); break;
-            case 4: k_noise_stats<4><<<grid, SNT, 0, st>>>(in, mean, var, nz, ny, nx, inv_wc, win * win * win, zchunk); break;
-            default: return cudaErrorInvalidValue;
-        }
+        fyzb::Params sp{};
+        sp.nz = nz; sp.ny = ny; sp.nx = nx;
+        sp.f0 = in; sp.o0 = mean; sp.o1 = var;
+        sp.inv_wc = inv_wc; sp.wci = win * win * win;
+        cudaError_t e0 = fyzb::launch<fyzb::ZB_NOISE>(sp, r, sms, st);
+        if (e0 != cudaSuccess) return e0;
         fy_prof_mark(st, "noise.stats");
     }
     const unsigned g = grid_sel(n, sms);

@@ -96,16 +96,24 @@ extern "C" int fy_gpu_restore_u8(const unsigned char* d_u8, float* d_out, int nz
         const int lz = (nz + s - 1) / s, ly = (ny + s - 1) / s, lx = (nx + s - 1) / s;
         int rl = radius / s; if (rl < 1) rl = 1;
         if (lz >= 2 && ly >= 2 && lx >= 2 && rl <= 4) {
-            if ((e = c.vout.ensure(3 * (size_t)lz * ly * lx * sizeof(float))) != cudaSuccess) return fail_cuda(e, what);
+            if ((e = c.vout.ensure(fy_guided_fast_scratch_floats(lz, ly, lx) * sizeof(float))) != cudaSuccess)
+                return fail_cuda(e, what);
             e = fy_launch_guided_fast(dec, d_out, c.vout.as<float>(), nz, ny, nx, radius, eps, s, c.sms, st, launches,
                                       eps_ptr);
         } else {
-            e = fy_launch_guided_fused(dec, d_out, nullptr, nz, ny, nx, radius, eps, 0, c.sms, st, eps_ptr);
-            launches += 1;
+            if ((e = c.aux.ensure(fy_guided_fused_scratch_floats(n) * sizeof(float))) != cudaSuccess)
+                return fail_cuda(e, what);
+            e = fy_launch_guided_fused(dec, d_out, nullptr, c.aux.as<float>(), nz, ny, nx, radius, eps, 0, c.sms, st,
+                                       eps_ptr);
+            launches += 2;
         }
     } else {
-        e = fy_launch_guided_fused(dec, d_out, nullptr, nz, ny, nx, radius, eps, 0, c.sms, st, eps_ptr);
-        launches += 1;
+        // a, b reuse the noise statistics' scratch: the model is final by now (stream order)
+        if ((e = c.aux.ensure(fy_guided_fused_scratch_floats(n) * sizeof(float))) != cudaSuccess)
+            return fail_cuda(e, what);
+        e = fy_launch_guided_fused(dec, d_out, nullptr, c.aux.as<float>(), nz, ny, nx, radius, eps, 0, c.sms, st,
+                                   eps_ptr);
+        launches += 2;
     }
     if (e != cudaSuccess) return fail_cuda(e, what);
     fy_prof_mark(st, "guided");

@@ -1,0 +1,327 @@
+// fy_zbox.cuh -- z-sliding 3-D box sums of two per-voxel quantities.
+//
+// Shared by the noise model's local statistics (noise.c:20-67) and the two passes of the
+// guided filter (guided.c:113-141). A CTA owns a 64 x 16 column tile and a chunk of z
+// planes. Per input plane zi:
+//   stage   cp.async copies the plane's tile plus halo (x0-4 .. x0+68, y0-R .. y0+16+R)
+//           into a 4-deep shared-memory ring, zero-filled outside the volume; planes
+//           zi+1 .. zi+3 are in flight while zi is reduced.
+//   X phase one item = 4 output columns of one staged row: three float4 reads, window
+//           sums of both quantities, two float4 stores.
+//   Y phase one thread = one output column x 4 output rows. Its (2R+1)-plane z ring of
+//           XY sums stays in registers and gives the box of plane zi - R to the epilogue.
+// Epilogues (KIND):
+//   ZB_NOISE      u = I - c (zero outside the volume), fixed divisor win^3: local mean and
+//                 variance as in noise.c:41-61, with the tile shift c removing the FP32
+//                 cancellation of E[I^2] - E[I]^2.
+//   ZB_GUIDED_AB  u = I - c, box MEANS over the in-bounds window taken axis by axis with
+//                 1.0f/(float)count (guided.c:22-28): var = max(corr - mean^2, 0),
+//                 a = var/(var + eps), b = mean*(1 - a) (guided.c:121-132) -> A, B.
+//   ZB_GUIDED_OUT box means of A and B -> out = box(a)*I + box(b) (guided.c:136-140), or
+//                 the two means themselves for the decimated variant (guided.c:181-182).
+// Window sums are direct (2R+1)-tap float sums in ascending order, started from the first
+// tap, so no running-sum chain accumulates error. Each output voxel is written once by one
+// thread, and ZB_GUIDED_OUT reads the guide only at the voxel it writes, so out may alias
+// the guide.
+#pragma once
+#include "fy_internal.h"
+
+namespace fyzb {
+
+constexpr int TX = 64, TY = 16, NT = 256, NS = 4;
+constexpr int SXW = TX + 8;                 // staged row: x0 - 4 .. x0 + TX + 4 (R <= 4)
+enum { ZB_NOISE = 0, ZB_GUIDED_AB = 1, ZB_GUIDED_OUT = 2 };
+
+struct Params {
+    const float* f0;       // I (NOISE, GUIDED_AB) or A (GUIDED_OUT)
+    const float* f1;       // B (GUIDED_OUT)
+    const float* guide;    // I (GUIDED_OUT, out_mode 0)
+    float* o0;             // mean | A | out (or box(a))
+    float* o1;             // var  | B | box(b) (out_mode 1)
+    const float* eps_ptr;  // GUIDED_AB: device eps (overrides eps when set)
+    float eps;
+    float inv_wc;          // NOISE: 1/win^3
+    int wci;               // NOISE: win^3
+    int out_mode;
+    int nz, ny, nx, zchunk;
+};
+
+template <int R, int NF>
+struct Geo {
+    static constexpr int NR = 2 * R + 1;
+    static constexpr int SY = TY + 2 * R;
+    static constexpr int STAGE = NF * SY * SXW;                 // floats per staged plane
+    static constexpr int XS = SY * TX;                          // floats per X-sum array
+    static constexpr size_t bytes = (size_t)(NS * STAGE + 2 * XS + TX + TY) * sizeof(float);
+};
+
+FY_D float recip_count(int p, int L, int r) {
+    const int lo = p - r < 0 ? 0 : p - r;
+    const int hi = p + r > L - 1 ? L - 1 : p + r;
+    return 1.0f / (float)(hi - lo + 1);                       // guided.c:26 (IEEE division)
+}
+
+FY_D void cp16(float* sdst, const float* gsrc, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+FY_D void cp4(float* sdst, const float* gsrc, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc), "r"(valid ? 4 : 0)
+                 : "memory");
+}
+FY_D void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+FY_D void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Stage plane zi (all NF fields) into dst; zero fill outside the volume.
+template <int R, int NF, bool VEC>
+FY_D void stage_plane(float* dst, const Params& p, int zi, int x0, int y0) {
+    using G = Geo<R, NF>;
+    const bool zin = zi >= 0 && zi < p.nz;
+    const size_t pbase = (size_t)(zin ? zi : 0) * p.ny * p.nx;
+    if (VEC) {
+        constexpr int Q = SXW / 4, PER = G::SY * Q;
+        for (int k = threadIdx.x; k < NF * PER; k += NT) {
+            const int f = NF == 1 ? 0 : k / PER;
+            const int rem = k - f * PER;
+            const int yy = rem / Q, q = rem - yy * Q;
+            const int gy = y0 - R + yy, gx = x0 - 4 + 4 * q;
+            const bool ok = zin && gy >= 0 && gy < p.ny && gx >= 0 && gx < p.nx;
+            const float* base = f ? p.f1 : p.f0;
+            cp16(dst + f * G::SY * SXW + yy * SXW + 4 * q, ok ? base + pbase + (size_t)gy * p.nx + gx : base, ok);
+        }
+    } else {
+        constexpr int PER = G::SY * SXW;
+        for (int k = threadIdx.x; k < NF * PER; k += NT) {
+            const int f = NF == 1 ? 0 : k / PER;
+            const int rem = k - f * PER;
+            const int yy = rem / SXW, xx = rem - yy * SXW;
+            const int gy = y0 - R + yy, gx = x0 - 4 + xx;
+            const bool ok = zin && gy >= 0 && gy < p.ny && gx >= 0 && gx < p.nx;
+            const float* base = f ? p.f1 : p.f0;
+            cp4(dst + f * G::SY * SXW + rem, ok ? base + pbase + (size_t)gy * p.nx + gx : base, ok);
+        }
+    }
+}
+
+template <int R, int KIND, bool VEC>
+__global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p) {
+    constexpr int NF = KIND == ZB_GUIDED_OUT ? 2 : 1;
+    using G = Geo<R, NF>;
+    constexpr int NR = G::NR;
+    extern __shared__ float4 zb_smem4[];
+    float* stage = reinterpret_cast<float*>(zb_smem4);
+    float* xs1 = stage + NS * G::STAGE;
+    float* xs2 = xs1 + G::XS;
+    float* rx = xs2 + G::XS;
+    float* ry = rx + TX;
+    const int t = threadIdx.x;
+    const int nz = p.nz, ny = p.ny, nx = p.nx;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int zs = blockIdx.z * p.zchunk, ze = min(nz, zs + p.zchunk);
+    const size_t plane = (size_t)ny * nx;
+    // per-tile shift: one constant for every window this CTA forms
+    const float c = KIND == ZB_GUIDED_OUT ? 0.f : __ldg(p.f0 + (size_t)zs * plane + (size_t)y0 * nx + x0);
+    float eps = p.eps;
+    if (KIND == ZB_GUIDED_AB && p.eps_ptr) eps = *p.eps_ptr;    // chained from the device noise model
+    if (t < TX) rx[t] = x0 + t < nx ? recip_count(x0 + t, nx, R) : 0.f;
+    if (t < TY) ry[t] = y0 + t < ny ? recip_count(y0 + t, ny, R) : 0.f;
+    const bool cols_in = x0 - 4 >= 0 && x0 + TX + 4 <= nx;       // no column of the staged rows is outside
+    const int zfirst = zs - R, zend = ze + R;
+#pragma unroll
+    for (int s = 0; s < NS - 1; ++s) {
+        if (zfirst + s < zend) stage_plane<R, NF, VEC>(stage + s * G::STAGE, p, zfirst + s, x0, y0);
+        cp_commit();
+    }
+    // Y-phase role: output column xc, output rows 4*rg .. 4*rg+3
+    const int xc = t & (TX - 1), rg = t >> 6;
+    const int gx = x0 + xc;
+    int cyx[4];                                                   // NOISE: in-bounds XY window size
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int gy = y0 + 4 * rg + k;
+        cyx[k] = (min(gy + R, ny - 1) - max(gy - R, 0) + 1) * (min(gx + R, nx - 1) - max(gx - R, 0) + 1);
+    }
+    float r1[NR][4], r2[NR][4];
+#pragma unroll
+    for (int q = 0; q < NR; ++q)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) r1[q][k] = r2[q][k] = 0.f;
+
+    // The plane loop is unrolled by NR so the z ring rotates by naming: plane zi lands in
+    // ring slot ph = (zi - zfirst) mod NR, and the window of plane zi - R is slots ph+1 ..
+    // ph+NR (mod NR) in ascending z.
+    for (int zi0 = zfirst; zi0 < zend; zi0 += NR) {
+#pragma unroll
+        for (int ph = 0; ph < NR; ++ph) {
+            const int zi = zi0 + ph;
+            if (zi >= zend) break;
+            const int slot = (zi - zfirst) & (NS - 1);
+            cp_wait<NS - 2>();
+            __syncthreads();             // plane zi landed for every thread; xs free again
+            {
+                const int zn = zi + NS - 1;
+                if (zn < zend) stage_plane<R, NF, VEC>(stage + ((zn - zfirst) & (NS - 1)) * G::STAGE, p, zn, x0, y0);
+                cp_commit();
+            }
+            const int zo = zi - R;
+            const bool emit = zo >= zs && zo < ze && gx < nx;
+            const size_t obase = (size_t)(emit ? zo : 0) * plane + (size_t)(y0 + 4 * rg) * nx + gx;
+            float gv[4] = {0.f, 0.f, 0.f, 0.f};
+            if (KIND == ZB_GUIDED_OUT && p.out_mode == 0 && emit) {   // issued early, used after the Y phase
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (y0 + 4 * rg + k < ny) gv[k] = __ldg(p.guide + obase + (size_t)k * nx);
+            }
+            const float* sp = stage + slot * G::STAGE;
+            const bool zin = zi >= 0 && zi < nz;
+            // X phase
+            for (int it = t; it < G::SY * (TX / 4); it += NT) {
+                const int yy = it >> 4, x4 = (it & 15) << 2;
+                const float* row = sp + yy * SXW + x4;
+                float q1[12], q2[12];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const float4 v = *reinterpret_cast<const float4*>(row + 4 * j);
+                    q1[4 * j] = v.x; q1[4 * j + 1] = v.y; q1[4 * j + 2] = v.z; q1[4 * j + 3] = v.w;
+                }
+                if (NF == 2) {
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        const float4 v = *reinterpret_cast<const float4*>(row + G::SY * SXW + 4 * j);
+                        q2[4 * j] = v.x; q2[4 * j + 1] = v.y; q2[4 * j + 2] = v.z; q2[4 * j + 3] = v.w;
+                    }
+                } else {
+                    const int gy = y0 - R + yy;
+                    const bool rin = zin && gy >= 0 && gy < ny;
+                    if (cols_in) {
+                        const float cs = rin ? c : 0.f;           // outside rows were staged as 0
+#pragma unroll
+                        for (int j = 4 - R; j < 8 + R; ++j) q1[j] = q1[j] - cs;
+                    } else {
+#pragma unroll
+                        for (int j = 4 - R; j < 8 + R; ++j) {
+                            const int gxj = x0 - 4 + x4 + j;
+                            q1[j] = (rin && gxj >= 0 && gxj < nx) ? q1[j] - c : 0.f;
+                        }
+                    }
+#pragma unroll
+                    for (int j = 4 - R; j < 8 + R; ++j) q2[j] = q1[j] * q1[j];
+                }
+                float o1[4], o2[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    float s1 = q1[4 + k - R], s2 = q2[4 + k - R];
+#pragma unroll
+                    for (int j = 5 + k - R; j <= 4 + k + R; ++j) { s1 += q1[j]; s2 += q2[j]; }
+                    if (KIND != ZB_NOISE) { const float f = rx[x4 + k]; s1 *= f; s2 *= f; }
+                    o1[k] = s1; o2[k] = s2;
+                }
+                *reinterpret_cast<float4*>(xs1 + yy * TX + x4) = make_float4(o1[0], o1[1], o1[2], o1[3]);
+                *reinterpret_cast<float4*>(xs2 + yy * TX + x4) = make_float4(o2[0], o2[1], o2[2], o2[3]);
+            }
+            __syncthreads();
+            // Y phase -> ring slot ph
+            {
+                float a1[4 + 2 * R], a2[4 + 2 * R];
+#pragma unroll
+                for (int j = 0; j < 4 + 2 * R; ++j) { a1[j] = xs1[(4 * rg + j) * TX + xc]; a2[j] = xs2[(4 * rg + j) * TX + xc]; }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    float s1 = a1[k], s2 = a2[k];
+#pragma unroll
+                    for (int j = 1; j <= 2 * R; ++j) { s1 += a1[k + j]; s2 += a2[k + j]; }
+                    if (KIND != ZB_NOISE) { const float f = ry[4 * rg + k]; s1 *= f; s2 *= f; }
+                    r1[ph][k] = s1; r2[ph][k] = s2;
+                }
+            }
+            if (!emit) continue;
+            const float rz = KIND == ZB_NOISE ? 0.f : recip_count(zo, nz, R);
+            const int cz = min(zo + R, nz - 1) - max(zo - R, 0) + 1;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (y0 + 4 * rg + k >= ny) continue;
+                float s1 = r1[(ph + 1) % NR][k], s2 = r2[(ph + 1) % NR][k];
+#pragma unroll
+                for (int q = 2; q <= NR; ++q) { s1 += r1[(ph + q) % NR][k]; s2 += r2[(ph + q) % NR][k]; }
+                const size_t o = obase + (size_t)k * nx;
+                if (KIND == ZB_NOISE) {
+                    const int nini = cz * cyx[k];
+                    const float nin = (float)nini;
+                    // raw sums: S1 = S1' + nin*c, S2 = S2' + 2c*S1' + nin*c^2
+                    const float m = (s1 + nin * c) * p.inv_wc;
+                    float v;
+                    if (nini == p.wci) {                           // interior: shifted, cancellation-free
+                        const float e1 = s1 * p.inv_wc;
+                        v = s2 * p.inv_wc - e1 * e1;
+                    } else {
+                        v = (s2 + 2.0f * c * s1 + nin * c * c) * p.inv_wc - m * m;
+                    }
+                    if (v < 0.f) v = 0.f;
+                    p.o0[o] = m;
+                    p.o1[o] = v;
+                } else if (KIND == ZB_GUIDED_AB) {
+                    const float e1 = s1 * rz, e2 = s2 * rz;        // E[I-c], E[(I-c)^2]
+                    float var = e2 - e1 * e1;
+                    if (var < 0.f) var = 0.f;
+                    const float mean = e1 + c;
+                    const float a = var / (var + eps);             // guided.c:129
+                    p.o0[o] = a;
+                    p.o1[o] = mean * (1.0f - a);                   // guided.c:131
+                } else {
+                    const float ma = s1 * rz, mb = s2 * rz;
+                    if (p.out_mode == 0) p.o0[o] = ma * gv[k] + mb;
+                    else { p.o0[o] = ma; p.o1[o] = mb; }
+                }
+            }
+        }
+    }
+    cp_wait<0>();
+}
+
+// Tiles and z chunks: ~6 CTAs per SM, chunks of >= 8R planes so the 2R-plane warm-up stays
+// a small fraction.
+inline dim3 grid_for(int nz, int ny, int nx, int r, int sms, int& zchunk) {
+    const int tx = (nx + TX - 1) / TX, ty = (ny + TY - 1) / TY;
+    const long txy = (long)tx * ty;
+    int nchunk = (int)((6L * sms + txy - 1) / txy);
+    const int min_chunk = 8 * r;
+    if (nchunk > nz / min_chunk) nchunk = nz / min_chunk;
+    if (nchunk < 1) nchunk = 1;
+    zchunk = (nz + nchunk - 1) / nchunk;
+    return dim3(tx, ty, (nz + zchunk - 1) / zchunk);
+}
+
+template <int KIND, int R, bool VEC>
+inline cudaError_t launch_r(const Params& p, dim3 grid, cudaStream_t st) {
+    constexpr int NF = KIND == ZB_GUIDED_OUT ? 2 : 1;
+    auto k = k_zbox<R, KIND, VEC>;
+    const size_t smem = Geo<R, NF>::bytes;
+    cudaError_t e = fy_smem_optin(k, smem);
+    if (e != cudaSuccess) return e;
+    k<<<grid, NT, smem, st>>>(p);
+    return cudaGetLastError();
+}
+
+// Enqueue one z-sliding box pass, radius r in [1, 4].
+template <int KIND>
+inline cudaError_t launch(Params p, int r, int sms, cudaStream_t st) {
+    const dim3 grid = grid_for(p.nz, p.ny, p.nx, r, sms, p.zchunk);
+    auto al = [](const void* q) { return ((uintptr_t)q & 15) == 0; };
+    const bool vec = p.nx % 4 == 0 && al(p.f0) && (KIND != ZB_GUIDED_OUT || al(p.f1));
+    switch (r * 2 + (vec ? 1 : 0)) {
+        case 2: return launch_r<KIND, 1, false>(p, grid, st);
+        case 3: return launch_r<KIND, 1, true>(p, grid, st);
+        case 4: return launch_r<KIND, 2, false>(p, grid, st);
+        case 5: return launch_r<KIND, 2, true>(p, grid, st);
+        case 6: return launch_r<KIND, 3, false>(p, grid, st);
+        case 7: return launch_r<KIND, 3, true>(p, grid, st);
+        case 8: return launch_r<KIND, 4, false>(p, grid, st);
+        case 9: return launch_r<KIND, 4, true>(p, grid, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace fyzb
