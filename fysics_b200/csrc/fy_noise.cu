@@ -25,7 +25,7 @@ constexpr int NT_MAX = 64;             // selection targets: 2 per bin + spare
 
 FY_D uint32_t fkey(float f) {
     const uint32_t u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return u ^ ((uint32_t)((int32_t)u >> 31) | 0x80000000u);   // negative: ~u, else u | sign
 }
 FY_HD float funkey(uint32_t k) {
 #ifdef __CUDA_ARCH__
@@ -89,115 +89,155 @@ FY_D int bin_of(float m, const float* __restrict__ fe, float lo_f, float scale) 
     return b;
 }
 
-// warp-aggregated shared-memory increment of h[code] (code < 0: nothing)
-FY_D void agg_inc(unsigned int* h, int code) {
-    const unsigned peers = __match_any_sync(0xffffffffu, code);
-    if (code >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[code], (unsigned)__popc(peers));
-}
+// Histogram increments with thread-local run merging: a thread's consecutive equal codes
+// are counted in a register and added with one shared atomic per run. Neighbouring voxels
+// mostly share intensity bins and high digits, so concentrated passes make few atomics,
+// and spread-out passes pay only bank conflicts; no warp collectives are needed.
+struct RunAcc {
+    int cur = -1;
+    unsigned int cnt = 0;
+    FY_D void add(unsigned int* h, int code) {
+        if (code != cur) {
+            if (cur >= 0) atomicAdd(&h[cur], cnt);
+            cur = code;
+            cnt = 0;
+        }
+        ++cnt;
+    }
+    FY_D void flush(unsigned int* h) {
+        if (cur >= 0) atomicAdd(&h[cur], cnt);
+        cur = -1;
+        cnt = 0;
+    }
+};
 
-// u8 bin id per voxel (255 = no bin) and per-bin counts
+// Streaming passes read SU float4 (and uchar4 bin labels) per thread before using any, so
+// enough bytes are in flight per SM to cover HBM latency. Full chunks of the grid-stride
+// loop run without per-element range checks; the one partial chunk is checked.
+constexpr int SU = 4;
+
+// u8 bin id per voxel (255 = no bin). Per-bin counts come from the first variance digit
+// pass, whose histogram covers every voxel of every bin (k_bin_targets).
 __global__ void __launch_bounds__(256) k_bin_assign(const float* __restrict__ mean, uint8_t* __restrict__ bin,
                                                     NoiseCtl* __restrict__ ctl) {
-    __shared__ unsigned int cnt[NB];
     __shared__ float fe[NB + 1];
-    if (threadIdx.x < NB) cnt[threadIdx.x] = 0;
     if (threadIdx.x <= NB) fe[threadIdx.x] = ctl->fedge[threadIdx.x];
     __syncthreads();
     const float lo_f = ctl->fedge[0], scale = ctl->fscale;
-    const long long n = ctl->n, n4 = (n + 3) / 4;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long base = (long long)blockIdx.x * blockDim.x; base < n4; base += stride) {
-        const long long q = base + threadIdx.x;
-        int b4[4] = {-1, -1, -1, -1};
-        if (q < n4) {
-            if (4 * q + 3 < n) {
-                const float4 m = __ldg(reinterpret_cast<const float4*>(mean) + q);
-                b4[0] = bin_of(m.x, fe, lo_f, scale); b4[1] = bin_of(m.y, fe, lo_f, scale);
-                b4[2] = bin_of(m.z, fe, lo_f, scale); b4[3] = bin_of(m.w, fe, lo_f, scale);
-                *reinterpret_cast<uchar4*>(bin + 4 * q) =
-                    make_uchar4(b4[0] < 0 ? 255 : b4[0], b4[1] < 0 ? 255 : b4[1], b4[2] < 0 ? 255 : b4[2],
-                                b4[3] < 0 ? 255 : b4[3]);
-            } else {
-                for (int j = 0; j < 4 && 4 * q + j < n; ++j) {
-                    b4[j] = bin_of(mean[4 * q + j], fe, lo_f, scale);
-                    bin[4 * q + j] = b4[j] < 0 ? 255 : (uint8_t)b4[j];
-                }
-            }
-        }
+    const long long n = ctl->n, n4 = (n + 3) / 4, n4f = n / 4;
+    const int step = blockDim.x;
+    const long long chunk = (long long)SU * step;
+    auto lab = [&](float m) -> unsigned { const int b = bin_of(m, fe, lo_f, scale); return b < 0 ? 255u : (unsigned)b; };
+    long long base = (long long)blockIdx.x * chunk;
+    for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
+        float4 x[SU];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) agg_inc(cnt, b4[j]);
+        for (int u = 0; u < SU; ++u) x[u] = __ldg(reinterpret_cast<const float4*>(mean) + base + threadIdx.x + (long long)u * step);
+#pragma unroll
+        for (int u = 0; u < SU; ++u)
+            reinterpret_cast<uchar4*>(bin)[base + threadIdx.x + (long long)u * step] =
+                make_uchar4(lab(x[u].x), lab(x[u].y), lab(x[u].z), lab(x[u].w));
     }
-    __syncthreads();
-    if (threadIdx.x < NB && cnt[threadIdx.x]) atomicAdd(&ctl->bcount[threadIdx.x], (unsigned long long)cnt[threadIdx.x]);
+    if (base < n4) {                                     // the grid's partial chunk
+        for (int u = 0; u < SU; ++u)
+            for (int j = 0; j < 4; ++j) {
+                const long long i = 4 * (base + threadIdx.x + (long long)u * step) + j;
+                if (i < n) bin[i] = (uint8_t)lab(__ldg(mean + i));
+            }
+    }
 }
 
 // One digit pass (bits [shift, shift + DB)) for every active target whose prefix matches.
-// mode 0: keys of mean, targets 0 and 1 over all voxels; mode 1: keys of var, target = bin;
-// mode 2: keys of var, target 0 over all voxels.
-template <int DB>
+// MODE 0: keys of mean, targets 0 and 1 over all voxels; MODE 1: keys of var, target = bin;
+// MODE 2: keys of var, target 0 over all voxels. A key matches at most one distinct prefix,
+// so in modes 0/2 targets whose prefixes are equal share one shared-memory histogram
+// (group) and every voxel makes at most one increment; the flush copies a group's counts
+// to each of its targets. Inactive targets and bin label 255 carry the prefix 0xffffffff,
+// which no key's high part (< 2^(32 - shift - DB)) can equal.
+template <int DB, int MODE>
 __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean, const float* __restrict__ var,
                                                   const uint8_t* __restrict__ bin, NoiseCtl* __restrict__ ctl,
-                                                  int shift, int want_mode) {
+                                                  int shift) {
     extern __shared__ unsigned int h[];
-    __shared__ uint32_t sp[NT_MAX];
-    __shared__ int sa[NT_MAX];
-    if (ctl->mode != want_mode) return;
+    __shared__ uint32_t sp[256];
+    if (ctl->mode != MODE) return;
     constexpr int NBK = 1 << DB;
     const int nt = ctl->ntarget;
-    for (int i = threadIdx.x; i < nt * NBK; i += blockDim.x) h[i] = 0;
-    for (int i = threadIdx.x; i < nt; i += blockDim.x) { sp[i] = ctl->tprefix[i]; sa[i] = ctl->tactive[i]; }
-    __syncthreads();
-    const int top = shift + DB;
-    const long long n = ctl->n, n4 = (n + 3) / 4;
-    const float* src = want_mode == 0 ? mean : var;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long base = (long long)blockIdx.x * blockDim.x; base < n4; base += stride) {
-        const long long q = base + threadIdx.x;
-        float v[4] = {0.f, 0.f, 0.f, 0.f};
-        int g[4] = {-1, -1, -1, -1};
-        if (q < n4) {
-            if (4 * q + 3 < n) {
-                const float4 x = __ldg(reinterpret_cast<const float4*>(src) + q);
-                v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
-                if (want_mode == 1) {
-                    const uchar4 bb = __ldg(reinterpret_cast<const uchar4*>(bin) + q);
-                    g[0] = bb.x; g[1] = bb.y; g[2] = bb.z; g[3] = bb.w;
-                } else {
-                    g[0] = g[1] = g[2] = g[3] = 0;
-                }
-            } else {
-                for (int j = 0; j < 4 && 4 * q + j < n; ++j) {
-                    v[j] = src[4 * q + j];
-                    g[j] = want_mode == 1 ? bin[4 * q + j] : 0;
-                }
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const uint32_t key = fkey(v[j]);
-            const uint32_t hb = top >= 32 ? 0u : (key >> top);
-            const int dig = (key >> shift) & (NBK - 1);
-            if (want_mode == 1) {
-                const int t = g[j];
-                const bool hit = t >= 0 && t < NB && sa[t] && sp[t] == hb;
-                agg_inc(h, hit ? t * NBK + dig : -1);
-            } else {
-                for (int t = 0; t < nt; ++t) {
-                    const bool hit = g[j] == 0 && sa[t] && sp[t] == hb;
-                    agg_inc(h, hit ? t * NBK + dig : -1);
-                }
-            }
+    if (MODE == 1)
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) sp[i] = i < nt && ctl->tactive[i] ? ctl->tprefix[i] : 0xffffffffu;
+    // modes 0/2: at most two targets; group of target 1 is 0 when it shares target 0's prefix
+    uint32_t p0 = 0xffffffffu, p1 = 0xffffffffu;
+    int g1 = 1;
+    if (MODE != 1) {
+        p0 = ctl->tactive[0] ? ctl->tprefix[0] : 0xffffffffu;
+        if (nt > 1 && ctl->tactive[1]) {
+            p1 = ctl->tprefix[1];
+            if (p1 == p0) { g1 = 0; p1 = 0xfffffffeu; }   // never matches: target 1 reads group 0
         }
     }
+    const int ngroup = MODE == 1 ? nt : 2;
+    for (int i = threadIdx.x; i < ngroup * NBK; i += blockDim.x) h[i] = 0;
     __syncthreads();
-    for (int i = threadIdx.x; i < nt * NBK; i += blockDim.x)
-        if (h[i]) atomicAdd(&ctl->hist[i], h[i]);
+    const int top = shift + DB;
+    const long long n = ctl->n, n4 = (n + 3) / 4, n4f = n / 4;
+    const float* src = MODE == 0 ? mean : var;
+    const int step = blockDim.x;
+    const long long chunk = (long long)SU * step;
+    RunAcc acc;
+    auto code_of = [&](float v, int g) -> int {
+        const uint32_t key = fkey(v);
+        const uint32_t hb = top >= 32 ? 0u : (key >> top);
+        const int dig = (key >> shift) & (NBK - 1);
+        if (MODE == 1) return sp[g] == hb ? g * NBK + dig : -1;
+        return hb == p0 ? dig : (hb == p1 ? NBK + dig : -1);
+    };
+    long long base = (long long)blockIdx.x * chunk;
+    for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
+        float4 x[SU];
+        uchar4 bb[SU];
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            const long long q = base + threadIdx.x + (long long)u * step;
+            x[u] = __ldg(reinterpret_cast<const float4*>(src) + q);
+            if (MODE == 1) bb[u] = __ldg(reinterpret_cast<const uchar4*>(bin) + q);
+        }
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            acc.add(h, code_of(x[u].x, MODE == 1 ? bb[u].x : 0));
+            acc.add(h, code_of(x[u].y, MODE == 1 ? bb[u].y : 0));
+            acc.add(h, code_of(x[u].z, MODE == 1 ? bb[u].z : 0));
+            acc.add(h, code_of(x[u].w, MODE == 1 ? bb[u].w : 0));
+        }
+    }
+    if (base < n4) {                                     // the grid's partial chunk
+        for (int u = 0; u < SU; ++u)
+            for (int j = 0; j < 4; ++j) {
+                const long long i = 4 * (base + threadIdx.x + (long long)u * step) + j;
+                if (i < n) acc.add(h, code_of(__ldg(src + i), MODE == 1 ? (int)__ldg(bin + i) : 0));
+            }
+    }
+    acc.flush(h);
+    __syncthreads();
+    if (MODE == 1) {
+        for (int i = threadIdx.x; i < nt * NBK; i += blockDim.x)
+            if (h[i]) atomicAdd(&ctl->hist[i], h[i]);
+    } else {
+        for (int i = threadIdx.x; i < nt * NBK; i += blockDim.x) {
+            const int t = i / NBK, grp = t == 0 ? 0 : g1;
+            const unsigned int cnt = h[grp * NBK + (i - t * NBK)];
+            if (cnt) atomicAdd(&ctl->hist[i], cnt);
+        }
+    }
 }
 
 // After a digit pass: target t (one block) finds the bucket holding its rank by a block
 // scan of the histogram, extends its prefix, records how many keys share the final key.
+// After the last digit, the next non-empty bucket of that digit is the smallest key above
+// the selected one within the prefix; k_sel_next scans only when there is none.
 __global__ void __launch_bounds__(256) k_sel_scan(NoiseCtl* __restrict__ ctl, int db, int want_mode, int last) {
     __shared__ unsigned long long part[256];
+    __shared__ int s_sel;
+    __shared__ unsigned int s_nextb;
     if (ctl->mode != want_mode) return;
     const int t = blockIdx.x;
     if (t >= ctl->ntarget || !ctl->tactive[t]) return;
@@ -207,6 +247,7 @@ __global__ void __launch_bounds__(256) k_sel_scan(NoiseCtl* __restrict__ ctl, in
     unsigned long long mine = 0;
     for (int b = b0; b < b0 + per && b < nbk; ++b) mine += h[b];
     part[threadIdx.x] = mine;
+    if (threadIdx.x == 0) { s_sel = nbk; s_nextb = 0xffffffffu; }
     __syncthreads();
     for (int off = 1; off < 256; off <<= 1) {                // inclusive scan
         const unsigned long long add = threadIdx.x >= off ? part[threadIdx.x - off] : 0ull;
@@ -223,20 +264,28 @@ __global__ void __launch_bounds__(256) k_sel_scan(NoiseCtl* __restrict__ ctl, in
                 ctl->trank[t] = r - (long long)acc;
                 ctl->tprefix[t] = (ctl->tprefix[t] << db) | (uint32_t)b;
                 if (last) ctl->teq[t] = h[b];
+                s_sel = b;
                 break;
             }
             acc += h[b];
         }
     }
     __syncthreads();
+    if (last) {
+        const int sel = s_sel;
+        for (int b = b0 > sel + 1 ? b0 : sel + 1; b < b0 + per && b < nbk; ++b)
+            if (h[b]) { atomicMin(&s_nextb, (unsigned)b); break; }
+    }
+    __syncthreads();
     for (int i = threadIdx.x; i < nbk; i += blockDim.x) h[i] = 0;
     if (last && threadIdx.x == 0) {
         ctl->tneed_next[t] = (ctl->trank[t] + 1 >= (long long)ctl->teq[t]) && (ctl->tk[t] + 1 < ctl->tgroup_n[t]);
-        ctl->tnext[t] = 0xffffffffu;
+        ctl->tnext[t] = s_nextb != 0xffffffffu ? ((ctl->tprefix[t] >> db) << db) | s_nextb : 0xffffffffu;
     }
 }
 
-// Smallest key greater than the selected key, for targets whose k+1 lies past it.
+// Smallest key greater than the selected key, for targets whose k+1 lies past it and whose
+// last digit histogram held no larger key (k_sel_scan resolves every other target).
 __global__ void __launch_bounds__(256) k_sel_next(const float* __restrict__ mean, const float* __restrict__ var,
                                                   const uint8_t* __restrict__ bin, NoiseCtl* __restrict__ ctl,
                                                   int want_mode) {
@@ -250,7 +299,7 @@ __global__ void __launch_bounds__(256) k_sel_next(const float* __restrict__ mean
     __syncthreads();
     for (int i = threadIdx.x; i < nt; i += blockDim.x) {
         sp[i] = ctl->tprefix[i];
-        sn[i] = ctl->tactive[i] && ctl->tneed_next[i];
+        sn[i] = ctl->tactive[i] && ctl->tneed_next[i] && ctl->tnext[i] == 0xffffffffu;
         smin[i] = 0xffffffffu;
         if (sn[i]) s_any = 1;
     }
@@ -258,21 +307,14 @@ __global__ void __launch_bounds__(256) k_sel_next(const float* __restrict__ mean
     if (!s_any) return;
     const long long n = ctl->n;
     const float* src = want_mode == 0 ? mean : var;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
-        const long long i = base + threadIdx.x;
-        uint32_t key = 0xffffffffu;
-        int g = -1;
-        if (i < n) {
-            key = fkey(__ldg(src + i));
-            g = want_mode == 1 ? (int)__ldg(bin + i) : 0;
-        }
-        for (int t = 0; t < nt; ++t) {
-            const bool mine = want_mode == 1 ? (g == t) : (g == 0);
-            const uint32_t cand = (mine && sn[t] && key > sp[t]) ? key : 0xffffffffu;
-            const uint32_t m = __reduce_min_sync(0xffffffffu, cand);
-            if ((threadIdx.x & 31) == 0 && m != 0xffffffffu) atomicMin(&smin[t], m);
-            if (want_mode == 1) {}   // every lane loops over all targets (warp-uniform)
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const uint32_t key = fkey(__ldg(src + i));
+        if (want_mode == 1) {            // one target per voxel: its bin
+            const int g = __ldg(bin + i);
+            if (g < NB && g < nt && sn[g] && key > sp[g] && key < smin[g]) atomicMin(&smin[g], key);
+        } else {
+            for (int t = 0; t < nt; ++t)
+                if (sn[t] && key > sp[t] && key < smin[t]) atomicMin(&smin[t], key);
         }
     }
     __syncthreads();
@@ -332,15 +374,32 @@ __global__ void k_noise_bins_setup(NoiseCtl* ctl) {
         ctl->fedge[k] = f;
     }
     ctl->fscale = (float)(NB / (hi - lo));
+    // first variance digit pass: every bin active with the empty prefix (its histogram
+    // gives the bin counts; k_bin_targets then sets the ranks)
+    for (int t = 0; t < NT_MAX; ++t) target_init(ctl, t, 0, 0, t < NB);
+    ctl->ntarget = NB;
     ctl->mode = 1;
 }
 
-// per-bin targets of the flat_pct percentile, bins with >= 200 voxels (noise.c:123)
-__global__ void k_bin_targets(NoiseCtl* ctl) {
-    ctl->ntarget = NB;
-    for (int b = 0; b < NB; ++b) {
-        const long long c = (long long)ctl->bcount[b];
-        const bool on = c >= 200;
+// After the first variance digit pass (one block per bin): the bin's count is the sum of its
+// histogram; targets of the flat_pct percentile for bins with >= 200 voxels (noise.c:123).
+// Bins below that drop out and their histogram is cleared.
+__global__ void __launch_bounds__(256) k_bin_targets(NoiseCtl* ctl) {
+    __shared__ unsigned long long part[256];
+    if (ctl->mode != 1) return;
+    const int b = blockIdx.x;
+    unsigned int* h = ctl->hist + (size_t)b * 256;
+    part[threadIdx.x] = h[threadIdx.x];
+    __syncthreads();
+    for (int off = 128; off > 0; off >>= 1) {
+        if (threadIdx.x < off) part[threadIdx.x] += part[threadIdx.x + off];
+        __syncthreads();
+    }
+    const long long c = (long long)part[0];
+    const bool on = c >= 200;
+    if (!on) h[threadIdx.x] = 0;
+    if (threadIdx.x == 0) {
+        ctl->bcount[b] = (unsigned long long)c;
         const double idx = ctl->flat_pct / 100.0 * (double)(c - 1);
         target_init(ctl, b, on ? (long long)idx : 0, c, on);
     }
@@ -445,7 +504,7 @@ __global__ void k_noise_fit(NoiseCtl* ctl, int stage) {
 }
 
 unsigned grid_sel(long long n, int sms) {
-    long long g = (n / 4 + 255) / 256;
+    long long g = (n / 4 + 256 * SU - 1) / (256 * SU);
     const long long cap = (long long)sms * 8;
     return (unsigned)(g < cap ? (g ? g : 1) : cap);
 }
@@ -491,18 +550,19 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     // 2a. 1st/99th percentile of the means: 11 + 11 + 10 bits, then the k+1 neighbours
     const int all_digits[3][2] = {{21, 11}, {10, 11}, {0, 10}};
     for (int i = 0; i < 3; ++i) {
-        if (all_digits[i][1] == 11) k_sel_hist<11><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0], 0);
-        else k_sel_hist<10><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0], 0);
+        if (all_digits[i][1] == 11) k_sel_hist<11, 0><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0]);
+        else k_sel_hist<10, 0><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0]);
         k_sel_scan<<<2, 256, 0, st>>>(ctl, all_digits[i][1], 0, i == 2);
     }
     k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 0);
     k_noise_bins_setup<<<1, 1, 0, st>>>(ctl);
     k_bin_assign<<<g, 256, 0, st>>>(mean, bin, ctl);
-    k_bin_targets<<<1, 1, 0, st>>>(ctl);
     fy_prof_mark(st, "noise.lohi+bins");
-    // 2b. per-bin flat_pct percentile of the variance: 4 x 8 bits, then the k+1 neighbours
+    // 2b. per-bin flat_pct percentile of the variance: 4 x 8 bits, then the k+1 neighbours;
+    // the first pass also yields the bin counts
     for (int sh = 24; sh >= 0; sh -= 8) {
-        k_sel_hist<8><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, sh, 1);
+        k_sel_hist<8, 1><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, sh);
+        if (sh == 24) k_bin_targets<<<NB, 256, 0, st>>>(ctl);
         k_sel_scan<<<NB, 256, 0, st>>>(ctl, 8, 1, sh == 0);
     }
     k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 1);
@@ -510,8 +570,8 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     fy_prof_mark(st, "noise.bin_select");
     // 2c. fallback (mode 2 only): flat_pct percentile over all voxels' variance
     for (int i = 0; i < 3; ++i) {
-        if (all_digits[i][1] == 11) k_sel_hist<11><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0], 2);
-        else k_sel_hist<10><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0], 2);
+        if (all_digits[i][1] == 11) k_sel_hist<11, 2><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0]);
+        else k_sel_hist<10, 2><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0]);
         k_sel_scan<<<1, 256, 0, st>>>(ctl, all_digits[i][1], 2, i == 2);
     }
     k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 2);
