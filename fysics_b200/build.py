@@ -71,7 +71,7 @@ def build(force: bool = False, ptxas_v: bool = False, verbose: bool = False) -> 
                 print(f"--- {s.name}\n{log}", file=sys.stderr)
     objs = [str(o) for o, _ in results]
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-Xlinker", "-Bsymbolic",
+    cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-Xlinker", "-Bsymbolic", "-Xlinker", "--no-undefined",
            "-cudart", "static", "-o", str(tmp), *objs, "-lpthread", "-ldl", "-lrt"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

@@ -1,0 +1,365 @@
+#pragma once
+// fy_deconv.cuh -- fused half-spectrum Wiener deconvolution (fy_deconvolve /
+// fy_deconvolve_matched, paganin.c:152-342) as five HBM passes:
+//
+//   P1 X  : gather rows (u8 dewindow or f32) with reflect padding in x, two rows per
+//           complex FFT, untangle -> half-spectrum rows         (paganin.c:165-194)
+//   P2 Y  : forward over py for each stored z plane, reflect/zero rows gathered on load
+//   P3 Z  : forward over pz (reflected planes gathered on load), radial weight from the
+//           4096-entry LUT over u = f^2 with linear interpolation (paganin.c:212-244),
+//           inverse over pz, store only the z < nz planes that survive the crop
+//   P4 Y  : inverse for z < nz, store only rows y < ny          (paganin.c:254-260)
+//   P5 X  : two-for-one C2R of surviving rows, x 1/(pz*py*px), crop (paganin.c:262-289)
+//
+// Algorithmic traffic at p = n (no padding): P1 4+4 (1+4 from u8), P2 8, P3 8, P4 8,
+// P5 4+4 bytes per voxel.
+//
+// Kernels take N > 0 for a compile-time FFT plan of length N on their axis (instantiated
+// for the common padded sizes in fy_deconv_ct_*.cu, compiled in parallel), or N = 0 for the
+// runtime plan (fy_deconv.cu). fy_deconv_pass<N> enqueues one of the five passes.
+#include "fy_internal.h"
+
+namespace {
+// Line transform with a compile-time plan when N > 0 (n == N, pitch PS), else the
+// runtime plan `pl` with pitch ps.
+constexpr int ct_pitch(int n) { return n > 0 ? ct_tile_lines(n) : 0; }
+constexpr int ct_e(int n) { return n % 3 == 0 ? (n >= 24 ? 24 : n) : (n >= 16 ? 16 : n); }
+template <int N, int E, int PS, int SIGN, class LD, class ST>
+FY_D void fft_line(float2* __restrict__ sline, int ps, int tl, const FftPlan& pl, const float2* __restrict__ tw,
+                   LD ld, ST st) {
+    if constexpr (N > 0) line_fft_ct<N, E, PS, SIGN>(sline, tl, tw, ld, st);
+    else line_fft<E>(sline, ps, tl, pl, tw, (float)SIGN, ld, st);
+}
+// Threads per CTA never exceed W*n/E: 512 for 2^k lines (E=16), 256 for 3*2^k (E=24).
+template <int E> struct KB { static constexpr int nt = (E % 3 == 0) ? 256 : 512; };
+
+
+// Thread -> (line l, thread-in-line tl) with the line index fastest.
+struct Lane {
+    int l, tl;
+    FY_D Lane(int wlog) : l(threadIdx.x & ((1 << wlog) - 1)), tl(threadIdx.x >> wlog) {}
+};
+
+// ---------------------------------------------------------------- P1
+// Rows q = z*ny + y (z < nz, y < ny) paired (2m, 2m+1) into one complex line; a CTA owns W
+// lines, staged line-major in shared memory (pitch px+1, odd: conflict-free for the FFT's
+// line-strided accesses). Each thread loads the same VEC-wide chunk of both rows of a line
+// pair, so it writes VEC consecutive complex values; reflect padding is filled from the
+// staged line afterwards.
+template <class T, int VEC> struct VecLoad;
+template <> struct VecLoad<float, 4> {
+    static FY_D void run(const float* p, float* v) {
+        const float4 x = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    }
+};
+template <> struct VecLoad<uint8_t, 4> {
+    static FY_D void run(const uint8_t* p, float* v) {
+        const uchar4 x = __ldg(reinterpret_cast<const uchar4*>(p));
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    }
+};
+template <class T> struct VecLoad<T, 1> {
+    static FY_D void run(const T* p, float* v) { v[0] = (float)__ldg(p); }
+};
+
+template <int N, int E, class T, int VEC>
+__global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(const T* __restrict__ src, float lo, float scale, int is_u8,
+                                                        float2* __restrict__ spec, SpecGeom g,
+                                                        const __grid_constant__ FftPlan pl,
+                                                        const float2* __restrict__ tw, int wlog, FastDiv dchunk,
+                                                        FastDiv dhx, FastDiv dpad) {
+    extern __shared__ float4 smem4[];
+    const int W = 1 << wlog, LPX = g.px + 1;
+    float2* s = reinterpret_cast<float2*>(smem4);
+    float2* stw = s + W * LPX;
+    const long Q = (long)g.nz * g.ny;
+    const long q0 = (long)blockIdx.x * 2 * W;
+    load_twiddles(stw, tw, pl.n);
+    const int nch = g.nx / VEC;
+    for (int it = threadIdx.x; it < W * nch; it += blockDim.x) {
+        const int l = dchunk.div(it), x = (it - l * nch) * VEC;
+        const long qa = q0 + 2 * l, qb = qa + 1;
+        float va[VEC], vb[VEC];
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) va[j] = vb[j] = 0.f;
+        if (qa < Q) VecLoad<T, VEC>::run(src + qa * g.nx + x, va);
+        if (qb < Q) VecLoad<T, VEC>::run(src + qb * g.nx + x, vb);
+        float2* dst = s + l * LPX + x;
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            float a = va[j], b = vb[j];
+            if (is_u8) {                                   // fy_u8_to_phys, FMA as the reference build
+                a = qa < Q ? __fmaf_rn(a, scale, lo) : 0.f;
+                b = qb < Q ? __fmaf_rn(b, scale, lo) : 0.f;
+            }
+            dst[j] = make_float2(a, b);
+        }
+    }
+    const int npad = g.px - g.nx;
+    if (npad > 0) {
+        __syncthreads();
+        for (int it = threadIdx.x; it < W * npad; it += blockDim.x) {
+            const int l = dpad.div(it), x = g.nx + (it - l * npad);
+            s[l * LPX + x] = g.zero_pad ? make_float2(0.f, 0.f) : s[l * LPX + reflect_idx(x, g.nx)];
+        }
+    }
+    __syncthreads();
+    const Lane ln(wlog);
+    float2* line = s + ln.l * LPX;
+    fft_line<N, E, 1, -1>(line, 1, ln.tl, pl, stw,
+                [&](int i) { return line[i]; },
+                [&](int i, float2 v) { line[i] = v; });
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < W * g.hx; idx += blockDim.x) {
+        const int l = dhx.div(idx), k = idx - l * g.hx;
+        const long qa = q0 + 2 * l, qb = qa + 1;
+        if (qa >= Q) continue;
+        const int mk = k == 0 ? 0 : g.px - k;
+        float2 A, B;
+        untangle(s[l * LPX + k], s[l * LPX + mk], A, B);
+        spec[((size_t)(qa / g.ny) * g.py + (qa % g.ny)) * g.hxp + k] = A;
+        if (qb < Q) spec[((size_t)(qb / g.ny) * g.py + (qb % g.ny)) * g.hxp + k] = B;
+    }
+}
+
+// ---------------------------------------------------------------- P2
+// CTA = (column tile of W half-spectrum columns, stored plane z). Pass-0 inputs come
+// straight from global memory (W consecutive columns = one 8W-byte run per point);
+// rows >= ny are the reflected (or zero) rows.
+template <int N, int E>
+__global__ void __launch_bounds__(KB<E>::nt, 2) k_y_fwd(float2* __restrict__ spec, SpecGeom g, const __grid_constant__ FftPlan pl,
+                                                 const float2* __restrict__ tw, int wlog) {
+    extern __shared__ float4 smem4[];
+    const int W = 1 << wlog;
+    float2* s = reinterpret_cast<float2*>(smem4);
+    float2* stw = s + pl.n * W;
+    const Lane ln(wlog);
+    float2* col = spec + (size_t)blockIdx.y * g.py * g.hxp + blockIdx.x * W + ln.l;
+    load_twiddles(stw, tw, pl.n);
+    __syncthreads();
+    fft_line<N, E, ct_pitch(N), -1>(s + ln.l, W, ln.tl, pl, stw,
+                [&](int i) {
+                    const int ys = i < g.ny ? i : (g.zero_pad ? -1 : reflect_idx(i, g.ny));
+                    return ys < 0 ? make_float2(0.f, 0.f) : col[(size_t)ys * g.hxp];
+                },
+                [&](int i, float2 v) { col[(size_t)i * g.hxp] = v; });
+}
+
+// ---------------------------------------------------------------- P3
+// CTA = (column tile, row y). Forward over z (reflected planes gathered on load), radial
+// LUT weight over the tile in shared memory, inverse over z, store z < nz.
+template <int N, int E>
+__global__ void __launch_bounds__(KB<E>::nt, 2) k_z_weight(float2* __restrict__ spec, SpecGeom g,
+                                                       const __grid_constant__ FftPlan pl,
+                                                       const float2* __restrict__ tw,
+                                                       const float* __restrict__ lut,
+                                                       const double* __restrict__ fz2,
+                                                       const double* __restrict__ fy2,
+                                                       const double* __restrict__ fx2, double us, int wlog) {
+    extern __shared__ float4 smem4[];
+    const int W = 1 << wlog;
+    float2* s = reinterpret_cast<float2*>(smem4);
+    float2* stw = s + pl.n * W;
+    double* sfz = reinterpret_cast<double*>(stw + pl.n);
+    float* slut = reinterpret_cast<float*>(sfz + pl.n);
+    const Lane ln(wlog);
+    const int c0 = blockIdx.x * W;
+    const size_t zstride = (size_t)g.py * g.hxp;
+    float2* col = spec + (size_t)blockIdx.y * g.hxp + c0 + ln.l;
+    load_twiddles(stw, tw, pl.n);
+    for (int i = threadIdx.x; i < pl.n; i += blockDim.x) sfz[i] = fz2[i];
+    for (int i = threadIdx.x; i <= FY_LUT_N; i += blockDim.x) slut[i] = lut[i];
+    __syncthreads();
+    fft_line<N, E, ct_pitch(N), -1>(s + ln.l, W, ln.tl, pl, stw,
+                [&](int i) {
+                    const int zs = i < g.nz ? i : (g.zero_pad ? -1 : reflect_idx(i, g.nz));
+                    return zs < 0 ? make_float2(0.f, 0.f) : col[(size_t)zs * zstride];
+                },
+                [&](int z, float2 v) { s[z * W + ln.l] = v; });
+    __syncthreads();
+    {   // weight: the same W-column slot for every element this thread touches
+        const int k = c0 + ln.l;
+        const double fyx = k < g.hx ? fy2[blockIdx.y] : 0.0;
+        const double fxx = k < g.hx ? __ldg(fx2 + k) : 0.0;
+        for (int z = ln.tl; z < pl.n; z += blockDim.x >> wlog) {
+            const double t = ((sfz[z] + fyx) + fxx) * us;    // paganin.c:234-236
+            int ti = (int)t;
+            if (ti >= FY_LUT_N) ti = FY_LUT_N - 1;
+            const float w = slut[ti] + (slut[ti + 1] - slut[ti]) * (float)(t - ti);
+            const float2 v = s[z * W + ln.l];
+            s[z * W + ln.l] = make_float2(v.x * w, v.y * w);
+        }
+    }
+    __syncthreads();
+    fft_line<N, E, ct_pitch(N), +1>(s + ln.l, W, ln.tl, pl, stw,
+                [&](int i) { return s[i * W + ln.l]; },
+                [&](int z, float2 v) { if (z < g.nz) col[(size_t)z * zstride] = v; });
+}
+
+// ---------------------------------------------------------------- P4
+template <int N, int E>
+__global__ void __launch_bounds__(KB<E>::nt, 2) k_y_inv(float2* __restrict__ spec, SpecGeom g, const __grid_constant__ FftPlan pl,
+                                                 const float2* __restrict__ tw, int keep_rows, int wlog) {
+    extern __shared__ float4 smem4[];
+    const int W = 1 << wlog;
+    float2* s = reinterpret_cast<float2*>(smem4);
+    float2* stw = s + pl.n * W;
+    const Lane ln(wlog);
+    float2* col = spec + (size_t)blockIdx.y * g.py * g.hxp + blockIdx.x * W + ln.l;
+    load_twiddles(stw, tw, pl.n);
+    __syncthreads();
+    fft_line<N, E, ct_pitch(N), +1>(s + ln.l, W, ln.tl, pl, stw,
+                [&](int i) { return col[(size_t)i * g.hxp]; },
+                [&](int i, float2 v) { if (i < keep_rows) col[(size_t)i * g.hxp] = v; });
+}
+
+// ---------------------------------------------------------------- P5
+// Line-major like P1; the two output rows of a line are written VEC floats at a time.
+template <int N, int E, int VEC>
+__global__ void __launch_bounds__(KB<E>::nt, 2) k_x_inv(const float2* __restrict__ spec, float* __restrict__ dst,
+                                                        SpecGeom g, const __grid_constant__ FftPlan pl,
+                                                        const float2* __restrict__ tw, float invN, int wlog,
+                                                        FastDiv dchunk, FastDiv dhx) {
+    extern __shared__ float4 smem4[];
+    const int W = 1 << wlog, LPX = g.px + 1;
+    float2* s = reinterpret_cast<float2*>(smem4);
+    float2* stw = s + W * LPX;
+    const long Q = (long)g.nz * g.ny;
+    const long q0 = (long)blockIdx.x * 2 * W;
+    load_twiddles(stw, tw, pl.n);
+    const int hi_max = g.px - g.hx;                 // m in [1, px-hx] mirrors to px-m
+    for (int idx = threadIdx.x; idx < W * g.hx; idx += blockDim.x) {
+        const int l = dhx.div(idx), k = idx - l * g.hx;
+        const long qa = q0 + 2 * l, qb = qa + 1;
+        const float2 A = qa < Q ? spec[((size_t)(qa / g.ny) * g.py + (qa % g.ny)) * g.hxp + k] : make_float2(0.f, 0.f);
+        const float2 B = qb < Q ? spec[((size_t)(qb / g.ny) * g.py + (qb % g.ny)) * g.hxp + k] : make_float2(0.f, 0.f);
+        s[l * LPX + k] = pack_lo(A, B);
+        if (k >= 1 && k <= hi_max) s[l * LPX + g.px - k] = pack_hi(A, B);
+    }
+    __syncthreads();
+    const Lane ln(wlog);
+    float2* line = s + ln.l * LPX;
+    fft_line<N, E, 1, +1>(line, 1, ln.tl, pl, stw,
+                [&](int i) { return line[i]; },
+                [&](int i, float2 v) { line[i] = v; });
+    __syncthreads();
+    const int nch = g.nx / VEC;
+    for (int it = threadIdx.x; it < W * nch; it += blockDim.x) {
+        const int l = dchunk.div(it), x = (it - l * nch) * VEC;
+        const long qa = q0 + 2 * l, qb = qa + 1;
+        if (qa >= Q) continue;
+        const float2* v = s + l * LPX + x;
+        if (VEC == 4) {
+            *reinterpret_cast<float4*>(dst + qa * g.nx + x) =
+                make_float4(v[0].x * invN, v[1].x * invN, v[2].x * invN, v[3].x * invN);
+            if (qb < Q)
+                *reinterpret_cast<float4*>(dst + qb * g.nx + x) =
+                    make_float4(v[0].y * invN, v[1].y * invN, v[2].y * invN, v[3].y * invN);
+        } else {
+            dst[qa * g.nx + x] = v[0].x * invN;
+            if (qb < Q) dst[qb * g.nx + x] = v[0].y * invN;
+        }
+    }
+}
+
+
+// Enqueue pass `pass` (1..5) with the compile-time plan of length N (N > 0, that pass's axis
+// length) or the runtime plans (N = 0).
+template <int N>
+cudaError_t fy_deconv_pass(int pass, const DeconvLaunch& d, cudaStream_t st) {
+    const SpecGeom& g = d.g;
+    const long Q = (long)g.nz * g.ny;
+    auto with_e = [&](int n, auto&& body) -> cudaError_t {
+        if constexpr (N > 0) return body(std::integral_constant<int, ct_e(N)>{});
+        else return fy_with_e(fy_fft_e(n), body);
+    };
+    switch (pass) {
+    case 1: {   // X forward, rows paired two per line (line-major staging)
+        const TileShape t = fy_tile_shape(g.px);
+        const size_t smem = (size_t)t.W * (g.px + 1) * sizeof(float2) + (size_t)g.px * sizeof(float2);
+        const unsigned grid = (unsigned)((Q + 2 * t.W - 1) / (2 * t.W));
+        const int esz = d.src_u8 ? 1 : 4;
+        const bool vec = g.nx % 4 == 0 && ((uintptr_t)d.src % (4 * esz)) == 0;
+        const int pad = g.px - g.nx > 0 ? g.px - g.nx : 1;
+        return with_e(g.px, [&](auto ec) -> cudaError_t {
+            constexpr int E = decltype(ec)::value;
+            cudaError_t e2 = cudaSuccess;
+            const FastDiv dch(vec ? g.nx / 4 : g.nx), dhx(g.hx), dpad(pad);
+#define FY_P1(T, V)                                                                                   \
+            { auto k = k_x_fwd<N, E, T, V>;                                                           \
+              if ((e2 = fy_smem_optin(k, smem)) != cudaSuccess) return e2;                            \
+              k<<<grid, t.NT, smem, st>>>((const T*)d.src, d.lo, d.scale, d.src_u8, d.spec, g, d.plx, d.twx, \
+                                          t.wlog, dch, dhx, dpad); }
+            if (d.src_u8) { if (vec) FY_P1(uint8_t, 4) else FY_P1(uint8_t, 1) }
+            else { if (vec) FY_P1(float, 4) else FY_P1(float, 1) }
+#undef FY_P1
+            return cudaGetLastError();
+        });
+    }
+    case 2:     // Y forward over the stored planes
+    case 4: {   // Y inverse, keep rows < ny
+        const TileShape t = fy_tile_shape(g.py);
+        const size_t smem = (size_t)g.py * t.W * sizeof(float2) + (size_t)g.py * sizeof(float2);
+        dim3 grid(ceil_div_i(g.hx, t.W), g.nz);
+        return with_e(g.py, [&](auto ec) -> cudaError_t {
+            constexpr int E = decltype(ec)::value;
+            if (pass == 2) {
+                auto k = k_y_fwd<N, E>;
+                cudaError_t e2 = fy_smem_optin(k, smem);
+                if (e2 != cudaSuccess) return e2;
+                k<<<grid, t.NT, smem, st>>>(d.spec, g, d.ply, d.twy, t.wlog);
+            } else {
+                auto k = k_y_inv<N, E>;
+                cudaError_t e2 = fy_smem_optin(k, smem);
+                if (e2 != cudaSuccess) return e2;
+                k<<<grid, t.NT, smem, st>>>(d.spec, g, d.ply, d.twy, g.ny, t.wlog);
+            }
+            return cudaGetLastError();
+        });
+    }
+    case 3: {   // Z forward, weight, Z inverse
+        const TileShape t = fy_tile_shape(g.pz);
+        const size_t smem = (size_t)g.pz * t.W * sizeof(float2) + (size_t)g.pz * sizeof(float2) +
+                            (size_t)g.pz * sizeof(double) + (FY_LUT_N + 1) * sizeof(float);
+        dim3 grid(ceil_div_i(g.hx, t.W), g.py);
+        return with_e(g.pz, [&](auto ec) -> cudaError_t {
+            constexpr int E = decltype(ec)::value;
+            auto k = k_z_weight<N, E>;
+            cudaError_t e2 = fy_smem_optin(k, smem);
+            if (e2 != cudaSuccess) return e2;
+            k<<<grid, t.NT, smem, st>>>(d.spec, g, d.plz, d.twz, d.lut, d.fz2, d.fy2, d.fx2, d.us, t.wlog);
+            return cudaGetLastError();
+        });
+    }
+    case 5: {   // X C2R, crop, 1/N (line-major staging, vector stores when rows are 16-byte aligned)
+        const TileShape t = fy_tile_shape(g.px);
+        const size_t smem = (size_t)t.W * (g.px + 1) * sizeof(float2) + (size_t)g.px * sizeof(float2);
+        const unsigned grid = (unsigned)((Q + 2 * t.W - 1) / (2 * t.W));
+        const float invN = 1.0f / ((float)g.pz * (float)g.py * (float)g.px);   // paganin.c:263
+        const bool vec = g.nx % 4 == 0 && ((uintptr_t)d.dst % 16) == 0;
+        return with_e(g.px, [&](auto ec) -> cudaError_t {
+            constexpr int E = decltype(ec)::value;
+            cudaError_t e2 = cudaSuccess;
+            const FastDiv dch(vec ? g.nx / 4 : g.nx), dhx(g.hx);
+            if (vec) {
+                auto k = k_x_inv<N, E, 4>;
+                if ((e2 = fy_smem_optin(k, smem)) != cudaSuccess) return e2;
+                k<<<grid, t.NT, smem, st>>>(d.spec, d.dst, g, d.plx, d.twx, invN, t.wlog, dch, dhx);
+            } else {
+                auto k = k_x_inv<N, E, 1>;
+                if ((e2 = fy_smem_optin(k, smem)) != cudaSuccess) return e2;
+                k<<<grid, t.NT, smem, st>>>(d.spec, d.dst, g, d.plx, d.twx, invN, t.wlog, dch, dhx);
+            }
+            return cudaGetLastError();
+        });
+    }
+    default:
+        return cudaErrorInvalidValue;
+    }
+}
+
+// One case of a compile-time dispatch switch over axis lengths.
+#define FY_DECONV_CT_CASE(NN) case NN: return fy_deconv_pass<NN>(pass, d, st);
+
+}  // namespace

@@ -219,6 +219,93 @@ FY_D void line_fft(float2* __restrict__ sline, int ps, int tl, const FftPlan& pl
     }
 }
 
+// ---------------------------------------------------------------- compile-time plans
+// The same transform with n, the pass sequence and the exchange pitch PS known at compile
+// time, so every index and twiddle offset folds to a constant or a single multiply-add.
+// Results are bit-identical to line_fft (same twiddles, same butterfly order).
+constexpr bool ct_has3(int n) { return n % 3 == 0; }
+constexpr int ct_log2(int m) { return m <= 1 ? 0 : 1 + ct_log2(m / 2); }
+constexpr int ct_lg(int n) { return ct_log2(ct_has3(n) ? n / 3 : n); }
+constexpr int ct_npass(int n) { return (ct_has3(n) ? 1 : 0) + ct_lg(n) / 3 + (ct_lg(n) % 3 ? 1 : 0); }
+constexpr int ct_radix(int n, int p) {
+    return (ct_has3(n) && p == 0) ? 3
+           : ((p - (ct_has3(n) ? 1 : 0)) < ct_lg(n) / 3 ? 8 : (ct_lg(n) % 3 == 2 ? 4 : 2));
+}
+constexpr int ct_nslog(int n, int p) { return (ct_has3(n) && p == 0) ? 0 : 3 * (p - (ct_has3(n) ? 1 : 0)); }
+constexpr int ct_odd(int n, int p) { return (ct_has3(n) && p > 0) ? 3 : 1; }
+constexpr int ct_tile_lines(int n) {
+    return n * 16 <= FY_FFT_TILE_ELEMS ? 16
+           : (n * 8 <= FY_FFT_TILE_ELEMS ? 8 : (n * 4 <= FY_FFT_TILE_ELEMS ? 4 : (n * 2 <= FY_FFT_TILE_ELEMS ? 2 : 1)));
+}
+
+template <int N, int E, int R, int PS, class LD>
+FY_D void ct_load(float2 (&v)[E], int tl, LD ld) {
+    constexpr int TPL = N / E, NR = N / R;
+#pragma unroll
+    for (int b = 0; b < E / R; ++b)
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[b * R + r] = ld(tl + TPL * b + r * NR);
+}
+
+template <int N, int E, int R, int C, int NSLOG, int SIGN>
+FY_D void ct_compute(float2 (&v)[E], int tl, const float2* __restrict__ tw) {
+    constexpr int TPL = N / E, NS = C << NSLOG, TWS = N / (NS * R);
+    if constexpr (NS > 1) {
+#pragma unroll
+        for (int b = 0; b < E / R; ++b) {
+            const int j = tl + TPL * b;
+            const int k = C == 1 ? (j & (NS - 1)) : j - ((j >> NSLOG) / C) * NS;   // j mod Ns
+            const int kt = k * TWS;
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                float2 w = tw[r * kt];
+                if (SIGN < 0) w.y = -w.y;
+                v[b * R + r] = cmul(v[b * R + r], w);
+            }
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < E / R; ++b) Bfly<R>::run(&v[b * R], (float)SIGN);
+}
+
+template <int N, int E, int R, int C, int NSLOG, class ST>
+FY_D void ct_store(const float2 (&v)[E], int tl, ST st) {
+    constexpr int TPL = N / E, NS = C << NSLOG;
+#pragma unroll
+    for (int b = 0; b < E / R; ++b) {
+        const int j = tl + TPL * b;
+        const int q = C == 1 ? (j >> NSLOG) : (j >> NSLOG) / C;
+        const int base = q * NS * R + (j - q * NS);
+#pragma unroll
+        for (int r = 0; r < R; ++r) st(base + r * NS, v[b * R + r]);
+    }
+}
+
+template <int N, int E, int PS, int SIGN, int P, class ST>
+FY_D void ct_passes(float2 (&v)[E], float2* __restrict__ sline, int tl, const float2* __restrict__ tw, ST st) {
+    constexpr int R = ct_radix(N, P), C = ct_odd(N, P), NSLOG = ct_nslog(N, P);
+    ct_compute<N, E, R, C, NSLOG, SIGN>(v, tl, tw);
+    if constexpr (P + 1 == ct_npass(N)) {
+        ct_store<N, E, R, C, NSLOG>(v, tl, st);
+    } else {
+        ct_store<N, E, R, C, NSLOG>(v, tl, [&](int i, float2 x) { sline[i * PS] = x; });
+        __syncthreads();
+        ct_load<N, E, ct_radix(N, P + 1), PS>(v, tl, [&](int i) { return sline[i * PS]; });
+        __syncthreads();
+        ct_passes<N, E, PS, SIGN, P + 1>(v, sline, tl, tw, st);
+    }
+}
+
+// Compile-time counterpart of line_fft (N >= 2): same contract, sign as SIGN = -1 / +1.
+template <int N, int E, int PS, int SIGN, class LD, class ST>
+FY_D void line_fft_ct(float2* __restrict__ sline, int tl, const float2* __restrict__ tw, LD ld, ST st) {
+    static_assert(N % E == 0 && E % ct_radix(N, 0) == 0, "E must hold whole radix groups");
+    float2 v[E];
+    ct_load<N, E, ct_radix(N, 0), PS>(v, tl, ld);
+    __syncthreads();
+    ct_passes<N, E, PS, SIGN, 0>(v, sline, tl, tw, st);
+}
+
 // cooperative copy of the n-entry twiddle table into shared memory
 FY_D void load_twiddles(float2* __restrict__ dst, const float2* __restrict__ src, int n) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];

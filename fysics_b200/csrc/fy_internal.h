@@ -24,6 +24,11 @@ struct DeconvLaunch {
     double us;                // LUT index scale FY_LUT_N / umax
 };
 cudaError_t fy_launch_deconv(const DeconvLaunch& d, cudaStream_t st);
+// Compile-time-plan pass `pass` (1..5) for axis length n; cudaErrorNotSupported when n has no
+// instantiation in that unit (a: 512, 96, 1024; b: 256, 384, 64; c: 128, 192, 768).
+cudaError_t fy_deconv_pass_ct_a(int pass, int n, const DeconvLaunch& d, cudaStream_t st);
+cudaError_t fy_deconv_pass_ct_b(int pass, int n, const DeconvLaunch& d, cudaStream_t st);
+cudaError_t fy_deconv_pass_ct_c(int pass, int n, const DeconvLaunch& d, cudaStream_t st);
 size_t fy_deconv_spec_elems(const SpecGeom& g);
 cudaError_t fy_launch_spec_y(float2* spec, const SpecGeom& g, const FftPlan& ply, const float2* twy, int nplanes,
                              int sign, int keep_rows, cudaStream_t st);
