@@ -39,7 +39,14 @@ class RestoreCfg(C.Structure):
                 ("dering", C.c_void_p), ("dering_accumulate", C.c_int), ("dering_ss", C.c_int),
                 ("dering_hp_win", C.c_int), ("dering_min_cnt", C.c_uint), ("dering_min_amp", C.c_double),
                 ("dering_max_amp", C.c_double), ("dering_scale", C.c_double),
-                ("z0", C.c_long), ("y0", C.c_long), ("x0", C.c_long)]
+                ("z0", C.c_long), ("y0", C.c_long), ("x0", C.c_long),
+                ("radial", C.c_void_p), ("radial_cy", C.c_double), ("radial_cx", C.c_double)]
+
+
+class RadialEps(C.Structure):
+    """fy_radial_eps (include/fysics_b200.h)."""
+    _fields_ = [("a", C.c_double), ("b", C.c_double), ("corr", C.c_double), ("median", C.c_double),
+                ("guided_eps", C.c_double), ("have", C.c_int), ("n", C.c_int)]
 
 
 class Dering(C.Structure):
@@ -110,6 +117,9 @@ SIGNATURES = {
     "fy_gpu_estimate_noise": (_i, [_P, _i, _i, _i, _i, _d, _d, _P, _P]),
     "fy_gpu_noise_model": (_i, [_P, _i, _i, _i, _PN, _P]),
     "fy_gpu_noise_eps": (_P, [_P, _i, _i, _i]),
+    "fy_gpu_fit_radial_eps": (_i, [_P, _P, _i, _d, _P, _P]),
+    "fy_fit_radial_eps": (_i, [_P, _P, _i, _d, C.POINTER(RadialEps)]),
+    "fy_radial_tile_eps": (_d, [C.POINTER(RadialEps), _d, _d, _d, _l, _l, _l, _l]),
     "fy_gpu_estimate_noise_noalloc": (_i, [_P, _i, _i, _i, _i, _d, _d, _P, _P, _P]),
     "fy_gpu_dering_create": (_i, [C.POINTER(_P), _l, _l, _l, _d, _d, _i, _i]),
     "fy_gpu_dering_destroy": (None, [_P]),

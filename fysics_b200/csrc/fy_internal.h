@@ -123,3 +123,7 @@ inline TileShape fy_tile_shape(int n) {
     t.NT = t.W * n / t.E;
     return t;
 }
+
+// Radial guided-eps model (fy_radial.cu): cube eps = base * radial scale, on the device.
+cudaError_t fy_launch_radial_tile_eps(const fy_radial_eps* d_fit, const float* base_dev, float base_host, double ecy,
+                                      double ecx, long y0, long x0, long ty, long tx, float* d_out, cudaStream_t st);

@@ -39,6 +39,8 @@ extern "C" void fy_restore_cfg_default(fy_restore_cfg* c) {
     c->dering_max_amp = 6.0;
     c->dering_scale = 1.0 / 255.0;
     c->z0 = c->y0 = c->x0 = 0;
+    c->radial = nullptr;
+    c->radial_cy = c->radial_cx = 0.0;
 }
 
 extern "C" int fy_gpu_restore_u8(const unsigned char* d_u8, float* d_out, int nz, int ny, int nx, double f32_min,
@@ -90,6 +92,16 @@ extern "C" int fy_gpu_restore_u8(const unsigned char* d_u8, float* d_out, int nz
         fy_prof_mark(st, "noise");
     }
     const float eps = (float)(cfg->guided_eps > 0 ? cfg->guided_eps : 0.0);
+    if (cfg->radial) {       // radial model: this cube's eps = base eps * clamp((fn(r)/median)^2, 0.4, 8)
+        const size_t off = fy_noise_ctl_bytes();
+        if ((e = c.small.ensure(off + 256)) != cudaSuccess) return fail_cuda(e, what);
+        float* d_eps = (float*)((char*)c.small.p + off);
+        if ((e = fy_launch_radial_tile_eps(cfg->radial, eps_ptr, eps, cfg->radial_cy, cfg->radial_cx, cfg->y0, cfg->x0,
+                                           ny, nx, d_eps, st)) != cudaSuccess)
+            return fail_cuda(e, what);
+        launches += 1;
+        eps_ptr = d_eps;
+    }
     // 4. guided filter dec -> d_out
     if (cfg->guided_s > 1) {
         const int s = cfg->guided_s;

@@ -227,6 +227,31 @@ int    fy_gpu_phase_correlate_batch(const float *d_fixed, const float *d_moving,
                                     double *shift, double *peak, long long *peak_index,
                                     int *status, void *stream);
 
+/* Radial guided-eps model. The reference computes it inside fy_run_pipeline
+ * (pipeline.c:851-891, 445-456) and has no public function for it. Least squares
+ * fn(r) = a + b*r of the calibration noise floors against their distance from the rotation
+ * axis, in FP64. have = 1 when the reference's gate passes: n >= 8, b > 0, corr >= 0.5,
+ * fn(0) > 0 and fn(rmax)/fn(0) >= 1.3. median is the median floor (0.015 without samples).
+ * guided_eps = (k*median)^2 with k = denoise_k (0 -> 4.2); 0 when denoise_k < 0. */
+typedef struct {
+    double a, b, corr;
+    double median;
+    double guided_eps;
+    int    have;
+    int    n;
+} fy_radial_eps;
+/* n <= 256 samples on the device; the model is written to d_fit (device memory). */
+int    fy_gpu_fit_radial_eps(const double *d_rads, const double *d_floors, int n, double denoise_k,
+                             fy_radial_eps *d_fit, void *stream);
+/* Host form of the same fit (runs on the device, synchronous). */
+int    fy_fit_radial_eps(const double *rads, const double *floors, int n, double denoise_k,
+                         fy_radial_eps *out);
+/* eps of the tile (y0, x0, ty, tx) around the axis (ecy, ecx): guided_eps times
+ * clamp((fn(r)/median)^2, 0.4, 8), or 0 when the model is off (pipeline.c:447-456).
+ * Host arithmetic only: no device is needed. */
+double fy_radial_tile_eps(const fy_radial_eps *fit, double guided_eps, double ecy, double ecx,
+                          long y0, long x0, long ty, long tx);
+
 /* The per-cube restoration chain on device buffers: dewindow (fused into the
  * deconvolution) -> Wiener deconvolution -> noise model -> guided filter with
  * eps = fy_guided_eps_for_noise(noise_ref) taken on the device -> ring subtraction.
@@ -248,7 +273,11 @@ typedef struct {
     unsigned int dering_min_cnt;
     double dering_min_amp, dering_max_amp;
     double dering_scale;         /* ring u8 units -> output units */
-    long   z0, y0, x0;           /* global offset of the cube (ring geometry) */
+    long   z0, y0, x0;           /* global offset of the cube (ring and radial geometry) */
+    const fy_radial_eps *radial; /* device model from fy_gpu_fit_radial_eps, or NULL: when it is
+                                    on, the guided eps is scaled for the cube centre's distance
+                                    from (radial_cy, radial_cx), as pipeline.c:447-456 */
+    double radial_cy, radial_cx;
 } fy_restore_cfg;
 void fy_restore_cfg_default(fy_restore_cfg *cfg);
 int  fy_gpu_restore_u8(const unsigned char *d_u8, float *d_out, int nz, int ny, int nx,

@@ -98,6 +98,9 @@ O64_SIGS = {
     "o64_dering_apply": (None, [_P, _i, _i, _i, _d, _d, _P, _l, _l, _l, _l, _l, _l, _d]),
     "o64_phase_correlate": (_i, [_P, _P, _i, _i, _i, _PDB, _PDB, _i, C.POINTER(_l)]),
     "o64_fit_radial_eps": (_i, [_P, _P, _i, _PDB, _PDB, _PDB]),
+    "o64_median_floor": (C.c_double, [_P, _i]),
+    "o64_radial_tile_eps": (C.c_double, [_i, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, C.c_long, C.c_long, C.c_long, C.c_long]),
 }
 
 _ref = None

@@ -672,3 +672,31 @@ int o64_fit_radial_eps(const double *rads, const double *floors, int n,
     if (corr) *corr = cc;
     return (bb > 0 && cc >= 0.5 && f0 > 0 && f1 / f0 >= 1.3) ? 1 : 0;
 }
+
+/* median_sorted (pipeline.c:74-78) on a copy; 0.015 without samples (pipeline.c:878). */
+static int o64_cmp_double(const void *a, const void *b) {
+    double x = *(const double *)a, y = *(const double *)b;
+    return (x > y) - (x < y);
+}
+double o64_median_floor(const double *v, int n) {
+    if (n <= 0) return 0.015;
+    double *w = (double *)malloc(sizeof(double) * (size_t)n);
+    if (!w) return -1;
+    memcpy(w, v, sizeof(double) * (size_t)n);
+    qsort(w, (size_t)n, sizeof(double), o64_cmp_double);
+    double m = (n & 1) ? w[n / 2] : 0.5 * (w[n / 2 - 1] + w[n / 2]);
+    free(w);
+    return m;
+}
+
+/* eps of a tile (pipeline.c:447-456): 0 when the radial model is off. */
+double o64_radial_tile_eps(int have, double a, double b, double median, double guided_eps,
+                           double ecy, double ecx, long y0, long x0, long ty, long tx) {
+    if (!have || guided_eps <= 0 || median <= 0) return 0.0;
+    double ry = y0 + ty / 2.0 - ecy, rx = x0 + tx / 2.0 - ecx;
+    double fn = a + b * sqrt(ry * ry + rx * rx);
+    double s = fn / median, s2 = s * s;
+    if (s2 < 0.4) s2 = 0.4;
+    if (s2 > 8.0) s2 = 8.0;
+    return guided_eps * s2;
+}

@@ -73,6 +73,11 @@ int    o64_phase_correlate(const double *fixed, const double *moving, int nz, in
 /* radial eps fit (pipeline.c:856-877): returns 1 and fills a,b when the gate passes */
 int    o64_fit_radial_eps(const double *rads, const double *floors, int n,
                           double *a, double *b, double *corr);
+/* median of the noise floors, pipeline.c:74-78 and :878 (0.015 when n == 0) */
+double o64_median_floor(const double *v, int n);
+/* per-tile eps, pipeline.c:447-456 (0 = use the global eps) */
+double o64_radial_tile_eps(int have, double a, double b, double median, double guided_eps,
+                           double ecy, double ecx, long y0, long x0, long ty, long tx);
 
 #ifdef __cplusplus
 }
