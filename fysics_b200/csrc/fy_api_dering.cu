@@ -344,6 +344,18 @@ extern "C" int fy_gpu_dering_finalize(fy_gpu_dering* h, int hp_win, unsigned int
     return FY_OK;
 }
 
+void fy_dering_ring_args(const fy_gpu_dering* h, long z0, long y0, long x0, double scale, RingApply* ra) {
+    ra->ring = h->dring;
+    ra->have = h->dhave;
+    ra->nslab = h->geo.nslab;
+    ra->nr = h->geo.nr;
+    ra->slab_z = h->geo.slab_z;
+    ra->cy = h->geo.cy;
+    ra->cx = h->geo.cx;
+    ra->z0 = z0; ra->y0 = y0; ra->x0 = x0;
+    ra->sc = (float)scale;
+}
+
 extern "C" int fy_gpu_dering_apply(const fy_gpu_dering* h, float* d_f, long z0, long y0, long x0, long dz, long dy,
                                    long dx, double scale, void* stream) {
     fy::enter();

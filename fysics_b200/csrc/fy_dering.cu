@@ -12,14 +12,17 @@
 //   k_dering_vote    per (slab, radius): sector sign-consistency vote, median, clamp
 //                    (dering.c:171-189)
 //   k_dering_apply   f = max(f - scale*ring[slab][r(y,x)], 0) for f > 0 (dering.c:200-248),
-//                    one thread per (y,x) column walking z.
+//                    one thread per (y,x) column walking a chunk of 32 planes.
 #include "fy_internal.h"
 
 namespace {
 
 // ---------------------------------------------------------------- accumulate
-// Grid: (x tiles of 256 samples, sampled rows * dz). Shared-memory histograms when the
-// bin count fits, else global atomics.
+// Grid: (x tiles, sampled rows * dz). Each thread takes 8 consecutive samples of a row and
+// merges runs that fall in the same (sector, radius) bin in registers, so neighbouring
+// samples (mostly one bin) cost one shared atomic per run. Shared-memory histograms when
+// the bin count fits, else global atomics.
+constexpr int ACC_K = 8;
 template <bool SMEM>
 __global__ void __launch_bounds__(256) k_dering_accum(const uint8_t* __restrict__ buf, const int* __restrict__ map,
                                                       unsigned long long* __restrict__ gsum,
@@ -33,19 +36,33 @@ __global__ void __launch_bounds__(256) k_dering_accum(const uint8_t* __restrict_
         for (int i = threadIdx.x; i < 2 * nbins; i += blockDim.x) sh[i] = 0;
         __syncthreads();
     }
+    auto flush = [&](int b, unsigned s_, unsigned c_) {
+        if (b < 0 || !c_) return;
+        if (SMEM) { atomicAdd(&ssum[b], s_); atomicAdd(&scnt[b], c_); }
+        else { atomicAdd(&gsum[b], (unsigned long long)s_); atomicAdd(&gcnt[b], c_); }
+    };
     const long nrows = dz * sy;
     const long r0 = (long)blockIdx.y * rows_per_cta;
     for (long rr = r0; rr < r0 + rows_per_cta && rr < nrows; ++rr) {
         const long z = rr / sy, yi = rr - z * sy;
         const uint8_t* row = buf + ((size_t)z * dy + (size_t)(yi * ss)) * dx;
         const int* mrow = map + yi * sx;
-        for (long xi = (long)blockIdx.x * blockDim.x + threadIdx.x; xi < sx; xi += (long)gridDim.x * blockDim.x) {
-            const unsigned v = __ldg(row + xi * ss);
-            if (!v) continue;                                   // masked voxels skipped
-            const int b = __ldg(mrow + xi);
-            if (b < 0) continue;
-            if (SMEM) { atomicAdd(&ssum[b], v); atomicAdd(&scnt[b], 1u); }
-            else { atomicAdd(&gsum[b], (unsigned long long)v); atomicAdd(&gcnt[b], 1u); }
+        for (long xb = ((long)blockIdx.x * blockDim.x + threadIdx.x) * ACC_K; xb < sx;
+             xb += (long)gridDim.x * blockDim.x * ACC_K) {
+            int cur = -1;
+            unsigned s_ = 0, c_ = 0;
+#pragma unroll
+            for (int j = 0; j < ACC_K; ++j) {
+                const long xi = xb + j;
+                if (xi >= sx) break;
+                const unsigned v = __ldg(row + xi * ss);
+                if (!v) continue;                               // masked voxels skipped
+                const int b = __ldg(mrow + xi);
+                if (b < 0) continue;
+                if (b != cur) { flush(cur, s_, c_); cur = b; s_ = 0; c_ = 0; }
+                s_ += v; ++c_;
+            }
+            flush(cur, s_, c_);
         }
     }
     if (SMEM) {
@@ -74,38 +91,49 @@ __global__ void __launch_bounds__(256) k_dering_smooth(const float* __restrict__
                                                        float* __restrict__ p, float* __restrict__ hp,
                                                        unsigned char* __restrict__ vd, int ns, int nr, int hw,
                                                        unsigned min_cnt) {
+    extern __shared__ float sm_f[];
+    float* sp = sm_f;                                  // p, hp and validity of this row in smem
+    float* shp = sp + nr;
+    unsigned char* svd = reinterpret_cast<unsigned char*>(shp + nr);
     __shared__ int s_first;
     const size_t off = (size_t)blockIdx.x * nr;       // (slab, sector) row
     if (threadIdx.x == 0) s_first = nr;
     for (int r = threadIdx.x; r < nr; r += blockDim.x) {
         const unsigned c = cnt[off + r];
         const unsigned char v = c >= min_cnt;
-        vd[off + r] = v;
-        p[off + r] = v ? sum_f[off + r] / (float)c : 0.0f;
+        svd[r] = v;
+        sp[r] = v ? sum_f[off + r] / (float)c : 0.0f;
     }
     __syncthreads();
     for (int r = threadIdx.x; r < nr; r += blockDim.x) {
-        if (!vd[off + r]) { hp[off + r] = 0.0f; continue; }
+        shp[r] = 0.0f;
+        if (!svd[r]) continue;
         double acc = 0;
         int c = 0;
         const int lo = r - hw < 0 ? 0 : r - hw, hi = r + hw >= nr ? nr - 1 : r + hw;
         for (int j = lo; j <= hi; ++j)
-            if (vd[off + j]) { acc += p[off + j]; ++c; }
-        if (c >= hw) hp[off + r] = p[off + r] - (float)(acc / c);
+            if (svd[j]) { acc += sp[j]; ++c; }
+        if (c >= hw) shp[r] = sp[r] - (float)(acc / c);
         else atomicMin(&s_first, r);
     }
     __syncthreads();
     if (threadIdx.x == 0 && s_first < nr) {           // rare: sequential from the first change
         for (int r = s_first; r < nr; ++r) {
-            if (!vd[off + r]) { hp[off + r] = 0.0f; continue; }
+            if (!svd[r]) { shp[r] = 0.0f; continue; }
             double acc = 0;
             int c = 0;
             const int lo = r - hw < 0 ? 0 : r - hw, hi = r + hw >= nr ? nr - 1 : r + hw;
             for (int j = lo; j <= hi; ++j)
-                if (vd[off + j]) { acc += p[off + j]; ++c; }
-            if (c >= hw) hp[off + r] = p[off + r] - (float)(acc / c);
-            else { hp[off + r] = 0.0f; vd[off + r] = 0; }
+                if (svd[j]) { acc += sp[j]; ++c; }
+            if (c >= hw) shp[r] = sp[r] - (float)(acc / c);
+            else { shp[r] = 0.0f; svd[r] = 0; }
         }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
+        p[off + r] = sp[r];
+        hp[off + r] = shp[r];
+        vd[off + r] = svd[r];
     }
 }
 
@@ -156,19 +184,21 @@ __global__ void __launch_bounds__(256) k_dering_apply(float* __restrict__ f, con
     if (have_rings && !*have_rings) return;                    // dering.c:202
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long y = blockIdx.y;
+    const long zc = (dz + gridDim.z - 1) / gridDim.z;
+    const long zb = (long)blockIdx.z * zc, zend = zb + zc < dz ? zb + zc : dz;
     if (x >= dx) return;
     const double gy = (double)(y0 + y) - cy, gx = (double)(x0 + x) - cx;
     const int ri = (int)(sqrt(gy * gy + gx * gx) + 0.5);
     if (ri >= nr) return;
     const size_t zs = (size_t)dy * dx;
     float* col = f + (size_t)y * dx + x;
-    for (long z = 0; z < dz; z += 4) {
+    for (long z = zb; z < zend; z += 4) {
         float v[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) v[k] = (z + k < dz) ? col[(size_t)(z + k) * zs] : 0.0f;   // 4 loads in flight
+        for (int k = 0; k < 4; ++k) v[k] = (z + k < zend) ? col[(size_t)(z + k) * zs] : 0.0f;   // 4 loads in flight
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            if (z + k >= dz || v[k] <= 0.0f) continue;     // masked voxels untouched
+            if (z + k >= zend || v[k] <= 0.0f) continue;   // masked voxels untouched
             long s = (z0 + z + k) / slab_z;
             if (s < 0) s = 0;
             if (s >= nslab) s = nslab - 1;
@@ -185,7 +215,8 @@ cudaError_t fy_launch_dering_accum(const uint8_t* buf, const int* map, unsigned 
     const long sy = (dy + ss - 1) / ss, sx = (dx + ss - 1) / ss;
     const long nrows = dz * sy;
     if (nrows <= 0 || sx <= 0) return cudaSuccess;
-    const int gx = (int)((sx + 255) / 256 < 4 ? (sx + 255) / 256 : 4);
+    const long xt = (sx + 256 * ACC_K - 1) / (256 * ACC_K);
+    const int gx = (int)(xt < 4 ? xt : 4);
     long want_ctas = (long)sms * 8 / gx;
     if (want_ctas < 1) want_ctas = 1;
     int rows_per_cta = (int)((nrows + want_ctas - 1) / want_ctas);
@@ -214,7 +245,10 @@ cudaError_t fy_launch_dering_finalize(const float* sum_f, const unsigned int* cn
     cudaError_t e = cudaMemsetAsync(detected, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     const int hw = hp_win / 2;
-    k_dering_smooth<<<nslab * ns, 256, 0, st>>>(sum_f, cnt, p, hp, vd, ns, nr, hw, min_cnt);
+    const size_t smem = (size_t)nr * (2 * sizeof(float) + 1);
+    e = fy_smem_optin(k_dering_smooth, smem);
+    if (e != cudaSuccess) return e;
+    k_dering_smooth<<<nslab * ns, 256, smem, st>>>(sum_f, cnt, p, hp, vd, ns, nr, hw, min_cnt);
     const long nv = (long)nslab * nr;
     k_dering_vote<<<(unsigned)((nv + 127) / 128), 128, 0, st>>>(hp, vd, ring, nslab, ns, nr, (float)min_amp,
                                                                 (float)max_amp, detected);
@@ -231,7 +265,7 @@ cudaError_t fy_launch_dering_apply(float* f, const float* ring, const int* have_
                                    int slab_z, double cy, double cx, long z0, long y0, long x0, long dz, long dy,
                                    long dx, double scale, cudaStream_t st) {
     if (dz <= 0 || dy <= 0 || dx <= 0) return cudaSuccess;
-    dim3 grid((unsigned)((dx + 255) / 256), (unsigned)dy);
+    dim3 grid((unsigned)((dx + 255) / 256), (unsigned)dy, (unsigned)((dz + 31) / 32));
     k_dering_apply<<<grid, 256, 0, st>>>(f, ring, have_rings, nslab, nr, slab_z, cy, cx, z0, y0, x0, dz, dy, dx,
                                          (float)scale);
     return cudaGetLastError();

@@ -99,7 +99,8 @@ size_t fy_guided_fused_scratch_floats(size_t n) { return 2 * round64(n); }
 // fy_guided_fused_scratch_floats(n) floats; out may alias in. mode 1 writes box(a) to out
 // and box(b) to out_b instead of the filtered volume.
 cudaError_t fy_launch_guided_fused(const float* in, float* out, float* out_b, float* ab_ws, int nz, int ny, int nx,
-                                   int r, float eps, int mode, int sms, cudaStream_t st, const float* eps_ptr) {
+                                   int r, float eps, int mode, int sms, cudaStream_t st, const float* eps_ptr,
+                                   const RingApply* rings) {
     if (r < 1 || r > 4) return cudaErrorInvalidValue;
     const size_t n = (size_t)nz * ny * nx;
     float* A = ab_ws;
@@ -112,6 +113,7 @@ cudaError_t fy_launch_guided_fused(const float* in, float* out, float* out_b, fl
     fyzb::Params q{};
     q.nz = nz; q.ny = ny; q.nx = nx;
     q.f0 = A; q.f1 = B; q.guide = in; q.o0 = out; q.o1 = out_b; q.out_mode = mode;
+    if (rings && mode == 0) q.ra = *rings;
     return fyzb::launch<fyzb::ZB_GUIDED_OUT>(q, r, sms, st);
 }
 

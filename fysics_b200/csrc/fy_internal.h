@@ -43,12 +43,25 @@ cudaError_t fy_launch_float_to_u8(const float* in, uint8_t* out, size_t n, cudaS
 cudaError_t fy_launch_u8_to_float(const uint8_t* in, float* out, size_t n, cudaStream_t st);
 
 // Guided filter / box mean (fy_guided.cu)
+// Ring subtraction folded into a producer's store (dering.c:200-248, the same arithmetic as
+// fy_dering_apply): ring == nullptr means none.
+struct RingApply {
+    const float* ring = nullptr;      // [nslab][nr] device ring profile
+    const int* have = nullptr;        // device have_rings flag (nullptr: apply unconditionally)
+    int nslab = 0, nr = 0, slab_z = 1;
+    double cy = 0.0, cx = 0.0;        // ring centre (global y, x)
+    long z0 = 0, y0 = 0, x0 = 0;      // global offset of the volume
+    float sc = 0.f;                   // ring units -> volume units
+};
+// Fill `ra` from a device ring handle (fy_api_dering.cu).
+void fy_dering_ring_args(const fy_gpu_dering* h, long z0, long y0, long x0, double scale, RingApply* ra);
+
 // exact r <= 4: ab_ws holds fy_guided_fused_scratch_floats(n); out may alias in
 size_t fy_guided_fused_scratch_floats(size_t n);
 size_t fy_guided_fast_scratch_floats(int lz, int ly, int lx);
 cudaError_t fy_launch_guided_fused(const float* in, float* out, float* out_b, float* ab_ws, int nz, int ny, int nx,
                                    int r, float eps, int mode, int sms, cudaStream_t st,
-                                   const float* eps_ptr = nullptr);
+                                   const float* eps_ptr = nullptr, const RingApply* rings = nullptr);
 cudaError_t fy_launch_guided_generic(const float* in, float* out, float* ws, int nz, int ny, int nx, int r,
                                      float eps, cudaStream_t st, int& launches);
 cudaError_t fy_launch_guided_fast(const float* in, float* out, float* ws, int nz, int ny, int nx, int r,

@@ -103,6 +103,7 @@ extern "C" int fy_gpu_restore_u8(const unsigned char* d_u8, float* d_out, int nz
         eps_ptr = d_eps;
     }
     // 4. guided filter dec -> d_out
+    bool rings_done = false;
     if (cfg->guided_s > 1) {
         const int s = cfg->guided_s;
         const int lz = (nz + s - 1) / s, ly = (ny + s - 1) / s, lx = (nx + s - 1) / s;
@@ -120,19 +121,24 @@ extern "C" int fy_gpu_restore_u8(const unsigned char* d_u8, float* d_out, int nz
             launches += 2;
         }
     } else {
-        // a, b reuse the noise statistics' scratch: the model is final by now (stream order)
+        // a, b reuse the noise statistics' scratch: the model is final by now (stream order);
+        // the ring subtraction is folded into the guided filter's output pass
         if ((e = c.aux.ensure(fy_guided_fused_scratch_floats(n) * sizeof(float))) != cudaSuccess)
             return fail_cuda(e, what);
+        RingApply ra;
+        if (cfg->dering) fy_dering_ring_args(cfg->dering, cfg->z0, cfg->y0, cfg->x0, cfg->dering_scale, &ra);
         e = fy_launch_guided_fused(dec, d_out, nullptr, c.aux.as<float>(), nz, ny, nx, radius, eps, 0, c.sms, st,
-                                   eps_ptr);
+                                   eps_ptr, cfg->dering ? &ra : nullptr);
         launches += 2;
+        rings_done = cfg->dering != nullptr;
     }
     if (e != cudaSuccess) return fail_cuda(e, what);
     fy_prof_mark(st, "guided");
     fy::count_launch(launches);
     fy::ws_release(st);
-    // 5. ring subtraction (no-op on the device when fewer than 2 radii were detected)
-    if (cfg->dering) {
+    // 5. ring subtraction (no-op on the device when fewer than 2 radii were detected), unless
+    // the exact guided filter already applied it
+    if (cfg->dering && !rings_done) {
         if ((rc = fy_gpu_dering_apply(cfg->dering, d_out, cfg->z0, cfg->y0, cfg->x0, nz, ny, nx, cfg->dering_scale,
                                       stream)))
             return rc;

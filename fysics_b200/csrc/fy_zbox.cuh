@@ -22,7 +22,8 @@
 // Window sums are direct (2R+1)-tap float sums in ascending order, started from the first
 // tap, so no running-sum chain accumulates error. Each output voxel is written once by one
 // thread, and ZB_GUIDED_OUT reads the guide only at the voxel it writes, so out may alias
-// the guide.
+// the guide. ZB_GUIDED_OUT can also subtract the ring profile from its output (the same
+// arithmetic as fy_dering_apply), which saves the separate read-modify-write pass.
 #pragma once
 #include "fy_internal.h"
 
@@ -44,6 +45,7 @@ struct Params {
     int wci;               // NOISE: win^3
     int out_mode;
     int nz, ny, nx, zchunk;
+    RingApply ra;          // GUIDED_OUT, out_mode 0: ring subtraction on the output (optional)
 };
 
 template <int R, int NF>
@@ -143,6 +145,18 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     for (int k = 0; k < 4; ++k) {
         const int gy = y0 + 4 * rg + k;
         cyx[k] = (min(gy + R, ny - 1) - max(gy - R, 0) + 1) * (min(gx + R, nx - 1) - max(gx - R, 0) + 1);
+    }
+    // GUIDED_OUT: ring radius of this thread's 4 output voxels (dering.c:200-248)
+    bool rings = false;
+    int ri[4] = {0, 0, 0, 0};
+    if (KIND == ZB_GUIDED_OUT && p.out_mode == 0 && p.ra.ring) {
+        rings = p.ra.have ? (*p.ra.have != 0) : true;
+        const double gxd = (double)(p.ra.x0 + gx) - p.ra.cx;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const double gyd = (double)(p.ra.y0 + y0 + 4 * rg + k) - p.ra.cy;
+            ri[k] = (int)(sqrt(gyd * gyd + gxd * gxd) + 0.5);
+        }
     }
     float r1[NR][4], r2[NR][4];
 #pragma unroll
@@ -272,8 +286,19 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                     p.o1[o] = mean * (1.0f - a);                   // guided.c:131
                 } else {
                     const float ma = s1 * rz, mb = s2 * rz;
-                    if (p.out_mode == 0) p.o0[o] = ma * gv[k] + mb;
-                    else { p.o0[o] = ma; p.o1[o] = mb; }
+                    if (p.out_mode == 0) {
+                        float w = ma * gv[k] + mb;
+                        if (rings && w > 0.f && ri[k] < p.ra.nr) {     // masked voxels untouched
+                            long sl = (p.ra.z0 + zo) / p.ra.slab_z;
+                            if (sl < 0) sl = 0;
+                            if (sl >= p.ra.nslab) sl = p.ra.nslab - 1;
+                            const float w2 = w - p.ra.sc * __ldg(p.ra.ring + (size_t)sl * p.ra.nr + ri[k]);
+                            w = w2 > 0.f ? w2 : 0.f;
+                        }
+                        p.o0[o] = w;
+                    } else {
+                        p.o0[o] = ma; p.o1[o] = mb;
+                    }
                 }
             }
         }

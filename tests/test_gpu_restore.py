@@ -130,6 +130,27 @@ def test_chain_equals_stages(gpu):
     assert np.abs(chain - steps).max() <= 1e-6
 
 
+def test_chain_ring_subtraction_matches_separate_apply(gpu):
+    """The chain folds the ring subtraction into the guided output pass; the result must
+    equal the chain without rings followed by fy_gpu_dering_apply (dering.c:200-248)."""
+    import torch
+    lib = gpu.load()
+    u8 = cube()
+    nz, ny, nx = u8.shape
+    fused = run_chain(gpu, u8, with_rings=True)
+    plain = torch.from_numpy(run_chain(gpu, u8, with_rings=False)).cuda()
+    d_u8 = torch.from_numpy(u8).cuda()
+    h = C.c_void_p()
+    assert lib.fy_gpu_dering_create(C.byref(h), nz, ny, nx, -1.0, -1.0, 512, 8) == 0
+    assert lib.fy_gpu_dering_accumulate_u8(h, C.c_void_p(d_u8.data_ptr()), 0, 0, 0, nz, ny, nx, 2, None) == 0
+    assert lib.fy_gpu_dering_finalize(h, 15, 20, 0.5, 6.0, None) == 0
+    assert lib.fy_gpu_dering_apply(h, C.c_void_p(plain.data_ptr()), 0, 0, 0, nz, ny, nx, 1.0 / 255.0, None) == 0
+    torch.cuda.synchronize()
+    lib.fy_gpu_dering_destroy(h)
+    sep = plain.cpu().numpy()
+    assert np.array_equal(fused, sep)
+
+
 @pytest.mark.skipif(not oracle.have_ref(), reason="reference library not built")
 def test_chain_vs_reference(gpu):
     u8 = cube()
