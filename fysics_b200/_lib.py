@@ -43,6 +43,28 @@ class RestoreCfg(C.Structure):
                 ("radial", C.c_void_p), ("radial_cy", C.c_double), ("radial_cx", C.c_double)]
 
 
+class ServerCfg(C.Structure):
+    """fy_server_cfg (include/fysics_b200.h)."""
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("workers", C.c_int), ("device", C.c_int)]
+
+
+class Request(C.Structure):
+    """fy_request (include/fysics_b200.h)."""
+    _fields_ = [("u8", C.c_void_p), ("out", C.c_void_p), ("nz", C.c_int), ("ny", C.c_int), ("nx", C.c_int),
+                ("f32_min", C.c_double), ("f32_max", C.c_double), ("phys", Physics), ("cfg", RestoreCfg)]
+
+
+class RequestResult(C.Structure):
+    """fy_request_result (include/fysics_b200.h)."""
+    _fields_ = [("status", C.c_int), ("queue_ms", C.c_double), ("run_ms", C.c_double), ("latency_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    """fy_server_stats (include/fysics_b200.h)."""
+    _fields_ = [("completed", C.c_longlong), ("voxels", C.c_double), ("mvox_per_s", C.c_double),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("inflight", C.c_int), ("queued", C.c_int)]
+
+
 class RadialEps(C.Structure):
     """fy_radial_eps (include/fysics_b200.h)."""
     _fields_ = [("a", C.c_double), ("b", C.c_double), ("corr", C.c_double), ("median", C.c_double),
@@ -117,6 +139,13 @@ SIGNATURES = {
     "fy_gpu_estimate_noise": (_i, [_P, _i, _i, _i, _i, _d, _d, _P, _P]),
     "fy_gpu_noise_model": (_i, [_P, _i, _i, _i, _PN, _P]),
     "fy_gpu_noise_eps": (_P, [_P, _i, _i, _i]),
+    "fy_server_cfg_default": (None, [C.POINTER(ServerCfg)]),
+    "fy_server_create": (_i, [C.POINTER(_P), C.POINTER(ServerCfg)]),
+    "fy_server_submit": (_i, [_P, C.POINTER(Request), C.POINTER(C.c_longlong)]),
+    "fy_server_wait": (_i, [_P, C.c_longlong, _d, C.POINTER(RequestResult)]),
+    "fy_server_get_stats": (_i, [_P, C.POINTER(ServerStats)]),
+    "fy_server_reset_stats": (None, [_P]),
+    "fy_server_destroy": (None, [_P]),
     "fy_gpu_fit_radial_eps": (_i, [_P, _P, _i, _d, _P, _P]),
     "fy_fit_radial_eps": (_i, [_P, _P, _i, _d, C.POINTER(RadialEps)]),
     "fy_radial_tile_eps": (_d, [C.POINTER(RadialEps), _d, _d, _d, _l, _l, _l, _l]),

@@ -1,0 +1,318 @@
+// fy_server.cu -- the request loop: continuous batching of restoration requests on one GPU.
+//
+// A viewer or exporter issues cubes as they are needed, from many threads, with sizes and
+// per-volume metadata that vary request by request. The server keeps a FIFO of submitted
+// requests and a pool of worker threads. Each worker owns a CUDA stream and its own
+// device workspaces (the per-thread context of the C-ABI), so the chains of different
+// requests run concurrently on the GPU, and one request's host<->device copies overlap
+// other requests' kernels. A request is admitted when a worker is free and the estimated
+// device footprint of everything in flight stays within the HBM budget; the head of the
+// queue waits rather than being overtaken, so no request starves. Each request's result is
+// the same as the single-cube fy_gpu_restore_u8 call on its own: the kernels are
+// deterministic and a worker's workspaces are private to the request it runs.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "fy_context.h"
+
+using fy::ctx;
+using fy::fail;
+using fy::fail_cuda;
+
+extern "C" int fy_gpu_restore_u8(const unsigned char* d_u8, float* d_out, int nz, int ny, int nx, double f32_min,
+                                 double f32_max, const fy_physics* p, const fy_restore_cfg* cfg, void* stream);
+
+namespace {
+
+double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Ticket {
+    fy_request req;
+    long long id = 0;
+    size_t footprint = 0;
+    double t_submit = 0, t_start = 0, t_done = 0;
+    int status = -1;          // -1 pending, else the chain's status
+    bool done = false;
+};
+
+// Worker-owned device and pinned buffers (grow-only).
+struct WorkerBufs {
+    fy::DevBuf d_in, d_out;
+    fy::HostBuf h_in, h_out;
+};
+
+}  // namespace
+
+struct fy_server {
+    fy_server_cfg cfg{};
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Ticket*> queue;
+    std::unordered_map<long long, Ticket*> tickets;
+    std::vector<std::thread> workers;
+    size_t inflight_bytes = 0;
+    int inflight = 0;
+    bool stop = false;
+    long long next_id = 1;
+    // completed-request statistics
+    std::vector<double> lat_ms;
+    double voxels = 0;
+    double first_start = 0, last_done = 0;
+    int init_status = 0;
+};
+
+namespace {
+
+// Device bytes a request holds while it runs: u8 in, f32 out, the deconvolved volume, the
+// half spectrum (<= 8 B per padded complex over half the x axis), the noise statistics
+// (9 B per voxel) and the guided filter's a/b fields reuse those; tables are small.
+size_t footprint_of(const fy_request& r) {
+    const size_t n = (size_t)r.nz * r.ny * r.nx;
+    const size_t pz = (size_t)fy_next_fft_size(r.nz), py = (size_t)fy_next_fft_size(r.ny);
+    const size_t px = (size_t)fy_next_fft_size(r.nx);
+    const size_t spec = r.nz * py * ((px / 2 + 1 + 15) & ~(size_t)15) * 8;
+    (void)pz;
+    return n + 4 * n + 4 * n + spec + 9 * n + (8u << 20);
+}
+
+void run_one(fy_server* s, Ticket* t, WorkerBufs& wb) {
+    const fy_request& r = t->req;
+    const size_t n = (size_t)r.nz * r.ny * r.nx;
+    fy::ThreadCtx& c = ctx();
+    cudaStream_t st = c.st;
+    cudaError_t e;
+    int rc = FY_OK;
+    const bool in_pinned = fy::is_pinned(r.u8), out_pinned = fy::is_pinned(r.out);
+    do {
+        if ((e = wb.d_in.ensure(n)) != cudaSuccess || (e = wb.d_out.ensure(4 * n)) != cudaSuccess) {
+            rc = fail_cuda(e, "fy_server");
+            break;
+        }
+        const unsigned char* src = r.u8;
+        if (!in_pinned) {                        // stage pageable input through pinned memory
+            if ((e = wb.h_in.ensure(n)) != cudaSuccess) { rc = fail_cuda(e, "fy_server"); break; }
+            memcpy(wb.h_in.p, r.u8, n);
+            src = (const unsigned char*)wb.h_in.p;
+        }
+        if ((e = cudaMemcpyAsync(wb.d_in.p, src, n, cudaMemcpyHostToDevice, st)) != cudaSuccess) {
+            rc = fail_cuda(e, "fy_server");
+            break;
+        }
+        rc = fy_gpu_restore_u8(wb.d_in.as<unsigned char>(), wb.d_out.as<float>(), r.nz, r.ny, r.nx, r.f32_min,
+                               r.f32_max, &r.phys, &r.cfg, st);
+        if (rc) break;
+        float* dst = r.out;
+        if (!out_pinned) {
+            if ((e = wb.h_out.ensure(4 * n)) != cudaSuccess) { rc = fail_cuda(e, "fy_server"); break; }
+            dst = (float*)wb.h_out.p;
+        }
+        if ((e = cudaMemcpyAsync(dst, wb.d_out.p, 4 * n, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+            rc = fail_cuda(e, "fy_server");
+            break;
+        }
+        if (!out_pinned) memcpy(r.out, wb.h_out.p, 4 * n);
+    } while (false);
+    std::lock_guard<std::mutex> lk(s->mu);
+    t->status = rc;
+    t->t_done = now_ms();
+    t->done = true;
+    s->inflight_bytes -= t->footprint;
+    s->inflight -= 1;
+    if (rc == FY_OK) {
+        s->lat_ms.push_back(t->t_done - t->t_submit);
+        s->voxels += (double)n;
+        s->last_done = t->t_done;
+    }
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+}
+
+void worker_main(fy_server* s, int idx) {
+    const int rc0 = fy_gpu_init(s->cfg.device);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (rc0 && !s->init_status) s->init_status = rc0;
+    }
+    WorkerBufs wb;
+    (void)idx;
+    for (;;) {
+        Ticket* t = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_work.wait(lk, [&] {
+                if (s->stop) return true;
+                if (s->queue.empty()) return false;
+                const Ticket* h = s->queue.front();
+                return s->inflight == 0 || s->inflight_bytes + h->footprint <= s->cfg.hbm_budget_bytes;
+            });
+            if (s->stop && s->queue.empty()) break;
+            if (s->stop) {                       // drain: cancel what never started
+                while (!s->queue.empty()) {
+                    Ticket* q = s->queue.front();
+                    s->queue.pop_front();
+                    q->status = FY_EBUSY;
+                    q->done = true;
+                }
+                s->cv_done.notify_all();
+                break;
+            }
+            t = s->queue.front();
+            s->queue.pop_front();
+            s->inflight_bytes += t->footprint;
+            s->inflight += 1;
+            t->t_start = now_ms();
+            if (s->first_start == 0) s->first_start = t->t_start;
+        }
+        if (rc0) {
+            std::lock_guard<std::mutex> lk(s->mu);
+            t->status = rc0;
+            t->done = true;
+            t->t_done = now_ms();
+            s->inflight_bytes -= t->footprint;
+            s->inflight -= 1;
+            s->cv_done.notify_all();
+            s->cv_work.notify_all();
+            continue;
+        }
+        run_one(s, t, wb);
+    }
+    wb.d_in.release();
+    wb.d_out.release();
+    wb.h_in.release();
+    wb.h_out.release();
+    fy_gpu_release();
+}
+
+}  // namespace
+
+extern "C" void fy_server_cfg_default(fy_server_cfg* c) {
+    c->hbm_budget_bytes = (size_t)150 << 30;    // 150 GB
+    c->workers = 4;
+    c->device = 0;
+}
+
+extern "C" int fy_server_create(fy_server** out, const fy_server_cfg* cfg) {
+    fy::enter();
+    if (!out) return fail(FY_EINVAL, "fy_server_create: null handle");
+    *out = nullptr;
+    int rc = fy::ensure_ctx();                  // fails with FY_ENODEV without a GPU
+    if (rc) return rc;
+    fy_server* s = new fy_server();
+    if (cfg) s->cfg = *cfg;
+    else fy_server_cfg_default(&s->cfg);
+    if (s->cfg.workers < 1) s->cfg.workers = 1;
+    if (s->cfg.workers > 64) s->cfg.workers = 64;
+    if (s->cfg.hbm_budget_bytes == 0) s->cfg.hbm_budget_bytes = (size_t)150 << 30;
+    for (int i = 0; i < s->cfg.workers; ++i) s->workers.emplace_back(worker_main, s, i);
+    *out = s;
+    return FY_OK;
+}
+
+extern "C" int fy_server_submit(fy_server* s, const fy_request* r, long long* ticket) {
+    fy::enter();
+    if (!s || !r || !ticket) return fail(FY_EINVAL, "fy_server_submit: null pointer");
+    if (!r->u8 || !r->out) return fail(FY_EINVAL, "fy_server_submit: null buffer");
+    if (r->nz < 1 || r->ny < 1 || r->nx < 1) return fail(FY_EINVAL, "fy_server_submit: bad dims");
+    if (r->cfg.dering && r->cfg.dering_accumulate)
+        return fail(FY_EINVAL, "fy_server_submit: ring accumulation into a shared handle is not allowed here");
+    Ticket* t = new Ticket();
+    t->req = *r;
+    t->footprint = footprint_of(*r);
+    if (t->footprint > s->cfg.hbm_budget_bytes) {
+        const size_t fp = t->footprint;
+        delete t;
+        return fail(FY_EUNSUPPORTED, "fy_server_submit: request needs ~%zu MB, above the HBM budget of %zu MB",
+                    fp >> 20, s->cfg.hbm_budget_bytes >> 20);
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) { delete t; return fail(FY_EBUSY, "fy_server_submit: server is stopping"); }
+    t->id = s->next_id++;
+    t->t_submit = now_ms();
+    s->tickets[t->id] = t;
+    s->queue.push_back(t);
+    *ticket = t->id;
+    s->cv_work.notify_one();
+    return FY_OK;
+}
+
+extern "C" int fy_server_wait(fy_server* s, long long ticket, double timeout_ms, fy_request_result* res) {
+    fy::enter();
+    if (!s) return fail(FY_EINVAL, "fy_server_wait: null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->tickets.find(ticket);
+    if (it == s->tickets.end()) return fail(FY_EINVAL, "fy_server_wait: unknown ticket %lld", ticket);
+    Ticket* t = it->second;
+    auto ready = [&] { return t->done; };
+    if (timeout_ms < 0) {
+        s->cv_done.wait(lk, ready);
+    } else if (!s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), ready)) {
+        return fail(FY_ETIMEDOUT, "fy_server_wait: ticket %lld not done after %.1f ms", ticket, timeout_ms);
+    }
+    if (res) {
+        res->status = t->status;
+        res->queue_ms = t->t_start > 0 ? t->t_start - t->t_submit : 0.0;
+        res->run_ms = t->t_start > 0 ? t->t_done - t->t_start : 0.0;
+        res->latency_ms = t->t_done - t->t_submit;
+    }
+    const int st = t->status;
+    s->tickets.erase(it);
+    delete t;
+    if (st) return fail(st, "fy_server_wait: request failed with status %d", st);
+    return FY_OK;
+}
+
+extern "C" int fy_server_get_stats(fy_server* s, fy_server_stats* out) {
+    fy::enter();
+    if (!s || !out) return fail(FY_EINVAL, "fy_server_get_stats: null pointer");
+    std::lock_guard<std::mutex> lk(s->mu);
+    out->completed = (long long)s->lat_ms.size();
+    out->voxels = s->voxels;
+    const double span = s->last_done - s->first_start;
+    out->mvox_per_s = span > 0 ? s->voxels / (span * 1e-3) / 1e6 : 0.0;
+    std::vector<double> v = s->lat_ms;
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double q) {            // nearest-rank percentile
+        if (v.empty()) return 0.0;
+        size_t k = (size_t)std::ceil(q / 100.0 * (double)v.size());
+        if (k < 1) k = 1;
+        return v[k - 1];
+    };
+    out->p50_ms = pct(50.0);
+    out->p99_ms = pct(99.0);
+    out->inflight = s->inflight;
+    out->queued = (int)s->queue.size();
+    return FY_OK;
+}
+
+extern "C" void fy_server_reset_stats(fy_server* s) {
+    if (!s) return;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->lat_ms.clear();
+    s->voxels = 0;
+    s->first_start = 0;
+    s->last_done = 0;
+}
+
+extern "C" void fy_server_destroy(fy_server* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    for (auto& w : s->workers) w.join();
+    for (auto& kv : s->tickets) delete kv.second;
+    delete s;
+}

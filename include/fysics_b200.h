@@ -284,6 +284,48 @@ int  fy_gpu_restore_u8(const unsigned char *d_u8, float *d_out, int nz, int ny, 
                        double f32_min, double f32_max, const fy_physics *p,
                        const fy_restore_cfg *cfg, void *stream);
 
+/* Request loop (continuous batching) on one GPU; no reference counterpart. Callers submit
+ * cubes from any thread as they need them. A pool of worker threads, each with its own CUDA
+ * stream and device workspaces, runs the restoration chain of several requests at once, so
+ * their kernels and their host<->device copies overlap on the device. A request is
+ * admitted in arrival order when a worker is free and the estimated device memory of the
+ * requests in flight stays within hbm_budget_bytes; a request larger than the whole budget
+ * is refused at submission. Each result equals the single-cube fy_gpu_restore_u8 call. */
+typedef struct fy_server fy_server;
+typedef struct {
+    size_t hbm_budget_bytes;     /* device memory admitted at once (default 150 GB) */
+    int    workers;              /* requests executing at once (default 4) */
+    int    device;
+} fy_server_cfg;
+typedef struct {
+    const unsigned char *u8;     /* host input, nz*ny*nx (pinned memory avoids a staging copy) */
+    float *out;                  /* host output, nz*ny*nx floats */
+    int    nz, ny, nx;
+    double f32_min, f32_max;     /* dewindow range (fy_u8_to_phys) */
+    fy_physics phys;
+    fy_restore_cfg cfg;          /* dering: a finalised handle, applied only (no accumulation) */
+} fy_request;
+typedef struct {
+    int    status;
+    double queue_ms, run_ms, latency_ms;   /* submit -> start, start -> done, submit -> done */
+} fy_request_result;
+typedef struct {
+    long long completed;
+    double voxels, mvox_per_s;   /* over completed requests, first start to last completion */
+    double p50_ms, p99_ms;       /* nearest-rank latency percentiles, submit -> done */
+    int    inflight, queued;
+} fy_server_stats;
+void fy_server_cfg_default(fy_server_cfg *cfg);
+int  fy_server_create(fy_server **out, const fy_server_cfg *cfg);
+/* The request's buffers must stay valid until fy_server_wait returns for its ticket. */
+int  fy_server_submit(fy_server *s, const fy_request *req, long long *ticket);
+/* timeout_ms < 0 waits without limit; FY_ETIMEDOUT leaves the ticket pending. */
+int  fy_server_wait(fy_server *s, long long ticket, double timeout_ms, fy_request_result *res);
+int  fy_server_get_stats(fy_server *s, fy_server_stats *out);
+void fy_server_reset_stats(fy_server *s);
+/* Finishes running requests, cancels queued ones (FY_EBUSY) and joins the workers. */
+void fy_server_destroy(fy_server *s);
+
 /* Per-kernel timing: CUDA events recorded on the launching stream after every launch of
  * the instrumented kernels. read(i) gives mark i's name and the ms since mark i-1, once
  * the stream has been synchronised. */

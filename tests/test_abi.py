@@ -89,3 +89,14 @@ def test_no_cpu_fallback_without_gpu(fy):
     f = np.full(16, -1.0, np.float32)
     lib.fy_u8_to_phys(u8.ctypes.data, f.ctypes.data, 16, 0.0, 1.0)
     assert lib.fy_gpu_last_status() == fy.FY_ENODEV and (f == -1.0).all()
+
+
+@pytest.mark.skipif(has_cuda(), reason="a GPU is present: the no-device contract is not observable")
+def test_server_refuses_without_gpu(fy):
+    lib = fy.load()
+    h = C.c_void_p(123)
+    cfg = fy.ServerCfg()
+    lib.fy_server_cfg_default(C.byref(cfg))
+    assert cfg.workers == 4 and cfg.hbm_budget_bytes == 150 << 30
+    assert lib.fy_server_create(C.byref(h), C.byref(cfg)) == fy.FY_ENODEV
+    assert h.value is None                                  # no handle, no worker threads
