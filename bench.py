@@ -209,8 +209,156 @@ def cpu_reference_sample(u8_host: np.ndarray, steps: int = 1, crop: int = 128, b
                       f"single-thread latency {t_one * 1e3:.0f} ms per {crop}^3 crop"}
 
 
+# ------------------------------------------------------------------------------ serving
+def _req(fb, u8_pinned, out_pinned, db, span, scale):
+    r = fb.Request()
+    r.u8 = u8_pinned.data_ptr()
+    r.out = out_pinned.data_ptr()
+    r.nz, r.ny, r.nx = u8_pinned.shape
+    r.f32_min, r.f32_max = 0.0, span
+    r.phys = fb.physics(delta_beta=db * scale, energy_kev=110.0, distance_mm=1200.0, pixel_um=2.4,
+                        unsharp_sigma=0.8, unsharp_coeff=0.5, psf_sigma_vox=1.0, psf_sigma_z_vox=1.17)
+    fb.load().fy_restore_cfg_default(C.byref(r.cfg))
+    r.cfg.deconv_kind = 1
+    r.cfg.deconv_param = 0.05
+    r.cfg.noise_win, r.cfg.noise_flat_pct, r.cfg.noise_ref_intensity = 5, 10.0, 0.4
+    r.cfg.guided_radius, r.cfg.guided_s = 2, 1
+    return r
+
+
+def _plain(fb, lib, reqs, dev):
+    """The same requests one at a time through the plain per-cube path: pinned H2D, the
+    chain (fy_gpu_restore_u8), D2H, synchronise; returns Mvox/s over the wall time."""
+    import torch
+    vox = 0
+    d_in = {}
+    d_out = {}
+    t0 = time.perf_counter()
+    for r in reqs:
+        shp = (r.nz, r.ny, r.nx)
+        if shp not in d_in:
+            d_in[shp] = torch.empty(shp, dtype=torch.uint8, device=f"cuda:{dev}")
+            d_out[shp] = torch.empty(shp, dtype=torch.float32, device=f"cuda:{dev}")
+        n = r.nz * r.ny * r.nx
+        src = torch.frombuffer((C.c_uint8 * n).from_address(r.u8), dtype=torch.uint8).view(shp)
+        d_in[shp].copy_(src, non_blocking=True)
+        fb.check(lib.fy_gpu_restore_u8(C.c_void_p(d_in[shp].data_ptr()), C.c_void_p(d_out[shp].data_ptr()),
+                                       r.nz, r.ny, r.nx, r.f32_min, r.f32_max, C.byref(r.phys), C.byref(r.cfg),
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream)), "fy_gpu_restore_u8")
+        dst = torch.frombuffer((C.c_float * n).from_address(r.out), dtype=torch.float32).view(shp)
+        dst.copy_(d_out[shp], non_blocking=True)
+        torch.cuda.synchronize()
+        vox += n
+    return vox / (time.perf_counter() - t0) / 1e6
+
+
+def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rate=500.0, n_batch=24):
+    """Config-5 sample (Poisson arrivals, 64:128:256:512 = 40:30:25:5) through the request
+    loop, and a config-3 sample (uneven cubes, dims per axis from {96..320}) submitted at
+    once; each next to the same requests on the plain per-cube path."""
+    import torch
+    import fysics_b200.phantom as ph
+    rng = np.random.default_rng(seed)
+    scfg = fb.ServerCfg()
+    lib.fy_server_cfg_default(C.byref(scfg))
+    srv = C.c_void_p()
+    fb.check(lib.fy_server_create(C.byref(srv), C.byref(scfg)), "fy_server_create")
+
+    def pinned_phantom(shape, s):
+        u = ph.phantom(shape, seed=s, delta_beta=500.0 * db_scale, pixel_um=2.4, fz2_scale=1.17 ** 2,
+                       device=f"cuda:{dev}")
+        h = torch.empty(shape, dtype=torch.uint8, pin_memory=True)
+        h.copy_(u.cpu())
+        return h
+
+    def run_all(reqs, arrivals=None):
+        lat = [0.0] * len(reqs)
+        tickets = [None] * len(reqs)
+        done = threading.Event()
+
+        def waiter():
+            for i in range(len(reqs)):
+                while tickets[i] is None:
+                    time.sleep(1e-4)
+                res = fb.RequestResult()
+                fb.check(lib.fy_server_wait(srv, tickets[i], -1.0, C.byref(res)), "fy_server_wait")
+                lat[i] = res.latency_ms
+            done.set()
+
+        lib.fy_server_reset_stats(srv)
+        th = threading.Thread(target=waiter)
+        th.start()
+        t0 = time.perf_counter()
+        for i, r in enumerate(reqs):
+            if arrivals is not None:
+                dt = arrivals[i] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+            t = C.c_longlong()
+            fb.check(lib.fy_server_submit(srv, C.byref(r), C.byref(t)), "fy_server_submit")
+            tickets[i] = t.value
+        th.join()
+        wall = time.perf_counter() - t0
+        st = fb.ServerStats()
+        lib.fy_server_get_stats(srv, C.byref(st))
+        return lat, wall, st
+
+    # ---- config-5 sample
+    sizes = [64, 128, 256, 512]
+    src = {s: pinned_phantom((s,) * 3, seed + s) for s in sizes}
+    outs = {s: [torch.empty((s,) * 3, dtype=torch.float32, pin_memory=True) for _ in range(6)] for s in sizes}
+    pick = rng.choice(len(sizes), n_requests, p=[0.40, 0.30, 0.25, 0.05])
+    reqs = []
+    for i, k in enumerate(pick):
+        s = sizes[k]
+        reqs.append(_req(fb, src[s], outs[s][i % 6], rng.uniform(200, 1000), float(rng.uniform(0.9, 1.1)), db_scale))
+    run_all([_req(fb, src[s], outs[s][0], 500.0, 1.0, db_scale) for s in sizes])          # warm-up
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    lat, wall, st = run_all(reqs, arrivals)
+    vox = sum(r.nz * r.ny * r.nx for r in reqs)
+    by = {}
+    for r, l in zip(reqs, lat):
+        by.setdefault(r.nz, []).append(l)
+    plain = _plain(fb, lib, reqs[: min(len(reqs), 120)], dev)
+    served = {
+        "workload": f"{n_requests} requests, Poisson arrivals at {rate:.0f}/s, sizes 64^3:128^3:256^3:512^3 = "
+                    "40:30:25:5, per-request delta_beta U[200,1000] and window span U[0.9,1.1]; host pinned "
+                    "buffers, H2D + chain + D2H per request",
+        "workers": scfg.workers, "hbm_budget_gb": scfg.hbm_budget_bytes / 2 ** 30,
+        "mvox_per_s": vox / wall / 1e6,
+        "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+        "p50_ms_by_size": {f"{k}^3": float(np.percentile(v, 50)) for k, v in sorted(by.items())},
+        "p99_ms_by_size": {f"{k}^3": float(np.percentile(v, 99)) for k, v in sorted(by.items())},
+        "plain_mvox_per_s": plain,
+        "plain": "the first 120 requests one at a time: pinned H2D, fy_gpu_restore_u8, D2H, synchronise",
+    }
+    # ---- config-3 sample: uneven cubes submitted at once
+    dims = [96, 128, 160, 200, 240, 256, 320]
+    bre = []
+    keep = []
+    for i in range(n_batch):
+        shape = tuple(int(d) for d in rng.choice(dims, 3))
+        h = pinned_phantom(shape, seed + 1000 + i)
+        o = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+        keep += [h, o]
+        bre.append(_req(fb, h, o, rng.uniform(200, 1000), 1.0, db_scale))
+    run_all(bre[:4])                                                                       # warm-up
+    _, bwall, _ = run_all(bre)
+    bvox = sum(r.nz * r.ny * r.nx for r in bre)
+    batched = {
+        "workload": f"{n_batch} cubes, dims per axis from {dims}, per-cube delta_beta U[200,1000], submitted "
+                    "at once to the request loop; host pinned buffers",
+        "mvox_per_s": bvox / bwall / 1e6,
+        "plain_mvox_per_s": _plain(fb, lib, bre, dev),
+    }
+    lib.fy_server_destroy(srv)
+    return served, batched
+
+
 # ------------------------------------------------------------------------------ main
-def dist_setup(n_gpus: int):
+def dist_setup(n_gpus: int, backend: str = "nccl"):
+    """One process per GPU (torchrun env). Replicas only: the only collectives are the
+    barrier and the max over ranks of the timed regions."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if world <= 1:
         return 0, 1, 0, None
@@ -218,10 +366,26 @@ def dist_setup(n_gpus: int):
     import torch.distributed as dist
     rank = int(os.environ["RANK"])
     local = int(os.environ.get("LOCAL_RANK", rank))
-    torch.cuda.set_device(local)
+    if backend == "nccl":
+        torch.cuda.set_device(local)
     import datetime
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return rank, world, local, dist
+
+
+def max_over_ranks(value: float, dist, device=None) -> float:
+    """The job's time is the slowest rank's (max over ranks); identity on one process."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mvox_per_s(world: int, vox_per_rank: int, steps: int, total_ms: float) -> float:
+    """Whole-job throughput: every rank processes its own cubes (weak scaling)."""
+    return world * vox_per_rank * steps / (total_ms * 1e-3) / 1e6
 
 
 def run_reference(args, rank, world):
@@ -262,6 +426,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--cpu-phantom", action="store_true")
     ap.add_argument("--size", type=int, default=512, help="cube edge (512 = the benchmark workload)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served / batched samples")
     args = ap.parse_args()
     global SHAPE, WORKLOAD
     if args.size != 512:
@@ -329,13 +494,9 @@ def main():
     launches = lib.fy_gpu_kernel_launches() - launches0
     prof = read_profile(lib)
     per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
-    total_ms = ev[0].elapsed_time(ev[args.steps])
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(ev[0].elapsed_time(ev[args.steps]), dist, f"cuda:{dev}")
     ms_step = total_ms / args.steps
-    value = world * n * args.steps / (total_ms * 1e-3) / 1e6
+    value = job_mvox_per_s(world, n, args.steps, total_ms)
 
     # ---- end to end through pinned host buffers
     h_in = torch.empty(SHAPE, dtype=torch.uint8, pin_memory=True)
@@ -355,12 +516,8 @@ def main():
     stream.synchronize()
     barrier()
     e2e_steps_ms = [ee[k].elapsed_time(ee[k + 1]) for k in range(e2e_steps)]
-    e2e_ms = ee[0].elapsed_time(ee[e2e_steps])
-    if dist:
-        t = torch.tensor([e2e_ms], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * n * e2e_steps / (e2e_ms * 1e-3) / 1e6
+    e2e_ms = max_over_ranks(ee[0].elapsed_time(ee[e2e_steps]), dist, f"cuda:{dev}")
+    e2e_value = job_mvox_per_s(world, n, e2e_steps, e2e_ms)
 
     # ---- roofline of the dominant kernel (live event timings above)
     peaks = {}
@@ -394,6 +551,13 @@ def main():
         except Exception as exc:       # the baseline is reported, never required
             cpu = {"value": None, "error": str(exc)[:200]}
 
+    served = batched = None
+    if not args.no_serve:
+        try:
+            served, batched = served_and_batched(fb, lib, dev, args.seed + 17 * rank, db_scale)
+        except Exception as exc:      # reported, never required
+            served = {"error": str(exc)[:300]}
+
     lat = sorted(per_step)
     line = {
         "metric": METRIC, "value": value, "unit": "Mvoxel/s", "n_gpus": world, "steps": args.steps,
@@ -411,6 +575,8 @@ def main():
         "kernels": kernels,
         "clocks": clock,
         "cpu_baseline": cpu,
+        "served": served,
+        "batched": batched,
     }
     lib.fy_gpu_dering_destroy(h)
     if rank == 0:
