@@ -498,25 +498,54 @@ def main():
     ms_step = total_ms / args.steps
     value = job_mvox_per_s(world, n, args.steps, total_ms)
 
-    # ---- end to end through pinned host buffers
+    # ---- end to end through pinned host buffers: the same chain through the public call,
+    # each cube's H2D and D2H inside the timed region. Two stream slots alternate (own
+    # buffers and ring handle each), so one cube's copies overlap the neighbouring cube's
+    # kernels; the chains themselves serialise on the thread's workspaces.
     h_in = torch.empty(SHAPE, dtype=torch.uint8, pin_memory=True)
     h_in.copy_(u8.cpu())
-    h_out = torch.empty(SHAPE, dtype=torch.float32, pin_memory=True)
-    d_in = torch.empty_like(u8)
-    e2e_steps = max(3, min(args.steps, 10))
-    ee = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps + 1)]
+    slots = []
+    for _ in range(2):
+        hs = C.c_void_p()
+        fb.check(lib.fy_gpu_dering_create(C.byref(hs), nz, ny, nx, -1.0, -1.0, 512, 8), "fy_gpu_dering_create")
+        slots.append({"st": torch.cuda.Stream(device=dev), "d_in": torch.empty_like(u8), "d_out": torch.empty_like(out),
+                      "h_out": torch.empty(SHAPE, dtype=torch.float32, pin_memory=True), "ring": hs,
+                      "cfg": restore_cfg(fb, hs)})
+    e2e_steps = max(4, min(args.steps, 10))
+    ev_a = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+    ev_b = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+
+    def e2e_cube(k):
+        sl = slots[k % 2]
+        st_ = sl["st"]
+        spk = C.c_void_p(st_.cuda_stream)
+        with torch.cuda.stream(st_):
+            ev_a[k].record(st_)
+            sl["d_in"].copy_(h_in, non_blocking=True)
+            fb.check(lib.fy_gpu_dering_reset(sl["ring"], spk), "fy_gpu_dering_reset")
+            fb.check(lib.fy_gpu_restore_u8(C.c_void_p(sl["d_in"].data_ptr()), C.c_void_p(sl["d_out"].data_ptr()),
+                                           nz, ny, nx, 0.0, 1.0, C.byref(p), C.byref(sl["cfg"]), spk),
+                     "fy_gpu_restore_u8")
+            sl["h_out"].copy_(sl["d_out"], non_blocking=True)
+            ev_b[k].record(st_)
+
+    for k in range(2):                                   # warm the second slot's buffers
+        e2e_cube(k)
+    torch.cuda.synchronize()
     barrier()
-    with torch.cuda.stream(stream):
-        ee[0].record(stream)
-        for k in range(e2e_steps):
-            d_in.copy_(h_in, non_blocking=True)
-            step(C.c_void_p(d_in.data_ptr()), C.c_void_p(out.data_ptr()))
-            h_out.copy_(out, non_blocking=True)
-            ee[k + 1].record(stream)
-    stream.synchronize()
+    t_e2e = time.perf_counter()
+    for k in range(e2e_steps):
+        if k >= 2:
+            ev_b[k - 2].synchronize()                    # the slot's previous cube is out
+        e2e_cube(k)
+    torch.cuda.synchronize()
     barrier()
-    e2e_steps_ms = [ee[k].elapsed_time(ee[k + 1]) for k in range(e2e_steps)]
-    e2e_ms = max_over_ranks(ee[0].elapsed_time(ee[e2e_steps]), dist, f"cuda:{dev}")
+    e2e_wall_ms = (time.perf_counter() - t_e2e) * 1e3
+    e2e_steps_ms = [ev_a[k].elapsed_time(ev_b[k]) for k in range(e2e_steps)]
+    e2e_dev_ms = ev_a[0].elapsed_time(ev_b[e2e_steps - 1])
+    for sl in slots:
+        lib.fy_gpu_dering_destroy(sl["ring"])
+    e2e_ms = max_over_ranks(max(e2e_dev_ms, e2e_wall_ms), dist, f"cuda:{dev}")
     e2e_value = job_mvox_per_s(world, n, e2e_steps, e2e_ms)
 
     # ---- roofline of the dominant kernel (live event timings above)
