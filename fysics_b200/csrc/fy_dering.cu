@@ -18,11 +18,8 @@
 namespace {
 
 // ---------------------------------------------------------------- accumulate
-// Grid: (x tiles, sampled rows * dz). Each thread takes 8 consecutive samples of a row and
-// merges runs that fall in the same (sector, radius) bin in registers, so neighbouring
-// samples (mostly one bin) cost one shared atomic per run. Shared-memory histograms when
-// the bin count fits, else global atomics.
-constexpr int ACC_K = 8;
+// Grid: (x tiles of 256 samples, sampled rows * dz). Shared-memory histograms when the
+// bin count fits, else global atomics.
 template <bool SMEM>
 __global__ void __launch_bounds__(256) k_dering_accum(const uint8_t* __restrict__ buf, const int* __restrict__ map,
                                                       unsigned long long* __restrict__ gsum,
@@ -36,33 +33,19 @@ __global__ void __launch_bounds__(256) k_dering_accum(const uint8_t* __restrict_
         for (int i = threadIdx.x; i < 2 * nbins; i += blockDim.x) sh[i] = 0;
         __syncthreads();
     }
-    auto flush = [&](int b, unsigned s_, unsigned c_) {
-        if (b < 0 || !c_) return;
-        if (SMEM) { atomicAdd(&ssum[b], s_); atomicAdd(&scnt[b], c_); }
-        else { atomicAdd(&gsum[b], (unsigned long long)s_); atomicAdd(&gcnt[b], c_); }
-    };
     const long nrows = dz * sy;
     const long r0 = (long)blockIdx.y * rows_per_cta;
     for (long rr = r0; rr < r0 + rows_per_cta && rr < nrows; ++rr) {
         const long z = rr / sy, yi = rr - z * sy;
         const uint8_t* row = buf + ((size_t)z * dy + (size_t)(yi * ss)) * dx;
         const int* mrow = map + yi * sx;
-        for (long xb = ((long)blockIdx.x * blockDim.x + threadIdx.x) * ACC_K; xb < sx;
-             xb += (long)gridDim.x * blockDim.x * ACC_K) {
-            int cur = -1;
-            unsigned s_ = 0, c_ = 0;
-#pragma unroll
-            for (int j = 0; j < ACC_K; ++j) {
-                const long xi = xb + j;
-                if (xi >= sx) break;
-                const unsigned v = __ldg(row + xi * ss);
-                if (!v) continue;                               // masked voxels skipped
-                const int b = __ldg(mrow + xi);
-                if (b < 0) continue;
-                if (b != cur) { flush(cur, s_, c_); cur = b; s_ = 0; c_ = 0; }
-                s_ += v; ++c_;
-            }
-            flush(cur, s_, c_);
+        for (long xi = (long)blockIdx.x * blockDim.x + threadIdx.x; xi < sx; xi += (long)gridDim.x * blockDim.x) {
+            const unsigned v = __ldg(row + xi * ss);
+            if (!v) continue;                                   // masked voxels skipped
+            const int b = __ldg(mrow + xi);
+            if (b < 0) continue;
+            if (SMEM) { atomicAdd(&ssum[b], v); atomicAdd(&scnt[b], 1u); }
+            else { atomicAdd(&gsum[b], (unsigned long long)v); atomicAdd(&gcnt[b], 1u); }
         }
     }
     if (SMEM) {
@@ -117,16 +100,41 @@ __global__ void __launch_bounds__(256) k_dering_smooth(const float* __restrict__
         else atomicMin(&s_first, r);
     }
     __syncthreads();
-    if (threadIdx.x == 0 && s_first < nr) {           // rare: sequential from the first change
-        for (int r = s_first; r < nr; ++r) {
-            if (!svd[r]) { shp[r] = 0.0f; continue; }
-            double acc = 0;
-            int c = 0;
-            const int lo = r - hw < 0 ? 0 : r - hw, hi = r + hw >= nr ? nr - 1 : r + hw;
-            for (int j = lo; j <= hi; ++j)
-                if (svd[j]) { acc += sp[j]; ++c; }
-            if (c >= hw) shp[r] = sp[r] - (float)(acc / c);
-            else { shp[r] = 0.0f; svd[r] = 0; }
+    if (threadIdx.x == 0 && s_first < nr) {           // sequential from the first change
+        if (hw <= 8) {
+            // the window's values are loaded together (independent loads), then summed in
+            // the reference's order (ascending j)
+            for (int r = s_first; r < nr; ++r) {
+                if (!svd[r]) { shp[r] = 0.0f; continue; }
+                const int lo = r - hw < 0 ? 0 : r - hw, hi = r + hw >= nr ? nr - 1 : r + hw;
+                float wv[17];
+                unsigned char wk[17];
+#pragma unroll
+                for (int q = 0; q < 17; ++q) {
+                    const int j = lo + q;
+                    const bool in = j <= hi;
+                    wv[q] = in ? sp[j] : 0.0f;
+                    wk[q] = in ? svd[j] : 0;
+                }
+                double acc = 0;
+                int c = 0;
+#pragma unroll
+                for (int q = 0; q < 17; ++q)
+                    if (wk[q]) { acc += wv[q]; ++c; }
+                if (c >= hw) shp[r] = sp[r] - (float)(acc / c);
+                else { shp[r] = 0.0f; svd[r] = 0; }
+            }
+        } else {
+            for (int r = s_first; r < nr; ++r) {
+                if (!svd[r]) { shp[r] = 0.0f; continue; }
+                double acc = 0;
+                int c = 0;
+                const int lo = r - hw < 0 ? 0 : r - hw, hi = r + hw >= nr ? nr - 1 : r + hw;
+                for (int j = lo; j <= hi; ++j)
+                    if (svd[j]) { acc += sp[j]; ++c; }
+                if (c >= hw) shp[r] = sp[r] - (float)(acc / c);
+                else { shp[r] = 0.0f; svd[r] = 0; }
+            }
         }
     }
     __syncthreads();
@@ -215,8 +223,7 @@ cudaError_t fy_launch_dering_accum(const uint8_t* buf, const int* map, unsigned 
     const long sy = (dy + ss - 1) / ss, sx = (dx + ss - 1) / ss;
     const long nrows = dz * sy;
     if (nrows <= 0 || sx <= 0) return cudaSuccess;
-    const long xt = (sx + 256 * ACC_K - 1) / (256 * ACC_K);
-    const int gx = (int)(xt < 4 ? xt : 4);
+    const int gx = (int)((sx + 255) / 256 < 4 ? (sx + 255) / 256 : 4);
     long want_ctas = (long)sms * 8 / gx;
     if (want_ctas < 1) want_ctas = 1;
     int rows_per_cta = (int)((nrows + want_ctas - 1) / want_ctas);

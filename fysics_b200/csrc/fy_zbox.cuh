@@ -149,6 +149,8 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     // GUIDED_OUT: ring radius of this thread's 4 output voxels (dering.c:200-248)
     bool rings = false;
     int ri[4] = {0, 0, 0, 0};
+    float rv[4] = {0.f, 0.f, 0.f, 0.f};                           // ring values of the cached slab
+    long rslab = -1;
     if (KIND == ZB_GUIDED_OUT && p.out_mode == 0 && p.ra.ring) {
         rings = p.ra.have ? (*p.ra.have != 0) : true;
         const double gxd = (double)(p.ra.x0 + gx) - p.ra.cx;
@@ -252,6 +254,17 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                 }
             }
             if (!emit) continue;
+            if (KIND == ZB_GUIDED_OUT && rings) {                // this plane's ring slab (dering.c:212-215)
+                long sl = (p.ra.z0 + zo) / p.ra.slab_z;
+                if (sl < 0) sl = 0;
+                if (sl >= p.ra.nslab) sl = p.ra.nslab - 1;
+                if (sl != rslab) {
+                    rslab = sl;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        rv[k] = ri[k] < p.ra.nr ? __ldg(p.ra.ring + (size_t)sl * p.ra.nr + ri[k]) : 0.f;
+                }
+            }
             const float rz = KIND == ZB_NOISE ? 0.f : recip_count(zo, nz, R);
             const int cz = min(zo + R, nz - 1) - max(zo - R, 0) + 1;
 #pragma unroll
@@ -289,10 +302,7 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                     if (p.out_mode == 0) {
                         float w = ma * gv[k] + mb;
                         if (rings && w > 0.f && ri[k] < p.ra.nr) {     // masked voxels untouched
-                            long sl = (p.ra.z0 + zo) / p.ra.slab_z;
-                            if (sl < 0) sl = 0;
-                            if (sl >= p.ra.nslab) sl = p.ra.nslab - 1;
-                            const float w2 = w - p.ra.sc * __ldg(p.ra.ring + (size_t)sl * p.ra.nr + ri[k]);
+                            const float w2 = w - p.ra.sc * rv[k];
                             w = w2 > 0.f ? w2 : 0.f;
                         }
                         p.o0[o] = w;
