@@ -116,37 +116,6 @@ struct RunAcc {
 // loop run without per-element range checks; the one partial chunk is checked.
 constexpr int SU = 4;
 
-// u8 bin id per voxel (255 = no bin). Per-bin counts come from the first variance digit
-// pass, whose histogram covers every voxel of every bin (k_bin_targets).
-__global__ void __launch_bounds__(256) k_bin_assign(const float* __restrict__ mean, uint8_t* __restrict__ bin,
-                                                    NoiseCtl* __restrict__ ctl) {
-    __shared__ float fe[NB + 1];
-    if (threadIdx.x <= NB) fe[threadIdx.x] = ctl->fedge[threadIdx.x];
-    __syncthreads();
-    const float lo_f = ctl->fedge[0], scale = ctl->fscale;
-    const long long n = ctl->n, n4 = (n + 3) / 4, n4f = n / 4;
-    const int step = blockDim.x;
-    const long long chunk = (long long)SU * step;
-    auto lab = [&](float m) -> unsigned { const int b = bin_of(m, fe, lo_f, scale); return b < 0 ? 255u : (unsigned)b; };
-    long long base = (long long)blockIdx.x * chunk;
-    for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
-        float4 x[SU];
-#pragma unroll
-        for (int u = 0; u < SU; ++u) x[u] = __ldg(reinterpret_cast<const float4*>(mean) + base + threadIdx.x + (long long)u * step);
-#pragma unroll
-        for (int u = 0; u < SU; ++u)
-            reinterpret_cast<uchar4*>(bin)[base + threadIdx.x + (long long)u * step] =
-                make_uchar4(lab(x[u].x), lab(x[u].y), lab(x[u].z), lab(x[u].w));
-    }
-    if (base < n4) {                                     // the grid's partial chunk
-        for (int u = 0; u < SU; ++u)
-            for (int j = 0; j < 4; ++j) {
-                const long long i = 4 * (base + threadIdx.x + (long long)u * step) + j;
-                if (i < n) bin[i] = (uint8_t)lab(__ldg(mean + i));
-            }
-    }
-}
-
 // One digit pass (bits [shift, shift + DB)) for every active target whose prefix matches.
 // MODE 0: keys of mean, targets 0 and 1 over all voxels; MODE 1: keys of var, target = bin;
 // MODE 2: keys of var, target 0 over all voxels. A key matches at most one distinct prefix,
@@ -154,13 +123,19 @@ __global__ void __launch_bounds__(256) k_bin_assign(const float* __restrict__ me
 // (group) and every voxel makes at most one increment; the flush copies a group's counts
 // to each of its targets. Inactive targets and bin label 255 carry the prefix 0xffffffff,
 // which no key's high part (< 2^(32 - shift - DB)) can equal.
-template <int DB, int MODE>
+// LABEL (the first variance pass only): the bin of each voxel is computed from its mean here
+// and its u8 label written for the later passes, so no separate labelling pass runs.
+template <int DB, int MODE, bool LABEL = false>
 __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean, const float* __restrict__ var,
-                                                  const uint8_t* __restrict__ bin, NoiseCtl* __restrict__ ctl,
+                                                  uint8_t* __restrict__ bin, NoiseCtl* __restrict__ ctl,
                                                   int shift) {
     extern __shared__ unsigned int h[];
     __shared__ uint32_t sp[256];
+    __shared__ float fe[NB + 1];
     if (ctl->mode != MODE) return;
+    if (LABEL && threadIdx.x <= NB) fe[threadIdx.x] = ctl->fedge[threadIdx.x];
+    const float lo_f = LABEL ? ctl->fedge[0] : 0.f, fscale = LABEL ? ctl->fscale : 0.f;
+    auto lab = [&](float m) -> unsigned { const int b = bin_of(m, fe, lo_f, fscale); return b < 0 ? 255u : (unsigned)b; };
     constexpr int NBK = 1 << DB;
     const int nt = ctl->ntarget;
     if (MODE == 1)
@@ -195,11 +170,20 @@ __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean
     for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
         float4 x[SU];
         uchar4 bb[SU];
+        float4 mm[LABEL ? SU : 1];
 #pragma unroll
         for (int u = 0; u < SU; ++u) {
             const long long q = base + threadIdx.x + (long long)u * step;
             x[u] = __ldg(reinterpret_cast<const float4*>(src) + q);
-            if (MODE == 1) bb[u] = __ldg(reinterpret_cast<const uchar4*>(bin) + q);
+            if (LABEL) mm[u] = __ldg(reinterpret_cast<const float4*>(mean) + q);
+            else if (MODE == 1) bb[u] = __ldg(reinterpret_cast<const uchar4*>(bin) + q);
+        }
+        if (LABEL) {
+#pragma unroll
+            for (int u = 0; u < SU; ++u) {
+                bb[u] = make_uchar4(lab(mm[u].x), lab(mm[u].y), lab(mm[u].z), lab(mm[u].w));
+                reinterpret_cast<uchar4*>(bin)[base + threadIdx.x + (long long)u * step] = bb[u];
+            }
         }
 #pragma unroll
         for (int u = 0; u < SU; ++u) {
@@ -213,7 +197,11 @@ __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean
         for (int u = 0; u < SU; ++u)
             for (int j = 0; j < 4; ++j) {
                 const long long i = 4 * (base + threadIdx.x + (long long)u * step) + j;
-                if (i < n) acc.add(h, code_of(__ldg(src + i), MODE == 1 ? (int)__ldg(bin + i) : 0));
+                if (i >= n) continue;
+                int g = 0;
+                if (LABEL) { g = (int)lab(__ldg(mean + i)); bin[i] = (uint8_t)g; }
+                else if (MODE == 1) g = (int)__ldg(bin + i);
+                acc.add(h, code_of(__ldg(src + i), g));
             }
     }
     acc.flush(h);
@@ -556,12 +544,12 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     }
     k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 0);
     k_noise_bins_setup<<<1, 1, 0, st>>>(ctl);
-    k_bin_assign<<<g, 256, 0, st>>>(mean, bin, ctl);
-    fy_prof_mark(st, "noise.lohi+bins");
+    fy_prof_mark(st, "noise.lohi");
     // 2b. per-bin flat_pct percentile of the variance: 4 x 8 bits, then the k+1 neighbours;
-    // the first pass also yields the bin counts
+    // the first pass also labels the voxels with their bins and yields the bin counts
     for (int sh = 24; sh >= 0; sh -= 8) {
-        k_sel_hist<8, 1><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, sh);
+        if (sh == 24) k_sel_hist<8, 1, true><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, sh);
+        else k_sel_hist<8, 1><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, sh);
         if (sh == 24) k_bin_targets<<<NB, 256, 0, st>>>(ctl);
         k_sel_scan<<<NB, 256, 0, st>>>(ctl, 8, 1, sh == 0);
     }
@@ -576,7 +564,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     }
     k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 2);
     k_noise_fit<<<1, 1, 0, st>>>(ctl, 1);
-    launches += 1 + 1 + 6 + 1 + 1 + 1 + 1 + 8 + 1 + 1 + 6 + 1 + 1;
+    launches += 1 + 1 + 6 + 1 + 1 + 1 + 8 + 1 + 1 + 6 + 1 + 1;
     return cudaGetLastError();
 }
 
