@@ -2,7 +2,7 @@
 //
 // A viewer or exporter issues cubes as they are needed, from many threads, with sizes and
 // per-volume metadata that vary request by request. The server keeps a FIFO of submitted
-// requests and a pool of worker threads. Each worker owns a CUDA stream and its own
+// requests and a pool of worker threads. Each worker owns CUDA streams and its own
 // device workspaces (the per-thread context of the C-ABI), so the chains of different
 // requests run concurrently on the GPU, and one request's host<->device copies overlap
 // other requests' kernels. A request is admitted when a worker is free and the estimated
@@ -46,11 +46,26 @@ struct Ticket {
     bool done = false;
 };
 
-// Worker-owned device and pinned buffers (grow-only).
+// Worker-owned device and pinned buffers (grow-only) and two streams: requests up to
+// priority_voxels run on the high-priority one, so the GPU's block scheduler serves their
+// kernels ahead of a large request's.
 struct WorkerBufs {
     fy::DevBuf d_in, d_out;
     fy::HostBuf h_in, h_out;
+    cudaStream_t hi = nullptr, lo = nullptr;
 };
+
+// Large copies go in chunks, so other requests' copies interleave with them on the link
+// instead of waiting behind one long transfer.
+constexpr size_t kCopyChunk = (size_t)32 << 20;
+cudaError_t copy_chunked(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st) {
+    for (size_t off = 0; off < bytes; off += kCopyChunk) {
+        const size_t len = bytes - off < kCopyChunk ? bytes - off : kCopyChunk;
+        const cudaError_t e = cudaMemcpyAsync((char*)dst + off, (const char*)src + off, len, kind, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
 
 }  // namespace
 
@@ -89,8 +104,7 @@ size_t footprint_of(const fy_request& r) {
 void run_one(fy_server* s, Ticket* t, WorkerBufs& wb) {
     const fy_request& r = t->req;
     const size_t n = (size_t)r.nz * r.ny * r.nx;
-    fy::ThreadCtx& c = ctx();
-    cudaStream_t st = c.st;
+    cudaStream_t st = n <= s->cfg.priority_voxels ? wb.hi : wb.lo;
     cudaError_t e;
     int rc = FY_OK;
     const bool in_pinned = fy::is_pinned(r.u8), out_pinned = fy::is_pinned(r.out);
@@ -105,7 +119,7 @@ void run_one(fy_server* s, Ticket* t, WorkerBufs& wb) {
             memcpy(wb.h_in.p, r.u8, n);
             src = (const unsigned char*)wb.h_in.p;
         }
-        if ((e = cudaMemcpyAsync(wb.d_in.p, src, n, cudaMemcpyHostToDevice, st)) != cudaSuccess) {
+        if ((e = copy_chunked(wb.d_in.p, src, n, cudaMemcpyHostToDevice, st)) != cudaSuccess) {
             rc = fail_cuda(e, "fy_server");
             break;
         }
@@ -117,7 +131,7 @@ void run_one(fy_server* s, Ticket* t, WorkerBufs& wb) {
             if ((e = wb.h_out.ensure(4 * n)) != cudaSuccess) { rc = fail_cuda(e, "fy_server"); break; }
             dst = (float*)wb.h_out.p;
         }
-        if ((e = cudaMemcpyAsync(dst, wb.d_out.p, 4 * n, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        if ((e = copy_chunked(dst, wb.d_out.p, 4 * n, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
             (e = cudaStreamSynchronize(st)) != cudaSuccess) {
             rc = fail_cuda(e, "fy_server");
             break;
@@ -147,6 +161,15 @@ void worker_main(fy_server* s, int idx) {
     }
     WorkerBufs wb;
     (void)idx;
+    int prio_lo = 0, prio_hi = 0;
+    if (!rc0) {
+        cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);      // (least, greatest)
+        if (cudaStreamCreateWithPriority(&wb.hi, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+            cudaStreamCreateWithPriority(&wb.lo, cudaStreamNonBlocking, prio_lo) != cudaSuccess) {
+            cudaGetLastError();
+            wb.hi = wb.lo = ctx().st;
+        }
+    }
     for (;;) {
         Ticket* t = nullptr;
         {
@@ -188,6 +211,8 @@ void worker_main(fy_server* s, int idx) {
         }
         run_one(s, t, wb);
     }
+    if (wb.hi && wb.hi != ctx().st) cudaStreamDestroy(wb.hi);
+    if (wb.lo && wb.lo != ctx().st) cudaStreamDestroy(wb.lo);
     wb.d_in.release();
     wb.d_out.release();
     wb.h_in.release();
@@ -201,6 +226,7 @@ extern "C" void fy_server_cfg_default(fy_server_cfg* c) {
     c->hbm_budget_bytes = (size_t)150 << 30;    // 150 GB
     c->workers = 4;
     c->device = 0;
+    c->priority_voxels = (size_t)256 * 256 * 256;
 }
 
 extern "C" int fy_server_create(fy_server** out, const fy_server_cfg* cfg) {

@@ -296,6 +296,9 @@ typedef struct {
     size_t hbm_budget_bytes;     /* device memory admitted at once (default 150 GB) */
     int    workers;              /* requests executing at once (default 4) */
     int    device;
+    size_t priority_voxels;      /* requests up to this size run on high-priority streams
+                                    (default 256^3), so small cubes keep low latency beside
+                                    large ones; copies move in 32 MB chunks for the same reason */
 } fy_server_cfg;
 typedef struct {
     const unsigned char *u8;     /* host input, nz*ny*nx (pinned memory avoids a staging copy) */
