@@ -46,6 +46,16 @@ struct Lane {
 // line-strided accesses). Each thread loads the same VEC-wide chunk of both rows of a line
 // pair, so it writes VEC consecutive complex values; reflect padding is filled from the
 // staged line afterwards.
+// Half-spectrum row offsets of the 2W rows (two per line) of a row tile, computed once per
+// CTA: row q = z*ny + y sits at (z*py + y)*hxp; -1 past the last row.
+FY_D void row_offsets(long long* off, long q0, int W, long Q, const SpecGeom& g) {
+    for (int i = threadIdx.x; i < 2 * W; i += blockDim.x) {
+        const long q = q0 + i;
+        const int qi = (int)q;                          // nz*ny < 2^31 (each padded axis <= 4096)
+        off[i] = q < Q ? ((long long)(qi / g.ny) * g.py + (qi % g.ny)) * g.hxp : -1;
+    }
+}
+
 template <class T, int VEC> struct VecLoad;
 template <> struct VecLoad<float, 4> {
     static FY_D void run(const float* p, float* v) {
@@ -73,9 +83,11 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(const T* __restrict__ sr
     const int W = 1 << wlog, LPX = g.px + 1;
     float2* s = reinterpret_cast<float2*>(smem4);
     float2* stw = s + W * LPX;
+    __shared__ long long soff[2 * 16];
     const long Q = (long)g.nz * g.ny;
     const long q0 = (long)blockIdx.x * 2 * W;
     load_twiddles(stw, tw, pl.n);
+    row_offsets(soff, q0, W, Q, g);
     const int nch = g.nx / VEC;
     for (int it = threadIdx.x; it < W * nch; it += blockDim.x) {
         const int l = dchunk.div(it), x = (it - l * nch) * VEC;
@@ -113,13 +125,13 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(const T* __restrict__ sr
     __syncthreads();
     for (int idx = threadIdx.x; idx < W * g.hx; idx += blockDim.x) {
         const int l = dhx.div(idx), k = idx - l * g.hx;
-        const long qa = q0 + 2 * l, qb = qa + 1;
-        if (qa >= Q) continue;
+        const long long oa = soff[2 * l], ob = soff[2 * l + 1];
+        if (oa < 0) continue;
         const int mk = k == 0 ? 0 : g.px - k;
         float2 A, B;
         untangle(s[l * LPX + k], s[l * LPX + mk], A, B);
-        spec[((size_t)(qa / g.ny) * g.py + (qa % g.ny)) * g.hxp + k] = A;
-        if (qb < Q) spec[((size_t)(qb / g.ny) * g.py + (qb % g.ny)) * g.hxp + k] = B;
+        spec[oa + k] = A;
+        if (ob >= 0) spec[ob + k] = B;
     }
 }
 
@@ -225,15 +237,18 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_inv(const float2* __restrict
     const int W = 1 << wlog, LPX = g.px + 1;
     float2* s = reinterpret_cast<float2*>(smem4);
     float2* stw = s + W * LPX;
+    __shared__ long long soff[2 * 16];
     const long Q = (long)g.nz * g.ny;
     const long q0 = (long)blockIdx.x * 2 * W;
     load_twiddles(stw, tw, pl.n);
+    row_offsets(soff, q0, W, Q, g);
+    __syncthreads();
     const int hi_max = g.px - g.hx;                 // m in [1, px-hx] mirrors to px-m
     for (int idx = threadIdx.x; idx < W * g.hx; idx += blockDim.x) {
         const int l = dhx.div(idx), k = idx - l * g.hx;
-        const long qa = q0 + 2 * l, qb = qa + 1;
-        const float2 A = qa < Q ? spec[((size_t)(qa / g.ny) * g.py + (qa % g.ny)) * g.hxp + k] : make_float2(0.f, 0.f);
-        const float2 B = qb < Q ? spec[((size_t)(qb / g.ny) * g.py + (qb % g.ny)) * g.hxp + k] : make_float2(0.f, 0.f);
+        const long long oa = soff[2 * l], ob = soff[2 * l + 1];
+        const float2 A = oa >= 0 ? spec[oa + k] : make_float2(0.f, 0.f);
+        const float2 B = ob >= 0 ? spec[ob + k] : make_float2(0.f, 0.f);
         s[l * LPX + k] = pack_lo(A, B);
         if (k >= 1 && k <= hi_max) s[l * LPX + g.px - k] = pack_hi(A, B);
     }
