@@ -6,8 +6,10 @@
 // device workspaces (the per-thread context of the C-ABI), so the chains of different
 // requests run concurrently on the GPU, and one request's host<->device copies overlap
 // other requests' kernels. A request is admitted when a worker is free and the estimated
-// device footprint of everything in flight stays within the HBM budget; the head of the
-// queue waits rather than being overtaken, so no request starves. Each request's result is
+// device footprint of everything in flight stays within the HBM budget. General workers take
+// the head of the queue, which is never overtaken by them, so no request starves; a few
+// reserved workers take the first small request instead, so small cubes do not wait for a
+// worker behind large ones. Each request's result is
 // the same as the single-cube fy_gpu_restore_u8 call on its own: the kernels are
 // deterministic and a worker's workspaces are private to the request it runs.
 #include <algorithm>
@@ -174,11 +176,29 @@ void worker_main(fy_server* s, int idx) {
         Ticket* t = nullptr;
         {
             std::unique_lock<std::mutex> lk(s->mu);
+            // Workers [0, small_workers) take only requests up to priority_voxels: the first
+            // such request in the queue, so small cubes never wait behind large ones for a
+            // worker. The others take the head of the queue.
+            const bool small_only = idx < s->cfg.small_workers;
+            auto fits = [&](const Ticket* q) {
+                return s->inflight == 0 || s->inflight_bytes + q->footprint <= s->cfg.hbm_budget_bytes;
+            };
+            auto pick = [&]() -> std::deque<Ticket*>::iterator {
+                if (!small_only) {
+                    auto it = s->queue.begin();
+                    return it != s->queue.end() && fits(*it) ? it : s->queue.end();
+                }
+                for (auto it = s->queue.begin(); it != s->queue.end(); ++it) {
+                    const fy_request& r = (*it)->req;
+                    if ((size_t)r.nz * r.ny * r.nx <= s->cfg.priority_voxels) return fits(*it) ? it : s->queue.end();
+                }
+                return s->queue.end();
+            };
+            std::deque<Ticket*>::iterator chosen = s->queue.end();
             s->cv_work.wait(lk, [&] {
                 if (s->stop) return true;
-                if (s->queue.empty()) return false;
-                const Ticket* h = s->queue.front();
-                return s->inflight == 0 || s->inflight_bytes + h->footprint <= s->cfg.hbm_budget_bytes;
+                chosen = pick();
+                return chosen != s->queue.end();
             });
             if (s->stop && s->queue.empty()) break;
             if (s->stop) {                       // drain: cancel what never started
@@ -191,8 +211,8 @@ void worker_main(fy_server* s, int idx) {
                 s->cv_done.notify_all();
                 break;
             }
-            t = s->queue.front();
-            s->queue.pop_front();
+            t = *chosen;
+            s->queue.erase(chosen);
             s->inflight_bytes += t->footprint;
             s->inflight += 1;
             t->t_start = now_ms();
@@ -224,9 +244,10 @@ void worker_main(fy_server* s, int idx) {
 
 extern "C" void fy_server_cfg_default(fy_server_cfg* c) {
     c->hbm_budget_bytes = (size_t)150 << 30;    // 150 GB
-    c->workers = 4;
+    c->workers = 8;
     c->device = 0;
     c->priority_voxels = (size_t)256 * 256 * 256;
+    c->small_workers = 2;
 }
 
 extern "C" int fy_server_create(fy_server** out, const fy_server_cfg* cfg) {
@@ -239,6 +260,8 @@ extern "C" int fy_server_create(fy_server** out, const fy_server_cfg* cfg) {
     if (cfg) s->cfg = *cfg;
     else fy_server_cfg_default(&s->cfg);
     if (s->cfg.workers < 1) s->cfg.workers = 1;
+    if (s->cfg.small_workers < 0) s->cfg.small_workers = 0;
+    if (s->cfg.small_workers >= s->cfg.workers) s->cfg.small_workers = s->cfg.workers - 1;
     if (s->cfg.workers > 64) s->cfg.workers = 64;
     if (s->cfg.hbm_budget_bytes == 0) s->cfg.hbm_budget_bytes = (size_t)150 << 30;
     for (int i = 0; i < s->cfg.workers; ++i) s->workers.emplace_back(worker_main, s, i);

@@ -289,16 +289,19 @@ int  fy_gpu_restore_u8(const unsigned char *d_u8, float *d_out, int nz, int ny, 
  * stream and device workspaces, runs the restoration chain of several requests at once, so
  * their kernels and their host<->device copies overlap on the device. A request is
  * admitted in arrival order when a worker is free and the estimated device memory of the
- * requests in flight stays within hbm_budget_bytes; a request larger than the whole budget
+ * requests in flight stays within hbm_budget_bytes (reserved small-request workers may take
+ * a small request out of order); a request larger than the whole budget
  * is refused at submission. Each result equals the single-cube fy_gpu_restore_u8 call. */
 typedef struct fy_server fy_server;
 typedef struct {
     size_t hbm_budget_bytes;     /* device memory admitted at once (default 150 GB) */
-    int    workers;              /* requests executing at once (default 4) */
+    int    workers;              /* requests executing at once (default 8) */
     int    device;
     size_t priority_voxels;      /* requests up to this size run on high-priority streams
                                     (default 256^3), so small cubes keep low latency beside
                                     large ones; copies move in 32 MB chunks for the same reason */
+    int    small_workers;        /* workers reserved for requests up to priority_voxels (default
+                                    2); they may take a small request from behind a large one */
 } fy_server_cfg;
 typedef struct {
     const unsigned char *u8;     /* host input, nz*ny*nx (pinned memory avoids a staging copy) */

@@ -97,6 +97,6 @@ def test_server_refuses_without_gpu(fy):
     h = C.c_void_p(123)
     cfg = fy.ServerCfg()
     lib.fy_server_cfg_default(C.byref(cfg))
-    assert cfg.workers == 4 and cfg.hbm_budget_bytes == 150 << 30
+    assert cfg.workers == 8 and cfg.small_workers == 2 and cfg.hbm_budget_bytes == 150 << 30
     assert lib.fy_server_create(C.byref(h), C.byref(cfg)) == fy.FY_ENODEV
     assert h.value is None                                  # no handle, no worker threads
