@@ -261,6 +261,7 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
     rng = np.random.default_rng(seed)
     scfg = fb.ServerCfg()
     lib.fy_server_cfg_default(C.byref(scfg))
+    scfg.reserve_nz = scfg.reserve_ny = scfg.reserve_nx = 512      # resident workspaces: largest cube
     srv = C.c_void_p()
     fb.check(lib.fy_server_create(C.byref(srv), C.byref(scfg)), "fy_server_create")
 
@@ -312,7 +313,7 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
     for i, k in enumerate(pick):
         s = sizes[k]
         reqs.append(_req(fb, src[s], outs[s][i % 6], rng.uniform(200, 1000), float(rng.uniform(0.9, 1.1)), db_scale))
-    run_all([_req(fb, src[s], outs[s][0], 500.0, 1.0, db_scale) for s in sizes] * 2)      # warm-up
+    run_all([_req(fb, src[s], outs[s][0], 500.0, 1.0, db_scale) for s in sizes] * scfg.workers)   # warm-up
     vox = sum(r.nz * r.ny * r.nx for r in reqs)
     points = []
     for rate in rates:
@@ -331,7 +332,8 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
         "workload": f"{n_requests} requests per point, Poisson arrivals, sizes 64^3:128^3:256^3:512^3 = "
                     "40:30:25:5, per-request delta_beta U[200,1000] and window span U[0.9,1.1]; host pinned "
                     "buffers, H2D + chain + D2H per request",
-        "workers": scfg.workers, "hbm_budget_gb": scfg.hbm_budget_bytes / 2 ** 30,
+        "workers": scfg.workers, "small_workers": scfg.small_workers, "resident_workspaces": "512^3",
+        "hbm_budget_gb": scfg.hbm_budget_bytes / 2 ** 30,
         "points": points,
         "mvox_per_s": max(pt["mvox_per_s"] for pt in points),
         "plain_mvox_per_s": plain,

@@ -46,7 +46,8 @@ class RestoreCfg(C.Structure):
 class ServerCfg(C.Structure):
     """fy_server_cfg (include/fysics_b200.h)."""
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("workers", C.c_int), ("device", C.c_int),
-                ("priority_voxels", C.c_size_t), ("small_workers", C.c_int)]
+                ("priority_voxels", C.c_size_t), ("small_workers", C.c_int),
+                ("reserve_nz", C.c_int), ("reserve_ny", C.c_int), ("reserve_nx", C.c_int)]
 
 
 class Request(C.Structure):

@@ -323,6 +323,24 @@ int host_deconv(const float* in, float* out, int nz, int ny, int nx, const fy_ph
 }
 }  // namespace
 
+// Size the calling thread's deconvolution workspaces (half spectrum, tables) for a cube shape,
+// so later calls up to that shape allocate nothing.
+int fy_deconv_reserve(int nz, int ny, int nx) {
+    SpecGeom g;
+    int rc = make_geom(nz, ny, nx, g, "fy_deconv_reserve");
+    if (rc) return rc;
+    if ((rc = fy::ensure_ctx())) return rc;
+    fy::ThreadCtx& c = ctx();
+    const size_t lut_bytes = ((FY_LUT_N + 1) * sizeof(float) + 15) & ~(size_t)15;
+    cudaError_t e;
+    if ((e = c.spec.ensure(fy_deconv_spec_elems(g) * sizeof(float2))) != cudaSuccess ||
+        (e = c.tab.buf.ensure(lut_bytes + sizeof(double) * ((size_t)g.pz + g.py + g.hx))) != cudaSuccess)
+        return fail_cuda(e, "fy_deconv_reserve");
+    if (!fy::twiddles(g.px) || !fy::twiddles(g.py) || !fy::twiddles(g.pz))
+        return fail(FY_ENOMEM, "fy_deconv_reserve: twiddle tables");
+    return FY_OK;
+}
+
 extern "C" int fy_deconvolve(const float* in, float* out, int nz, int ny, int nx, const fy_physics* p,
                              double reg) {
     fy::enter();

@@ -140,3 +140,7 @@ inline TileShape fy_tile_shape(int n) {
 // Radial guided-eps model (fy_radial.cu): cube eps = base * radial scale, on the device.
 cudaError_t fy_launch_radial_tile_eps(const fy_radial_eps* d_fit, const float* base_dev, float base_host, double ecy,
                                       double ecx, long y0, long x0, long ty, long tx, float* d_out, cudaStream_t st);
+
+// Workspace reservation for a cube shape on the calling thread (fy_api.cu, fy_restore.cu).
+int fy_deconv_reserve(int nz, int ny, int nx);
+int fy_restore_reserve(int nz, int ny, int nx);

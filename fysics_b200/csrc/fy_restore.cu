@@ -146,3 +146,20 @@ extern "C" int fy_gpu_restore_u8(const unsigned char* d_u8, float* d_out, int nz
     }
     return FY_OK;
 }
+
+// Size every workspace the chain uses for a cube shape (exact guided path), so later calls
+// up to that shape allocate nothing: growing a workspace frees the old buffer, and a free
+// synchronises the whole device.
+int fy_restore_reserve(int nz, int ny, int nx) {
+    int rc = fy_deconv_reserve(nz, ny, nx);
+    if (rc) return rc;
+    fy::ThreadCtx& c = ctx();
+    const size_t n = (size_t)nz * ny * nx;
+    size_t aux = fy_noise_scratch_floats(n);
+    if (fy_guided_fused_scratch_floats(n) > aux) aux = fy_guided_fused_scratch_floats(n);
+    cudaError_t e;
+    if ((e = c.aux2.ensure(n * sizeof(float))) != cudaSuccess || (e = c.aux.ensure(aux * sizeof(float))) != cudaSuccess ||
+        (e = c.small.ensure(fy_noise_ctl_bytes() + 256)) != cudaSuccess)
+        return fail_cuda(e, "fy_restore_reserve");
+    return FY_OK;
+}

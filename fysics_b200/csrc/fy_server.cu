@@ -164,6 +164,13 @@ void worker_main(fy_server* s, int idx) {
     WorkerBufs wb;
     (void)idx;
     int prio_lo = 0, prio_hi = 0;
+    if (!rc0 && s->cfg.reserve_nz > 0 && s->cfg.reserve_ny > 0 && s->cfg.reserve_nx > 0) {
+        // resident workspaces for the largest expected cube: no allocation while serving
+        const size_t rn = (size_t)s->cfg.reserve_nz * s->cfg.reserve_ny * s->cfg.reserve_nx;
+        if (fy_restore_reserve(s->cfg.reserve_nz, s->cfg.reserve_ny, s->cfg.reserve_nx) != FY_OK ||
+            wb.d_in.ensure(rn) != cudaSuccess || wb.d_out.ensure(4 * rn) != cudaSuccess)
+            cudaGetLastError();                    // serving still works; buffers grow on demand
+    }
     if (!rc0) {
         cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);      // (least, greatest)
         if (cudaStreamCreateWithPriority(&wb.hi, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
@@ -248,6 +255,7 @@ extern "C" void fy_server_cfg_default(fy_server_cfg* c) {
     c->device = 0;
     c->priority_voxels = (size_t)256 * 256 * 256;
     c->small_workers = 2;
+    c->reserve_nz = c->reserve_ny = c->reserve_nx = 0;
 }
 
 extern "C" int fy_server_create(fy_server** out, const fy_server_cfg* cfg) {

@@ -302,6 +302,10 @@ typedef struct {
                                     large ones; copies move in 32 MB chunks for the same reason */
     int    small_workers;        /* workers reserved for requests up to priority_voxels (default
                                     2); they may take a small request from behind a large one */
+    int    reserve_nz, reserve_ny, reserve_nx;  /* > 0: every worker sizes its device workspaces for
+                                    this cube at start, so serving up to that size allocates
+                                    nothing (a workspace that grows frees its old buffer, and a
+                                    free synchronises the device); 0: grow on demand */
 } fy_server_cfg;
 typedef struct {
     const unsigned char *u8;     /* host input, nz*ny*nx (pinned memory avoids a staging copy) */
