@@ -362,6 +362,88 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
     return served, batched
 
 
+# ------------------------------------------------------------------------------ registration
+def phasecorr_sample(fb, lib, dev, seed, db_scale, npairs=64, n=256, distinct=8, cpu_budget_s=10.0):
+    """Config-4 sample: npairs pairs of n^3 f32 volumes; the moving volume is an FP64 Fourier
+    shift of the fixed one (integer U[-40,40] + subvoxel U[-0.5,0.5] per axis), each with
+    independent noise var = 0.002*I + 1e-4. `distinct` different pairs are tiled to npairs.
+    One batched call (fy_gpu_phase_correlate_batch, window 0) is timed; the reference CPU path
+    runs a bounded sample of the same pairs, one per host thread."""
+    import torch
+    import fysics_b200.phantom as ph
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=f"cuda:{dev}").manual_seed(int(seed))
+    u = ph.phantom((n, n, n), seed=seed, delta_beta=500.0 * db_scale, pixel_um=2.4, device=f"cuda:{dev}")
+    f = u.to(torch.float64) / 255.0
+    F = torch.fft.fftn(f)
+    k = torch.fft.fftfreq(n, device=f"cuda:{dev}", dtype=torch.float64) * n
+    k[n // 2] = n // 2                           # the reference keeps k = n/2 positive
+    truths, fixed, moving = [], [], []
+    for i in range(distinct):
+        s = rng.integers(-40, 41, 3) + rng.uniform(-0.5, 0.5, 3)
+        ph_ = -2 * np.pi * (k[:, None, None] * s[0] + k[None, :, None] * s[1] + k[None, None, :] * s[2]) / n
+        m = torch.fft.ifftn(F * torch.exp(1j * ph_)).real
+        noise = lambda v: v + torch.sqrt(0.002 * v.clamp(min=0) + 1e-4) * torch.randn(v.shape, generator=g,
+                                                                                      device=v.device, dtype=v.dtype)
+        fixed.append(noise(f).float())
+        moving.append(noise(m).float())
+        truths.append(s)
+    del F
+    d_fixed = torch.stack([fixed[i % distinct] for i in range(npairs)])
+    d_moving = torch.stack([moving[i % distinct] for i in range(npairs)])
+    scratch = torch.empty(lib.fy_gpu_phase_correlate_scratch_bytes(n, n, n), dtype=torch.uint8, device=f"cuda:{dev}")
+    sh = (C.c_double * (3 * npairs))()
+    pk = (C.c_double * npairs)()
+    st = (C.c_int * npairs)()
+    args = (C.c_void_p(d_fixed.data_ptr()), C.c_void_p(d_moving.data_ptr()), npairs, n, n, n, 0,
+            C.c_void_p(scratch.data_ptr()), sh, pk, None, st, None)
+    torch.cuda.synchronize()
+    fb.check(lib.fy_gpu_phase_correlate_batch(*args[:2], min(npairs, 2), *args[3:]), "phase correlate warm-up")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    fb.check(lib.fy_gpu_phase_correlate_batch(*args), "fy_gpu_phase_correlate_batch")
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    got = np.array(sh[:]).reshape(npairs, 3)
+    want = np.array([truths[i % distinct] for i in range(npairs)])
+    err = np.abs(got - want)
+    res = {"workload": f"{npairs} pairs of {n}^3 f32 ({distinct} distinct pairs tiled), FP64 Fourier shift "
+                       "integer U[-40,40] + subvoxel U[-0.5,0.5] per axis, noise var = 0.002*I + 1e-4, window 0; "
+                       "inputs resident on the device, one batched call",
+           "pairs_per_s": npairs / dt, "mvox_pairs_per_s": npairs * n ** 3 / dt / 1e6,
+           "ms_per_pair": dt * 1e3 / npairs, "status_ok": int(sum(1 for i in range(npairs) if st[i] == 0)),
+           "integer_exact": int(np.sum(np.all(np.round(got) == np.round(want), axis=1))),
+           "mean_abs_err_vox": float(err.mean()), "max_abs_err_vox": float(err.max())}
+    # reference CPU path on a bounded sample: one pair per host thread
+    try:
+        import oracle
+        from concurrent.futures import ThreadPoolExecutor
+        if oracle.have_ref() and cpu_budget_s > 0:
+            L = oracle.ref()
+            hf = [fixed[i].cpu().numpy() for i in range(distinct)]
+            hm = [moving[i].cpu().numpy() for i in range(distinct)]
+
+            def one(i):
+                s3 = (C.c_double * 3)()
+                p1 = C.c_double()
+                L.fy_phase_correlate(oracle.p(hf[i % distinct]), oracle.p(hm[i % distinct]), n, n, n, s3, C.byref(p1), 0)
+                return 1
+
+            t1 = time.perf_counter()
+            one(0)
+            t_one = time.perf_counter() - t1
+            cores = os.cpu_count() or 1
+            jobs = cores if t_one < cpu_budget_s else 1      # one wave of pairs, one per thread
+            t1 = time.perf_counter()
+            with ThreadPoolExecutor(max_workers=cores) as ex:
+                done = sum(ex.map(one, range(jobs)))
+            res["cpu_reference"] = {"pairs_per_s": done / (time.perf_counter() - t1), "cores": cores,
+                                    "sample": f"{done} pairs, one per host thread; single-thread {t_one:.2f} s per pair"}
+    except Exception as exc:             # reported, never required
+        res["cpu_reference"] = {"error": str(exc)[:200]}
+    return res
+
+
 # ------------------------------------------------------------------------------ main
 def dist_setup(n_gpus: int, backend: str = "nccl"):
     """One process per GPU (torchrun env). Replicas only: the only collectives are the
@@ -434,6 +516,7 @@ def main():
     ap.add_argument("--cpu-phantom", action="store_true")
     ap.add_argument("--size", type=int, default=512, help="cube edge (512 = the benchmark workload)")
     ap.add_argument("--no-serve", action="store_true", help="skip the served / batched samples")
+    ap.add_argument("--no-phasecorr", action="store_true", help="skip the registration sample")
     args = ap.parse_args()
     global SHAPE, WORKLOAD
     if args.size != 512:
@@ -594,6 +677,14 @@ def main():
         except Exception as exc:      # reported, never required
             served = {"error": str(exc)[:300]}
 
+    phasecorr = None
+    if not args.no_phasecorr:
+        try:
+            phasecorr = phasecorr_sample(fb, lib, dev, args.seed + 31 * rank, db_scale,
+                                         cpu_budget_s=0.0 if args.no_cpu else 10.0)
+        except Exception as exc:      # reported, never required
+            phasecorr = {"error": str(exc)[:300]}
+
     lat = sorted(per_step)
     line = {
         "metric": METRIC, "value": value, "unit": "Mvoxel/s", "n_gpus": world, "steps": args.steps,
@@ -613,6 +704,7 @@ def main():
         "cpu_baseline": cpu,
         "served": served,
         "batched": batched,
+        "phasecorr": phasecorr,
     }
     lib.fy_gpu_dering_destroy(h)
     if rank == 0:
