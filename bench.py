@@ -137,7 +137,7 @@ def algorithmic_bytes(name: str, n: int, geo: dict) -> float | None:
         "deconv.y_inv": nz * geo["py"] * hx * 8 + half,
         "deconv.x_inv": half + n * 4,
         "noise.stats": n * 12,                 # box pass: I read, mean + var written
-        "noise.lohi": n * 12,                  # 3 digit passes over mean
+        "noise.lohi": n * 8,                   # digit passes 2 and 3 over mean (the first is in noise.stats)
         "noise.bin_select": n * 24,            # mean + var read, labels written; 3 passes over var + labels
         "guided": n * 28,                      # I -> a, b (12 B); a, b, I -> out (16 B)
         "dering.accumulate+vote": n * 1,
