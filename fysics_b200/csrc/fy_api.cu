@@ -230,8 +230,20 @@ int deconv_tables(const SpecGeom& g, const fy_physics* p, double param, int kind
         }
         cudaError_t e = c.tab.buf.ensure(bytes);
         if (e != cudaSuccess) return fail_cuda(e, "deconv tables");
-        if ((e = cudaMemcpyAsync(c.tab.buf.p, h.data(), bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        // Stage through pinned memory so the upload is an ordinary asynchronous copy (a
+        // pageable one waits for the stream and shares the driver's staging path); the
+        // staging buffer is reused only once the previous upload has been read.
+        if (c.tab_pending && (e = cudaEventSynchronize(c.tab_done)) != cudaSuccess)
             return fail_cuda(e, "deconv tables upload");
+        c.tab_pending = false;
+        if ((e = c.tab_pin.ensure(bytes)) != cudaSuccess) return fail_cuda(e, "deconv tables");
+        if (!c.tab_done && (e = cudaEventCreateWithFlags(&c.tab_done, cudaEventDisableTiming)) != cudaSuccess)
+            return fail_cuda(e, "deconv tables");
+        memcpy(c.tab_pin.p, h.data(), bytes);
+        if ((e = cudaMemcpyAsync(c.tab.buf.p, c.tab_pin.p, bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+            (e = cudaEventRecord(c.tab_done, st)) != cudaSuccess)
+            return fail_cuda(e, "deconv tables upload");
+        c.tab_pending = true;
         memcpy(c.tab.key, &key, sizeof key);
         c.tab.keylen = sizeof key;
         c.tab.us = us;
@@ -334,7 +346,8 @@ int fy_deconv_reserve(int nz, int ny, int nx) {
     const size_t lut_bytes = ((FY_LUT_N + 1) * sizeof(float) + 15) & ~(size_t)15;
     cudaError_t e;
     if ((e = c.spec.ensure(fy_deconv_spec_elems(g) * sizeof(float2))) != cudaSuccess ||
-        (e = c.tab.buf.ensure(lut_bytes + sizeof(double) * ((size_t)g.pz + g.py + g.hx))) != cudaSuccess)
+        (e = c.tab.buf.ensure(lut_bytes + sizeof(double) * ((size_t)g.pz + g.py + g.hx))) != cudaSuccess ||
+        (e = c.tab_pin.ensure(lut_bytes + sizeof(double) * ((size_t)g.pz + g.py + g.hx))) != cudaSuccess)
         return fail_cuda(e, "fy_deconv_reserve");
     if (!fy::twiddles(g.px) || !fy::twiddles(g.py) || !fy::twiddles(g.pz))
         return fail(FY_ENOMEM, "fy_deconv_reserve: twiddle tables");

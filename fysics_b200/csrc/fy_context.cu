@@ -206,5 +206,8 @@ void fy_gpu_release(void) {
     c.aux.release(); c.aux2.release(); c.small.release();
     c.pin.release(); c.pin2.release();
     c.tab.buf.release(); c.tab.valid = false;
+    c.tab_pin.release();
+    if (c.tab_done) { cudaEventDestroy(c.tab_done); c.tab_done = nullptr; }
+    c.tab_pending = false;
 }
 }

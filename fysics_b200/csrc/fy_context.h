@@ -46,6 +46,9 @@ struct ThreadCtx {
     // deconvolution table cache (one live entry per thread)
     struct TabEntry { unsigned char key[160]; size_t keylen = 0; DevBuf buf; double us = 0; bool valid = false; };
     TabEntry tab;
+    HostBuf tab_pin;                   // pinned staging of the table upload (asynchronous copy)
+    cudaEvent_t tab_done = nullptr;    // the last upload from tab_pin has been read
+    bool tab_pending = false;
 };
 
 ThreadCtx& ctx();
