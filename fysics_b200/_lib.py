@@ -132,6 +132,7 @@ SIGNATURES = {
     "fy_gpu_last_error": (C.c_char_p, []),
     "fy_gpu_release": (None, []),
     "fy_gpu_kernel_launches": (C.c_ulonglong, []),
+    "fy_gpu_kernel_timeouts": (_i, []),
     "fy_gpu_u8_to_phys": (_i, [_P, _P, _sz, _d, _d, _P]),
     "fy_gpu_phys_to_u8": (_i, [_P, _P, _sz, _d, _d, _P]),
     "fy_gpu_deconvolve_ex": (_i, [_P, _i, _d, _d, _P, _i, _i, _i, _PP, _d, _i, _d, _P]),

@@ -199,6 +199,10 @@ int fy_gpu_init(int device) {
 int fy_gpu_last_status(void) { return fy::ctx().status; }
 const char* fy_gpu_last_error(void) { return fy::ctx().err.c_str(); }
 unsigned long long fy_gpu_kernel_launches(void) { return fy::ctx().launches; }
+int fy_gpu_kernel_timeouts(void) {
+    const int a = fy_guided_wait_timeouts(), b = fy_noise_wait_timeouts();
+    return a < 0 || b < 0 ? -1 : a + b;
+}
 void fy_gpu_release(void) {
     fy::ThreadCtx& c = fy::ctx();
     if (c.st) cudaStreamSynchronize(c.st);

@@ -214,3 +214,6 @@ cudaError_t fy_launch_box_mean(const float* in, float* out, float* tmp, int nz, 
                                cudaStream_t st, int& launches) {
     return box3(in, out, tmp, nz, ny, nx, r, st, launches);
 }
+
+// Bounded waits of this unit's box passes that expired (see fy_zbox.cuh); 0 expected.
+int fy_guided_wait_timeouts() { return fyzb::timeouts(); }

@@ -144,3 +144,5 @@ cudaError_t fy_launch_radial_tile_eps(const fy_radial_eps* d_fit, const float* b
 // Workspace reservation for a cube shape on the calling thread (fy_api.cu, fy_restore.cu).
 int fy_deconv_reserve(int nz, int ny, int nx);
 int fy_restore_reserve(int nz, int ny, int nx);
+int fy_guided_wait_timeouts();
+int fy_noise_wait_timeouts();

@@ -603,3 +603,6 @@ cudaError_t fy_noise_store(const void* ctl_mem, void* d_model, float* d_eps, cud
     k_noise_store<<<1, 1, 0, st>>>((const NoiseCtl*)ctl_mem, (fy_noise_model*)d_model, d_eps);
     return cudaGetLastError();
 }
+
+// Bounded waits of this unit's box passes that expired (see fy_zbox.cuh); 0 expected.
+int fy_noise_wait_timeouts() { return fyzb::timeouts(); }

@@ -3,9 +3,11 @@
 // Shared by the noise model's local statistics (noise.c:20-67) and the two passes of the
 // guided filter (guided.c:113-141). A CTA owns a 64 x 16 column tile and a chunk of z
 // planes. Per input plane zi:
-//   stage   cp.async copies the plane's tile plus halo (x0-4 .. x0+68, y0-R .. y0+16+R)
-//           into a 4-deep shared-memory ring, zero-filled outside the volume; planes
-//           zi+1 .. zi+3 are in flight while zi is reduced.
+//   stage   the plane's tile plus halo (x0-4 .. x0+68, y0-R .. y0+16+R) lands in a 4-deep
+//           shared-memory ring, zero-filled outside the volume; planes zi+1 .. zi+3 are in
+//           flight while zi is reduced. 16-byte-aligned rows: one thread issues a 3-D tensor
+//           copy (TMA) per field, completing on the slot's mbarrier. Other shapes: cp.async
+//           by all threads.
 //   X phase one item = 4 output columns of one staged row: three float4 reads, window
 //           sums of both quantities, two float4 stores.
 //   Y phase one thread = one output column x 4 output rows. Its (2R+1)-plane z ring of
@@ -25,6 +27,8 @@
 // the guide. ZB_GUIDED_OUT can also subtract the ring profile from its output (the same
 // arithmetic as fy_dering_apply), which saves the separate read-modify-write pass.
 #pragma once
+#include <cuda.h>
+#include <mutex>
 #include "fy_internal.h"
 
 namespace fyzb {
@@ -61,9 +65,10 @@ template <int R, int NF>
 struct Geo {
     static constexpr int NR = 2 * R + 1;
     static constexpr int SY = TY + 2 * R;
-    static constexpr int STAGE = NF * SY * SXW;                 // floats per staged plane
+    static constexpr int FS = (SY * SXW + 31) / 32 * 32;        // floats per staged field (128 B multiple)
+    static constexpr int STAGE = NF * FS;                       // floats per staged plane
     static constexpr int XS = SY * TX;                          // floats per X-sum array
-    static constexpr size_t bytes = (size_t)(NS * STAGE + 2 * XS + TX + TY) * sizeof(float);
+    static constexpr size_t bytes = (size_t)(NS * STAGE + 2 * XS + TX + TY) * sizeof(float) + 128;   // + alignment
 };
 
 FY_D float recip_count(int p, int L, int r) {
@@ -86,6 +91,56 @@ FY_D void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 FY_D void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// ---- TMA staging: one thread copies a plane's tile (per field) with cp.async.bulk.tensor,
+// completion tracked by one mbarrier per ring slot. Waits are bounded: on expiry the kernel
+// raises zb_timeout, waits (bounded) for its own copies in flight and returns.
+struct TmaMaps {
+    CUtensorMap m0, m1;                // field 0 and field 1 (GUIDED_OUT); 64-byte aligned type
+};
+static __device__ int zb_timeout;      // set when a bounded wait expires (never expected)
+constexpr int kWaitSpins = 1 << 20;
+
+FY_D unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+FY_D void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+FY_D void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+FY_D bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+FY_D bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    for (int i = 0; i < kWaitSpins; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+FY_D void tma_load_3d(float* dst, const CUtensorMap* map, int x, int y, int z, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Issue plane zi (all NF fields) into slot `dst` (thread 0 only). x starts at x0 - 4, a
+// multiple of 4 floats (16 bytes) as the tensor copy requires; rows and planes outside the
+// volume, negative ones included, are zero-filled by the copy.
+template <int R, int NF>
+FY_D void tma_stage(float* dst, const TmaMaps& tm, unsigned long long* bar, int zi, int x0, int y0) {
+    using G = Geo<R, NF>;
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // prior generic reads of the slot
+    mbar_expect_tx(bar, (unsigned)(NF * G::SY * SXW * sizeof(float)));
+    tma_load_3d(dst, &tm.m0, x0 - 4, y0 - R, zi, bar);
+    if (NF == 2) tma_load_3d(dst + G::FS, &tm.m1, x0 - 4, y0 - R, zi, bar);
+}
+
 // Stage plane zi (all NF fields) into dst; zero fill outside the volume.
 template <int R, int NF, bool VEC>
 FY_D void stage_plane(float* dst, const Params& p, int zi, int x0, int y0) {
@@ -101,7 +156,7 @@ FY_D void stage_plane(float* dst, const Params& p, int zi, int x0, int y0) {
             const int gy = y0 - R + yy, gx = x0 - 4 + 4 * q;
             const bool ok = zin && gy >= 0 && gy < p.ny && gx >= 0 && gx < p.nx;
             const float* base = f ? p.f1 : p.f0;
-            cp16(dst + f * G::SY * SXW + yy * SXW + 4 * q, ok ? base + pbase + (size_t)gy * p.nx + gx : base, ok);
+            cp16(dst + f * G::FS + yy * SXW + 4 * q, ok ? base + pbase + (size_t)gy * p.nx + gx : base, ok);
         }
     } else {
         constexpr int PER = G::SY * SXW;
@@ -112,18 +167,19 @@ FY_D void stage_plane(float* dst, const Params& p, int zi, int x0, int y0) {
             const int gy = y0 - R + yy, gx = x0 - 4 + xx;
             const bool ok = zin && gy >= 0 && gy < p.ny && gx >= 0 && gx < p.nx;
             const float* base = f ? p.f1 : p.f0;
-            cp4(dst + f * G::SY * SXW + rem, ok ? base + pbase + (size_t)gy * p.nx + gx : base, ok);
+            cp4(dst + f * G::FS + rem, ok ? base + pbase + (size_t)gy * p.nx + gx : base, ok);
         }
     }
 }
 
-template <int R, int KIND, bool VEC>
-__global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p) {
+template <int R, int KIND, bool VEC, bool TMA>
+__global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p, const __grid_constant__ TmaMaps tm) {
     constexpr int NF = KIND == ZB_GUIDED_OUT ? 2 : 1;
     using G = Geo<R, NF>;
     constexpr int NR = G::NR;
     extern __shared__ float4 zb_smem4[];
-    float* stage = reinterpret_cast<float*>(zb_smem4);
+    __shared__ __align__(8) unsigned long long bars[NS];
+    float* stage = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(zb_smem4) + 127) & ~(uintptr_t)127);
     float* xs1 = stage + NS * G::STAGE;
     float* xs2 = xs1 + G::XS;
     float* rx = xs2 + G::XS;
@@ -147,10 +203,21 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     if (t < TY) ry[t] = y0 + t < ny ? recip_count(y0 + t, ny, R) : 0.f;
     const bool cols_in = x0 - 4 >= 0 && x0 + TX + 4 <= nx;       // no column of the staged rows is outside
     const int zfirst = zs - R, zend = ze + R;
+    if (TMA) {
+        if (t == 0) {
+            for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
+            asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        }
+        __syncthreads();
+        if (t == 0)
+            for (int s = 0; s < NS - 1; ++s)
+                if (zfirst + s < zend) tma_stage<R, NF>(stage + s * G::STAGE, tm, &bars[s], zfirst + s, x0, y0);
+    } else {
 #pragma unroll
-    for (int s = 0; s < NS - 1; ++s) {
-        if (zfirst + s < zend) stage_plane<R, NF, VEC>(stage + s * G::STAGE, p, zfirst + s, x0, y0);
-        cp_commit();
+        for (int s = 0; s < NS - 1; ++s) {
+            if (zfirst + s < zend) stage_plane<R, NF, VEC>(stage + s * G::STAGE, p, zfirst + s, x0, y0);
+            cp_commit();
+        }
     }
     // Y-phase role: output column xc, output rows 4*rg .. 4*rg+3
     const int xc = t & (TX - 1), rg = t >> 6;
@@ -190,9 +257,25 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
             const int zi = zi0 + ph;
             if (zi >= zend) break;
             const int slot = (zi - zfirst) & (NS - 1);
-            cp_wait<NS - 2>();
-            __syncthreads();             // plane zi landed for every thread; xs free again
-            {
+            if (TMA) {
+                const bool ok = mbar_wait_bounded(&bars[slot], (unsigned)(((zi - zfirst) / NS) & 1));
+                if (__syncthreads_or(!ok)) {      // plane zi never landed: flag, drain, return
+                    if (t == 0) {
+                        atomicExch(&zb_timeout, 1);
+                        const int zlast = min(zi + NS - 2, zend - 1);   // loads issued so far
+                        for (int zq = zi; zq <= zlast; ++zq)
+                            mbar_wait_bounded(&bars[(zq - zfirst) & (NS - 1)], (unsigned)(((zq - zfirst) / NS) & 1));
+                    }
+                    __syncthreads();
+                    return;
+                }
+                const int zn = zi + NS - 1;       // plane zi landed for every thread; xs free again
+                if (t == 0 && zn < zend)
+                    tma_stage<R, NF>(stage + ((zn - zfirst) & (NS - 1)) * G::STAGE, tm, &bars[(zn - zfirst) & (NS - 1)],
+                                     zn, x0, y0);
+            } else {
+                cp_wait<NS - 2>();
+                __syncthreads();             // plane zi landed for every thread; xs free again
                 const int zn = zi + NS - 1;
                 if (zn < zend) stage_plane<R, NF, VEC>(stage + ((zn - zfirst) & (NS - 1)) * G::STAGE, p, zn, x0, y0);
                 cp_commit();
@@ -221,7 +304,7 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                 if (NF == 2) {
 #pragma unroll
                     for (int j = 0; j < 3; ++j) {
-                        const float4 v = *reinterpret_cast<const float4*>(row + G::SY * SXW + 4 * j);
+                        const float4 v = *reinterpret_cast<const float4*>(row + G::FS + 4 * j);
                         q2[4 * j] = v.x; q2[4 * j + 1] = v.y; q2[4 * j + 2] = v.z; q2[4 * j + 3] = v.w;
                     }
                 } else {
@@ -337,7 +420,7 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
             }
         }
     }
-    cp_wait<0>();
+    if (!TMA) cp_wait<0>();
     if (want_hist) {
         if (hcur >= 0) atomicAdd(&h0[hcur], hcnt);
         __syncthreads();
@@ -361,15 +444,63 @@ inline dim3 grid_for(int nz, int ny, int nx, int r, int sms, int& zchunk) {
     return dim3(tx, ty, (nz + zchunk - 1) / zchunk);
 }
 
+// Tensor map of one f32 volume field for the TMA staging: box (x0-4 .. x0+TX+4, SY rows, 1
+// plane), zero fill outside. The encoder comes from the driver through the runtime, so the
+// library needs no link-time driver dependency. Returns false when unavailable.
+inline bool make_tma_map(CUtensorMap* m, const float* base, int nz, int ny, int nx, int sy) {
+    using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static EncodeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeFn>(f);
+        else
+            cudaGetLastError();
+    });
+    if (!fn || ((uintptr_t)base & 15) || (nx % 4)) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)SXW, (cuuint32_t)sy, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int KIND, int R, bool VEC>
 inline cudaError_t launch_r(const Params& p, dim3 grid, cudaStream_t st) {
     constexpr int NF = KIND == ZB_GUIDED_OUT ? 2 : 1;
-    auto k = k_zbox<R, KIND, VEC>;
     const size_t smem = Geo<R, NF>::bytes + (KIND == ZB_NOISE ? HIST0_BINS * sizeof(unsigned int) : 0);
-    cudaError_t e = fy_smem_optin(k, smem);
-    if (e != cudaSuccess) return e;
-    k<<<grid, NT, smem, st>>>(p);
+    TmaMaps tm;
+    memset(&tm, 0, sizeof tm);
+    bool tma = false;
+    if (VEC) {
+        tma = make_tma_map(&tm.m0, p.f0, p.nz, p.ny, p.nx, Geo<R, NF>::SY) &&
+              (NF == 1 || make_tma_map(&tm.m1, p.f1, p.nz, p.ny, p.nx, Geo<R, NF>::SY));
+    }
+    cudaError_t e;
+    if (tma) {
+        auto k = k_zbox<R, KIND, true, true>;
+        if ((e = fy_smem_optin(k, smem)) != cudaSuccess) return e;
+        k<<<grid, NT, smem, st>>>(p, tm);
+    } else {
+        auto k = k_zbox<R, KIND, VEC, false>;
+        if ((e = fy_smem_optin(k, smem)) != cudaSuccess) return e;
+        k<<<grid, NT, smem, st>>>(p, tm);
+    }
     return cudaGetLastError();
+}
+
+// Number of bounded waits that expired in this translation unit's box passes (0 expected).
+static inline int timeouts() {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, zb_timeout, sizeof v) != cudaSuccess) { cudaGetLastError(); return -1; }
+    return v;
 }
 
 // Enqueue one z-sliding box pass, radius r in [1, 4].

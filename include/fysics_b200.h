@@ -142,6 +142,10 @@ const char *fy_gpu_last_error(void);
 void        fy_gpu_release(void);
 /* Launch counter: number of kernels this thread has launched (for measurement). */
 unsigned long long fy_gpu_kernel_launches(void);
+/* Number of bounded in-kernel waits (tensor-copy completions of the box passes) that gave
+ * up since the library loaded on this device; the kernel then returned without finishing.
+ * 0 in normal operation; -1 without a device. */
+int fy_gpu_kernel_timeouts(void);
 
 /* Device-pointer forms of the drop-in calls, enqueued on `stream` (a cudaStream_t, NULL =
  * legacy default stream) and NOT synchronised: results are valid once the stream reaches

@@ -125,3 +125,12 @@ def test_device_inplace(gpu):
     assert rc == 0
     torch.cuda.synchronize()
     assert np.array_equal(d.cpu().numpy(), want)
+
+
+def test_box_pass_waits_never_expired(gpu):
+    """The box passes' bounded waits on tensor-copy completion never gave up during the
+    GPU tests run so far (their expiry would leave the output unfinished)."""
+    vol = np.random.default_rng(2).uniform(0, 1, (40, 64, 64)).astype(np.float32)
+    out = np.empty_like(vol)
+    assert gpu.load().fy_guided_denoise(p(vol), p(out), *vol.shape, 2, 1e-3) == 0
+    assert gpu.load().fy_gpu_kernel_timeouts() == 0
