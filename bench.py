@@ -137,13 +137,22 @@ def algorithmic_bytes(name: str, n: int, geo: dict) -> float | None:
         "deconv.y_inv": nz * geo["py"] * hx * 8 + half,
         "deconv.x_inv": half + n * 4,
         "noise.stats": n * 12,                 # box pass: I read, mean + var written
-        "noise.lohi": n * 8,                   # digit passes 2 and 3 over mean (the first is in noise.stats)
+        "noise.lohi": n * 12,                  # 3 digit passes over mean
         "noise.bin_select": n * 24,            # mean + var read, labels written; 3 passes over var + labels
         "guided": n * 28,                      # I -> a, b (12 B); a, b, I -> out (16 B)
         "dering.accumulate+vote": n * 1,
         "dering.apply": n * 8,
     }
     return table.get(name)
+
+
+# DRAM bytes per voxel of each instrumented span, from a one-pass ncu capture of the 512^3
+# chain (dram__bytes_read.sum + dram__bytes_write.sum per launch; profiles/dram_restore_512.md).
+DRAM_BYTES_PER_VOXEL = {
+    "deconv.x_fwd": 4.654, "deconv.y_fwd": 8.032, "deconv.z_weight": 8.284, "deconv.y_inv": 8.027,
+    "deconv.x_inv": 7.877, "noise.stats": 11.638, "noise.lohi": 12.006, "noise.bin_select": 23.93,
+    "guided": 27.617, "dering.accumulate+vote": 0.507,
+}
 
 
 def read_profile(lib):
@@ -657,8 +666,11 @@ def main():
     roof = None
     if dom:
         ach = kernels[dom]["gbs"]
+        tpv = DRAM_BYTES_PER_VOXEL.get(dom)
         roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
-                "frac": ach / hbm_peak, "traffic": None, "peak_source": peak_src,
+                "frac": ach / hbm_peak, "traffic": tpv * n if tpv is not None and SHAPE == (512, 512, 512) else None,
+                "traffic_source": "ncu one-pass capture of the 512^3 chain (profiles/dram_restore_512.md)",
+                "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": algorithmic_bytes(dom, n, geo)}
 
     cpu = None

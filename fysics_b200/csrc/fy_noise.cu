@@ -526,22 +526,19 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     cudaError_t e;
     if ((e = cudaMemsetAsync(hist, 0, hist_bytes, st)) != cudaSuccess) return e;
     k_noise_setup<<<1, 1, 0, st>>>(ctl, n, flat_pct, ref_intensity);
-    {   // 1. stats; the epilogue also builds the first digit histogram of the means (top 11 bits)
+    {   // 1. stats
         fyzb::Params sp{};
         sp.nz = nz; sp.ny = ny; sp.nx = nx;
         sp.f0 = in; sp.o0 = mean; sp.o1 = var;
         sp.inv_wc = inv_wc; sp.wci = win * win * win;
-        sp.hist0 = hist;
         cudaError_t e0 = fyzb::launch<fyzb::ZB_NOISE>(sp, r, sms, st);
         if (e0 != cudaSuccess) return e0;
         fy_prof_mark(st, "noise.stats");
     }
-    // 2a. 1st/99th percentile of the means: 11 (from the stats pass) + 11 + 10 bits, then the
-    // k+1 neighbours
+    // 2a. 1st/99th percentile of the means: 11 + 11 + 10 bits, then the k+1 neighbours
     const int all_digits[3][2] = {{21, 11}, {10, 11}, {0, 10}};
     for (int i = 0; i < 3; ++i) {
-        if (i == 0) { /* histogram already built by the stats pass */ }
-        else if (all_digits[i][1] == 11) k_sel_hist<11, 0><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0]);
+        if (all_digits[i][1] == 11) k_sel_hist<11, 0><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0]);
         else k_sel_hist<10, 0><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0]);
         k_sel_scan<<<2, 256, 0, st>>>(ctl, all_digits[i][1], 0, i == 2);
     }
@@ -567,7 +564,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     }
     k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 2);
     k_noise_fit<<<1, 1, 0, st>>>(ctl, 1);
-    launches += 1 + 1 + 5 + 1 + 1 + 1 + 8 + 1 + 1 + 6 + 1 + 1;
+    launches += 1 + 1 + 6 + 1 + 1 + 1 + 8 + 1 + 1 + 6 + 1 + 1;
     return cudaGetLastError();
 }
 

@@ -50,16 +50,7 @@ struct Params {
     int out_mode;
     int nz, ny, nx, zchunk;
     RingApply ra;          // GUIDED_OUT, out_mode 0: ring subtraction on the output (optional)
-    unsigned int* hist0;   // NOISE (optional): 2 x 2048-bin histograms of the top 11 bits of the
-                           // means' orderable keys, the first digit pass of their percentiles
 };
-
-// Orderable 32-bit key of a float (total order of the values, -0 < +0).
-FY_D uint32_t order_key(float f) {
-    const uint32_t u = __float_as_uint(f);
-    return u ^ ((uint32_t)((int32_t)u >> 31) | 0x80000000u);
-}
-constexpr int HIST0_BINS = 2048;
 
 template <int R, int NF>
 struct Geo {
@@ -184,13 +175,7 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     float* xs2 = xs1 + G::XS;
     float* rx = xs2 + G::XS;
     float* ry = rx + TX;
-    unsigned int* h0 = reinterpret_cast<unsigned int*>(ry + TY);   // NOISE with hist0
     const int t = threadIdx.x;
-    const bool want_hist = KIND == ZB_NOISE && p.hist0 != nullptr;
-    if (want_hist)
-        for (int i = t; i < HIST0_BINS; i += NT) h0[i] = 0;      // first use follows a barrier
-    int hcur = -1;
-    unsigned int hcnt = 0;
     const int nz = p.nz, ny = p.ny, nx = p.nx;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int zs = blockIdx.z * p.zchunk, ze = min(nz, zs + p.zchunk);
@@ -387,15 +372,6 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                     if (v < 0.f) v = 0.f;
                     p.o0[o] = m;
                     p.o1[o] = v;
-                    if (want_hist) {                               // run-merged shared increments
-                        const int code = (int)(order_key(m) >> 21);
-                        if (code != hcur) {
-                            if (hcur >= 0) atomicAdd(&h0[hcur], hcnt);
-                            hcur = code;
-                            hcnt = 0;
-                        }
-                        ++hcnt;
-                    }
                 } else if (KIND == ZB_GUIDED_AB) {
                     const float e1 = s1 * rz, e2 = s2 * rz;        // E[I-c], E[(I-c)^2]
                     float var = e2 - e1 * e1;
@@ -421,14 +397,6 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
         }
     }
     if (!TMA) cp_wait<0>();
-    if (want_hist) {
-        if (hcur >= 0) atomicAdd(&h0[hcur], hcnt);
-        __syncthreads();
-        for (int i = t; i < HIST0_BINS; i += NT) {
-            const unsigned int c = h0[i];
-            if (c) { atomicAdd(&p.hist0[i], c); atomicAdd(&p.hist0[HIST0_BINS + i], c); }
-        }
-    }
 }
 
 // Tiles and z chunks: ~6 CTAs per SM, chunks of >= 8R planes so the 2R-plane warm-up stays
@@ -475,7 +443,7 @@ inline bool make_tma_map(CUtensorMap* m, const float* base, int nz, int ny, int 
 template <int KIND, int R, bool VEC>
 inline cudaError_t launch_r(const Params& p, dim3 grid, cudaStream_t st) {
     constexpr int NF = KIND == ZB_GUIDED_OUT ? 2 : 1;
-    const size_t smem = Geo<R, NF>::bytes + (KIND == ZB_NOISE ? HIST0_BINS * sizeof(unsigned int) : 0);
+    const size_t smem = Geo<R, NF>::bytes;
     TmaMaps tm;
     memset(&tm, 0, sizeof tm);
     bool tma = false;
