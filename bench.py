@@ -35,6 +35,10 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+# Hardware work queues per context (CUDA default 8). The request loop runs a stream pair per
+# worker; with fewer queues than busy streams, unrelated streams share a queue and a small
+# request's kernels wait behind a large one's. Must be set before CUDA is initialised.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 METRIC = "Mvoxel/s deconv+denoise and p50/p99 cube latency, served vs plain, same B200"
 SHAPE = (512, 512, 512)
@@ -283,6 +287,7 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
 
     def run_all(reqs, arrivals=None):
         lat = [0.0] * len(reqs)
+        phases = [None] * len(reqs)
         tickets = [None] * len(reqs)
         done = threading.Event()
 
@@ -293,6 +298,7 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
                 res = fb.RequestResult()
                 fb.check(lib.fy_server_wait(srv, tickets[i], -1.0, C.byref(res)), "fy_server_wait")
                 lat[i] = res.latency_ms
+                phases[i] = (res.queue_ms, res.h2d_ms, res.chain_ms, res.d2h_ms)
             done.set()
 
         lib.fy_server_reset_stats(srv)
@@ -311,7 +317,7 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
         wall = time.perf_counter() - t0
         st = fb.ServerStats()
         lib.fy_server_get_stats(srv, C.byref(st))
-        return lat, wall, st
+        return lat, wall, st, phases
 
     # ---- config-5 sample at a latency point and a saturating throughput point
     sizes = [64, 128, 256, 512]
@@ -327,15 +333,20 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
     points = []
     for rate in rates:
         arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
-        lat, wall, st = run_all(reqs, arrivals)
-        by = {}
-        for r, l in zip(reqs, lat):
+        lat, wall, st, phases = run_all(reqs, arrivals)
+        by, ph_by = {}, {}
+        for r, l, f in zip(reqs, lat, phases):
             by.setdefault(r.nz, []).append(l)
+            ph_by.setdefault(r.nz, []).append(f)
         points.append({
             "arrival_rps": rate, "offered_mvox_per_s": vox / arrivals[-1] / 1e6, "mvox_per_s": vox / wall / 1e6,
             "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
             "p50_ms_by_size": {f"{k}^3": float(np.percentile(v, 50)) for k, v in sorted(by.items())},
-            "p99_ms_by_size": {f"{k}^3": float(np.percentile(v, 99)) for k, v in sorted(by.items())}})
+            "p99_ms_by_size": {f"{k}^3": float(np.percentile(v, 99)) for k, v in sorted(by.items())},
+            # per-size p50/p99 of each phase: queue wait, H2D, chain (incl. waiting for the GPU), D2H
+            "phases_ms_by_size": {f"{k}^3": {name: [round(float(np.percentile(col, q)), 3) for q in (50, 99)]
+                                             for name, col in zip(("queue", "h2d", "chain", "d2h"), zip(*v))}
+                                  for k, v in sorted(ph_by.items())}})
     plain = _plain(fb, lib, reqs[: min(len(reqs), 120)], dev)
     served = {
         "workload": f"{n_requests} requests per point, Poisson arrivals, sizes 64^3:128^3:256^3:512^3 = "
@@ -343,6 +354,7 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
                     "buffers, H2D + chain + D2H per request",
         "workers": scfg.workers, "small_workers": scfg.small_workers, "resident_workspaces": "512^3",
         "hbm_budget_gb": scfg.hbm_budget_bytes / 2 ** 30,
+        "cuda_device_max_connections": int(os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS", "8")),
         "points": points,
         "mvox_per_s": max(pt["mvox_per_s"] for pt in points),
         "plain_mvox_per_s": plain,
@@ -359,7 +371,7 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
         keep += [h, o]
         bre.append(_req(fb, h, o, rng.uniform(200, 1000), 1.0, db_scale))
     run_all(bre[:4])                                                                       # warm-up
-    _, bwall, _ = run_all(bre)
+    _, bwall, _, _ = run_all(bre)
     bvox = sum(r.nz * r.ny * r.nx for r in bre)
     batched = {
         "workload": f"{n_batch} cubes, dims per axis from {dims}, per-cube delta_beta U[200,1000], submitted "

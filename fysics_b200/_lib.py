@@ -58,7 +58,8 @@ class Request(C.Structure):
 
 class RequestResult(C.Structure):
     """fy_request_result (include/fysics_b200.h)."""
-    _fields_ = [("status", C.c_int), ("queue_ms", C.c_double), ("run_ms", C.c_double), ("latency_ms", C.c_double)]
+    _fields_ = [("status", C.c_int), ("queue_ms", C.c_double), ("run_ms", C.c_double), ("latency_ms", C.c_double),
+                ("h2d_ms", C.c_double), ("chain_ms", C.c_double), ("d2h_ms", C.c_double)]
 
 
 class ServerStats(C.Structure):

@@ -1,7 +1,8 @@
 // fy_dering.cu -- residual ring detection and removal (dering.c:78-248) on the GPU.
 //
 //   k_dering_accum   per (sector, radius) sums of nonzero u8 samples on an ss-stride
-//                    (dering.c:78-116), exact integer arithmetic, shared-memory privatised.
+//                    (dering.c:78-116), exact integer arithmetic, summed along z per
+//                    sampled column before one atomic per column and z range.
 //                    The (y,x) -> sector*nr + radius map is built on the host with the
 //                    reference's own double-precision sqrt/atan2 formula (dering.c:89-99)
 //                    so every sample lands in the same bin.
@@ -18,44 +19,43 @@
 namespace {
 
 // ---------------------------------------------------------------- accumulate
-// Grid: (x tiles of 256 samples, sampled rows * dz). Shared-memory histograms when the
-// bin count fits, else global atomics.
-template <bool SMEM>
+// The bin of a sample depends on its (y, x) only, so a thread owns one sampled column
+// (yi, xi) and a range of z planes: it sums the column's samples and counts the nonzero
+// ones (zero samples add nothing to either), then adds both to the column's bin with one
+// pair of global atomics. Integer arithmetic throughout, so the totals equal the
+// per-sample accumulation exactly. Consecutive threads take consecutive xi of a row, and
+// each thread has 8 loads in flight.
 __global__ void __launch_bounds__(256) k_dering_accum(const uint8_t* __restrict__ buf, const int* __restrict__ map,
                                                       unsigned long long* __restrict__ gsum,
-                                                      unsigned int* __restrict__ gcnt, int nbins, long dz,
-                                                      long dy, long dx, int ss, long sy, long sx,
-                                                      int rows_per_cta) {
-    extern __shared__ unsigned int sh[];
-    unsigned int* ssum = sh;
-    unsigned int* scnt = sh + nbins;
-    if (SMEM) {
-        for (int i = threadIdx.x; i < 2 * nbins; i += blockDim.x) sh[i] = 0;
-        __syncthreads();
+                                                      unsigned int* __restrict__ gcnt, long dz, long dy, long dx,
+                                                      int ss, long sy, long sx, long zchunk) {
+    const long ncol = sy * sx;
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const long yi = col / sx, xi = col - yi * sx;
+    const int b = __ldg(map + col);
+    if (b < 0) return;
+    const long z0 = (long)blockIdx.y * zchunk;
+    const long z1 = z0 + zchunk < dz ? z0 + zchunk : dz;
+    const size_t zs = (size_t)dy * dx;
+    const uint8_t* p = buf + (size_t)z0 * zs + (size_t)(yi * ss) * dx + (size_t)xi * ss;
+    unsigned int s = 0, c = 0;
+    long z = z0;
+    for (; z + 8 <= z1; z += 8, p += 8 * zs) {
+        unsigned int v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = __ldg(p + (size_t)u * zs);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) { s += v[u]; c += v[u] != 0u; }
     }
-    const long nrows = dz * sy;
-    const long r0 = (long)blockIdx.y * rows_per_cta;
-    for (long rr = r0; rr < r0 + rows_per_cta && rr < nrows; ++rr) {
-        const long z = rr / sy, yi = rr - z * sy;
-        const uint8_t* row = buf + ((size_t)z * dy + (size_t)(yi * ss)) * dx;
-        const int* mrow = map + yi * sx;
-        for (long xi = (long)blockIdx.x * blockDim.x + threadIdx.x; xi < sx; xi += (long)gridDim.x * blockDim.x) {
-            const unsigned v = __ldg(row + xi * ss);
-            if (!v) continue;                                   // masked voxels skipped
-            const int b = __ldg(mrow + xi);
-            if (b < 0) continue;
-            if (SMEM) { atomicAdd(&ssum[b], v); atomicAdd(&scnt[b], 1u); }
-            else { atomicAdd(&gsum[b], (unsigned long long)v); atomicAdd(&gcnt[b], 1u); }
-        }
+    for (; z < z1; ++z, p += zs) {
+        const unsigned int v = __ldg(p);
+        s += v;
+        c += v != 0u;
     }
-    if (SMEM) {
-        __syncthreads();
-        for (int i = threadIdx.x; i < nbins; i += blockDim.x) {
-            if (scnt[i]) {
-                atomicAdd(&gsum[i], (unsigned long long)ssum[i]);
-                atomicAdd(&gcnt[i], scnt[i]);
-            }
-        }
+    if (c) {
+        atomicAdd(&gsum[b], (unsigned long long)s);
+        atomicAdd(&gcnt[b], c);
     }
 }
 
@@ -64,11 +64,12 @@ __global__ void __launch_bounds__(256) k_dering_accum(const uint8_t* __restrict_
 // float), so p = sum/cnt is the same IEEE float division.
 //
 // The reference sweeps radii in order and invalidates bin r when fewer than hw valid bins
-// lie within +-hw, which later bins then see (dering.c:161-169). One block per (slab,
-// sector): all radii are evaluated in parallel against the original validity; if no bin
-// would be invalidated, that IS the sequential result (the first invalidation in the sweep
-// would have been seen with unmodified validity). Otherwise one thread resumes the sweep
-// sequentially from the first invalidated radius, which reproduces it exactly.
+// lie within +-hw, which later bins then see (dering.c:161-169). At step r the window's bins
+// below r carry their final validity and the bins from r up their original one, and only
+// the COUNT of valid bins decides an invalidation. So one thread first runs the sweep on
+// counts alone (a running count, O(1) per radius), and then every radius forms its window
+// mean in parallel, in the reference's order (ascending j, FP64), over exactly the bins the
+// sequential sweep would have seen. One block per (slab, sector).
 __global__ void __launch_bounds__(256) k_dering_smooth(const float* __restrict__ sum_f,
                                                        const unsigned int* __restrict__ cnt,
                                                        float* __restrict__ p, float* __restrict__ hp,
@@ -77,71 +78,44 @@ __global__ void __launch_bounds__(256) k_dering_smooth(const float* __restrict__
     extern __shared__ float sm_f[];
     float* sp = sm_f;                                  // p, hp and validity of this row in smem
     float* shp = sp + nr;
-    unsigned char* svd = reinterpret_cast<unsigned char*>(shp + nr);
-    __shared__ int s_first;
+    unsigned char* svo = reinterpret_cast<unsigned char*>(shp + nr);   // original validity
+    unsigned char* svf = svo + nr;                                     // after the sweep
     const size_t off = (size_t)blockIdx.x * nr;       // (slab, sector) row
-    if (threadIdx.x == 0) s_first = nr;
     for (int r = threadIdx.x; r < nr; r += blockDim.x) {
         const unsigned c = cnt[off + r];
         const unsigned char v = c >= min_cnt;
-        svd[r] = v;
+        svo[r] = v;
         sp[r] = v ? sum_f[off + r] / (float)c : 0.0f;
     }
     __syncthreads();
-    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
-        shp[r] = 0.0f;
-        if (!svd[r]) continue;
-        double acc = 0;
-        int c = 0;
-        const int lo = r - hw < 0 ? 0 : r - hw, hi = r + hw >= nr ? nr - 1 : r + hw;
-        for (int j = lo; j <= hi; ++j)
-            if (svd[j]) { acc += sp[j]; ++c; }
-        if (c >= hw) shp[r] = sp[r] - (float)(acc / c);
-        else atomicMin(&s_first, r);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0 && s_first < nr) {           // sequential from the first change
-        if (hw <= 8) {
-            // the window's values are loaded together (independent loads), then summed in
-            // the reference's order (ascending j)
-            for (int r = s_first; r < nr; ++r) {
-                if (!svd[r]) { shp[r] = 0.0f; continue; }
-                const int lo = r - hw < 0 ? 0 : r - hw, hi = r + hw >= nr ? nr - 1 : r + hw;
-                float wv[17];
-                unsigned char wk[17];
-#pragma unroll
-                for (int q = 0; q < 17; ++q) {
-                    const int j = lo + q;
-                    const bool in = j <= hi;
-                    wv[q] = in ? sp[j] : 0.0f;
-                    wk[q] = in ? svd[j] : 0;
-                }
-                double acc = 0;
-                int c = 0;
-#pragma unroll
-                for (int q = 0; q < 17; ++q)
-                    if (wk[q]) { acc += wv[q]; ++c; }
-                if (c >= hw) shp[r] = sp[r] - (float)(acc / c);
-                else { shp[r] = 0.0f; svd[r] = 0; }
-            }
-        } else {
-            for (int r = s_first; r < nr; ++r) {
-                if (!svd[r]) { shp[r] = 0.0f; continue; }
-                double acc = 0;
-                int c = 0;
-                const int lo = r - hw < 0 ? 0 : r - hw, hi = r + hw >= nr ? nr - 1 : r + hw;
-                for (int j = lo; j <= hi; ++j)
-                    if (svd[j]) { acc += sp[j]; ++c; }
-                if (c >= hw) shp[r] = sp[r] - (float)(acc / c);
-                else { shp[r] = 0.0f; svd[r] = 0; }
-            }
+    if (threadIdx.x == 0) {
+        // cf = final-valid bins in [r - hw, r - 1], co = originally valid bins in [r, r + hw]
+        int cf = 0, co = 0;
+        for (int j = 0; j <= hw && j < nr; ++j) co += svo[j];
+        for (int r = 0; r < nr; ++r) {
+            unsigned char f = 0;
+            if (svo[r]) f = cf + co >= hw;
+            svf[r] = f;
+            cf += f;
+            if (r - hw >= 0) cf -= svf[r - hw];
+            co -= svo[r];
+            if (r + 1 + hw < nr) co += svo[r + 1 + hw];
         }
     }
     __syncthreads();
     for (int r = threadIdx.x; r < nr; r += blockDim.x) {
+        float h = 0.0f;
+        if (svf[r]) {
+            double acc = 0;
+            int c = 0;
+            const int lo = r - hw < 0 ? 0 : r - hw, hi = r + hw >= nr ? nr - 1 : r + hw;
+            for (int j = lo; j <= hi; ++j)
+                if (j < r ? svf[j] : svo[j]) { acc += sp[j]; ++c; }
+            h = sp[r] - (float)(acc / c);
+        }
         p[off + r] = sp[r];
-        hp[off + r] = shp[r];
-        vd[off + r] = svd[r];
+        hp[off + r] = h;
+        vd[off + r] = svf[r];
     }
 }
 
@@ -220,23 +194,18 @@ __global__ void __launch_bounds__(256) k_dering_apply(float* __restrict__ f, con
 
 cudaError_t fy_launch_dering_accum(const uint8_t* buf, const int* map, unsigned long long* sum, unsigned int* cnt,
                                    int nbins, long dz, long dy, long dx, int ss, int sms, cudaStream_t st) {
+    (void)nbins;
     const long sy = (dy + ss - 1) / ss, sx = (dx + ss - 1) / ss;
-    const long nrows = dz * sy;
-    if (nrows <= 0 || sx <= 0) return cudaSuccess;
-    const int gx = (int)((sx + 255) / 256 < 4 ? (sx + 255) / 256 : 4);
-    long want_ctas = (long)sms * 8 / gx;
-    if (want_ctas < 1) want_ctas = 1;
-    int rows_per_cta = (int)((nrows + want_ctas - 1) / want_ctas);
-    if (rows_per_cta < 1) rows_per_cta = 1;
-    dim3 grid(gx, (unsigned)((nrows + rows_per_cta - 1) / rows_per_cta));
-    const size_t smem = 2 * (size_t)nbins * sizeof(unsigned int);
-    if (smem <= 96 * 1024) {
-        cudaError_t e = fy_smem_optin(k_dering_accum<true>, smem);
-        if (e != cudaSuccess) return e;
-        k_dering_accum<true><<<grid, 256, smem, st>>>(buf, map, sum, cnt, nbins, dz, dy, dx, ss, sy, sx, rows_per_cta);
-    } else {
-        k_dering_accum<false><<<grid, 256, 0, st>>>(buf, map, sum, cnt, nbins, dz, dy, dx, ss, sy, sx, rows_per_cta);
-    }
+    const long ncol = sy * sx;
+    if (dz <= 0 || ncol <= 0) return cudaSuccess;
+    // z chunks: about one full wave of threads, each column sum at most 255 * zchunk < 2^32
+    long nchunk = ((long)sms * 2048 + ncol - 1) / ncol;
+    if (nchunk > dz) nchunk = dz;
+    if (nchunk > 65535) nchunk = 65535;
+    if (nchunk < 1) nchunk = 1;
+    const long zchunk = (dz + nchunk - 1) / nchunk;
+    const dim3 grid((unsigned)((ncol + 255) / 256), (unsigned)((dz + zchunk - 1) / zchunk));
+    k_dering_accum<<<grid, 256, 0, st>>>(buf, map, sum, cnt, dz, dy, dx, ss, sy, sx, zchunk);
     return cudaGetLastError();
 }
 
@@ -252,7 +221,7 @@ cudaError_t fy_launch_dering_finalize(const float* sum_f, const unsigned int* cn
     cudaError_t e = cudaMemsetAsync(detected, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     const int hw = hp_win / 2;
-    const size_t smem = (size_t)nr * (2 * sizeof(float) + 1);
+    const size_t smem = (size_t)nr * (2 * sizeof(float) + 2);
     e = fy_smem_optin(k_dering_smooth, smem);
     if (e != cudaSuccess) return e;
     k_dering_smooth<<<nslab * ns, 256, smem, st>>>(sum_f, cnt, p, hp, vd, ns, nr, hw, min_cnt);

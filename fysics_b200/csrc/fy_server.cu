@@ -9,7 +9,9 @@
 // device footprint of everything in flight stays within the HBM budget. General workers take
 // the head of the queue, which is never overtaken by them, so no request starves; a few
 // reserved workers take the first small request instead, so small cubes do not wait for a
-// worker behind large ones. Each request's result is
+// worker behind large ones. All host<->device copies go through one scheduler per link
+// direction that serves the request with the fewest bytes left first (Link below), so a small
+// result never queues behind a large one on the copy engine. Each request's result is
 // the same as the single-cube fy_gpu_restore_u8 call on its own: the kernels are
 // deterministic and a worker's workspaces are private to the request it runs.
 #include <algorithm>
@@ -44,6 +46,7 @@ struct Ticket {
     long long id = 0;
     size_t footprint = 0;
     double t_submit = 0, t_start = 0, t_done = 0;
+    float h2d_ms = 0, chain_ms = 0, d2h_ms = 0;   // copies: host clock incl. link wait; chain: CUDA events
     int status = -1;          // -1 pending, else the chain's status
     bool done = false;
 };
@@ -55,24 +58,170 @@ struct WorkerBufs {
     fy::DevBuf d_in, d_out;
     fy::HostBuf h_in, h_out;
     cudaStream_t hi = nullptr, lo = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};   // chain start, chain end
 };
 
-// Large copies go in chunks, so other requests' copies interleave with them on the link
-// instead of waiting behind one long transfer.
-constexpr size_t kCopyChunk = (size_t)32 << 20;
-cudaError_t copy_chunked(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st) {
-    for (size_t off = 0; off < bytes; off += kCopyChunk) {
-        const size_t len = bytes - off < kCopyChunk ? bytes - off : kCopyChunk;
-        const cudaError_t e = cudaMemcpyAsync((char*)dst + off, (const char*)src + off, len, kind, st);
-        if (e != cudaSuccess) return e;
+// One direction of the host<->device link, shared by all workers. A copy engine runs one
+// direction's copies in the order they were issued, so a small request's result would wait
+// behind every queued chunk of a large one. Instead one scheduler thread per direction
+// issues the copies chunk by chunk on its own stream, keeps at most kInflight chunks queued
+// on the engine (enough to keep the link busy), and always issues next from the job with
+// the fewest bytes left (ties: the earlier job). A small request then waits for at most the
+// chunks already queued.
+constexpr size_t kLinkChunk = (size_t)8 << 20;
+constexpr int kInflight = 2;
+
+struct LinkJob {
+    char* dst;
+    const char* src;
+    size_t bytes, issued = 0, done = 0;
+    long long seq = 0;
+    cudaError_t err = cudaSuccess;
+    bool finished = false;
+};
+
+class Link {
+  public:
+    // Starts the scheduler thread on `device`; returns once its stream and events exist.
+    cudaError_t start(int device, cudaMemcpyKind kind) {
+        device_ = device;
+        kind_ = kind;
+        th_ = std::thread([this] { run(); });
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_done_.wait(lk, [&] { return ready_; });
+        if (init_err_ != cudaSuccess) {
+            lk.unlock();
+            th_.join();
+        }
+        return init_err_;
     }
-    return cudaSuccess;
-}
+    // Copies bytes and returns when they have landed (or with the first error).
+    cudaError_t copy(void* dst, const void* src, size_t bytes) {
+        if (!bytes) return cudaSuccess;
+        LinkJob job;
+        job.dst = (char*)dst;
+        job.src = (const char*)src;
+        job.bytes = bytes;
+        std::unique_lock<std::mutex> lk(mu_);
+        job.seq = seq_++;
+        pending_.push_back(&job);
+        cv_.notify_one();
+        cv_done_.wait(lk, [&] { return job.finished; });
+        return job.err;
+    }
+    void stop() {
+        if (th_.joinable()) {
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                stopping_ = true;
+            }
+            cv_.notify_one();
+            th_.join();
+        }
+        release();
+    }
+
+  private:
+    struct Slot {
+        LinkJob* job;
+        size_t len;
+    };
+    void release() {
+        for (cudaEvent_t& ev : ev_)
+            if (ev) { cudaEventDestroy(ev); ev = nullptr; }
+        if (st_) { cudaStreamDestroy(st_); st_ = nullptr; }
+    }
+    // Caller holds mu_. Completed bytes of a job; the last ones finish it.
+    void complete(LinkJob* j, size_t len, cudaError_t e) {
+        if (e != cudaSuccess && j->err == cudaSuccess) j->err = e;
+        j->done += len;
+        if (j->done == j->bytes) {
+            j->finished = true;
+            cv_done_.notify_all();
+        }
+    }
+    void run() {
+        cudaError_t e0 = cudaSetDevice(device_);
+        if (e0 == cudaSuccess) e0 = cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking);
+        for (int i = 0; i < kInflight && e0 == cudaSuccess; ++i)
+            e0 = cudaEventCreateWithFlags(&ev_[i], cudaEventDisableTiming);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            if (e0 != cudaSuccess) { cudaGetLastError(); release(); }
+            init_err_ = e0;
+            ready_ = true;
+            cv_done_.notify_all();
+        }
+        if (e0 != cudaSuccess) return;
+        Slot slot[kInflight];
+        int head = 0, n = 0;
+        for (;;) {
+            LinkJob* pick = nullptr;
+            size_t off = 0, len = 0;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                if (n == 0) cv_.wait(lk, [&] { return stopping_ || !pending_.empty(); });
+                if (n == 0 && pending_.empty()) break;           // stopping, nothing left
+                if (n < kInflight && !pending_.empty()) {
+                    auto best = pending_.begin();
+                    for (auto it = pending_.begin(); it != pending_.end(); ++it) {
+                        const size_t left = (*it)->bytes - (*it)->issued, bl = (*best)->bytes - (*best)->issued;
+                        if (left < bl || (left == bl && (*it)->seq < (*best)->seq)) best = it;
+                    }
+                    pick = *best;
+                    off = pick->issued;
+                    len = pick->bytes - off < kLinkChunk ? pick->bytes - off : kLinkChunk;
+                    pick->issued += len;
+                    if (pick->issued == pick->bytes) pending_.erase(best);
+                }
+            }
+            if (pick) {
+                const int k = (head + n) % kInflight;
+                cudaError_t e = cudaMemcpyAsync(pick->dst + off, pick->src + off, len, kind_, st_);
+                if (e == cudaSuccess) e = cudaEventRecord(ev_[k], st_);
+                if (e != cudaSuccess) {                            // drop the job's unissued rest
+                    cudaGetLastError();
+                    std::lock_guard<std::mutex> lk(mu_);
+                    const size_t rest = pick->bytes - pick->issued;
+                    if (rest) {
+                        pick->issued = pick->bytes;
+                        pending_.erase(std::find(pending_.begin(), pending_.end(), pick));
+                    }
+                    complete(pick, len + rest, e);
+                    continue;
+                }
+                slot[k] = Slot{pick, len};
+                ++n;
+                continue;                                          // fill the next slot first
+            }
+            const cudaError_t e = cudaEventSynchronize(ev_[head]);   // oldest chunk in flight
+            if (e != cudaSuccess) cudaGetLastError();
+            const Slot sl = slot[head];
+            head = (head + 1) % kInflight;
+            --n;
+            std::lock_guard<std::mutex> lk(mu_);
+            complete(sl.job, sl.len, e);
+        }
+    }
+
+    int device_ = 0;
+    cudaMemcpyKind kind_ = cudaMemcpyHostToDevice;
+    cudaStream_t st_ = nullptr;
+    cudaEvent_t ev_[kInflight] = {};
+    std::mutex mu_;
+    std::condition_variable cv_, cv_done_;
+    std::vector<LinkJob*> pending_;
+    long long seq_ = 0;
+    bool stopping_ = false, ready_ = false;
+    cudaError_t init_err_ = cudaSuccess;
+    std::thread th_;
+};
 
 }  // namespace
 
 struct fy_server {
     fy_server_cfg cfg{};
+    Link h2d, d2h;                 // the two directions of the host<->device link
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Ticket*> queue;
@@ -110,6 +259,7 @@ void run_one(fy_server* s, Ticket* t, WorkerBufs& wb) {
     cudaError_t e;
     int rc = FY_OK;
     const bool in_pinned = fy::is_pinned(r.u8), out_pinned = fy::is_pinned(r.out);
+    const bool timed = wb.ev[1] != nullptr;
     do {
         if ((e = wb.d_in.ensure(n)) != cudaSuccess || (e = wb.d_out.ensure(4 * n)) != cudaSuccess) {
             rc = fail_cuda(e, "fy_server");
@@ -121,23 +271,33 @@ void run_one(fy_server* s, Ticket* t, WorkerBufs& wb) {
             memcpy(wb.h_in.p, r.u8, n);
             src = (const unsigned char*)wb.h_in.p;
         }
-        if ((e = copy_chunked(wb.d_in.p, src, n, cudaMemcpyHostToDevice, st)) != cudaSuccess) {
+        double t0 = now_ms();
+        if ((e = s->h2d.copy(wb.d_in.p, src, n)) != cudaSuccess) {
             rc = fail_cuda(e, "fy_server");
             break;
         }
+        t->h2d_ms = (float)(now_ms() - t0);
+        if (timed) cudaEventRecord(wb.ev[0], st);
         rc = fy_gpu_restore_u8(wb.d_in.as<unsigned char>(), wb.d_out.as<float>(), r.nz, r.ny, r.nx, r.f32_min,
                                r.f32_max, &r.phys, &r.cfg, st);
         if (rc) break;
+        if (timed) cudaEventRecord(wb.ev[1], st);
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) {
+            rc = fail_cuda(e, "fy_server");
+            break;
+        }
+        if (timed && cudaEventElapsedTime(&t->chain_ms, wb.ev[0], wb.ev[1]) != cudaSuccess) cudaGetLastError();
         float* dst = r.out;
         if (!out_pinned) {
             if ((e = wb.h_out.ensure(4 * n)) != cudaSuccess) { rc = fail_cuda(e, "fy_server"); break; }
             dst = (float*)wb.h_out.p;
         }
-        if ((e = copy_chunked(dst, wb.d_out.p, 4 * n, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-            (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+        t0 = now_ms();
+        if ((e = s->d2h.copy(dst, wb.d_out.p, 4 * n)) != cudaSuccess) {
             rc = fail_cuda(e, "fy_server");
             break;
         }
+        t->d2h_ms = (float)(now_ms() - t0);
         if (!out_pinned) memcpy(r.out, wb.h_out.p, 4 * n);
     } while (false);
     std::lock_guard<std::mutex> lk(s->mu);
@@ -178,6 +338,11 @@ void worker_main(fy_server* s, int idx) {
             cudaGetLastError();
             wb.hi = wb.lo = ctx().st;
         }
+        for (cudaEvent_t& ev : wb.ev)
+            if (cudaEventCreate(&ev) != cudaSuccess) { cudaGetLastError(); ev = nullptr; }
+        if (!wb.ev[0] || !wb.ev[1])                                      // untimed unless both exist
+            for (cudaEvent_t& ev : wb.ev)
+                if (ev) { cudaEventDestroy(ev); ev = nullptr; }
     }
     for (;;) {
         Ticket* t = nullptr;
@@ -240,6 +405,8 @@ void worker_main(fy_server* s, int idx) {
     }
     if (wb.hi && wb.hi != ctx().st) cudaStreamDestroy(wb.hi);
     if (wb.lo && wb.lo != ctx().st) cudaStreamDestroy(wb.lo);
+    for (cudaEvent_t ev : wb.ev)
+        if (ev) cudaEventDestroy(ev);
     wb.d_in.release();
     wb.d_out.release();
     wb.h_in.release();
@@ -272,6 +439,12 @@ extern "C" int fy_server_create(fy_server** out, const fy_server_cfg* cfg) {
     if (s->cfg.small_workers >= s->cfg.workers) s->cfg.small_workers = s->cfg.workers - 1;
     if (s->cfg.workers > 64) s->cfg.workers = 64;
     if (s->cfg.hbm_budget_bytes == 0) s->cfg.hbm_budget_bytes = (size_t)150 << 30;
+    cudaError_t e = s->h2d.start(s->cfg.device, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && (e = s->d2h.start(s->cfg.device, cudaMemcpyDeviceToHost)) != cudaSuccess) s->h2d.stop();
+    if (e != cudaSuccess) {
+        delete s;
+        return fail_cuda(e, "fy_server_create: link scheduler");
+    }
     for (int i = 0; i < s->cfg.workers; ++i) s->workers.emplace_back(worker_main, s, i);
     *out = s;
     return FY_OK;
@@ -322,6 +495,9 @@ extern "C" int fy_server_wait(fy_server* s, long long ticket, double timeout_ms,
         res->queue_ms = t->t_start > 0 ? t->t_start - t->t_submit : 0.0;
         res->run_ms = t->t_start > 0 ? t->t_done - t->t_start : 0.0;
         res->latency_ms = t->t_done - t->t_submit;
+        res->h2d_ms = t->h2d_ms;
+        res->chain_ms = t->chain_ms;
+        res->d2h_ms = t->d2h_ms;
     }
     const int st = t->status;
     s->tickets.erase(it);
@@ -370,6 +546,8 @@ extern "C" void fy_server_destroy(fy_server* s) {
     }
     s->cv_work.notify_all();
     for (auto& w : s->workers) w.join();
+    s->h2d.stop();
+    s->d2h.stop();
     for (auto& kv : s->tickets) delete kv.second;
     delete s;
 }

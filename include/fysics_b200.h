@@ -322,6 +322,9 @@ typedef struct {
 typedef struct {
     int    status;
     double queue_ms, run_ms, latency_ms;   /* submit -> start, start -> done, submit -> done */
+    /* device-side phases from CUDA events on the worker's stream: input copy, the chain
+     * (including time its kernels waited for other requests' work), output copy */
+    double h2d_ms, chain_ms, d2h_ms;
 } fy_request_result;
 typedef struct {
     long long completed;
