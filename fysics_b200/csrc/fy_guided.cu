@@ -95,24 +95,21 @@ static size_t round64(size_t v) { return (v + 63) & ~(size_t)63; }
 size_t fy_guided_fused_scratch_floats(size_t n) { return 2 * round64(n); }
 
 // Exact guided filter for r in [1, 4] as two z-sliding box passes (fy_zbox.cuh):
-// in -> (a, b) into ab_ws, then box(a), box(b) -> out. ab_ws holds
+// in -> interleaved (a, b) pairs into ab_ws, then box(a), box(b) -> out. ab_ws holds
 // fy_guided_fused_scratch_floats(n) floats; out may alias in. mode 1 writes box(a) to out
 // and box(b) to out_b instead of the filtered volume.
 cudaError_t fy_launch_guided_fused(const float* in, float* out, float* out_b, float* ab_ws, int nz, int ny, int nx,
                                    int r, float eps, int mode, int sms, cudaStream_t st, const float* eps_ptr,
                                    const RingApply* rings) {
     if (r < 1 || r > 4) return cudaErrorInvalidValue;
-    const size_t n = (size_t)nz * ny * nx;
-    float* A = ab_ws;
-    float* B = ab_ws + round64(n);
     fyzb::Params p{};
     p.nz = nz; p.ny = ny; p.nx = nx;
-    p.f0 = in; p.o0 = A; p.o1 = B; p.eps = eps; p.eps_ptr = eps_ptr;
+    p.f0 = in; p.o0 = ab_ws; p.eps = eps; p.eps_ptr = eps_ptr;
     cudaError_t e = fyzb::launch<fyzb::ZB_GUIDED_AB>(p, r, sms, st);
     if (e != cudaSuccess) return e;
     fyzb::Params q{};
     q.nz = nz; q.ny = ny; q.nx = nx;
-    q.f0 = A; q.f1 = B; q.guide = in; q.o0 = out; q.o1 = out_b; q.out_mode = mode;
+    q.f0 = ab_ws; q.guide = in; q.o0 = out; q.o1 = out_b; q.out_mode = mode;
     if (rings && mode == 0) q.ra = *rings;
     return fyzb::launch<fyzb::ZB_GUIDED_OUT>(q, r, sms, st);
 }

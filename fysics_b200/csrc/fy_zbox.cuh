@@ -6,21 +6,26 @@
 //   stage   the plane's tile plus halo (x0-4 .. x0+68, y0-R .. y0+16+R) lands in a 4-deep
 //           shared-memory ring, zero-filled outside the volume; planes zi+1 .. zi+3 are in
 //           flight while zi is reduced. 16-byte-aligned rows: one thread issues a 3-D tensor
-//           copy (TMA) per field, completing on the slot's mbarrier. Other shapes: cp.async
+//           copy (TMA) per plane, completing on the slot's mbarrier. Other shapes: cp.async
 //           by all threads.
-//   X phase one item = 4 output columns of one staged row: three float4 reads, window
+//   X phase one item = 4 output columns of one staged row: the row's values, the window
 //           sums of both quantities, two float4 stores.
 //   Y phase one thread = one output column x 4 output rows. Its (2R+1)-plane z ring of
 //           XY sums stays in registers and gives the box of plane zi - R to the epilogue.
+// The two quantities travel as one float2 through all three window sums, so each tap is
+// one paired FP32 add (__fadd2_rn: two IEEE round-to-nearest adds, the same results as two
+// scalar adds in the same order) and the XY sums are stored and read as pairs.
 // Epilogues (KIND):
 //   ZB_NOISE      u = I - c (zero outside the volume), fixed divisor win^3: local mean and
 //                 variance as in noise.c:41-61, with the tile shift c removing the FP32
 //                 cancellation of E[I^2] - E[I]^2.
 //   ZB_GUIDED_AB  u = I - c, box MEANS over the in-bounds window taken axis by axis with
 //                 1.0f/(float)count (guided.c:22-28): var = max(corr - mean^2, 0),
-//                 a = var/(var + eps), b = mean*(1 - a) (guided.c:121-132) -> A, B.
-//   ZB_GUIDED_OUT box means of A and B -> out = box(a)*I + box(b) (guided.c:136-140), or
-//                 the two means themselves for the decimated variant (guided.c:181-182).
+//                 a = var/(var + eps), b = mean*(1 - a) (guided.c:121-132) -> interleaved
+//                 (a, b) pairs, one 8-byte store per voxel.
+//   ZB_GUIDED_OUT box means of the (a, b) pairs -> out = box(a)*I + box(b)
+//                 (guided.c:136-140), or the two means themselves for the decimated variant
+//                 (guided.c:181-182). The pairs are staged as one interleaved field.
 // Window sums are direct (2R+1)-tap float sums in ascending order, started from the first
 // tap, so no running-sum chain accumulates error. Each output voxel is written once by one
 // thread, and ZB_GUIDED_OUT reads the guide only at the voxel it writes, so out may alias
@@ -38,11 +43,10 @@ constexpr int SXW = TX + 8;                 // staged row: x0 - 4 .. x0 + TX + 4
 enum { ZB_NOISE = 0, ZB_GUIDED_AB = 1, ZB_GUIDED_OUT = 2 };
 
 struct Params {
-    const float* f0;       // I (NOISE, GUIDED_AB) or A (GUIDED_OUT)
-    const float* f1;       // B (GUIDED_OUT)
+    const float* f0;       // I (NOISE, GUIDED_AB) or the interleaved (a, b) pairs (GUIDED_OUT)
     const float* guide;    // I (GUIDED_OUT, out_mode 0)
-    float* o0;             // mean | A | out (or box(a))
-    float* o1;             // var  | B | box(b) (out_mode 1)
+    float* o0;             // mean | (a, b) pairs | out (or box(a))
+    float* o1;             // var  | -      | box(b) (out_mode 1)
     const float* eps_ptr;  // GUIDED_AB: device eps (overrides eps when set)
     float eps;
     float inv_wc;          // NOISE: 1/win^3
@@ -52,13 +56,14 @@ struct Params {
     RingApply ra;          // GUIDED_OUT, out_mode 0: ring subtraction on the output (optional)
 };
 
-template <int R, int NF>
+// C = floats per staged voxel: 1 (I) or 2 (interleaved a, b).
+template <int R, int C>
 struct Geo {
     static constexpr int NR = 2 * R + 1;
     static constexpr int SY = TY + 2 * R;
-    static constexpr int FS = (SY * SXW + 31) / 32 * 32;        // floats per staged field (128 B multiple)
-    static constexpr int STAGE = NF * FS;                       // floats per staged plane
-    static constexpr int XS = SY * TX;                          // floats per X-sum array
+    static constexpr int RW = C * SXW;                           // floats per staged row
+    static constexpr int STAGE = (SY * RW + 31) / 32 * 32;      // floats per staged plane (128 B multiple)
+    static constexpr int XS = SY * TX;                          // float2 per X-sum array
     static constexpr size_t bytes = (size_t)(NS * STAGE + 2 * XS + TX + TY) * sizeof(float) + 128;   // + alignment
 };
 
@@ -67,6 +72,9 @@ FY_D float recip_count(int p, int L, int r) {
     const int hi = p + r > L - 1 ? L - 1 : p + r;
     return 1.0f / (float)(hi - lo + 1);                       // guided.c:26 (IEEE division)
 }
+
+FY_D float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+FY_D float2 mul2(float2 a, float f) { return __fmul2_rn(a, make_float2(f, f)); }
 
 FY_D void cp16(float* sdst, const float* gsrc, bool valid) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
@@ -82,11 +90,11 @@ FY_D void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 FY_D void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// ---- TMA staging: one thread copies a plane's tile (per field) with cp.async.bulk.tensor,
-// completion tracked by one mbarrier per ring slot. Waits are bounded: on expiry the kernel
-// raises zb_timeout, waits (bounded) for its own copies in flight and returns.
+// ---- TMA staging: one thread copies a plane's tile with cp.async.bulk.tensor, completion
+// tracked by one mbarrier per ring slot. Waits are bounded: on expiry the kernel raises
+// zb_timeout, waits (bounded) for its own copies in flight and returns.
 struct TmaMaps {
-    CUtensorMap m0, m1;                // field 0 and field 1 (GUIDED_OUT); 64-byte aligned type
+    CUtensorMap m0;                    // the staged field; 64-byte aligned type
 };
 static __device__ int zb_timeout;      // set when a bounded wait expires (never expected)
 constexpr int kWaitSpins = 1 << 20;
@@ -120,60 +128,52 @@ FY_D void tma_load_3d(float* dst, const CUtensorMap* map, int x, int y, int z, u
         : "memory");
 }
 
-// Issue plane zi (all NF fields) into slot `dst` (thread 0 only). x starts at x0 - 4, a
+// Issue plane zi into slot `dst` (thread 0 only). The innermost coordinate C*(x0 - 4) is a
 // multiple of 4 floats (16 bytes) as the tensor copy requires; rows and planes outside the
 // volume, negative ones included, are zero-filled by the copy.
-template <int R, int NF>
+template <int R, int C>
 FY_D void tma_stage(float* dst, const TmaMaps& tm, unsigned long long* bar, int zi, int x0, int y0) {
-    using G = Geo<R, NF>;
+    using G = Geo<R, C>;
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // prior generic reads of the slot
-    mbar_expect_tx(bar, (unsigned)(NF * G::SY * SXW * sizeof(float)));
-    tma_load_3d(dst, &tm.m0, x0 - 4, y0 - R, zi, bar);
-    if (NF == 2) tma_load_3d(dst + G::FS, &tm.m1, x0 - 4, y0 - R, zi, bar);
+    mbar_expect_tx(bar, (unsigned)(G::SY * G::RW * sizeof(float)));
+    tma_load_3d(dst, &tm.m0, C * (x0 - 4), y0 - R, zi, bar);
 }
 
-// Stage plane zi (all NF fields) into dst; zero fill outside the volume.
-template <int R, int NF, bool VEC>
+// Stage plane zi into dst with cp.async; zero fill outside the volume. VEC: 16-byte copies
+// (nx % 4 == 0, so a copy never straddles the volume's x edge).
+template <int R, int C, bool VEC>
 FY_D void stage_plane(float* dst, const Params& p, int zi, int x0, int y0) {
-    using G = Geo<R, NF>;
+    using G = Geo<R, C>;
     const bool zin = zi >= 0 && zi < p.nz;
     const size_t pbase = (size_t)(zin ? zi : 0) * p.ny * p.nx;
     if (VEC) {
-        constexpr int Q = SXW / 4, PER = G::SY * Q;
-        for (int k = threadIdx.x; k < NF * PER; k += NT) {
-            const int f = NF == 1 ? 0 : k / PER;
-            const int rem = k - f * PER;
-            const int yy = rem / Q, q = rem - yy * Q;
-            const int gy = y0 - R + yy, gx = x0 - 4 + 4 * q;
+        constexpr int Q = G::RW / 4;
+        for (int k = threadIdx.x; k < G::SY * Q; k += NT) {
+            const int yy = k / Q, q = k - yy * Q;
+            const int gy = y0 - R + yy, gx = x0 - 4 + 4 * q / C;
             const bool ok = zin && gy >= 0 && gy < p.ny && gx >= 0 && gx < p.nx;
-            const float* base = f ? p.f1 : p.f0;
-            cp16(dst + f * G::FS + yy * SXW + 4 * q, ok ? base + pbase + (size_t)gy * p.nx + gx : base, ok);
+            cp16(dst + yy * G::RW + 4 * q, ok ? p.f0 + (pbase + (size_t)gy * p.nx + gx) * C : p.f0, ok);
         }
     } else {
-        constexpr int PER = G::SY * SXW;
-        for (int k = threadIdx.x; k < NF * PER; k += NT) {
-            const int f = NF == 1 ? 0 : k / PER;
-            const int rem = k - f * PER;
-            const int yy = rem / SXW, xx = rem - yy * SXW;
-            const int gy = y0 - R + yy, gx = x0 - 4 + xx;
+        for (int k = threadIdx.x; k < G::SY * G::RW; k += NT) {
+            const int yy = k / G::RW, e = k - yy * G::RW;
+            const int gy = y0 - R + yy, gx = x0 - 4 + e / C;
             const bool ok = zin && gy >= 0 && gy < p.ny && gx >= 0 && gx < p.nx;
-            const float* base = f ? p.f1 : p.f0;
-            cp4(dst + f * G::FS + rem, ok ? base + pbase + (size_t)gy * p.nx + gx : base, ok);
+            cp4(dst + k, ok ? p.f0 + (pbase + (size_t)gy * p.nx + gx) * C + (e - (e / C) * C) : p.f0, ok);
         }
     }
 }
 
 template <int R, int KIND, bool VEC, bool TMA>
 __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p, const __grid_constant__ TmaMaps tm) {
-    constexpr int NF = KIND == ZB_GUIDED_OUT ? 2 : 1;
-    using G = Geo<R, NF>;
+    constexpr int C = KIND == ZB_GUIDED_OUT ? 2 : 1;
+    using G = Geo<R, C>;
     constexpr int NR = G::NR;
     extern __shared__ float4 zb_smem4[];
     __shared__ __align__(8) unsigned long long bars[NS];
     float* stage = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(zb_smem4) + 127) & ~(uintptr_t)127);
-    float* xs1 = stage + NS * G::STAGE;
-    float* xs2 = xs1 + G::XS;
-    float* rx = xs2 + G::XS;
+    float2* xs = reinterpret_cast<float2*>(stage + NS * G::STAGE);   // X sums of both quantities, [SY][TX]
+    float* rx = reinterpret_cast<float*>(xs + G::XS);
     float* ry = rx + TX;
     const int t = threadIdx.x;
     const int nz = p.nz, ny = p.ny, nx = p.nx;
@@ -196,11 +196,11 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
         __syncthreads();
         if (t == 0)
             for (int s = 0; s < NS - 1; ++s)
-                if (zfirst + s < zend) tma_stage<R, NF>(stage + s * G::STAGE, tm, &bars[s], zfirst + s, x0, y0);
+                if (zfirst + s < zend) tma_stage<R, C>(stage + s * G::STAGE, tm, &bars[s], zfirst + s, x0, y0);
     } else {
 #pragma unroll
         for (int s = 0; s < NS - 1; ++s) {
-            if (zfirst + s < zend) stage_plane<R, NF, VEC>(stage + s * G::STAGE, p, zfirst + s, x0, y0);
+            if (zfirst + s < zend) stage_plane<R, C, VEC>(stage + s * G::STAGE, p, zfirst + s, x0, y0);
             cp_commit();
         }
     }
@@ -227,11 +227,11 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
             ri[k] = (int)(sqrt(gyd * gyd + gxd * gxd) + 0.5);
         }
     }
-    float r1[NR][4], r2[NR][4];
+    float2 rz2[NR][4];                                            // z ring of XY sums
 #pragma unroll
     for (int q = 0; q < NR; ++q)
 #pragma unroll
-        for (int k = 0; k < 4; ++k) r1[q][k] = r2[q][k] = 0.f;
+        for (int k = 0; k < 4; ++k) rz2[q][k] = make_float2(0.f, 0.f);
 
     // The plane loop is unrolled by NR so the z ring rotates by naming: plane zi lands in
     // ring slot ph = (zi - zfirst) mod NR, and the window of plane zi - R is slots ph+1 ..
@@ -256,13 +256,13 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                 }
                 const int zn = zi + NS - 1;       // plane zi landed for every thread; xs free again
                 if (t == 0 && zn < zend)
-                    tma_stage<R, NF>(stage + ((zn - zfirst) & (NS - 1)) * G::STAGE, tm, &bars[(zn - zfirst) & (NS - 1)],
-                                     zn, x0, y0);
+                    tma_stage<R, C>(stage + ((zn - zfirst) & (NS - 1)) * G::STAGE, tm, &bars[(zn - zfirst) & (NS - 1)],
+                                    zn, x0, y0);
             } else {
                 cp_wait<NS - 2>();
                 __syncthreads();             // plane zi landed for every thread; xs free again
                 const int zn = zi + NS - 1;
-                if (zn < zend) stage_plane<R, NF, VEC>(stage + ((zn - zfirst) & (NS - 1)) * G::STAGE, p, zn, x0, y0);
+                if (zn < zend) stage_plane<R, C, VEC>(stage + ((zn - zfirst) & (NS - 1)) * G::STAGE, p, zn, x0, y0);
                 cp_commit();
             }
             const int zo = zi - R;
@@ -276,23 +276,26 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
             }
             const float* sp = stage + slot * G::STAGE;
             const bool zin = zi >= 0 && zi < nz;
-            // X phase
+            // X phase: P[j] = both quantities of staged column x0 - 4 + x4 + j
             for (int it = t; it < G::SY * (TX / 4); it += NT) {
                 const int yy = it >> 4, x4 = (it & 15) << 2;
-                const float* row = sp + yy * SXW + x4;
-                float q1[12], q2[12];
+                float2 P[12];
+                if (C == 2) {                    // interleaved pairs: float4 = two columns
+                    const float* row = sp + yy * G::RW + 2 * x4;
 #pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const float4 v = *reinterpret_cast<const float4*>(row + 4 * j);
-                    q1[4 * j] = v.x; q1[4 * j + 1] = v.y; q1[4 * j + 2] = v.z; q1[4 * j + 3] = v.w;
-                }
-                if (NF == 2) {
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        const float4 v = *reinterpret_cast<const float4*>(row + G::FS + 4 * j);
-                        q2[4 * j] = v.x; q2[4 * j + 1] = v.y; q2[4 * j + 2] = v.z; q2[4 * j + 3] = v.w;
+                    for (int j2 = (4 - R) / 2; j2 <= (7 + R) / 2; ++j2) {
+                        const float4 v = *reinterpret_cast<const float4*>(row + 4 * j2);
+                        P[2 * j2] = make_float2(v.x, v.y);
+                        P[2 * j2 + 1] = make_float2(v.z, v.w);
                     }
                 } else {
+                    const float* row = sp + yy * G::RW + x4;
+                    float q1[12];
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        const float4 v = *reinterpret_cast<const float4*>(row + 4 * j);
+                        q1[4 * j] = v.x; q1[4 * j + 1] = v.y; q1[4 * j + 2] = v.z; q1[4 * j + 3] = v.w;
+                    }
                     const int gy = y0 - R + yy;
                     const bool rin = zin && gy >= 0 && gy < ny;
                     if (cols_in) {
@@ -307,33 +310,34 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                         }
                     }
 #pragma unroll
-                    for (int j = 4 - R; j < 8 + R; ++j) q2[j] = q1[j] * q1[j];
+                    for (int j = 4 - R; j < 8 + R; ++j) P[j] = make_float2(q1[j], q1[j] * q1[j]);
                 }
-                float o1[4], o2[4];
+                float2 o[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    float s1 = q1[4 + k - R], s2 = q2[4 + k - R];
+                    float2 sm = P[4 + k - R];
 #pragma unroll
-                    for (int j = 5 + k - R; j <= 4 + k + R; ++j) { s1 += q1[j]; s2 += q2[j]; }
-                    if (KIND != ZB_NOISE) { const float f = rx[x4 + k]; s1 *= f; s2 *= f; }
-                    o1[k] = s1; o2[k] = s2;
+                    for (int j = 5 + k - R; j <= 4 + k + R; ++j) sm = add2(sm, P[j]);
+                    if (KIND != ZB_NOISE) sm = mul2(sm, rx[x4 + k]);
+                    o[k] = sm;
                 }
-                *reinterpret_cast<float4*>(xs1 + yy * TX + x4) = make_float4(o1[0], o1[1], o1[2], o1[3]);
-                *reinterpret_cast<float4*>(xs2 + yy * TX + x4) = make_float4(o2[0], o2[1], o2[2], o2[3]);
+                float4* dst = reinterpret_cast<float4*>(xs + yy * TX + x4);
+                dst[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+                dst[1] = make_float4(o[2].x, o[2].y, o[3].x, o[3].y);
             }
             __syncthreads();
             // Y phase -> ring slot ph
             {
-                float a1[4 + 2 * R], a2[4 + 2 * R];
+                float2 a[4 + 2 * R];
 #pragma unroll
-                for (int j = 0; j < 4 + 2 * R; ++j) { a1[j] = xs1[(4 * rg + j) * TX + xc]; a2[j] = xs2[(4 * rg + j) * TX + xc]; }
+                for (int j = 0; j < 4 + 2 * R; ++j) a[j] = xs[(4 * rg + j) * TX + xc];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    float s1 = a1[k], s2 = a2[k];
+                    float2 sm = a[k];
 #pragma unroll
-                    for (int j = 1; j <= 2 * R; ++j) { s1 += a1[k + j]; s2 += a2[k + j]; }
-                    if (KIND != ZB_NOISE) { const float f = ry[4 * rg + k]; s1 *= f; s2 *= f; }
-                    r1[ph][k] = s1; r2[ph][k] = s2;
+                    for (int j = 1; j <= 2 * R; ++j) sm = add2(sm, a[k + j]);
+                    if (KIND != ZB_NOISE) sm = mul2(sm, ry[4 * rg + k]);
+                    rz2[ph][k] = sm;
                 }
             }
             if (!emit) continue;
@@ -353,9 +357,10 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 if (y0 + 4 * rg + k >= ny) continue;
-                float s1 = r1[(ph + 1) % NR][k], s2 = r2[(ph + 1) % NR][k];
+                float2 sm = rz2[(ph + 1) % NR][k];
 #pragma unroll
-                for (int q = 2; q <= NR; ++q) { s1 += r1[(ph + q) % NR][k]; s2 += r2[(ph + q) % NR][k]; }
+                for (int q = 2; q <= NR; ++q) sm = add2(sm, rz2[(ph + q) % NR][k]);
+                const float s1 = sm.x, s2 = sm.y;
                 const size_t o = obase + (size_t)k * nx;
                 if (KIND == ZB_NOISE) {
                     const int nini = cz * cyx[k];
@@ -373,24 +378,23 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                     p.o0[o] = m;
                     p.o1[o] = v;
                 } else if (KIND == ZB_GUIDED_AB) {
-                    const float e1 = s1 * rz, e2 = s2 * rz;        // E[I-c], E[(I-c)^2]
-                    float var = e2 - e1 * e1;
+                    const float2 e = mul2(sm, rz);                 // E[I-c], E[(I-c)^2]
+                    float var = e.y - e.x * e.x;
                     if (var < 0.f) var = 0.f;
-                    const float mean = e1 + c;
+                    const float mean = e.x + c;
                     const float a = var / (var + eps);             // guided.c:129
-                    p.o0[o] = a;
-                    p.o1[o] = mean * (1.0f - a);                   // guided.c:131
+                    reinterpret_cast<float2*>(p.o0)[o] = make_float2(a, mean * (1.0f - a));   // guided.c:131
                 } else {
-                    const float ma = s1 * rz, mb = s2 * rz;
+                    const float2 mab = mul2(sm, rz);
                     if (p.out_mode == 0) {
-                        float w = ma * gv[k] + mb;
+                        float w = mab.x * gv[k] + mab.y;
                         if (rings && w > 0.f && ri[k] < p.ra.nr) {     // masked voxels untouched
                             const float w2 = w - p.ra.sc * rv[k];
                             w = w2 > 0.f ? w2 : 0.f;
                         }
                         p.o0[o] = w;
                     } else {
-                        p.o0[o] = ma; p.o1[o] = mb;
+                        p.o0[o] = mab.x; p.o1[o] = mab.y;
                     }
                 }
             }
@@ -412,10 +416,11 @@ inline dim3 grid_for(int nz, int ny, int nx, int r, int sms, int& zchunk) {
     return dim3(tx, ty, (nz + zchunk - 1) / zchunk);
 }
 
-// Tensor map of one f32 volume field for the TMA staging: box (x0-4 .. x0+TX+4, SY rows, 1
-// plane), zero fill outside. The encoder comes from the driver through the runtime, so the
-// library needs no link-time driver dependency. Returns false when unavailable.
-inline bool make_tma_map(CUtensorMap* m, const float* base, int nz, int ny, int nx, int sy) {
+// Tensor map of one f32 volume field of C floats per voxel for the TMA staging: box
+// (C*(x0-4) .. C*(x0+TX+4), SY rows, 1 plane), zero fill outside. The encoder comes from the
+// driver through the runtime, so the library needs no link-time driver dependency. Returns
+// false when unavailable.
+inline bool make_tma_map(CUtensorMap* m, const float* base, int nz, int ny, int nx, int c, int sy) {
     using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -431,9 +436,9 @@ inline bool make_tma_map(CUtensorMap* m, const float* base, int nz, int ny, int 
             cudaGetLastError();
     });
     if (!fn || ((uintptr_t)base & 15) || (nx % 4)) return false;
-    const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
-    const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4};
-    const cuuint32_t box[3] = {(cuuint32_t)SXW, (cuuint32_t)sy, 1};
+    const cuuint64_t dims[3] = {(cuuint64_t)nx * c, (cuuint64_t)ny, (cuuint64_t)nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)nx * c * 4, (cuuint64_t)nx * ny * c * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)(SXW * c), (cuuint32_t)sy, 1};
     const cuuint32_t es[3] = {1, 1, 1};
     return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -442,15 +447,11 @@ inline bool make_tma_map(CUtensorMap* m, const float* base, int nz, int ny, int 
 
 template <int KIND, int R, bool VEC>
 inline cudaError_t launch_r(const Params& p, dim3 grid, cudaStream_t st) {
-    constexpr int NF = KIND == ZB_GUIDED_OUT ? 2 : 1;
-    const size_t smem = Geo<R, NF>::bytes;
+    constexpr int C = KIND == ZB_GUIDED_OUT ? 2 : 1;
+    const size_t smem = Geo<R, C>::bytes;
     TmaMaps tm;
     memset(&tm, 0, sizeof tm);
-    bool tma = false;
-    if (VEC) {
-        tma = make_tma_map(&tm.m0, p.f0, p.nz, p.ny, p.nx, Geo<R, NF>::SY) &&
-              (NF == 1 || make_tma_map(&tm.m1, p.f1, p.nz, p.ny, p.nx, Geo<R, NF>::SY));
-    }
+    const bool tma = VEC && make_tma_map(&tm.m0, p.f0, p.nz, p.ny, p.nx, C, Geo<R, C>::SY);
     cudaError_t e;
     if (tma) {
         auto k = k_zbox<R, KIND, true, true>;
@@ -476,7 +477,7 @@ template <int KIND>
 inline cudaError_t launch(Params p, int r, int sms, cudaStream_t st) {
     const dim3 grid = grid_for(p.nz, p.ny, p.nx, r, sms, p.zchunk);
     auto al = [](const void* q) { return ((uintptr_t)q & 15) == 0; };
-    const bool vec = p.nx % 4 == 0 && al(p.f0) && (KIND != ZB_GUIDED_OUT || al(p.f1));
+    const bool vec = p.nx % 4 == 0 && al(p.f0);
     switch (r * 2 + (vec ? 1 : 0)) {
         case 2: return launch_r<KIND, 1, false>(p, grid, st);
         case 3: return launch_r<KIND, 1, true>(p, grid, st);
