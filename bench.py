@@ -140,10 +140,13 @@ def algorithmic_bytes(name: str, n: int, geo: dict) -> float | None:
         "deconv.z_weight": 2 * nz * geo["py"] * hx * 8,
         "deconv.y_inv": nz * geo["py"] * hx * 8 + half,
         "deconv.x_inv": half + n * 4,
-        "noise.stats": n * 12,                 # box pass: I read, mean + var written
+        # box pass: I read, mean + var written (+ the guided (mean, var) pairs when the noise
+        # window is the guided window: the chain then skips the guided a/b pass)
+        "noise.stats": n * (20 if geo.get("shared_window") else 12),
         "noise.lohi": n * 12,                  # 3 digit passes over mean
         "noise.bin_select": n * 24,            # mean + var read, labels written; 3 passes over var + labels
-        "guided": n * 28,                      # I -> a, b (12 B); a, b, I -> out (16 B)
+        # (mean, var) pairs + I -> out (16 B); without the shared window I -> a, b (12 B) first
+        "guided": n * (16 if geo.get("shared_window") else 28),
         "dering.accumulate+vote": n * 1,
         "dering.apply": n * 8,
     }
@@ -153,9 +156,9 @@ def algorithmic_bytes(name: str, n: int, geo: dict) -> float | None:
 # DRAM bytes per voxel of each instrumented span, from a one-pass ncu capture of the 512^3
 # chain (dram__bytes_read.sum + dram__bytes_write.sum per launch; profiles/dram_restore_512.md).
 DRAM_BYTES_PER_VOXEL = {
-    "deconv.x_fwd": 4.654, "deconv.y_fwd": 8.032, "deconv.z_weight": 8.284, "deconv.y_inv": 8.027,
-    "deconv.x_inv": 7.877, "noise.stats": 11.638, "noise.lohi": 12.006, "noise.bin_select": 23.93,
-    "guided": 27.617, "dering.accumulate+vote": 0.507,
+    "deconv.x_fwd": 4.653, "deconv.y_fwd": 8.031, "deconv.z_weight": 8.290, "deconv.y_inv": 8.031,
+    "deconv.x_inv": 7.880, "noise.stats": 19.647, "noise.lohi": 12.003, "noise.bin_select": 23.931,
+    "guided": 15.938, "dering.accumulate+vote": 0.507,
 }
 
 
@@ -667,7 +670,8 @@ def main():
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    geo = {"shape": SHAPE, "px": fb.load().fy_next_fft_size(nx), "py": fb.load().fy_next_fft_size(ny)}
+    geo = {"shape": SHAPE, "px": fb.load().fy_next_fft_size(nx), "py": fb.load().fy_next_fft_size(ny),
+           "shared_window": cfg.noise_win == 2 * cfg.guided_radius + 1 and cfg.guided_s <= 1}
     kernels = {}
     for name, v in prof.items():
         avg = sum(v) / len(v)

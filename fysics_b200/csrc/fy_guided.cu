@@ -10,7 +10,9 @@
 // from box means of (I - c) and (I - c)^2 with a per-tile shift c, which makes
 // E[(I-c)^2] - E[I-c]^2 = E[I^2] - E[I]^2 exactly while removing most of the FP32
 // cancellation that dominates the reference's error (guided.c:127); the second boxes a and
-// b and applies them. 12 + 16 B/voxel of HBM traffic.
+// b and applies them. 12 + 16 B/voxel of HBM traffic. In a chain whose noise model uses the
+// same window, the noise statistics pass also writes (mean, var) and only the second pass
+// runs here (fy_launch_guided_apply_mv).
 //
 // Generic path (any r, and fy_box_smooth): separable direct-sum box passes along x, y, z
 // plus elementwise a/b and output kernels.
@@ -112,6 +114,21 @@ cudaError_t fy_launch_guided_fused(const float* in, float* out, float* out_b, fl
     q.f0 = ab_ws; q.guide = in; q.o0 = out; q.o1 = out_b; q.out_mode = mode;
     if (rings && mode == 0) q.ra = *rings;
     return fyzb::launch<fyzb::ZB_GUIDED_OUT>(q, r, sms, st);
+}
+
+// Output pass alone, from the guided (mean, var) pairs that the noise model's statistics pass
+// wrote for the same window (fy_launch_estimate_noise with guided_mv): (a, b) are formed per
+// staged voxel with the a/b pass's expressions, then boxed and applied as above. eps (or
+// *eps_ptr) must be > 0.
+cudaError_t fy_launch_guided_apply_mv(const float* mv, const float* in, float* out, int nz, int ny, int nx, int r,
+                                      float eps, int sms, cudaStream_t st, const float* eps_ptr,
+                                      const RingApply* rings) {
+    if (r < 1 || r > 4) return cudaErrorInvalidValue;
+    fyzb::Params q{};
+    q.nz = nz; q.ny = ny; q.nx = nx;
+    q.f0 = mv; q.guide = in; q.o0 = out; q.out_mode = 0; q.eps = eps; q.eps_ptr = eps_ptr;
+    if (rings) q.ra = *rings;
+    return fyzb::launch<fyzb::ZB_GUIDED_OUT_MV>(q, r, sms, st);
 }
 
 // ---------------------------------------------------------------- fast (s-decimated) variant

@@ -69,13 +69,17 @@ cudaError_t fy_launch_guided_fast(const float* in, float* out, float* ws, int nz
                                   const float* eps_ptr = nullptr);
 cudaError_t fy_launch_box_mean(const float* in, float* out, float* tmp, int nz, int ny, int nx, int r,
                                cudaStream_t st, int& launches);
+// output pass from guided (mean, var) pairs written by the noise statistics pass (r = win/2)
+cudaError_t fy_launch_guided_apply_mv(const float* mv, const float* in, float* out, int nz, int ny, int nx, int r,
+                                      float eps, int sms, cudaStream_t st, const float* eps_ptr,
+                                      const RingApply* rings);
 
 // Noise model (fy_noise.cu)
 size_t fy_noise_ctl_bytes();
 size_t fy_noise_scratch_floats(size_t n);
 cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, int win, double flat_pct,
                                      double ref_intensity, float* scratch, void* ctl_mem, int sms,
-                                     cudaStream_t st, int& launches);
+                                     cudaStream_t st, int& launches, float* guided_mv = nullptr);
 cudaError_t fy_noise_read(const void* ctl_mem, double* g, double* b, double* noise_ref, double* ref_intensity,
                           int* used, cudaStream_t st);
 const float* fy_noise_eps_ptr(const void* ctl_mem);

@@ -507,10 +507,12 @@ static size_t round64(size_t v) { return (v + 63) & ~(size_t)63; }
 size_t fy_noise_scratch_floats(size_t n) { return 2 * round64(n) + round64((n + 3) / 4); }
 
 // Enqueue the whole estimate. scratch: 2n floats (mean, var) + n bytes (bin ids);
-// ctl: fy_noise_ctl_bytes(). Supports win in {3..9} (r = win/2 <= 4).
+// ctl: fy_noise_ctl_bytes(). Supports win in {3..9} (r = win/2 <= 4). guided_mv (optional,
+// 2n floats): the statistics pass also writes the guided filter's (mean, var) pairs of the
+// same window, for fy_launch_guided_apply_mv with r = win/2.
 cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, int win, double flat_pct,
                                      double ref_intensity, float* scratch, void* ctl_mem, int sms,
-                                     cudaStream_t st, int& launches) {
+                                     cudaStream_t st, int& launches, float* guided_mv) {
     NoiseCtl* ctl = (NoiseCtl*)ctl_mem;
     const long long n = (long long)nz * ny * nx;
     const size_t nr = ((size_t)n + 63) & ~(size_t)63;
@@ -529,7 +531,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     {   // 1. stats
         fyzb::Params sp{};
         sp.nz = nz; sp.ny = ny; sp.nx = nx;
-        sp.f0 = in; sp.o0 = mean; sp.o1 = var;
+        sp.f0 = in; sp.o0 = mean; sp.o1 = var; sp.o2 = guided_mv;
         sp.inv_wc = inv_wc; sp.wci = win * win * win;
         cudaError_t e0 = fyzb::launch<fyzb::ZB_NOISE>(sp, r, sms, st);
         if (e0 != cudaSuccess) return e0;

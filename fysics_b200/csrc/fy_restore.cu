@@ -78,15 +78,22 @@ extern "C" int fy_gpu_restore_u8(const unsigned char* d_u8, float* d_out, int nz
                                    cfg->deconv_kind, cfg->fz2_scale, stream)))
         return rc;
     fy::ws_acquire(st);
-    // 3. noise model on the deconvolved volume -> device eps
+    // 3. noise model on the deconvolved volume -> device eps. When the noise window is the
+    // exact guided filter's window, the statistics pass also writes the guided (mean, var)
+    // pairs (after the noise scratch), and the guided filter runs its output pass only.
     const float* eps_ptr = nullptr;
     int launches = 0;
-    if (!(cfg->guided_eps > 0)) {
-        if ((e = c.aux.ensure(fy_noise_scratch_floats(n) * sizeof(float))) != cudaSuccess) return fail_cuda(e, what);
+    const bool noise = !(cfg->guided_eps > 0);
+    const bool shared_window = noise && cfg->guided_s <= 1 && win == 2 * radius + 1;
+    const size_t mv_off = fy_noise_scratch_floats(n);
+    if (noise) {
+        const size_t need = mv_off + (shared_window ? fy_guided_fused_scratch_floats(n) : 0);
+        if ((e = c.aux.ensure(need * sizeof(float))) != cudaSuccess) return fail_cuda(e, what);
         if ((e = c.small.ensure(fy_noise_ctl_bytes())) != cudaSuccess) return fail_cuda(e, what);
         double pct = cfg->noise_flat_pct <= 0 ? 10.0 : cfg->noise_flat_pct;
         if ((e = fy_launch_estimate_noise(dec, nz, ny, nx, win, pct, cfg->noise_ref_intensity, c.aux.as<float>(),
-                                          c.small.p, c.sms, st, launches)) != cudaSuccess)
+                                          c.small.p, c.sms, st, launches,
+                                          shared_window ? c.aux.as<float>() + mv_off : nullptr)) != cudaSuccess)
             return fail_cuda(e, what);
         eps_ptr = fy_noise_eps_ptr(c.small.p);
         fy_prof_mark(st, "noise");
@@ -121,15 +128,21 @@ extern "C" int fy_gpu_restore_u8(const unsigned char* d_u8, float* d_out, int nz
             launches += 2;
         }
     } else {
-        // a, b reuse the noise statistics' scratch: the model is final by now (stream order);
         // the ring subtraction is folded into the guided filter's output pass
-        if ((e = c.aux.ensure(fy_guided_fused_scratch_floats(n) * sizeof(float))) != cudaSuccess)
-            return fail_cuda(e, what);
         RingApply ra;
         if (cfg->dering) fy_dering_ring_args(cfg->dering, cfg->z0, cfg->y0, cfg->x0, cfg->dering_scale, &ra);
-        e = fy_launch_guided_fused(dec, d_out, nullptr, c.aux.as<float>(), nz, ny, nx, radius, eps, 0, c.sms, st,
-                                   eps_ptr, cfg->dering ? &ra : nullptr);
-        launches += 2;
+        if (shared_window) {
+            e = fy_launch_guided_apply_mv(c.aux.as<float>() + mv_off, dec, d_out, nz, ny, nx, radius, eps, c.sms, st,
+                                          eps_ptr, cfg->dering ? &ra : nullptr);
+            launches += 1;
+        } else {
+            // a, b reuse the noise statistics' scratch: the model is final by now (stream order)
+            if ((e = c.aux.ensure(fy_guided_fused_scratch_floats(n) * sizeof(float))) != cudaSuccess)
+                return fail_cuda(e, what);
+            e = fy_launch_guided_fused(dec, d_out, nullptr, c.aux.as<float>(), nz, ny, nx, radius, eps, 0, c.sms, st,
+                                       eps_ptr, cfg->dering ? &ra : nullptr);
+            launches += 2;
+        }
         rings_done = cfg->dering != nullptr;
     }
     if (e != cudaSuccess) return fail_cuda(e, what);
@@ -155,8 +168,7 @@ int fy_restore_reserve(int nz, int ny, int nx) {
     if (rc) return rc;
     fy::ThreadCtx& c = ctx();
     const size_t n = (size_t)nz * ny * nx;
-    size_t aux = fy_noise_scratch_floats(n);
-    if (fy_guided_fused_scratch_floats(n) > aux) aux = fy_guided_fused_scratch_floats(n);
+    size_t aux = fy_noise_scratch_floats(n) + fy_guided_fused_scratch_floats(n);   // noise + guided (mean, var)
     cudaError_t e;
     if ((e = c.aux2.ensure(n * sizeof(float))) != cudaSuccess || (e = c.aux.ensure(aux * sizeof(float))) != cudaSuccess ||
         (e = c.small.ensure(fy_noise_ctl_bytes() + 256)) != cudaSuccess)

@@ -242,14 +242,14 @@ namespace {
 
 // Device bytes a request holds while it runs: u8 in, f32 out, the deconvolved volume, the
 // half spectrum (<= 8 B per padded complex over half the x axis), the noise statistics
-// (9 B per voxel) and the guided filter's a/b fields reuse those; tables are small.
+// (9 B per voxel) and the guided filter's (mean, var) pairs (8 B per voxel); tables are small.
 size_t footprint_of(const fy_request& r) {
     const size_t n = (size_t)r.nz * r.ny * r.nx;
     const size_t pz = (size_t)fy_next_fft_size(r.nz), py = (size_t)fy_next_fft_size(r.ny);
     const size_t px = (size_t)fy_next_fft_size(r.nx);
     const size_t spec = r.nz * py * ((px / 2 + 1 + 15) & ~(size_t)15) * 8;
     (void)pz;
-    return n + 4 * n + 4 * n + spec + 9 * n + (8u << 20);
+    return n + 4 * n + 4 * n + spec + 9 * n + 8 * n + (8u << 20);
 }
 
 void run_one(fy_server* s, Ticket* t, WorkerBufs& wb) {

@@ -19,13 +19,20 @@
 //   ZB_NOISE      u = I - c (zero outside the volume), fixed divisor win^3: local mean and
 //                 variance as in noise.c:41-61, with the tile shift c removing the FP32
 //                 cancellation of E[I^2] - E[I]^2.
-//   ZB_GUIDED_AB  u = I - c, box MEANS over the in-bounds window taken axis by axis with
-//                 1.0f/(float)count (guided.c:22-28): var = max(corr - mean^2, 0),
-//                 a = var/(var + eps), b = mean*(1 - a) (guided.c:121-132) -> interleaved
-//                 (a, b) pairs, one 8-byte store per voxel.
+//                 With o2 set it also writes the guided filter's (mean, var) pair of the
+//                 same window (ZB_GUIDED_AB's formulas): a chain whose noise window equals
+//                 the guided window then needs no ZB_GUIDED_AB pass.
+//   ZB_GUIDED_AB  u = I - c, box MEANS over the in-bounds window: the window sum times
+//                 the reciprocal in-bounds counts 1.0f/(float)count of the three axes
+//                 (guided.c:22-28): var = max(corr - mean^2, 0), a = var/(var + eps),
+//                 b = mean*(1 - a) (guided.c:121-132) -> interleaved (a, b) pairs, one 8-byte
+//                 store per voxel.
 //   ZB_GUIDED_OUT box means of the (a, b) pairs -> out = box(a)*I + box(b)
 //                 (guided.c:136-140), or the two means themselves for the decimated variant
 //                 (guided.c:181-182). The pairs are staged as one interleaved field.
+//   ZB_GUIDED_OUT_MV  the same from staged (mean, var) pairs, turned into (a, b) as the X
+//                 phase reads them, with ZB_GUIDED_AB's expressions, so the output equals the
+//                 two-pass filter's bit for bit (eps > 0).
 // Window sums are direct (2R+1)-tap float sums in ascending order, started from the first
 // tap, so no running-sum chain accumulates error. Each output voxel is written once by one
 // thread, and ZB_GUIDED_OUT reads the guide only at the voxel it writes, so out may alias
@@ -40,14 +47,16 @@ namespace fyzb {
 
 constexpr int TX = 64, TY = 16, NT = 256, NS = 4;
 constexpr int SXW = TX + 8;                 // staged row: x0 - 4 .. x0 + TX + 4 (R <= 4)
-enum { ZB_NOISE = 0, ZB_GUIDED_AB = 1, ZB_GUIDED_OUT = 2 };
+enum { ZB_NOISE = 0, ZB_GUIDED_AB = 1, ZB_GUIDED_OUT = 2, ZB_GUIDED_OUT_MV = 3 };
+__host__ __device__ constexpr bool out_kind(int k) { return k == ZB_GUIDED_OUT || k == ZB_GUIDED_OUT_MV; }
 
 struct Params {
-    const float* f0;       // I (NOISE, GUIDED_AB) or the interleaved (a, b) pairs (GUIDED_OUT)
-    const float* guide;    // I (GUIDED_OUT, out_mode 0)
+    const float* f0;       // I (NOISE, GUIDED_AB) or interleaved (a, b) | (mean, var) pairs (OUT kinds)
+    const float* guide;    // I (OUT kinds, out_mode 0)
     float* o0;             // mean | (a, b) pairs | out (or box(a))
     float* o1;             // var  | -      | box(b) (out_mode 1)
-    const float* eps_ptr;  // GUIDED_AB: device eps (overrides eps when set)
+    float* o2;             // NOISE: guided (mean, var) pairs, optional
+    const float* eps_ptr;  // GUIDED_AB, GUIDED_OUT_MV: device eps (overrides eps when set)
     float eps;
     float inv_wc;          // NOISE: 1/win^3
     int wci;               // NOISE: win^3
@@ -75,6 +84,22 @@ FY_D float recip_count(int p, int L, int r) {
 
 FY_D float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 FY_D float2 mul2(float2 a, float f) { return __fmul2_rn(a, make_float2(f, f)); }
+
+// Guided (mean, var) of a window from its shifted sums and the product of the three axes'
+// reciprocal in-bounds counts (guided.c:121-128).
+FY_D float2 guided_mv(float2 sums, float rxyz, float c) {
+    const float2 e = mul2(sums, rxyz);                 // E[I-c], E[(I-c)^2]
+    float var = e.y - e.x * e.x;
+    if (var < 0.f) var = 0.f;
+    return make_float2(e.x + c, var);
+}
+// (a, b) from (mean, var) (guided.c:129-131). a = var/(var + eps) uses the fast division
+// (<= 2 ulp for the denominators here, var + eps in [eps, ~1]); the a/b pass and the
+// output pass from (mean, var) share it, so both forms of the filter agree bit for bit.
+FY_D float2 guided_ab(float2 mv, float eps) {
+    const float a = __fdividef(mv.y, mv.y + eps);
+    return make_float2(a, mv.x * (1.0f - a));
+}
 
 FY_D void cp16(float* sdst, const float* gsrc, bool valid) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
@@ -166,7 +191,7 @@ FY_D void stage_plane(float* dst, const Params& p, int zi, int x0, int y0) {
 
 template <int R, int KIND, bool VEC, bool TMA>
 __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p, const __grid_constant__ TmaMaps tm) {
-    constexpr int C = KIND == ZB_GUIDED_OUT ? 2 : 1;
+    constexpr int C = out_kind(KIND) ? 2 : 1;
     using G = Geo<R, C>;
     constexpr int NR = G::NR;
     extern __shared__ float4 zb_smem4[];
@@ -181,9 +206,9 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     const int zs = blockIdx.z * p.zchunk, ze = min(nz, zs + p.zchunk);
     const size_t plane = (size_t)ny * nx;
     // per-tile shift: one constant for every window this CTA forms
-    const float c = KIND == ZB_GUIDED_OUT ? 0.f : __ldg(p.f0 + (size_t)zs * plane + (size_t)y0 * nx + x0);
+    const float c = out_kind(KIND) ? 0.f : __ldg(p.f0 + (size_t)zs * plane + (size_t)y0 * nx + x0);
     float eps = p.eps;
-    if (KIND == ZB_GUIDED_AB && p.eps_ptr) eps = *p.eps_ptr;    // chained from the device noise model
+    if ((KIND == ZB_GUIDED_AB || KIND == ZB_GUIDED_OUT_MV) && p.eps_ptr) eps = *p.eps_ptr;   // device noise model
     if (t < TX) rx[t] = x0 + t < nx ? recip_count(x0 + t, nx, R) : 0.f;
     if (t < TY) ry[t] = y0 + t < ny ? recip_count(y0 + t, ny, R) : 0.f;
     const bool cols_in = x0 - 4 >= 0 && x0 + TX + 4 <= nx;       // no column of the staged rows is outside
@@ -218,7 +243,7 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     int ri[4] = {0, 0, 0, 0};
     float rv[4] = {0.f, 0.f, 0.f, 0.f};                           // ring values of the cached slab
     long rslab = -1;
-    if (KIND == ZB_GUIDED_OUT && p.out_mode == 0 && p.ra.ring) {
+    if (out_kind(KIND) && p.out_mode == 0 && p.ra.ring) {
         rings = p.ra.have ? (*p.ra.have != 0) : true;
         const double gxd = (double)(p.ra.x0 + gx) - p.ra.cx;
 #pragma unroll
@@ -269,7 +294,7 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
             const bool emit = zo >= zs && zo < ze && gx < nx;
             const size_t obase = (size_t)(emit ? zo : 0) * plane + (size_t)(y0 + 4 * rg) * nx + gx;
             float gv[4] = {0.f, 0.f, 0.f, 0.f};
-            if (KIND == ZB_GUIDED_OUT && p.out_mode == 0 && emit) {   // issued early, used after the Y phase
+            if (out_kind(KIND) && p.out_mode == 0 && emit) {   // issued early, used after the Y phase
 #pragma unroll
                 for (int k = 0; k < 4; ++k)
                     if (y0 + 4 * rg + k < ny) gv[k] = __ldg(p.guide + obase + (size_t)k * nx);
@@ -287,6 +312,10 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                         const float4 v = *reinterpret_cast<const float4*>(row + 4 * j2);
                         P[2 * j2] = make_float2(v.x, v.y);
                         P[2 * j2 + 1] = make_float2(v.z, v.w);
+                    }
+                    if (KIND == ZB_GUIDED_OUT_MV) {          // (mean, var) -> (a, b)
+#pragma unroll
+                        for (int j = 4 - R; j < 8 + R; ++j) P[j] = guided_ab(P[j], eps);
                     }
                 } else {
                     const float* row = sp + yy * G::RW + x4;
@@ -318,7 +347,7 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                     float2 sm = P[4 + k - R];
 #pragma unroll
                     for (int j = 5 + k - R; j <= 4 + k + R; ++j) sm = add2(sm, P[j]);
-                    if (KIND != ZB_NOISE) sm = mul2(sm, rx[x4 + k]);
+                    if (out_kind(KIND)) sm = mul2(sm, rx[x4 + k]);
                     o[k] = sm;
                 }
                 float4* dst = reinterpret_cast<float4*>(xs + yy * TX + x4);
@@ -336,12 +365,12 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                     float2 sm = a[k];
 #pragma unroll
                     for (int j = 1; j <= 2 * R; ++j) sm = add2(sm, a[k + j]);
-                    if (KIND != ZB_NOISE) sm = mul2(sm, ry[4 * rg + k]);
+                    if (out_kind(KIND)) sm = mul2(sm, ry[4 * rg + k]);
                     rz2[ph][k] = sm;
                 }
             }
             if (!emit) continue;
-            if (KIND == ZB_GUIDED_OUT && rings) {                // this plane's ring slab (dering.c:212-215)
+            if (out_kind(KIND) && rings) {                        // this plane's ring slab (dering.c:212-215)
                 long sl = (p.ra.z0 + zo) / p.ra.slab_z;
                 if (sl < 0) sl = 0;
                 if (sl >= p.ra.nslab) sl = p.ra.nslab - 1;
@@ -352,7 +381,7 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                         rv[k] = ri[k] < p.ra.nr ? __ldg(p.ra.ring + (size_t)sl * p.ra.nr + ri[k]) : 0.f;
                 }
             }
-            const float rz = KIND == ZB_NOISE ? 0.f : recip_count(zo, nz, R);
+            const float rz = recip_count(zo, nz, R);
             const int cz = min(zo + R, nz - 1) - max(zo - R, 0) + 1;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
@@ -377,13 +406,10 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                     if (v < 0.f) v = 0.f;
                     p.o0[o] = m;
                     p.o1[o] = v;
+                    if (p.o2)
+                        reinterpret_cast<float2*>(p.o2)[o] = guided_mv(sm, rx[xc] * ry[4 * rg + k] * rz, c);
                 } else if (KIND == ZB_GUIDED_AB) {
-                    const float2 e = mul2(sm, rz);                 // E[I-c], E[(I-c)^2]
-                    float var = e.y - e.x * e.x;
-                    if (var < 0.f) var = 0.f;
-                    const float mean = e.x + c;
-                    const float a = var / (var + eps);             // guided.c:129
-                    reinterpret_cast<float2*>(p.o0)[o] = make_float2(a, mean * (1.0f - a));   // guided.c:131
+                    reinterpret_cast<float2*>(p.o0)[o] = guided_ab(guided_mv(sm, rx[xc] * ry[4 * rg + k] * rz, c), eps);
                 } else {
                     const float2 mab = mul2(sm, rz);
                     if (p.out_mode == 0) {
@@ -447,7 +473,7 @@ inline bool make_tma_map(CUtensorMap* m, const float* base, int nz, int ny, int 
 
 template <int KIND, int R, bool VEC>
 inline cudaError_t launch_r(const Params& p, dim3 grid, cudaStream_t st) {
-    constexpr int C = KIND == ZB_GUIDED_OUT ? 2 : 1;
+    constexpr int C = out_kind(KIND) ? 2 : 1;
     const size_t smem = Geo<R, C>::bytes;
     TmaMaps tm;
     memset(&tm, 0, sizeof tm);

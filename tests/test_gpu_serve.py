@@ -103,7 +103,7 @@ def test_budget_admits_one_at_a_time_and_refuses_oversize(gpu):
     outs = [np.zeros(s, np.float32) for s in shapes]
     reqs = [request(gpu, u, o, 7 + i) for i, (u, o) in enumerate(zip(ins, outs))]
     n = 96 ** 3
-    srv = make_server(gpu, budget=40 * n, workers=3)  # about one 96^3 request's footprint
+    srv = make_server(gpu, budget=48 * n, workers=3)  # one 96^3 request's footprint (~40 B/voxel), not two
     ts = []
     for r in reqs:
         t = C.c_longlong()
