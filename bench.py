@@ -143,7 +143,7 @@ def algorithmic_bytes(name: str, n: int, geo: dict) -> float | None:
         # box pass: I read, mean + var written (+ the guided (mean, var) pairs when the noise
         # window is the guided window: the chain then skips the guided a/b pass)
         "noise.stats": n * (20 if geo.get("shared_window") else 12),
-        "noise.lohi": n * 12,                  # 3 digit passes over mean
+        "noise.lohi": n * 4,                   # one window pass over mean (candidates ~1%: small)
         "noise.bin_select": n * 24,            # mean + var read, labels written; 3 passes over var + labels
         # (mean, var) pairs + I -> out (16 B); without the shared window I -> a, b (12 B) first
         "guided": n * (16 if geo.get("shared_window") else 28),
@@ -157,7 +157,7 @@ def algorithmic_bytes(name: str, n: int, geo: dict) -> float | None:
 # chain (dram__bytes_read.sum + dram__bytes_write.sum per launch; profiles/dram_restore_512.md).
 DRAM_BYTES_PER_VOXEL = {
     "deconv.x_fwd": 4.653, "deconv.y_fwd": 8.031, "deconv.z_weight": 8.290, "deconv.y_inv": 8.031,
-    "deconv.x_inv": 7.880, "noise.stats": 19.647, "noise.lohi": 12.003, "noise.bin_select": 23.931,
+    "deconv.x_inv": 7.880, "noise.stats": 19.647, "noise.lohi": 4.402, "noise.bin_select": 23.931,
     "guided": 15.938, "dering.accumulate+vote": 0.507,
 }
 

@@ -3,7 +3,8 @@
 // fy_gpu_estimate_noise_noalloc serves callers that may not allocate device memory while
 // they run: a serving loop whose HBM is committed to its own pool (a cudaMalloc there can
 // fail, or synchronise the device), or a caller that budgets every byte ahead of time. The
-// scratch -- mean/variance fields, the bin labels and the selection control block -- lives in
+// scratch -- mean/variance fields, the bin labels, the selection control blocks, the sample
+// and the candidate list -- lives in
 // g_noise_scratch below, sized for FY_NOISE_NOALLOC_MAX_VOXELS voxels. It is part of the
 // library's device image, so every GPU that loads the library holds it until exit. Nothing
 // here calls cudaMalloc, cudaFree or any other allocating routine.
@@ -26,7 +27,12 @@ constexpr size_t kMaxVoxels = FY_NOISE_NOALLOC_MAX_VOXELS;
 constexpr size_t round64(size_t v) { return (v + 63) & ~(size_t)63; }
 // control block first (it holds the 64 KB selection histograms), fields after it
 constexpr size_t kCtlBytes = 128 << 10;
-constexpr size_t kFieldFloats = 2 * round64(kMaxVoxels) + round64((kMaxVoxels + 3) / 4);
+// mean, var, bin labels, the candidate selection's control block (<= 128 KB), the sample
+// (16384 floats) and the candidate list (n/8 + 4096 values and labels); checked against
+// fy_noise_scratch_floats at run time
+constexpr size_t kCandMax = (kMaxVoxels + 7) / 8 + 4096;
+constexpr size_t kFieldFloats = 2 * round64(kMaxVoxels) + round64((kMaxVoxels + 3) / 4) + (128 << 10) / 4 +
+                                16384 + round64(kCandMax) + round64((kCandMax + 3) / 4);
 constexpr size_t kScratchBytes = kCtlBytes + kFieldFloats * sizeof(float);
 static_assert(kCtlBytes % 256 == 0, "fields must start 256-byte aligned");
 
@@ -69,6 +75,7 @@ extern "C" int fy_gpu_estimate_noise_noalloc(const float* d_in, int nz, int ny, 
         return fail(FY_EUNSUPPORTED, "%s: %dx%dx%d = %lld voxels exceeds the static scratch limit of %lld voxels",
                     what, nz, ny, nx, n, (long long)kMaxVoxels);
     if (fy_noise_ctl_bytes() > kCtlBytes) return fail(FY_EUNSUPPORTED, "%s: control block too large", what);
+    if (fy_noise_scratch_floats((size_t)n) > kFieldFloats) return fail(FY_EUNSUPPORTED, "%s: scratch layout too large", what);
 
     int dev = -1, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);

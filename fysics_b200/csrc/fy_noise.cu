@@ -6,10 +6,12 @@
 //      (2r+1)-tap float sums of (I - c) and (I - c)^2 with a per-tile shift c, and interior
 //      voxels use v = S2'/wc - (S1'/wc)^2, which equals the reference's S2/wc - (S1/wc)^2
 //      without its cancellation.
-//   2. Exact order statistics by radix select on orderable 32-bit float keys: the 1st and
-//      99th percentiles of m (noise.c:104-108) and, per intensity bin with >= 200 voxels,
-//      the flat_pct percentile of v (noise.c:117-134), each interpolated between
-//      order statistics k and k+1 exactly as percentile() does (noise.c:66-73).
+//   2. Exact order statistics on orderable 32-bit float keys: the 1st and 99th percentiles
+//      of m (noise.c:104-108) through a sample-guided window, one pass over m and a radix
+//      select of the window's candidates (falling back to radix passes over m when the
+//      window misses), and, per intensity bin with >= 200 voxels, the flat_pct percentile of
+//      v (noise.c:117-134) by radix passes; each interpolated between order statistics k and
+//      k+1 exactly as percentile() does (noise.c:66-73).
 //   3. k_noise_fit: one thread, FP64: IRLS line fit var = g*I + b (noise.c:137-172) and
 //      noise_ref = sqrt(max(g*ref + b, ..))*1.15 (noise.c:181-187), plus the guided eps
 //      (3*noise_ref)^2 floored at 1e-8 (noise.c:197-202).
@@ -22,6 +24,10 @@ namespace {
 
 constexpr int NB = 24;                 // intensity bins, noise.c:111
 constexpr int NT_MAX = 64;             // selection targets: 2 per bin + spare
+// ctl->mode: 0 mean percentiles by radix passes, 1 bin percentiles by radix passes, 2
+// variance fallback, 3 done; kModeWin0: the mean percentiles through the sample-guided
+// window (section 2w), which falls back to mode 0 when the window misses.
+constexpr int kModeWin0 = 4;
 
 FY_D uint32_t fkey(float f) {
     const uint32_t u = __float_as_uint(f);
@@ -69,6 +75,12 @@ struct NoiseCtl {
     int out_used;
     float eps;                         // fy_guided_eps_for_noise(noise_ref), for a chained guided filter
     unsigned int hist[NT_MAX * 256];   // per-target histogram (bins: 24 x 256; whole: 2 x 2048)
+    // Sample-guided window (section 2w): per target the window keys [wlo, whi] and the count
+    // of keys below wlo.
+    uint32_t wlo[2], whi[2];
+    unsigned long long wbelow[2];
+    unsigned long long ncand;          // candidates appended (may exceed the capacity)
+    int wfail;                         // the window missed: the radix passes run instead
 };
 
 namespace {
@@ -336,7 +348,7 @@ __global__ void k_noise_setup(NoiseCtl* ctl, long long n, double flat_pct, doubl
     ctl->n = n;
     ctl->flat_pct = flat_pct;
     ctl->ref_intensity = ref_intensity;
-    ctl->mode = 0;
+    ctl->mode = kModeWin0;                 // the radix passes run only if the windows fail
     for (int t = 0; t < NT_MAX; ++t) target_init(ctl, t, 0, 0, false);
     const double i1 = 1.0 / 100.0 * (double)(n - 1), i99 = 99.0 / 100.0 * (double)(n - 1);
     target_init(ctl, 0, (long long)i1, n, true);              // 1st percentile of the means
@@ -390,6 +402,293 @@ __global__ void __launch_bounds__(256) k_bin_targets(NoiseCtl* ctl) {
         ctl->bcount[b] = (unsigned long long)c;
         const double idx = ctl->flat_pct / 100.0 * (double)(c - 1);
         target_init(ctl, b, on ? (long long)idx : 0, c, on);
+    }
+}
+
+// ---------------------------------------------------------------- 2w. sample-guided window
+// The 1st/99th percentiles of the means by radix selection read the mean field once per
+// digit (3 passes). Here they read it once:
+//   sample   m <= kSampleMax means at positions (A*i + B) mod n, a bijection of [0, n) when
+//            gcd(A, n) = 1, spread evenly over the volume.
+//   window   per target, the sample's order statistics kWinSigmas binomial standard
+//            deviations either side of the target's expected sample rank give a key window
+//            [wlo, whi] that holds the target's order statistics k and k+1 with
+//            overwhelming probability (one CTA per target and window end, radix select in
+//            shared memory).
+//   count    one pass over the means counts, per target, the keys below wlo and appends the
+//            keys inside [wlo, whi] with their target label to a candidate list.
+//   select   the radix passes of mode 1 over the candidates with a second control block,
+//            targets = labels: the first digit pass's per-target sums are the inside counts,
+//            so the target ranks r = k - below are set after it (as the bin counts are in
+//            the bin selection). A rank outside [0, inside) -- k or k+1 not in the window --
+//            or a candidate list over its capacity sends the selection to the radix passes
+//            over the whole field (mode 0), which are exact in every case.
+//   finish   the keys of k and k+1 go into the main block in the form the fit reads.
+// The result is the same exact order statistics as the radix path: only which pass finds
+// them changes. (The per-bin variance percentiles keep the radix path: their counting pass
+// must bin every voxel, which costs as much as the radix path's labelling pass.)
+constexpr int kSampleMax = 16384;
+constexpr int kBoundThreads = 512;
+constexpr double kWinSigmas = 5.0;
+
+// Block radix select over keys in shared memory: the rank-th smallest (0-based) of keys[0, c),
+// c <= kSampleMax, by kBoundThreads threads. Four 8-bit digit passes; each thread counts its
+// own keys (<= 32) in a private byte column of hist8 ([256 digits][kBoundThreads]), so no
+// atomics are needed; two threads then sum each digit's row.
+FY_D uint32_t block_select(const uint32_t* keys, int c, long long rank, unsigned char* hist8,
+                           unsigned long long* part, uint32_t* s_sel) {
+    constexpr int NTB = kBoundThreads, RW = NTB / 4;    // threads, words per digit row
+    const int t = threadIdx.x;
+    uint32_t prefix = 0, pmask = 0;
+    uint32_t* h32 = reinterpret_cast<uint32_t*>(hist8);
+    for (int sh = 24; sh >= 0; sh -= 8) {
+        for (int i = t; i < 256 * RW; i += NTB) h32[i] = 0;
+        __syncthreads();
+        for (int i = t; i < c; i += NTB) {
+            const uint32_t k = keys[i];
+            if ((k & pmask) == prefix) ++hist8[((k >> sh) & 255u) * NTB + t];
+        }
+        __syncthreads();
+        unsigned long long mine = 0;                   // half of digit t/2's row
+        const uint32_t* row = h32 + (t >> 1) * RW + (t & 1) * (RW / 2);
+        for (int w = 0; w < RW / 2; ++w) {
+            const uint32_t v = row[w];
+            mine += (v & 255u) + ((v >> 8) & 255u) + ((v >> 16) & 255u) + (v >> 24);
+        }
+        part[t] = mine;
+        __syncthreads();
+        unsigned long long dsum = 0;
+        if (t < 256) dsum = part[2 * t] + part[2 * t + 1];
+        __syncthreads();
+        if (t < 256) part[t] = dsum;
+        __syncthreads();
+        for (int off = 1; off < 256; off <<= 1) {      // inclusive scan over digits
+            const unsigned long long add = (t < 256 && t >= off) ? part[t - off] : 0ull;
+            __syncthreads();
+            if (t < 256) part[t] += add;
+            __syncthreads();
+        }
+        if (t < 256) {
+            const unsigned long long before = t ? part[t - 1] : 0ull;
+            if ((unsigned long long)rank >= before && (unsigned long long)rank < part[t]) {
+                s_sel[0] = (uint32_t)t;
+                s_sel[1] = (uint32_t)(rank - (long long)before);
+            }
+        }
+        __syncthreads();
+        prefix |= s_sel[0] << sh;
+        pmask |= 255u << sh;
+        rank = s_sel[1];
+        __syncthreads();
+    }
+    return prefix;
+}
+
+__global__ void __launch_bounds__(256) k_win_sample(const float* __restrict__ mean, const NoiseCtl* __restrict__ ctl,
+                                                    float* __restrict__ sm, long long m, unsigned long long A,
+                                                    unsigned long long B) {
+    if (ctl->mode != kModeWin0) return;
+    const unsigned long long n = (unsigned long long)ctl->n;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+        sm[i] = __ldg(mean + (A * (unsigned long long)i + B) % n);
+}
+
+// One CTA (kBoundThreads threads) per target (blockIdx.x 0/1: 1st/99th percentile) and window
+// end (blockIdx.y 0: wlo, 1: whi). Dynamic shared memory: kSampleMax keys, then the private
+// digit counts (256 x kBoundThreads bytes).
+__global__ void __launch_bounds__(kBoundThreads) k_win_bounds(const float* __restrict__ sm,
+                                                              NoiseCtl* __restrict__ ctl, long long m) {
+    extern __shared__ uint32_t wkeys[];
+    unsigned char* hist8 = reinterpret_cast<unsigned char*>(wkeys + kSampleMax);
+    __shared__ unsigned long long part[kBoundThreads];
+    __shared__ uint32_t s_sel[2];
+    if (ctl->mode != kModeWin0) return;
+    const int t = blockIdx.x;
+    const int c = (int)(m < kSampleMax ? m : kSampleMax);
+    for (int i = threadIdx.x; i < c; i += blockDim.x) wkeys[i] = fkey(sm[i]);
+    __syncthreads();
+    const double q = (double)ctl->tk[t] / (double)(ctl->n > 1 ? ctl->n - 1 : 1);   // the target's quantile
+    const bool upper = blockIdx.y == 1;
+    uint32_t w = upper ? 0xffffffffu : 0u;
+    if (c >= 64) {                                      // fewer samples: the whole key range
+        const double qc = q < 1.0 / c ? 1.0 / c : (q > 1.0 - 1.0 / c ? 1.0 - 1.0 / c : q);
+        const long long ks = (long long)(q * (double)(c - 1));
+        const long long d = (long long)ceil(kWinSigmas * sqrt((double)c * qc * (1.0 - qc))) + 4;
+        if (!upper && ks - d >= 0) w = block_select(wkeys, c, ks - d, hist8, part, s_sel);
+        if (upper && ks + d + 1 < c) w = block_select(wkeys, c, ks + d + 1, hist8, part, s_sel);
+    }
+    if (threadIdx.x == 0) {
+        if (upper) {
+            ctl->whi[t] = w;
+        } else {
+            ctl->wlo[t] = w;
+            ctl->wbelow[t] = 0;
+            if (t == 0) ctl->ncand = 0;
+        }
+    }
+}
+
+// Candidate appends go through a per-warp shared buffer; a full buffer is copied out with one
+// global atomic for its whole run, so the list's counter sees one atomic per ~kWarpBuf
+// candidates instead of one per warp and element.
+constexpr int kWarpBuf = 256;
+struct WarpCands {
+    float* v;                          // this warp's kWarpBuf values in shared memory
+    uint8_t* l;                        // and labels
+    int cnt = 0;                       // warp-uniform fill
+    FY_D void flush(float* __restrict__ cval, uint8_t* __restrict__ clab, unsigned long long* ncand, long long cap) {
+        const unsigned full = 0xffffffffu;
+        __syncwarp();
+        if (cnt) {
+            unsigned long long base = 0;
+            if ((threadIdx.x & 31) == 0) base = atomicAdd(ncand, (unsigned long long)cnt);
+            base = __shfl_sync(full, base, 0);
+            for (int i = threadIdx.x & 31; i < cnt; i += 32)
+                if ((long long)(base + i) < cap) { cval[base + i] = v[i]; clab[base + i] = l[i]; }
+        }
+        cnt = 0;
+        __syncwarp();
+    }
+    // every lane of the warp calls
+    FY_D void add(bool take, float val, uint8_t label, float* __restrict__ cval, uint8_t* __restrict__ clab,
+                  unsigned long long* ncand, long long cap) {
+        const unsigned bal = __ballot_sync(0xffffffffu, take);
+        if (!bal) return;
+        const int lane = threadIdx.x & 31;
+        if (take) {
+            const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+            v[pos] = val;
+            l[pos] = label;
+        }
+        cnt += __popc(bal);
+        if (cnt > kWarpBuf - 32) flush(cval, clab, ncand, cap);
+    }
+};
+
+// The counting pass: mean keys against the windows of targets 0 and 1. The counts below each
+// window stay in registers until one warp reduction at the end; the keys inside a window go
+// to the candidate list.
+__global__ void __launch_bounds__(256) k_win_count(const float* __restrict__ mean, NoiseCtl* __restrict__ ctl,
+                                                   float* __restrict__ cval, uint8_t* __restrict__ clab,
+                                                   long long cap) {
+    __shared__ float bufv[256 / 32][kWarpBuf];
+    __shared__ uint8_t bufl[256 / 32][kWarpBuf];
+    if (ctl->mode != kModeWin0) return;
+    const unsigned full = 0xffffffffu;
+    const int t = threadIdx.x;
+    WarpCands wc;
+    wc.v = bufv[t >> 5];
+    wc.l = bufl[t >> 5];
+    const long long n = ctl->n, n4 = (n + 3) / 4, n4f = n / 4;
+    const uint32_t lo0 = ctl->wlo[0], hi0 = ctl->whi[0], lo1 = ctl->wlo[1], hi1 = ctl->whi[1];
+    unsigned int bel0 = 0, bel1 = 0;
+    const long long chunk = (long long)SU * 256;
+    long long base = (long long)blockIdx.x * chunk;
+    for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
+        float4 x[SU];
+#pragma unroll
+        for (int u = 0; u < SU; ++u) x[u] = __ldg(reinterpret_cast<const float4*>(mean) + base + t + (long long)u * 256);
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            const float mv[4] = {x[u].x, x[u].y, x[u].z, x[u].w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t k = fkey(mv[j]);
+                bel0 += k < lo0;
+                bel1 += k < lo1;
+                const bool in0 = k >= lo0 && k <= hi0, in1 = k >= lo1 && k <= hi1;
+                if (__any_sync(full, in0 || in1)) {
+                    wc.add(in0, mv[j], 0, cval, clab, &ctl->ncand, cap);
+                    wc.add(in1, mv[j], 1, cval, clab, &ctl->ncand, cap);
+                }
+            }
+        }
+    }
+    if (base < n4) {                                     // the grid's partial chunk
+        for (int u = 0; u < SU; ++u)
+            for (int j = 0; j < 4; ++j) {
+                const long long i = 4 * (base + t + (long long)u * 256) + j;
+                if (i >= n) continue;
+                const float mv = __ldg(mean + i);
+                const uint32_t k = fkey(mv);
+                bel0 += k < lo0;
+                bel1 += k < lo1;
+                for (int g = 0; g < 2; ++g)
+                    if (k >= (g ? lo1 : lo0) && k <= (g ? hi1 : hi0)) {
+                        const unsigned long long pos = atomicAdd(&ctl->ncand, 1ull);
+                        if ((long long)pos < cap) { cval[pos] = mv; clab[pos] = (uint8_t)g; }
+                    }
+            }
+    }
+    wc.flush(cval, clab, &ctl->ncand, cap);
+    const unsigned int s0 = __reduce_add_sync(full, bel0), s1 = __reduce_add_sync(full, bel1);
+    if ((t & 31) == 0) {
+        if (s0) atomicAdd(&ctl->wbelow[0], (unsigned long long)s0);
+        if (s1) atomicAdd(&ctl->wbelow[1], (unsigned long long)s1);
+    }
+}
+
+// After the counting pass (one thread): arms the candidate block for its first digit pass
+// (both targets active with the empty prefix, like the bin selection's labelling pass), or,
+// when the candidate list overflowed, sends the selection to the radix passes.
+__global__ void k_win_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc, long long cap) {
+    if (ctl->mode != kModeWin0) { cc->mode = 3; return; }
+    for (int t = 0; t < NT_MAX; ++t) target_init(cc, t, 0, 0, t < 2);
+    cc->ntarget = 2;
+    cc->n = (long long)(ctl->ncand < (unsigned long long)cap ? ctl->ncand : (unsigned long long)cap);
+    ctl->wfail = 0;
+    if ((long long)ctl->ncand > cap) {
+        cc->mode = 3;
+        ctl->wfail = 1;
+    } else {
+        cc->mode = 1;
+    }
+}
+
+// After the candidates' first digit pass (one block per target): the target's inside count
+// is the sum of its histogram; its rank among the candidates is r = k - below, which must
+// leave k and (when it exists) k+1 inside. Otherwise the selection fails (k_win_check).
+__global__ void __launch_bounds__(256) k_win_targets(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) {
+    __shared__ unsigned long long part[256];
+    if (cc->mode != 1) return;
+    const int t = blockIdx.x;
+    if (t >= cc->ntarget) return;
+    unsigned int* h = cc->hist + (size_t)t * 256;
+    part[threadIdx.x] = h[threadIdx.x];
+    __syncthreads();
+    for (int off = 128; off > 0; off >>= 1) {
+        if (threadIdx.x < off) part[threadIdx.x] += part[threadIdx.x + off];
+        __syncthreads();
+    }
+    const long long in = (long long)part[0];
+    const long long k = ctl->tk[t];
+    const long long r = k - (long long)ctl->wbelow[t];
+    const bool has_next = k + 1 < ctl->n;
+    const bool ok = r >= 0 && r < in && (!has_next || r + 1 < in);
+    __syncthreads();
+    if (!ok) h[threadIdx.x] = 0;                         // inactive: its histogram is cleared
+    if (threadIdx.x == 0) {
+        target_init(cc, t, ok ? r : 0, in, ok);
+        if (!ok) atomicExch(&ctl->wfail, 1);
+    }
+}
+
+// One thread: a failed window sends the selection to the radix passes over the whole field.
+__global__ void k_win_check(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) {
+    if (ctl->mode != kModeWin0 || !ctl->wfail) return;
+    cc->mode = 3;
+    ctl->mode = 0;
+}
+
+// Keys of order statistics k and k+1 into the main block's targets 0/1 (interp / next_value
+// form); the radix passes of mode 0 then stand aside.
+__global__ void k_win_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restrict__ cc) {
+    if (ctl->mode != kModeWin0) return;
+    for (int t = 0; t < 2; ++t) {
+        ctl->tprefix[t] = cc->tprefix[t];
+        ctl->tnext[t] = cc->tneed_next[t] ? cc->tnext[t] : cc->tprefix[t];
+        ctl->tneed_next[t] = 1;
+        ctl->tactive[t] = 1;
     }
 }
 
@@ -500,14 +799,45 @@ unsigned grid_sel(long long n, int sms) {
 }  // namespace
 
 size_t fy_noise_ctl_bytes() { return (sizeof(NoiseCtl) + 255) & ~(size_t)255; }
-// Scratch layout (floats): mean [0, nr), var [nr, 2nr), bin ids (bytes) from 2nr, with
-// nr = n rounded up to 64 floats so every sub-array (and the control block after the
-// scratch) starts 256-byte aligned for the vector loads.
-static size_t round64(size_t v) { return (v + 63) & ~(size_t)63; }
-size_t fy_noise_scratch_floats(size_t n) { return 2 * round64(n) + round64((n + 3) / 4); }
 
-// Enqueue the whole estimate. scratch: 2n floats (mean, var) + n bytes (bin ids);
-// ctl: fy_noise_ctl_bytes(). Supports win in {3..9} (r = win/2 <= 4). guided_mv (optional,
+namespace {
+// Scratch layout (floats; every sub-array 256-byte aligned for the vector loads): mean, var,
+// bin labels (bytes), the candidates' control block, the sample of means, and the candidate
+// list (values, then labels) of capacity n/8 + 4096 (the window holds ~1% of the voxels).
+size_t round64(size_t v) { return (v + 63) & ~(size_t)63; }
+struct NoiseLayout {
+    size_t mean, var, bin, cc, samp, cval, clab, total;
+    long long cap;
+};
+NoiseLayout noise_layout(size_t n) {
+    NoiseLayout L;
+    const size_t nr = round64(n);
+    L.mean = 0;
+    L.var = nr;
+    L.bin = 2 * nr;
+    L.cc = L.bin + round64((n + 3) / 4);
+    L.samp = L.cc + round64((sizeof(NoiseCtl) + 3) / 4);
+    L.cap = (long long)((n + 7) / 8 + 4096);
+    L.cval = L.samp + (size_t)kSampleMax;
+    L.clab = L.cval + round64((size_t)L.cap);
+    L.total = L.clab + round64(((size_t)L.cap + 3) / 4);
+    return L;
+}
+// Weyl step for the sample positions: a prime a with gcd(a, n) = 1, reduced mod n (for a
+// prime a that means n < a, or a not dividing n).
+unsigned long long weyl_step(unsigned long long n) {
+    if (n <= 1) return 1;
+    const unsigned long long primes[4] = {2654435761ull, 2246822519ull, 3266489917ull, 668265263ull};
+    for (unsigned long long a : primes)
+        if (n < a || n % a != 0) return a % n;
+    return 1;
+}
+}  // namespace
+
+size_t fy_noise_scratch_floats(size_t n) { return noise_layout(n).total; }
+
+// Enqueue the whole estimate. scratch: fy_noise_scratch_floats(n) floats; ctl:
+// fy_noise_ctl_bytes(). Supports win in {3..9} (r = win/2 <= 4). guided_mv (optional,
 // 2n floats): the statistics pass also writes the guided filter's (mean, var) pairs of the
 // same window, for fy_launch_guided_apply_mv with r = win/2.
 cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, int win, double flat_pct,
@@ -515,18 +845,25 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
                                      cudaStream_t st, int& launches, float* guided_mv) {
     NoiseCtl* ctl = (NoiseCtl*)ctl_mem;
     const long long n = (long long)nz * ny * nx;
-    const size_t nr = ((size_t)n + 63) & ~(size_t)63;
-    float* mean = scratch;
-    float* var = scratch + nr;
-    uint8_t* bin = (uint8_t*)(scratch + 2 * nr);
+    const NoiseLayout L = noise_layout((size_t)n);
+    float* mean = scratch + L.mean;
+    float* var = scratch + L.var;
+    uint8_t* bin = (uint8_t*)(scratch + L.bin);
+    NoiseCtl* cc = (NoiseCtl*)(scratch + L.cc);
+    float* sm = scratch + L.samp;
+    float* cval = scratch + L.cval;
+    uint8_t* clab = (uint8_t*)(scratch + L.clab);
     const int r = win / 2;
     const float inv_wc = (float)(1.0 / ((double)win * win * win));
-    const unsigned g = grid_sel(n, sms);
-    unsigned int* hist = ctl->hist;
-    const size_t hist_bytes = sizeof(ctl->hist);
+    const unsigned g = grid_sel(n, sms), gc = grid_sel(L.cap, sms);
     const size_t smem_all = 2 * 2048 * sizeof(unsigned int), smem_bin = NB * 256 * sizeof(unsigned int);
+    const size_t smem_keys = kSampleMax * sizeof(uint32_t) + 256 * kBoundThreads;   // keys + private digit counts
+    const long long m = n < kSampleMax ? n : kSampleMax;
+    const unsigned long long wa = weyl_step((unsigned long long)n), wb = (unsigned long long)n / 3;
     cudaError_t e;
-    if ((e = cudaMemsetAsync(hist, 0, hist_bytes, st)) != cudaSuccess) return e;
+    if ((e = fy_smem_optin(k_win_bounds, smem_keys)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(ctl->hist, 0, sizeof(ctl->hist), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(cc->hist, 0, sizeof(cc->hist), st)) != cudaSuccess) return e;
     k_noise_setup<<<1, 1, 0, st>>>(ctl, n, flat_pct, ref_intensity);
     {   // 1. stats
         fyzb::Params sp{};
@@ -537,7 +874,24 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
         if (e0 != cudaSuccess) return e0;
         fy_prof_mark(st, "noise.stats");
     }
-    // 2a. 1st/99th percentile of the means: 11 + 11 + 10 bits, then the k+1 neighbours
+    // 2a. 1st/99th percentile of the means: sample-guided window pass, then the radix passes
+    // of mode 1 over the candidates (control block cc, targets = labels); the radix passes
+    // over the whole field (11 + 11 + 10 bits, then the k+1 neighbours) run only if the
+    // window misses
+    k_win_sample<<<64, 256, 0, st>>>(mean, ctl, sm, m, wa, wb);
+    k_win_bounds<<<dim3(2, 2), kBoundThreads, smem_keys, st>>>(sm, ctl, m);
+    k_win_count<<<g, 256, 0, st>>>(mean, ctl, cval, clab, L.cap);
+    k_win_arm<<<1, 1, 0, st>>>(ctl, cc, L.cap);
+    for (int sh = 24; sh >= 0; sh -= 8) {
+        k_sel_hist<8, 1><<<gc, 256, smem_bin, st>>>(nullptr, cval, clab, cc, sh);
+        if (sh == 24) {
+            k_win_targets<<<2, 256, 0, st>>>(ctl, cc);
+            k_win_check<<<1, 1, 0, st>>>(ctl, cc);
+        }
+        k_sel_scan<<<2, 256, 0, st>>>(cc, 8, 1, sh == 0);
+    }
+    k_sel_next<<<gc, 256, 0, st>>>(nullptr, cval, clab, cc, 1);
+    k_win_finish<<<1, 1, 0, st>>>(ctl, cc);
     const int all_digits[3][2] = {{21, 11}, {10, 11}, {0, 10}};
     for (int i = 0; i < 3; ++i) {
         if (all_digits[i][1] == 11) k_sel_hist<11, 0><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0]);
@@ -566,7 +920,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     }
     k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 2);
     k_noise_fit<<<1, 1, 0, st>>>(ctl, 1);
-    launches += 1 + 1 + 6 + 1 + 1 + 1 + 8 + 1 + 1 + 6 + 1 + 1;
+    launches += 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 7 + 1 + 10 + 1 + 1 + 7 + 1;
     return cudaGetLastError();
 }
 

@@ -116,3 +116,24 @@ def test_device_eps_chain(gpu):
     off = eps_ptr - scratch.data_ptr()
     eps = scratch[off:off + 4].cpu().numpy().view(np.float32)[0]
     assert eps == np.float32(lib.fy_guided_eps_for_noise(host.noise_ref))
+
+
+def test_noise_window_overflow_falls_back(gpu):
+    """The mean percentiles come from a sample-guided window and a candidate list of n/8 +
+    4096 entries. A volume whose low 60% is one constant ties the 1st percentile across far
+    more voxels than that, so the window's candidate list overflows and the exact radix
+    passes over the whole field run instead: the model must still equal the oracle's."""
+    rng = np.random.default_rng(7)
+    shape = (64, 64, 64)
+    vol = np.full(shape, 0.1, np.float32)
+    z, y, x = np.meshgrid(*[np.linspace(0, 1, s) for s in shape], indexing="ij")
+    upper = z > 0.6
+    sig = (0.3 + 0.5 * x * y)[upper]
+    vol[upper] = (sig + rng.standard_normal(sig.shape) * np.sqrt(0.002 * sig + 1e-4)).astype(np.float32)
+    g, o = gpu_noise(gpu, vol, 5, 10.0, 0.4), o64_noise(vol, 5, 10.0, 0.4)
+    assert g.n_bins_used == o.n_bins_used
+    assert close(g.noise_ref, o.noise_ref)
+    if oracle.have_ref():
+        r = ref_noise(vol, 5, 10.0, 0.4)
+        assert g.n_bins_used == r.n_bins_used
+        assert close(g.noise_ref, r.noise_ref)
