@@ -31,6 +31,16 @@ class NoiseModel(C.Structure):
                 ("ref_intensity", C.c_double), ("n_bins_used", C.c_int)]
 
 
+class HistState(C.Structure):
+    """fy_hist_state (fysics.h:54): 256 u8 counts and their total."""
+    _fields_ = [("hist", C.c_long * 256), ("total", C.c_long)]
+
+
+class AnisoResult(C.Structure):
+    """fy_aniso_result (include/fysics_b200.h)."""
+    _fields_ = [("rho_z", C.c_double), ("rho_xy", C.c_double), ("status", C.c_int)]
+
+
 class RestoreCfg(C.Structure):
     """fy_restore_cfg (include/fysics_b200.h)."""
     _fields_ = [("deconv_kind", C.c_int), ("deconv_param", C.c_double), ("fz2_scale", C.c_double),
@@ -127,6 +137,17 @@ SIGNATURES = {
     "fy_dering_finalize": (_l, [_PD, _i, C.c_uint, _d, _d]),
     "fy_dering_apply": (None, [_PD, _P, _l, _l, _l, _l, _l, _l, _d]),
     "fy_phase_correlate": (_i, [_P, _P, _i, _i, _i, _PDBL, _PDBL, _i]),
+    "fy_hist_init": (None, [C.POINTER(HistState)]),
+    "fy_hist_accumulate_u8": (None, [C.POINTER(HistState), _P, _sz]),
+    "fy_hist_merge": (None, [C.POINTER(HistState), C.POINTER(HistState)]),
+    "fy_hist_percentile_u8": (_i, [C.POINTER(HistState), _d]),
+    "fy_hist_percentile_u8_inner": (_i, [C.POINTER(HistState), _d]),
+    "fy_flat_noise": (_d, [_P, _i, _i, _i, _i]),
+    "fy_noise_aniso": (_i, [_P, _i, _i, _i, _PDBL, _PDBL]),
+    "fy_gpu_hist_accumulate_u8": (_i, [_P, _sz, _P, _P]),
+    "fy_gpu_calib_scratch_bytes": (_sz, [_i, _i, _i, _i]),
+    "fy_gpu_flat_noise": (_i, [_P, _i, _i, _i, _i, _P, _P, _P]),
+    "fy_gpu_noise_aniso": (_i, [_P, _i, _i, _i, _P, _P, _P]),
     # ---- fy_gpu_* extension
     "fy_gpu_init": (_i, [_i]),
     "fy_gpu_last_status": (_i, []),

@@ -120,6 +120,20 @@ void fy_dering_apply(const fy_dering *d, float *f, long z0, long y0, long x0, lo
 int fy_phase_correlate(const float *fixed, const float *moving, int nz, int ny, int nx,
                        double *shift, double *peak, int window);
 
+/* calibration statistics (pass 1), fysics.h:54, 78-82, 95, 214-215. The histogram state is
+ * layout-identical; fy_hist_init/merge/percentile* are O(256) host bookkeeping on it, the
+ * per-voxel counting of fy_hist_accumulate_u8 runs on the GPU. fy_flat_noise returns NaN
+ * (reason in fy_gpu_last_error) when it cannot run; fy_noise_aniso returns 1 as the
+ * reference does for too few blocks, and an FY_E* code above 1 when it cannot run. */
+typedef struct { long hist[256]; long total; } fy_hist_state;
+void   fy_hist_init(fy_hist_state *s);
+void   fy_hist_accumulate_u8(fy_hist_state *s, const unsigned char *chunk, size_t n);
+void   fy_hist_merge(fy_hist_state *dst, const fy_hist_state *src);
+int    fy_hist_percentile_u8(const fy_hist_state *s, double pct);
+int    fy_hist_percentile_u8_inner(const fy_hist_state *s, double pct);
+double fy_flat_noise(const float *v, int nz, int ny, int nx, int blk);
+int    fy_noise_aniso(const float *v, int nz, int ny, int nx, double *rho_z, double *rho_xy);
+
 /* ================================================================== part 2: fy_gpu_* */
 
 /* status codes (0 = success; 1 is the reference's generic failure) */
@@ -200,6 +214,24 @@ const float *fy_gpu_noise_eps(const void *d_scratch, int nz, int ny, int nx);
 int    fy_gpu_estimate_noise_noalloc(const float *d_in, int nz, int ny, int nx, int win,
                                      double flat_pct, double ref_intensity,
                                      fy_noise_model *d_model, float *d_eps, void *stream);
+
+/* Calibration statistics on device data (fy_hist_accumulate_u8, fy_flat_noise,
+ * fy_noise_aniso; fysics.h:79, 95, 214-215). fy_gpu_hist_accumulate_u8 adds the counts of a
+ * device u8 chunk to d_hist, 256 unsigned 64-bit counters in device memory. The other two
+ * take d_scratch of fy_gpu_calib_scratch_bytes(nz, ny, nx, blk) bytes (blk: the noise
+ * floor's block size; the anisotropy uses 8) and leave their result in device memory: the
+ * noise floor as one double, the anisotropy as an fy_aniso_result whose status is
+ * fy_noise_aniso's return value. All enqueue on `stream` without synchronising, except
+ * fy_gpu_noise_aniso on a volume of fewer than 64 blocks, which writes status 1 and
+ * waits for that copy. */
+typedef struct { double rho_z, rho_xy; int status; } fy_aniso_result;
+int    fy_gpu_hist_accumulate_u8(const unsigned char *d_chunk, size_t n, unsigned long long *d_hist,
+                                 void *stream);
+size_t fy_gpu_calib_scratch_bytes(int nz, int ny, int nx, int blk);
+int    fy_gpu_flat_noise(const float *d_v, int nz, int ny, int nx, int blk, double *d_floor,
+                         void *d_scratch, void *stream);
+int    fy_gpu_noise_aniso(const float *d_v, int nz, int ny, int nx, fy_aniso_result *d_out,
+                          void *d_scratch, void *stream);
 
 /* Device-resident ring state for chains (fy_dering's arrays live on the GPU). accumulate
  * adds a device u8 region at global (z0,y0,x0) into slab z0/slab_z (accumulate + merge);

@@ -41,6 +41,11 @@ class RefDering(C.Structure):
                 ("ring", C.POINTER(C.c_float)), ("have_rings", C.c_int)]
 
 
+class RefHist(C.Structure):
+    """fy_hist_state (fysics.h:54): 256 u8 counts and their total."""
+    _fields_ = [("hist", C.c_long * 256), ("total", C.c_long)]
+
+
 _P, _i, _l, _d, _sz = C.c_void_p, C.c_int, C.c_long, C.c_double, C.c_size_t
 _PP = C.POINTER(RefPhysics)
 _PDB = C.POINTER(C.c_double)
@@ -77,6 +82,13 @@ REF_SIGS = {
     "fy_dering_finalize": (_l, [C.POINTER(RefDering), _i, C.c_uint, _d, _d]),
     "fy_dering_apply": (None, [C.POINTER(RefDering), _P, _l, _l, _l, _l, _l, _l, _d]),
     "fy_phase_correlate": (_i, [_P, _P, _i, _i, _i, _PDB, _PDB, _i]),
+    "fy_hist_init": (None, [C.POINTER(RefHist)]),
+    "fy_hist_accumulate_u8": (None, [C.POINTER(RefHist), _P, _sz]),
+    "fy_hist_merge": (None, [C.POINTER(RefHist), C.POINTER(RefHist)]),
+    "fy_hist_percentile_u8": (_i, [C.POINTER(RefHist), _d]),
+    "fy_hist_percentile_u8_inner": (_i, [C.POINTER(RefHist), _d]),
+    "fy_flat_noise": (_d, [_P, _i, _i, _i, _i]),
+    "fy_noise_aniso": (_i, [_P, _i, _i, _i, _PDB, _PDB]),
 }
 
 O64_SIGS = {
@@ -99,6 +111,9 @@ O64_SIGS = {
     "o64_phase_correlate": (_i, [_P, _P, _i, _i, _i, _PDB, _PDB, _i, C.POINTER(_l)]),
     "o64_fit_radial_eps": (_i, [_P, _P, _i, _PDB, _PDB, _PDB]),
     "o64_median_floor": (C.c_double, [_P, _i]),
+    "o64_hist_u8": (None, [_P, _sz, _P]),
+    "o64_flat_noise": (_d, [_P, _i, _i, _i, _i]),
+    "o64_noise_aniso": (_i, [_P, _i, _i, _i, _PDB, _PDB]),
     "o64_radial_tile_eps": (C.c_double, [_i, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                          C.c_double, C.c_long, C.c_long, C.c_long, C.c_long]),
 }

@@ -700,3 +700,116 @@ double o64_radial_tile_eps(int have, double a, double b, double median, double g
     if (s2 > 8.0) s2 = 8.0;
     return guided_eps * s2;
 }
+
+/* ---------------------------------------------------------------- calibration statistics */
+/* Histogram of u8 values (stream.c:76-86): every value counted once. */
+void o64_hist_u8(const uint8_t *v, size_t n, long long *hist) {
+    for (size_t i = 0; i < n; ++i) hist[v[i]] += 1;
+}
+
+/* Flat-region noise floor (stream.c:174-200). Blocks of blk^3 voxels tile the volume from
+ * the origin (partial blocks at the far edges are skipped). A block's sums run in voxel
+ * order in double; the squares are float products, as the reference's `val*val` on a float
+ * is. Blocks whose mean exceeds 0.1 contribute sqrt(max(var, 0)); the answer is the order
+ * statistic m/10 (0-based) of those stds, ascending. */
+double o64_flat_noise(const float *v, int nz, int ny, int nx, int blk) {
+    if (blk < 4) blk = 8;
+    const int bz = nz / blk, by = ny / blk, bx = nx / blk;
+    const long nb = (long)bz * by * bx;
+    if (nb <= 0) return 0;
+    double *std_of = (double *)malloc(sizeof(double) * (size_t)nb);
+    if (!std_of) return -1;
+    long m = 0;
+    const double cnt = (double)blk * blk * blk;
+    for (long b = 0; b < nb; ++b) {
+        const long z0 = (b / ((long)by * bx)) * blk, y0 = ((b / bx) % by) * blk, x0 = (b % bx) * blk;
+        double s = 0, s2 = 0;
+        for (int k = 0; k < blk * blk * blk; ++k) {
+            const long z = z0 + k / (blk * blk), y = y0 + (k / blk) % blk, x = x0 + k % blk;
+            const float t = v[((size_t)z * ny + y) * nx + x];
+            const float t2 = t * t;
+            s += t;
+            s2 += t2;
+        }
+        const double mean = s / cnt, var = s2 / cnt - mean * mean;
+        if (mean > 0.1) std_of[m++] = sqrt(var > 0 ? var : 0);
+    }
+    double out = 0;
+    if (m > 0) {
+        qsort(std_of, (size_t)m, sizeof(double), o64_cmp_double);
+        out = std_of[m / 10];
+    }
+    free(std_of);
+    return out;
+}
+
+/* Noise anisotropy (noise.c:210-269). 8^3 blocks from the origin; a block with any voxel
+ * <= 0 is skipped (a NaN voxel does not skip it). Block variance in double from double sums of t and t^2, stored as a
+ * float; the threshold is the order statistic nv/5 (0-based) of those floats. Blocks whose
+ * variance (double) is at most the threshold give residuals r = (float)(t - (float)mean)
+ * and add r*r to the denominator and the products of each r with its +z, +y, +x neighbour
+ * inside the block to the three lag-1 sums (all double). rho = 8/7 * lag sum / denominator,
+ * rho_xy the mean of the y and x ones. Returns 1 with fewer than 64 blocks, 64 non-zero
+ * blocks, 32 flat blocks, or a zero denominator. */
+static int o64_cmp_float(const void *a, const void *b) {
+    float x = *(const float *)a, y = *(const float *)b;
+    return (x > y) - (x < y);
+}
+int o64_noise_aniso(const float *v, int nz, int ny, int nx, double *rho_z, double *rho_xy) {
+    enum { B = 8, B3 = B * B * B };
+    const int bz = nz / B, by = ny / B, bx = nx / B;
+    const long nb = (long)bz * by * bx;
+    if (nb < 64) return 1;
+    float *bvar = (float *)malloc(sizeof(float) * (size_t)nb);
+    signed char *state = (signed char *)malloc((size_t)nb);       /* 0 skipped, 1 kept */
+    double *mean_of = (double *)malloc(sizeof(double) * (size_t)nb);
+    double *var_of = (double *)malloc(sizeof(double) * (size_t)nb);
+    if (!bvar || !state || !mean_of || !var_of) { free(bvar); free(state); free(mean_of); free(var_of); return 1; }
+    long nv = 0;
+    for (long b = 0; b < nb; ++b) {
+        const long z0 = (b / ((long)by * bx)) * B, y0 = ((b / bx) % by) * B, x0 = (b % bx) * B;
+        double s = 0, s2 = 0;
+        int positive = 1;
+        for (int k = 0; k < B3; ++k) {
+            const float t = v[((size_t)(z0 + k / (B * B)) * ny + y0 + (k / B) % B) * nx + x0 + k % B];
+            if (t <= 0) positive = 0;
+            s += t;
+            s2 += (double)t * t;
+        }
+        state[b] = (signed char)positive;
+        mean_of[b] = s / B3;
+        var_of[b] = s2 / B3 - mean_of[b] * mean_of[b];
+        if (positive) bvar[nv++] = (float)var_of[b];
+    }
+    int rc = 1;
+    if (nv >= 64) {
+        qsort(bvar, (size_t)nv, sizeof(float), o64_cmp_float);
+        const float thresh = bvar[nv / 5];
+        double nzs = 0, nys = 0, nxs = 0, den = 0;
+        long used = 0;
+        float r[B3];
+        for (long b = 0; b < nb; ++b) {
+            if (!state[b] || var_of[b] > thresh) continue;
+            const long z0 = (b / ((long)by * bx)) * B, y0 = ((b / bx) % by) * B, x0 = (b % bx) * B;
+            const float fm = (float)mean_of[b];
+            for (int k = 0; k < B3; ++k)
+                r[k] = v[((size_t)(z0 + k / (B * B)) * ny + y0 + (k / B) % B) * nx + x0 + k % B] - fm;
+            for (int k = 0; k < B3; ++k) {
+                const int dz = k / (B * B), dy = (k / B) % B, dx = k % B;
+                den += (double)r[k] * r[k];
+                if (dz + 1 < B) nzs += (double)r[k] * r[k + B * B];
+                if (dy + 1 < B) nys += (double)r[k] * r[k + B];
+                if (dx + 1 < B) nxs += (double)r[k] * r[k + 1];
+            }
+            ++used;
+        }
+        if (used >= 32 && den > 0) {
+            const double corr = (double)B / (B - 1);
+            *rho_z = corr * nzs / den;
+            *rho_xy = corr * 0.5 * (nys + nxs) / den;
+            rc = 0;
+        }
+    }
+    free(bvar); free(state); free(mean_of); free(var_of);
+    return rc;
+}

@@ -79,6 +79,15 @@ double o64_median_floor(const double *v, int n);
 double o64_radial_tile_eps(int have, double a, double b, double median, double guided_eps,
                            double ecy, double ecx, long y0, long x0, long ty, long tx);
 
+/* calibration statistics (pass 1 of the pipeline) */
+/* counts of every u8 value of v[0, n) added to hist[256] (stream.c:76-86) */
+void   o64_hist_u8(const uint8_t *v, size_t n, long long *hist);
+/* 10th-percentile std over the bright (mean > 0.1) non-overlapping blk^3 blocks
+ * (stream.c:174-200); blk < 4 means 8; 0 without blocks */
+double o64_flat_noise(const float *v, int nz, int ny, int nx, int blk);
+/* lag-1 noise autocorrelation per axis in flat 8^3 blocks (noise.c:210-269); 0 on success */
+int    o64_noise_aniso(const float *v, int nz, int ny, int nx, double *rho_z, double *rho_xy);
+
 #ifdef __cplusplus
 }
 #endif
