@@ -617,50 +617,66 @@ def main():
     value = job_mvox_per_s(world, n, args.steps, total_ms)
 
     # ---- end to end through pinned host buffers: the same chain through the public call,
-    # each cube's H2D and D2H inside the timed region. Two stream slots alternate (own
-    # buffers and ring handle each), so one cube's copies overlap the neighbouring cube's
-    # kernels; the chains themselves serialise on the thread's workspaces.
+    # each cube's H2D and D2H inside the timed region. Three streams form a pipeline -- input
+    # copies, chains, output copies -- linked by events, over NSLOT buffer slots (device
+    # input and output, pinned result and ring handle each). The output link, which bounds
+    # this leg (537 MB of f32 per cube), then carries one result after another while the
+    # next inputs land and the next chain runs.
+    NSLOT = 3
     h_in = torch.empty(SHAPE, dtype=torch.uint8, pin_memory=True)
     h_in.copy_(u8.cpu())
+    st_in, st_run, st_out = (torch.cuda.Stream(device=dev) for _ in range(3))
     slots = []
-    for _ in range(2):
+    for _ in range(NSLOT):
         hs = C.c_void_p()
         fb.check(lib.fy_gpu_dering_create(C.byref(hs), nz, ny, nx, -1.0, -1.0, 512, 8), "fy_gpu_dering_create")
-        slots.append({"st": torch.cuda.Stream(device=dev), "d_in": torch.empty_like(u8), "d_out": torch.empty_like(out),
+        slots.append({"d_in": torch.empty_like(u8), "d_out": torch.empty_like(out),
                       "h_out": torch.empty(SHAPE, dtype=torch.float32, pin_memory=True), "ring": hs,
                       "cfg": restore_cfg(fb, hs)})
     e2e_steps = max(4, min(args.steps, 10))
-    ev_a = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
-    ev_b = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+    spr = C.c_void_p(st_run.cuda_stream)
 
-    def e2e_cube(k):
-        sl = slots[k % 2]
-        st_ = sl["st"]
-        spk = C.c_void_p(st_.cuda_stream)
-        with torch.cuda.stream(st_):
-            ev_a[k].record(st_)
+    def new_events(k):
+        return [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(k)]
+
+    def e2e_cube(k, ev):
+        """ev[k] = input copy start, input landed, chain done, result landed."""
+        sl = slots[k % NSLOT]
+        if k >= NSLOT:
+            st_in.wait_event(ev[k - NSLOT][2])           # d_in free: the slot's last chain read it
+            st_run.wait_event(ev[k - NSLOT][3])          # d_out free: the slot's last result is out
+        with torch.cuda.stream(st_in):
+            ev[k][0].record(st_in)
             sl["d_in"].copy_(h_in, non_blocking=True)
-            fb.check(lib.fy_gpu_dering_reset(sl["ring"], spk), "fy_gpu_dering_reset")
+            ev[k][1].record(st_in)
+        st_run.wait_event(ev[k][1])
+        with torch.cuda.stream(st_run):
+            fb.check(lib.fy_gpu_dering_reset(sl["ring"], spr), "fy_gpu_dering_reset")
             fb.check(lib.fy_gpu_restore_u8(C.c_void_p(sl["d_in"].data_ptr()), C.c_void_p(sl["d_out"].data_ptr()),
-                                           nz, ny, nx, 0.0, 1.0, C.byref(p), C.byref(sl["cfg"]), spk),
+                                           nz, ny, nx, 0.0, 1.0, C.byref(p), C.byref(sl["cfg"]), spr),
                      "fy_gpu_restore_u8")
+            ev[k][2].record(st_run)
+        st_out.wait_event(ev[k][2])
+        with torch.cuda.stream(st_out):
             sl["h_out"].copy_(sl["d_out"], non_blocking=True)
-            ev_b[k].record(st_)
+            ev[k][3].record(st_out)
 
-    for k in range(2):                                   # warm the second slot's buffers
-        e2e_cube(k)
+    warm = new_events(NSLOT)
+    for k in range(NSLOT):                               # warm every slot's buffers
+        e2e_cube(k, warm)
     torch.cuda.synchronize()
+    ev = new_events(e2e_steps)
     barrier()
     t_e2e = time.perf_counter()
     for k in range(e2e_steps):
-        if k >= 2:
-            ev_b[k - 2].synchronize()                    # the slot's previous cube is out
-        e2e_cube(k)
+        if k >= NSLOT:
+            ev[k - NSLOT][3].synchronize()               # the caller has the slot's last result
+        e2e_cube(k, ev)
     torch.cuda.synchronize()
     barrier()
     e2e_wall_ms = (time.perf_counter() - t_e2e) * 1e3
-    e2e_steps_ms = [ev_a[k].elapsed_time(ev_b[k]) for k in range(e2e_steps)]
-    e2e_dev_ms = ev_a[0].elapsed_time(ev_b[e2e_steps - 1])
+    e2e_steps_ms = [ev[k][0].elapsed_time(ev[k][3]) for k in range(e2e_steps)]
+    e2e_dev_ms = ev[0][0].elapsed_time(ev[e2e_steps - 1][3])
     for sl in slots:
         lib.fy_gpu_dering_destroy(sl["ring"])
     e2e_ms = max_over_ranks(max(e2e_dev_ms, e2e_wall_ms), dist, f"cuda:{dev}")
