@@ -53,6 +53,29 @@ class RestoreCfg(C.Structure):
                 ("radial", C.c_void_p), ("radial_cy", C.c_double), ("radial_cx", C.c_double)]
 
 
+class PipelineCfg(C.Structure):
+    """fy_pipeline_cfg (fysics.h:436-491), field for field."""
+    _fields_ = ([(n, C.c_double) for n in ("delta_beta", "energy_kev", "distance_mm", "pixel_um", "unsharp_sigma",
+                                           "unsharp_coeff", "machine_current_start", "machine_current_stop",
+                                           "window_lo", "window_hi")] +
+                [("do_deconv", C.c_int), ("use_matched_deconv", C.c_int), ("psf_sigma_vox", C.c_double),
+                 ("deconv_tikhonov", C.c_double), ("guided_eps", C.c_double), ("do_air_zero", C.c_int),
+                 ("air_cut_u8", C.c_int), ("air_cut_band", C.c_int), ("air_thresh", C.c_double),
+                 ("air_cut_aggr", C.c_double), ("air_min_component", C.c_int), ("denoise_k", C.c_double),
+                 ("scratch_passes", C.c_int), ("do_normalize", C.c_int), ("norm_lo", C.c_int), ("norm_hi", C.c_int),
+                 ("do_zdrift", C.c_int), ("zdrift_factor", C.POINTER(C.c_float)), ("do_dering", C.c_int),
+                 ("calib_budget_gb", C.c_double), ("dering_cy", C.c_double), ("dering_cx", C.c_double),
+                 ("psf_p5", C.c_double), ("psf_med", C.c_double), ("do_musica", C.c_int), ("musica_p", C.c_double),
+                 ("musica_levels", C.c_int), ("musica_core", C.c_double), ("guided_subsample", C.c_int),
+                 ("no_dither", C.c_int), ("halo", C.c_int), ("have_norm", C.c_int), ("have_zdrift", C.c_int),
+                 ("have_dec_range", C.c_int), ("have_dering", C.c_int), ("dering", C.c_void_p),
+                 ("psf_z_ratio", C.c_double), ("have_eps_r", C.c_int), ("eps_fn_a", C.c_double),
+                 ("eps_fn_b", C.c_double), ("eps_fn_med", C.c_double), ("dec_lo", C.c_double),
+                 ("dec_hi", C.c_double), ("vol_z", C.c_long), ("noise_floor", C.c_double),
+                 ("occ", C.c_void_p), ("occ_ncz", C.c_long), ("occ_ncy", C.c_long), ("occ_ncx", C.c_long),
+                 ("occ_cz", C.c_long), ("occ_cy", C.c_long), ("occ_cx", C.c_long)])
+
+
 class ServerCfg(C.Structure):
     """fy_server_cfg (include/fysics_b200.h)."""
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("workers", C.c_int), ("device", C.c_int),
@@ -148,6 +171,12 @@ SIGNATURES = {
     "fy_gpu_calib_scratch_bytes": (_sz, [_i, _i, _i, _i]),
     "fy_gpu_flat_noise": (_i, [_P, _i, _i, _i, _i, _P, _P, _P]),
     "fy_gpu_noise_aniso": (_i, [_P, _i, _i, _i, _P, _P, _P]),
+    "fy_valley_depth": (_d, [_P, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
+    "fy_process_buffer": (_i, [C.POINTER(PipelineCfg), _P, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l,
+                               _P, C.POINTER(_i)]),
+    "fy_gpu_process_buffer": (_i, [C.POINTER(PipelineCfg), _P, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l,
+                                   _l, _P, C.POINTER(_i), _P]),
+    "fy_process_buffer_air_state": (_i, [_P, _P]),
     # ---- fy_gpu_* extension
     "fy_gpu_init": (_i, [_i]),
     "fy_gpu_last_status": (_i, []),

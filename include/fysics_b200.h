@@ -134,6 +134,59 @@ int    fy_hist_percentile_u8_inner(const fy_hist_state *s, double pct);
 double fy_flat_noise(const float *v, int nz, int ny, int nx, int blk);
 int    fy_noise_aniso(const float *v, int nz, int ny, int nx, double *rho_z, double *rho_xy);
 
+/* histogram valley (fysics.h:92, stream.c:138-168): O(256) host arithmetic on counts */
+double fy_valley_depth(const long hist[256], int *dark_out, int *light_out, int *valley_out);
+
+/* ---- the per-tile chain of the export tool (fysics.h:436-511, pipeline.c:252-510).
+ * fy_pipeline_cfg is layout-identical to the reference's; fy_process_buffer reads the
+ * fields the tile chain uses (physics, window, do_deconv/use_matched_deconv/psf/tikhonov,
+ * dec range, guided_eps/subsample and the radial eps fit, air-zero settings, norm, dither,
+ * rings through `dering`, z drift through `zdrift_factor`) and ignores the rest. */
+typedef struct {
+    double delta_beta, energy_kev, distance_mm, pixel_um, unsharp_sigma, unsharp_coeff;
+    double machine_current_start, machine_current_stop;
+    double window_lo, window_hi;
+    int    do_deconv;
+    int    use_matched_deconv;
+    double psf_sigma_vox, deconv_tikhonov;
+    double guided_eps;
+    int    do_air_zero; int air_cut_u8, air_cut_band; double air_thresh;
+    double air_cut_aggr;
+    int    air_min_component;
+    double denoise_k;
+    int    scratch_passes;
+    int    do_normalize; int norm_lo, norm_hi;
+    int    do_zdrift; float *zdrift_factor;
+    int    do_dering;
+    double calib_budget_gb;
+    double dering_cy, dering_cx;
+    double psf_p5, psf_med;
+    int    do_musica; double musica_p; int musica_levels; double musica_core;
+    int    guided_subsample;
+    int    no_dither;
+    int    halo;
+    int    have_norm, have_zdrift, have_dec_range;
+    int    have_dering; fy_dering *dering;
+    double psf_z_ratio;
+    int    have_eps_r; double eps_fn_a, eps_fn_b, eps_fn_med;
+    double dec_lo, dec_hi;
+    long   vol_z;
+    double noise_floor;
+    const unsigned char *occ;
+    long   occ_ncz, occ_ncy, occ_ncx;
+    long   occ_cz, occ_cy, occ_cx;
+} fy_pipeline_cfg;
+/* One inner tile from a haloed u8 buffer (fysics.h:507-511): u8buf is hz*hy*hx at global
+ * origin (rz0, ry0, rx0); the inner tile (z0, y0, x0, tz, ty, tx) lies inside it; vol_y and
+ * vol_x are the full volume's (rotation axis default). Writes tz*ty*tx u8 to out and sets
+ * *all_air. Runs on the GPU and returns when out is written; thread-safe (each host thread
+ * has its own stream and workspaces). Returns 0, or an FY_E* code: FY_EINVAL for a
+ * tile outside the buffer, FY_EUNSUPPORTED for do_musica (not on this path). */
+int    fy_process_buffer(const fy_pipeline_cfg *cfg, const unsigned char *u8buf,
+                         long rz0, long ry0, long rx0, long hz, long hy, long hx,
+                         long z0, long y0, long x0, long tz, long ty, long tx,
+                         long vol_y, long vol_x, unsigned char *out, int *all_air);
+
 /* ================================================================== part 2: fy_gpu_* */
 
 /* status codes (0 = success; 1 is the reference's generic failure) */
@@ -319,6 +372,19 @@ void fy_restore_cfg_default(fy_restore_cfg *cfg);
 int  fy_gpu_restore_u8(const unsigned char *d_u8, float *d_out, int nz, int ny, int nx,
                        double f32_min, double f32_max, const fy_physics *p,
                        const fy_restore_cfg *cfg, void *stream);
+
+/* fy_process_buffer on device buffers: d_u8 (hz*hy*hx) in, d_out (tz*ty*tx) out, on
+ * `stream`. Synchronises the stream twice: after the all-air test (an empty buffer skips
+ * the chain, as the reference does) and at the end, so that *all_air and the status are
+ * final on return. */
+int    fy_gpu_process_buffer(const fy_pipeline_cfg *cfg, const unsigned char *d_u8,
+                             long rz0, long ry0, long rx0, long hz, long hy, long hx,
+                             long z0, long y0, long x0, long tz, long ty, long tx,
+                             long vol_y, long vol_x, unsigned char *d_out, int *all_air, void *stream);
+/* Air-cut state of the calling thread's last fy_process_buffer / fy_gpu_process_buffer:
+ * the 256-bin histogram of the scratch smooth and (cut, uniform cut, textured cut) in u8
+ * levels. Returns 0, or 1 when that call ran no air cut. */
+int    fy_process_buffer_air_state(long hist[256], int cuts[3]);
 
 /* Request loop (continuous batching) on one GPU; no reference counterpart. Callers submit
  * cubes from any thread as they need them. A pool of worker threads, each with its own CUDA

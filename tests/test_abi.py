@@ -32,6 +32,8 @@ def test_header_declares_the_drop_in_set():
         "fy_estimate_noise", "fy_guided_eps_for_noise", "fy_dering_init", "fy_dering_free",
         "fy_dering_tile_init", "fy_dering_tile_reset", "fy_dering_accumulate_u8",
         "fy_dering_merge_tile", "fy_dering_finalize", "fy_dering_apply", "fy_phase_correlate",
+        # the per-tile chain and pass-1 helpers (survey rows f1, f2)
+        "fy_process_buffer", "fy_valley_depth", "fy_hist_accumulate_u8", "fy_flat_noise", "fy_noise_aniso",
     }
     assert required <= names, sorted(required - names)
 
@@ -51,6 +53,11 @@ def test_struct_layouts_match_reference():
     assert C.sizeof(fb.Physics) == 64                      # fysics.h:23-35, 8 doubles
     assert C.sizeof(fb.NoiseModel) == 40                    # 4 doubles + int (+pad)
     assert fb.Dering.ring.offset == 72 and C.sizeof(fb.Dering) == 88
+    # fy_pipeline_cfg (fysics.h:436-491): 440 bytes on LP64, the ring handle at 304
+    assert C.sizeof(fb.PipelineCfg) == 440 and fb.PipelineCfg.dering.offset == 304
+    import oracle
+    assert [(n, getattr(fb.PipelineCfg, n).offset) for n, _ in fb.PipelineCfg._fields_] == \
+        [(n, getattr(oracle.RefPipelineCfg, n).offset) for n, _ in oracle.RefPipelineCfg._fields_]
 
 
 def test_scalar_helpers_match_reference(fy):
