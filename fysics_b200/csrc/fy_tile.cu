@@ -312,11 +312,23 @@ __global__ void __launch_bounds__(kTpb) k_air_apply(AirArgs a) {
 // ---------------------------------------------------------------- connected components
 __device__ __forceinline__ int uf_find(int* L, int i, int* err) {
     for (int it = 0; it < kUfMaxIter; ++it) {
-        const int p = L[i];
+        const int p = __ldcg(L + i);     // L2 reads: links made by other threads are seen
         if (p == i) return i;
-        const int g = L[p];
+        const int g = __ldcg(L + p);
         if (g != p) L[i] = g;            // path halving: g is an ancestor of i
         i = g;
+    }
+    *err = 1;
+    return i;
+}
+
+// Read-only walk to the root: the flatten pass uses it, so that no store of another walk can
+// land on a label after its final root was written.
+__device__ __forceinline__ int uf_root(const int* L, int i, int* err) {
+    for (int it = 0; it < kUfMaxIter; ++it) {
+        const int p = __ldcg(L + i);
+        if (p == i) return i;
+        i = p;
     }
     *err = 1;
     return i;
@@ -344,43 +356,67 @@ struct CcArgs {
     int min_size;
 };
 
-__global__ void __launch_bounds__(256) k_cc_init(CcArgs a, size_t n) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        a.lab[i] = a.f[i] > 0.0f ? (int)i : -1;
+// Labels start as x-runs: each material voxel points at the first voxel of its run within
+// its 32-voxel warp chunk of the row (a forest of depth one); info is cleared.
+__global__ void __launch_bounds__(kTpb) k_cc_init(CcArgs a) {
+    const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    const int lane = threadIdx.x & 31;
+    for (long z = blockIdx.z; z < a.nz; z += gridDim.z) {
+        const size_t i = ((size_t)z * a.ny + y) * a.nx + x;
+        const bool mat = x < a.nx && a.f[i] > 0.0f;
+        const unsigned bits = __ballot_sync(0xffffffffu, mat);
+        if (x >= a.nx) continue;
+        const unsigned gaps = ~bits & ((1u << lane) - 1u);      // non-material lanes below this one
+        const int start = gaps ? 32 - __clz(gaps) : 0;          // first lane of this run in the chunk
+        a.lab[i] = mat ? (int)(i - (size_t)(lane - start)) : -1;
         a.info[i] = 0u;
     }
 }
 
+// Join runs: across a chunk boundary in x, and to the -y and -z neighbours where a run
+// overlap starts (if the left neighbours are both material, they already joined the runs).
 __global__ void __launch_bounds__(kTpb) k_cc_union(CcArgs a) {
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= a.nx) return;
+    const long plane = a.ny * a.nx;
     for (long z = blockIdx.z; z < a.nz; z += gridDim.z) {
         const int i = (int)(((size_t)z * a.ny + y) * a.nx + x);
         if (a.lab[i] < 0) continue;
-        if (x > 0 && a.lab[i - 1] >= 0) uf_union(a.lab, i, i - 1, a.err);
-        if (y > 0 && a.lab[i - a.nx] >= 0) uf_union(a.lab, i, i - (int)a.nx, a.err);
-        if (z > 0 && a.lab[i - a.ny * a.nx] >= 0) uf_union(a.lab, i, i - (int)(a.ny * a.nx), a.err);
+        const bool left = x > 0 && a.lab[i - 1] >= 0;
+        if (left && (x & 31) == 0) uf_union(a.lab, i, i - 1, a.err);
+        if (y > 0 && a.lab[i - a.nx] >= 0 && !(left && a.lab[i - 1 - a.nx] >= 0))
+            uf_union(a.lab, i, i - (int)a.nx, a.err);
+        if (z > 0 && a.lab[i - plane] >= 0 && !(left && a.lab[i - 1 - plane] >= 0))
+            uf_union(a.lab, i, i - (int)plane, a.err);
     }
 }
 
+__global__ void __launch_bounds__(256) k_cc_flatten(CcArgs a, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (a.lab[i] >= 0) a.lab[i] = uf_root(a.lab, (int)i, a.err);
+}
+
+// Component sizes and face contact, one atomic per distinct root per warp.
 __global__ void __launch_bounds__(kTpb) k_cc_count(CcArgs a) {
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= a.nx) return;
+    const int lane = threadIdx.x & 31;
     for (long z = blockIdx.z; z < a.nz; z += gridDim.z) {
-        const int i = (int)(((size_t)z * a.ny + y) * a.nx + x);
-        if (a.lab[i] < 0) continue;
-        const int root = uf_find(a.lab, i, a.err);
-        const bool edge = z == 0 || z == a.nz - 1 || y == 0 || y == a.ny - 1 || x == 0 || x == a.nx - 1;
-        atomicAdd(&a.info[root], 1u);
-        if (edge) atomicOr(&a.info[root], kEdge);
+        const size_t i = ((size_t)z * a.ny + y) * a.nx + x;
+        const int root = x < a.nx ? a.lab[i] : -1;
+        const bool edge = root >= 0 && (z == 0 || z == a.nz - 1 || y == 0 || y == a.ny - 1 || x == 0 || x == a.nx - 1);
+        const unsigned peers = __match_any_sync(0xffffffffu, root);
+        const unsigned epeers = __ballot_sync(0xffffffffu, edge) & peers;
+        if (root >= 0 && lane == __ffs(peers) - 1) {
+            atomicAdd(&a.info[root], (unsigned)__popc(peers));
+            if (epeers) atomicOr(&a.info[root], kEdge);
+        }
     }
 }
 
 __global__ void __launch_bounds__(256) k_cc_zero(CcArgs a, size_t n) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int l = a.lab[i];
-        if (l < 0) continue;
-        const int root = uf_find(a.lab, l, a.err);   // the labels are roots' descendants
+        const int root = a.lab[i];
+        if (root < 0) continue;
         const unsigned v = a.info[root];
         if (!(v & kEdge) && (long)(v & ~kEdge) < a.min_size) a.f[i] = 0.0f;
     }
@@ -598,26 +634,33 @@ int tile_chain(const fy_pipeline_cfg* c, const uint8_t* d_u8, long rz0, long ry0
         TRY(box_pass(orig, t1, (int)mx, r, mz, my, d * hy * hx, d * hx, d, mp, mx, 1, st));
         TRY(box_pass(t1, t2, (int)my, r, mz, mx, mp, 1, mx, mp, 1, mx, st));
         TRY(box_pass(t2, sm, (int)mz, r, my, mx, mx, 1, mp, mx, 1, mp, st));
+        fy_prof_mark(st, "tile.scratch_box");
         k_air_hist<<<grid1(m, 256, cx.sms), 256, 0, st>>>(sm, m, ctl);
         TRY(cudaGetLastError());
         k_air_cut<<<1, 1, 0, st>>>(ctl, c->air_cut_u8, c->air_cut_band, c->air_thresh, c->air_cut_aggr);
         TRY(cudaGetLastError());
+        fy_prof_mark(st, "tile.air_cut");
         AirArgs aa{f, orig, sm, ctl, hz, hy, hx, lz, ly, lx, lowres ? 1 : 0};
         k_air_apply<<<grid_rows(hx, hy, hz), kTpb, 0, st>>>(aa);
         TRY(cudaGetLastError());
         launches += 6;
-        fy_prof_mark(st, "tile.air");
+        fy_prof_mark(st, "tile.air_apply");
         if (c->air_min_component > 0) {
             TRY(w.lab.ensure(hn * sizeof(int)));
             TRY(w.info.ensure(hn * sizeof(unsigned)));
             CcArgs ca{f, w.lab.as<int>(), w.info.as<unsigned>(), &ctl->err, hz, hy, hx, c->air_min_component};
-            k_cc_init<<<grid1(hn, 256, cx.sms), 256, 0, st>>>(ca, hn);
+            k_cc_init<<<grid_rows(hx, hy, hz), kTpb, 0, st>>>(ca);
+            fy_prof_mark(st, "tile.cc_init");
             k_cc_union<<<grid_rows(hx, hy, hz), kTpb, 0, st>>>(ca);
+            fy_prof_mark(st, "tile.cc_union");
+            k_cc_flatten<<<grid1(hn, 256, cx.sms), 256, 0, st>>>(ca, hn);
+            fy_prof_mark(st, "tile.cc_flatten");
             k_cc_count<<<grid_rows(hx, hy, hz), kTpb, 0, st>>>(ca);
+            fy_prof_mark(st, "tile.cc_count");
             k_cc_zero<<<grid1(hn, 256, cx.sms), 256, 0, st>>>(ca, hn);
             TRY(cudaGetLastError());
-            launches += 4;
-            fy_prof_mark(st, "tile.despeckle");
+            launches += 5;
+            fy_prof_mark(st, "tile.cc_zero");
         }
     }
 
