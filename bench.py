@@ -391,6 +391,238 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
 
 
 # ------------------------------------------------------------------------------ registration
+class WorkerPool:
+    """`n` persistent host threads. run(fn, items) hands out 0..items-1 through a shared
+    counter and returns the wall time; run_each(fn) runs fn once on every thread (the
+    warm-up, so that each thread's library workspaces exist before anything is timed).
+    fn(worker, item) returns 0 or an error code. close() releases every thread's library
+    workspaces (fy_gpu_release) and joins the threads."""
+
+    def __init__(self, n, lib):
+        self.n, self.lib = n, lib
+        self.go, self.done = threading.Barrier(n + 1), threading.Barrier(n + 1)
+        self.lock = threading.Lock()
+        self.fn, self.items, self.next, self.each, self.errs = None, 0, 0, False, []
+        self.threads = [threading.Thread(target=self._loop, args=(w,), daemon=True) for w in range(n)]
+        for t in self.threads:
+            t.start()
+
+    def _loop(self, w):
+        while True:
+            self.go.wait()
+            if self.fn is None:
+                self.lib.fy_gpu_release()
+                self.done.wait()
+                return
+            if self.each:
+                rc = self.fn(w, w)
+                if rc:
+                    self.errs.append(rc)
+            else:
+                while True:
+                    with self.lock:
+                        k = self.next
+                        self.next += 1
+                    if k >= self.items:
+                        break
+                    rc = self.fn(w, k)
+                    if rc:
+                        self.errs.append(rc)
+            self.done.wait()
+
+    def _start(self, fn, items, each):
+        self.fn, self.items, self.next, self.each, self.errs = fn, items, 0, each, []
+        t0 = time.perf_counter()
+        self.go.wait()
+        self.done.wait()
+        dt = time.perf_counter() - t0
+        if self.errs:
+            raise RuntimeError(f"worker call failed: {self.errs[:3]} {self.lib.fy_gpu_last_error()}")
+        return dt
+
+    def run(self, fn, items):
+        return self._start(fn, items, False)
+
+    def run_each(self, fn):
+        return self._start(fn, self.n, True)
+
+    def close(self):
+        self.fn = None
+        self.go.wait()
+        self.done.wait()
+        for t in self.threads:
+            t.join()
+
+
+def tiles_sample(fb, lib, dev, seed, threads=8, passes=3, cpu_budget_s=10.0):
+    """The export tool's per-tile chain (fy_process_buffer, pipeline.c:467-510) as its worker
+    pool calls it (mca_export.c:634-660): 16 inner tiles of 128^3 with an 8-voxel halo
+    (144^3 u8 buffers) from a synthetic 144 x 528 x 528 scroll band, with the export
+    settings: no deconvolution, guided eps 8e-4 on 2x-subsampled coefficients, air cut,
+    despeckle of islands under 64 voxels, recenter [40, 200], dithered u8.
+      e2e       `threads` host threads take tiles from a shared queue and call
+                fy_process_buffer on pageable host buffers (copies inside the timing);
+      resident  the same threads call fy_gpu_process_buffer on device-resident buffers,
+                one CUDA stream each;
+      reference the reference's fy_process_buffer, one tile per host thread (bounded)."""
+    import torch
+    import fysics_b200.phantom as ph
+    vol = ph.scroll_volume((144, 528, 528), seed=seed)
+    halo, T = 8, 128
+    tiles = []
+    for ty in range(4):
+        for tx in range(4):
+            z0, y0, x0 = halo, halo + T * ty, halo + T * tx
+            org = (z0 - halo, y0 - halo, x0 - halo)
+            buf = np.ascontiguousarray(vol[org[0]:z0 + T + halo, org[1]:y0 + T + halo, org[2]:x0 + T + halo])
+            tiles.append((buf, org, (z0, y0, x0, T, T, T)))
+    vyx = vol.shape[1:]
+    cfgd = dict(delta_beta=1000.0, energy_kev=78.0, distance_mm=220.0, pixel_um=2.4, unsharp_sigma=1.2,
+                unsharp_coeff=4.0, use_matched_deconv=1, psf_sigma_vox=1.0, deconv_tikhonov=0.05, guided_eps=8e-4,
+                do_air_zero=1, air_cut_u8=-1, air_cut_band=8, air_thresh=0.05, air_cut_aggr=0.5,
+                air_min_component=64, scratch_passes=5, have_norm=1, norm_lo=40, norm_hi=200, halo=halo,
+                dering_cy=-1.0, dering_cx=-1.0)
+    cfg = fb.PipelineCfg()
+    for k, v in cfgd.items():
+        setattr(cfg, k, v)
+    inner_vox = T ** 3
+
+    outs = [np.empty((T, T, T), np.uint8) for _ in range(len(tiles))]
+
+    def host_work(wid, k):
+        buf, org, inner = tiles[k % len(tiles)]
+        air = C.c_int()
+        return lib.fy_process_buffer(C.byref(cfg), buf.ctypes.data, *org, *buf.shape, *inner, *vyx,
+                                     outs[k % len(tiles)].ctypes.data, C.byref(air))
+
+    d_bufs = [torch.from_numpy(t[0]).to(f"cuda:{dev}") for t in tiles]
+    d_outs = [torch.empty((T, T, T), dtype=torch.uint8, device=f"cuda:{dev}") for _ in range(threads)]
+    streams = [torch.cuda.Stream(device=dev) for _ in range(threads)]
+    torch.cuda.synchronize()
+
+    def dev_work(wid, k):
+        buf, org, inner = tiles[k % len(tiles)]
+        k = k % len(tiles)
+        air = C.c_int()
+        return lib.fy_gpu_process_buffer(C.byref(cfg), C.c_void_p(d_bufs[k].data_ptr()), *org, *buf.shape, *inner,
+                                         *vyx, C.c_void_p(d_outs[wid].data_ptr()), C.byref(air),
+                                         C.c_void_p(streams[wid].cuda_stream))
+
+    n_items = passes * len(tiles)
+    pool = WorkerPool(threads, lib)
+    try:
+        pool.run_each(host_work)                       # warm-up: every thread's workspaces
+        pool.run(host_work, len(tiles))
+        t_host = pool.run(host_work, n_items)
+        pool.run_each(dev_work)
+        pool.run(dev_work, len(tiles))
+        t_dev = pool.run(dev_work, n_items)
+    finally:
+        pool.close()
+    res = {"workload": "16 tiles of 128^3 (8-voxel halo, 144^3 u8 buffers) from a synthetic 144x528x528 scroll "
+                       "band; export settings: no deconvolution, guided eps 8e-4 subsample 2, air cut, despeckle "
+                       "< 64 voxels, recenter [40, 200], dithered u8",
+           "threads": threads, "tiles_timed": n_items,
+           "e2e": {"tiles_per_s": n_items / t_host, "mvox_per_s": n_items * inner_vox / t_host / 1e6,
+                   "ms_per_tile": t_host * 1e3 / n_items, "api": "fy_process_buffer, pageable host buffers"},
+           "resident": {"tiles_per_s": n_items / t_dev, "mvox_per_s": n_items * inner_vox / t_dev / 1e6,
+                        "ms_per_tile": t_dev * 1e3 / n_items, "api": "fy_gpu_process_buffer, one stream per thread"}}
+    try:
+        import oracle
+        from concurrent.futures import ThreadPoolExecutor
+        if oracle.have_ref() and cpu_budget_s > 0:
+            L = oracle.ref()
+            rcfg = oracle.ref_pipeline_cfg(oracle.pipeline_defaults(**cfgd))
+            ref_out = [np.empty((T, T, T), np.uint8) for _ in range(len(tiles))]
+
+            def one(k):
+                buf, org, inner = tiles[k % len(tiles)]
+                air = C.c_int()
+                L.fy_process_buffer(C.byref(rcfg), oracle.p(buf), *org, *buf.shape, *inner, *vyx,
+                                    oracle.p(ref_out[k % len(tiles)]), C.byref(air))
+                return 1
+
+            t1 = time.perf_counter()
+            one(0)
+            t_one = time.perf_counter() - t1
+            cores = os.cpu_count() or 1
+            jobs = max(1, min(len(tiles), int(cpu_budget_s / max(t_one, 1e-3)) * cores // 2, cores))
+            t1 = time.perf_counter()
+            with ThreadPoolExecutor(max_workers=cores) as ex:
+                done = sum(ex.map(one, range(jobs)))
+            dt = time.perf_counter() - t1
+            res["cpu_reference"] = {"tiles_per_s": done / dt, "mvox_per_s": done * inner_vox / dt / 1e6,
+                                    "cores": cores, "kind": "reference",
+                                    "sample": f"{done} tiles, one per host thread; single-thread {t_one * 1e3:.0f} ms "
+                                              "per tile"}
+            same = [np.count_nonzero(ref_out[k] != outs[k]) for k in range(min(done, len(tiles)))]
+            res["u8_voxels_differing_from_reference"] = {"tiles": len(same), "voxels": int(sum(same)),
+                                                         "of": len(same) * inner_vox}
+    except Exception as exc:          # reported, never required
+        res["cpu_reference"] = {"error": str(exc)[:200]}
+    return res
+
+
+def viewer_slab_sample(fb, lib, dev, seed, reps=40, cpu_budget_s=5.0):
+    """The viewer path (README.md:109-118, :190): fy_deconvolve (auto reg) on 8x512x512 f32
+    slabs with the reference physics, as an interactive caller issues it. Host API on pageable
+    buffers, one call at a time (copies inside each call), and the device form on resident
+    buffers; beside them the reference's fy_deconvolve on the host."""
+    import torch
+    rng = np.random.default_rng(seed)
+    shape = (8, 512, 512)
+    n = int(np.prod(shape))
+    slab = rng.uniform(0.0, 1.0, shape).astype(np.float32)
+    out = np.empty_like(slab)
+    ph = fb.physics()
+    t_host = []
+    for i in range(reps + 3):
+        t0 = time.perf_counter()
+        fb.check(lib.fy_deconvolve(slab.ctypes.data, out.ctypes.data, *shape, C.byref(ph), -1.0), "fy_deconvolve")
+        if i >= 3:
+            t_host.append(time.perf_counter() - t0)
+    d_in = torch.from_numpy(slab).to(f"cuda:{dev}")
+    d_out = torch.empty_like(d_in)
+    st = torch.cuda.Stream(device=dev)
+    args = (C.c_void_p(d_in.data_ptr()), 0, 0.0, 0.0, C.c_void_p(d_out.data_ptr()), *shape, C.byref(ph), -1.0, 0, 1.0,
+            C.c_void_p(st.cuda_stream))
+    for _ in range(3):
+        fb.check(lib.fy_gpu_deconvolve_ex(*args), "fy_gpu_deconvolve_ex")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(reps):
+        lib.fy_gpu_deconvolve_ex(*args)
+    e1.record(st)
+    e1.synchronize()
+    dev_ms = e0.elapsed_time(e1) / reps
+    p50 = float(np.percentile(t_host, 50)) * 1e3
+    res = {"workload": "fy_deconvolve, auto reg, reference physics, 8x512x512 f32 slab (uniform [0,1])",
+           "e2e": {"ms_p50": p50, "ms_p99": float(np.percentile(t_host, 99)) * 1e3, "mvox_per_s": n / p50 / 1e3,
+                   "api": "fy_deconvolve, pageable host buffers, one call at a time",
+                   "h2d_bytes": 4 * n, "d2h_bytes": 4 * n},
+           "resident": {"ms_per_slab": dev_ms, "mvox_per_s": n / dev_ms / 1e3,
+                        "api": "fy_gpu_deconvolve_ex, device buffers, back to back on one stream"}}
+    try:
+        import oracle
+        if oracle.have_ref() and cpu_budget_s > 0:
+            rph = oracle.RefPhysics(*[getattr(ph, k) for k, _ in ph._fields_])
+            ts = []
+            t_end = time.perf_counter() + cpu_budget_s
+            while time.perf_counter() < t_end and len(ts) < 20:
+                t0 = time.perf_counter()
+                oracle.ref_deconvolve(slab, rph, -1.0)
+                ts.append(time.perf_counter() - t0)
+            ms = float(np.median(ts)) * 1e3
+            res["cpu_reference"] = {"ms_per_slab": ms, "mvox_per_s": n / ms / 1e3, "cores": os.cpu_count(),
+                                    "kind": "reference",
+                                    "sample": f"{len(ts)} calls of the reference's fy_deconvolve (its own "
+                                              "OpenMP threads), median"}
+    except Exception as exc:          # reported, never required
+        res["cpu_reference"] = {"error": str(exc)[:200]}
+    return res
+
+
 def phasecorr_sample(fb, lib, dev, seed, db_scale, npairs=64, n=256, distinct=8, cpu_budget_s=10.0):
     """Config-4 sample: npairs pairs of n^3 f32 volumes; the moving volume is an FP64 Fourier
     shift of the fixed one (integer U[-40,40] + subvoxel U[-0.5,0.5] per axis), each with
@@ -545,6 +777,8 @@ def main():
     ap.add_argument("--size", type=int, default=512, help="cube edge (512 = the benchmark workload)")
     ap.add_argument("--no-serve", action="store_true", help="skip the served / batched samples")
     ap.add_argument("--no-phasecorr", action="store_true", help="skip the registration sample")
+    ap.add_argument("--no-tiles", action="store_true", help="skip the per-tile export chain sample")
+    ap.add_argument("--no-viewer", action="store_true", help="skip the viewer slab sample")
     args = ap.parse_args()
     global SHAPE, WORKLOAD
     if args.size != 512:
@@ -733,6 +967,20 @@ def main():
         except Exception as exc:      # reported, never required
             phasecorr = {"error": str(exc)[:300]}
 
+    tiles = None
+    if not args.no_tiles:
+        try:
+            tiles = tiles_sample(fb, lib, dev, args.seed + 43 * rank, cpu_budget_s=0.0 if args.no_cpu else 10.0)
+        except Exception as exc:      # reported, never required
+            tiles = {"error": str(exc)[:300]}
+
+    viewer = None
+    if not args.no_viewer:
+        try:
+            viewer = viewer_slab_sample(fb, lib, dev, args.seed + 59 * rank, cpu_budget_s=0.0 if args.no_cpu else 5.0)
+        except Exception as exc:      # reported, never required
+            viewer = {"error": str(exc)[:300]}
+
     lat = sorted(per_step)
     line = {
         "metric": METRIC, "value": value, "unit": "Mvoxel/s", "n_gpus": world, "steps": args.steps,
@@ -753,6 +1001,8 @@ def main():
         "served": served,
         "batched": batched,
         "phasecorr": phasecorr,
+        "tiles": tiles,
+        "viewer_slab": viewer,
     }
     lib.fy_gpu_dering_destroy(h)
     if rank == 0:

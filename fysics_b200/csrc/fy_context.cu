@@ -206,6 +206,7 @@ int fy_gpu_kernel_timeouts(void) {
 void fy_gpu_release(void) {
     fy::ThreadCtx& c = fy::ctx();
     if (c.st) cudaStreamSynchronize(c.st);
+    fy_tile_release();
     c.vin.release(); c.vout.release(); c.spec.release(); c.spec2.release();
     c.aux.release(); c.aux2.release(); c.small.release();
     c.pin.release(); c.pin2.release();

@@ -148,5 +148,7 @@ cudaError_t fy_launch_radial_tile_eps(const fy_radial_eps* d_fit, const float* b
 // Workspace reservation for a cube shape on the calling thread (fy_api.cu, fy_restore.cu).
 int fy_deconv_reserve(int nz, int ny, int nx);
 int fy_restore_reserve(int nz, int ny, int nx);
+// Free the calling thread's per-tile chain workspaces (fy_tile.cu); part of fy_gpu_release.
+void fy_tile_release();
 int fy_guided_wait_timeouts();
 int fy_noise_wait_timeouts();

@@ -8,10 +8,12 @@
 //   deconvolution   fy_gpu_deconvolve_ex in place: plain auto-reg, or matched (:273-275)
 //   k_tile_unwin    re-window, dec-range rescale, clamp to [0, 1] (:277-288)
 //   guided filter   fy_gpu_guided, r = 2, subsampled coefficients by default (:290-297)
-//   air zero        k_box_line x3 over the 2x-decimated orig (the sliding sums of
+//   air zero        k_box_line_smem x3 over the 2x-decimated orig (the sliding sums of
 //                   guided.c:34-98), k_air_hist, k_air_cut (stream.c:138-168 and
-//                   pipeline.c:330-364), k_air_apply (the texture split, :355-399)
-//   despeckle       union-find over 6-connected material (:223-250, :400-405)
+//                   pipeline.c:330-364), k_air_apply (the texture split, :355-399), which
+//                   also writes the despeckle's x-run labels
+//   despeckle       union-find over 6-connected material (:223-250, :400-405): k_cc_union,
+//                   k_cc_count (roots, sizes, face contact), k_cc_zero
 //   k_tile_quant    recenter (:407-421) and the dithered quantiser (:53-65, :501-506) over
 //                   the inner tile
 //
@@ -24,6 +26,7 @@
 #include "fy_context.h"
 
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 #include <algorithm>
 
@@ -125,8 +128,8 @@ __global__ void __launch_bounds__(256) k_tile_any(const uint8_t* __restrict__ u8
 struct PrepArgs {
     const uint8_t* u8;
     float* orig;
-    float* work;
-    long hz, hy, hx, zc;
+    float* work;              // the deconvolution's input (windowed), or nullptr
+    long hz, hy, hx;
     // rings: rows [s0, s0 + rows) of the [nslab][nr] table, or ring == nullptr
     const float* ring;
     long s0, nslab, slab_z;
@@ -139,29 +142,56 @@ struct PrepArgs {
     float wlo, wspan;
 };
 
-__global__ void __launch_bounds__(kTpb) k_tile_prep(PrepArgs a) {
-    const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= a.hx) return;
-    const long zb = (long)blockIdx.z * a.zc, ze = zb + a.zc < a.hz ? zb + a.zc : a.hz;
-    int ri = -1;
-    if (a.ring) {
-        const double gy = (double)(a.ry0 + y) - a.cy, gx = (double)(a.rx0 + x) - a.cx;
-        const int r = (int)(sqrt(gy * gy + gx * gx) + 0.5);
-        ri = r < a.nr ? r : -1;
-    }
-    const size_t plane = (size_t)a.hy * a.hx;
-    size_t i = (size_t)zb * plane + (size_t)y * a.hx + x;
-    for (long z = zb; z < ze; ++z, i += plane) {
-        float f = __fmul_rn((float)a.u8[i], 1.0f / 255.0f);
-        if (ri >= 0 && f > 0.0f) {
-            long s = (a.rz0 + z) / a.slab_z;
-            s = s < 0 ? 0 : (s >= a.nslab ? a.nslab - 1 : s);
-            const float w = __fmaf_rn(-a.sc, __ldg(a.ring + (size_t)(s - a.s0) * a.nr + ri), f);
-            f = w > 0.0f ? w : 0.0f;
+// Four consecutive voxels per thread (one 4-byte load, 16-byte stores when aligned).
+// Coordinates are derived only when rings or z drift need them.
+__device__ __forceinline__ float prep_one(const PrepArgs& a, unsigned u, size_t i, unsigned plane) {
+    float f = __fmul_rn((float)u, 1.0f / 255.0f);
+    if (a.ring || a.zdrift) {
+        const unsigned ii = (unsigned)i;            // hz*hy*hx < 2^31
+        const unsigned z = ii / plane, rem = ii - z * plane;
+        if (a.ring && f > 0.0f) {
+            const unsigned y = rem / (unsigned)a.hx, x = rem - y * (unsigned)a.hx;
+            const double gy = (double)(a.ry0 + y) - a.cy, gx = (double)(a.rx0 + x) - a.cx;
+            const int r = (int)(sqrt(gy * gy + gx * gx) + 0.5);
+            if (r < a.nr) {
+                long s = (a.rz0 + (long)z) / a.slab_z;
+                s = s < 0 ? 0 : (s >= a.nslab ? a.nslab - 1 : s);
+                const float w = __fmaf_rn(-a.sc, __ldg(a.ring + (size_t)(s - a.s0) * a.nr + r), f);
+                f = w > 0.0f ? w : 0.0f;
+            }
         }
         if (a.zdrift) f = __fmul_rn(f, __ldg(a.zdrift + z));
-        a.orig[i] = f;
-        a.work[i] = a.windowed ? __fmaf_rn(f, a.wspan, a.wlo) : f;
+    }
+    return f;
+}
+
+__global__ void __launch_bounds__(256) k_tile_prep(PrepArgs a) {
+    const size_t n = (size_t)a.hz * a.hy * a.hx;
+    const unsigned plane = (unsigned)(a.hy * a.hx);
+    const bool vec = ((uintptr_t)a.u8 & 3) == 0;
+    for (size_t q = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 4; q < n;
+         q += (size_t)gridDim.x * blockDim.x * 4) {
+        unsigned u[4] = {0, 0, 0, 0};
+        if (vec && q + 4 <= n) {
+            const uchar4 v = *reinterpret_cast<const uchar4*>(a.u8 + q);
+            u[0] = v.x; u[1] = v.y; u[2] = v.z; u[3] = v.w;
+        } else {
+            for (int k = 0; k < 4 && q + k < n; k++) u[k] = a.u8[q + k];
+        }
+        float f[4], w[4];
+        for (int k = 0; k < 4; k++) {
+            f[k] = prep_one(a, u[k], q + k, plane);
+            w[k] = a.windowed ? __fmaf_rn(f[k], a.wspan, a.wlo) : f[k];
+        }
+        if (q + 4 <= n) {                           // orig and work are 256-byte aligned, q % 4 == 0
+            *reinterpret_cast<float4*>(a.orig + q) = make_float4(f[0], f[1], f[2], f[3]);
+            if (a.work) *reinterpret_cast<float4*>(a.work + q) = make_float4(w[0], w[1], w[2], w[3]);
+        } else {
+            for (int k = 0; q + k < n; k++) {
+                a.orig[q + k] = f[k];
+                if (a.work) a.work[q + k] = w[k];
+            }
+        }
     }
 }
 
@@ -204,6 +234,58 @@ __global__ void __launch_bounds__(kTpb) k_box_line(LineArgs a) {
     }
 }
 
+// The same sliding sums with the lines staged through shared memory: a CTA takes kLines
+// consecutive lines, loads them with coalesced requests (along the line when it is
+// contiguous, across lines otherwise), walks its line in shared memory and stores the
+// means back the same way. Shared memory: 2 * L * (kLines + 1) floats.
+constexpr int kLines = 32;               // lines per CTA: ~5000 lines per pass at 144^3 -> 160 CTAs
+constexpr int kLp = kLines + 1;
+__global__ void __launch_bounds__(kLines) k_box_line_smem(LineArgs a, int along) {
+    extern __shared__ float sl[];
+    float* so = sl + (size_t)a.L * kLp;
+    const long lines = a.A * a.B, t0 = (long)blockIdx.x * kLines;
+    const int tid = threadIdx.x;
+    const int nl = (int)(lines - t0 < kLines ? lines - t0 : kLines);
+    if (along) {                        // contiguous lines: the CTA reads each line in turn
+        for (int j = 0; j < nl; ++j) {
+            const long t = t0 + j, ai = t / a.B, bi = t - ai * a.B;
+            const float* in = a.in + ai * a.ia + bi * a.ib;
+            for (int e = tid; e < a.L; e += kLines) sl[e * kLp + j] = in[e * a.il];
+        }
+    } else if (tid < nl) {              // neighbouring lines are neighbouring addresses
+        const long t = t0 + tid, ai = t / a.B, bi = t - ai * a.B;
+        const float* in = a.in + ai * a.ia + bi * a.ib;
+        for (int e = 0; e < a.L; ++e) sl[e * kLp + tid] = in[e * a.il];
+    }
+    __syncthreads();
+    if (tid < nl) {
+        const float* in = sl + tid;
+        float* out = so + tid;
+        const float rin = __frcp_rn((float)(2 * a.r + 1));
+        float s = 0.0f;
+        for (int i = 0; i <= a.r && i < a.L; ++i) s = __fadd_rn(s, in[i * kLp]);
+        for (int i = 0; i < a.L; ++i) {
+            const int lo = i - a.r < 0 ? 0 : i - a.r, hi = i + a.r > a.L - 1 ? a.L - 1 : i + a.r;
+            const int cnt = hi - lo + 1;
+            out[i * kLp] = __fmul_rn(s, cnt == 2 * a.r + 1 ? rin : __frcp_rn((float)cnt));
+            if (i + a.r + 1 < a.L) s = __fadd_rn(s, in[(i + a.r + 1) * kLp]);
+            if (i - a.r >= 0) s = __fsub_rn(s, in[(i - a.r) * kLp]);
+        }
+    }
+    __syncthreads();
+    if (along) {
+        for (int j = 0; j < nl; ++j) {
+            const long t = t0 + j, ai = t / a.B, bi = t - ai * a.B;
+            float* out = a.out + ai * a.oa + bi * a.ob;
+            for (int e = tid; e < a.L; e += kLines) out[e * a.ol] = so[e * kLp + j];
+        }
+    } else if (tid < nl) {
+        const long t = t0 + tid, ai = t / a.B, bi = t - ai * a.B;
+        float* out = a.out + ai * a.oa + bi * a.ob;
+        for (int e = 0; e < a.L; ++e) out[e * a.ol] = so[e * kLp + tid];
+    }
+}
+
 __global__ void __launch_bounds__(256) k_air_hist(const float* __restrict__ sm, size_t n, TileCtl* ctl) {
     __shared__ unsigned h[256];
     h[threadIdx.x] = 0;
@@ -217,25 +299,100 @@ __global__ void __launch_bounds__(256) k_air_hist(const float* __restrict__ sm, 
     if (h[threadIdx.x]) atomicAdd(&ctl->hist[threadIdx.x], h[threadIdx.x]);
 }
 
-// the value cut and its texture split, pipeline.c:330-378
-__global__ void k_air_cut(TileCtl* ctl, int air_cut_u8, int air_cut_band, double air_thresh, double air_cut_aggr) {
-    long hist[256];
-    for (int i = 0; i < 256; i++) hist[i] = ctl->hist[i];
+// The valley (stream.c:138-168) and the value cut with its texture split (pipeline.c:330-378),
+// one CTA of 256 threads, a thread per bin: smoothed counts, their maximum, the local-maximum
+// candidates and the valley's first minimum in parallel; the peak merge, which is sequential
+// by definition, walks the candidate bits on one thread. Same arithmetic as valley_depth_hd.
+__global__ void __launch_bounds__(256) k_air_cut(TileCtl* ctl, int air_cut_u8, int air_cut_band, double air_thresh,
+                                                 double air_cut_aggr) {
+    __shared__ double hf[256];
+    __shared__ double wmax[8];
+    __shared__ unsigned cand[8];
+    __shared__ int s_ab[3];
+    __shared__ double wmin[8];
+    __shared__ int wmini[8];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    long sum = 0;
+    int cnt = 0;
+    for (int j = t - 2; j <= t + 2; j++)
+        if (j >= 0 && j < 256) { sum += ctl->hist[j]; cnt++; }
+    double h = (double)sum / cnt;
+    if (t == 0 || t == 254 || t == 255) h = 0;
+    hf[t] = h;
+    double m = h;
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) wmax[warp] = m;
+    __syncthreads();
+    double mx = wmax[0];
+    for (int k = 1; k < 8; k++) mx = fmax(mx, wmax[k]);
+    const bool c = t >= 3 && t < 253 && hf[t] >= hf[t - 1] && hf[t] >= hf[t + 1] && hf[t] > 0.05 * mx;
+    const unsigned bal = __ballot_sync(0xffffffffu, c);
+    if (lane == 0) cand[warp] = bal;
+    __syncthreads();
+    if (t == 0) {
+        int ok = 0, a = 0, b = 0;
+        if (mx > 0) {
+            int pk[32], np = 0;           // kept peaks are > 10 bins apart: at most 23 in [3, 253)
+            for (int w = 0; w < 8; w++)
+                for (unsigned bits = cand[w]; bits; bits &= bits - 1) {
+                    const int u = w * 32 + __ffs(bits) - 1;
+                    if (np > 0 && u - pk[np - 1] <= 10) {
+                        if (hf[u] > hf[pk[np - 1]]) pk[np - 1] = u;
+                    } else if (np < 32) {
+                        pk[np++] = u;
+                    }
+                }
+            if (np >= 2) {
+                int p1 = pk[0], p2 = pk[1];
+                for (int i = 0; i < np; i++) {
+                    const int u = pk[i];
+                    if (hf[u] > hf[p1]) { p2 = p1; p1 = u; }
+                    else if (hf[u] > hf[p2] && u != p1) p2 = u;
+                }
+                a = p1 < p2 ? p1 : p2;
+                b = p1 < p2 ? p2 : p1;
+                ok = 1;
+            }
+        }
+        s_ab[0] = a; s_ab[1] = b; s_ab[2] = ok;
+    }
+    __syncthreads();
+    const int a = s_ab[0], b = s_ab[1], ok = s_ab[2];
+    // first minimum over [a, b] (strict <, so the lowest bin among equal minima)
+    double vm = (ok && t >= a && t <= b) ? hf[t] : INFINITY;
+    int vi = (ok && t >= a && t <= b) ? t : 1 << 30;
+    for (int o = 16; o; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, vm, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, vi, o);
+        if (ov < vm || (ov == vm && oi < vi)) { vm = ov; vi = oi; }
+    }
+    if (lane == 0) { wmin[warp] = vm; wmini[warp] = vi; }
+    __syncthreads();
+    if (t != 0) return;
     int dark = 0, light = 0, valley = 0;
-    const double d = valley_depth_hd(hist, &dark, &light, &valley);
+    double d = -1;
+    if (ok) {
+        double vmin = wmin[0];
+        int v = wmini[0];
+        for (int k = 1; k < 8; k++)
+            if (wmin[k] < vmin || (wmin[k] == vmin && wmini[k] < v)) { vmin = wmin[k]; v = wmini[k]; }
+        dark = a; light = b; valley = v;
+        const double mn = hf[a] < hf[b] ? hf[a] : hf[b];
+        d = 1.0 - vmin / (mn + 1e-12);
+    }
     const int pf = air_thresh > 0 ? (int)__fma_rn(air_thresh, 255.0, 0.5) : 39;
     int cut;
     if (air_cut_u8 >= 0) {
         const int gg = air_cut_u8, band = air_cut_band;
         if (d >= 0) {
-            double a = air_cut_aggr;
-            a = a < 0 ? 0 : (a > 2 ? 2 : a);
+            double g = air_cut_aggr;
+            g = g < 0 ? 0 : (g > 2 ? 2 : g);
             int local;
             if (valley <= pf) local = pf;
-            else if (a <= 1.0) local = (int)__dadd_rn(__fma_rn(a, (double)(valley - pf), (double)pf), 0.5);
+            else if (g <= 1.0) local = (int)__dadd_rn(__fma_rn(g, (double)(valley - pf), (double)pf), 0.5);
             else
                 local = (int)__dadd_rn(
-                    __fma_rn(__dsub_rn(a, 1.0), (double)(light > valley ? light - valley : 0), (double)valley), 0.5);
+                    __fma_rn(__dsub_rn(g, 1.0), (double)(light > valley ? light - valley : 0), (double)valley), 0.5);
             cut = local < gg - band ? gg - band : (local > gg + band ? gg + band : local);
         } else {
             cut = gg;
@@ -259,12 +416,14 @@ __global__ void k_air_cut(TileCtl* ctl, int air_cut_u8, int air_cut_band, double
 }
 
 struct AirArgs {
-    float* f;
+    float* f;                 // may alias orig: each voxel reads orig and writes f at itself
     const float* orig;
     const float* sm;
     const TileCtl* ctl;
     long nz, ny, nx, lz, ly, lx;
     int lowres;
+    int* lab;                 // despeckle on: x-run labels of the material (f > 0) written here
+    unsigned* info;
 };
 
 __device__ __forceinline__ float blend4(const float* s, size_t r00, size_t r01, size_t r10, size_t r11, long k,
@@ -278,34 +437,50 @@ __device__ __forceinline__ float blend4(const float* s, size_t r00, size_t r01, 
 // the cut chosen by the local texture |orig - smooth| (pipeline.c:355-399)
 __global__ void __launch_bounds__(kTpb) k_air_apply(AirArgs a) {
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= a.nx) return;
+    const int lane = threadIdx.x & 31;
+    const bool in = x < a.nx;
     const float cu = a.ctl->cutf_uni, ct = a.ctl->cutf_tex;
     for (long z = blockIdx.z; z < a.nz; z += gridDim.z) {
         const size_t i = ((size_t)z * a.ny + y) * a.nx + x;
-        float v;
-        if (a.lowres) {
-            long z0 = z >> 1, y0 = y >> 1, x0 = x >> 1;
-            if (z0 > a.lz - 2) z0 = a.lz - 2;
-            if (y0 > a.ly - 2) y0 = a.ly - 2;
-            if (x0 > a.lx - 2) x0 = a.lx - 2;
-            float zf = __fsub_rn(__fmul_rn(0.5f, (float)z), (float)z0);
-            float yf = __fsub_rn(__fmul_rn(0.5f, (float)y), (float)y0);
-            float fx = __fsub_rn(__fmul_rn(0.5f, (float)x), (float)x0);
-            zf = zf > 1.0f ? 1.0f : zf;
-            yf = yf > 1.0f ? 1.0f : yf;
-            fx = fx > 1.0f ? 1.0f : fx;
-            const float w00 = __fmul_rn(1.0f - zf, 1.0f - yf), w01 = __fmul_rn(1.0f - zf, yf);
-            const float w10 = __fmul_rn(zf, 1.0f - yf), w11 = __fmul_rn(zf, yf);
-            const size_t r00 = ((size_t)z0 * a.ly + y0) * a.lx, r01 = r00 + a.lx;
-            const size_t r10 = r00 + (size_t)a.ly * a.lx, r11 = r10 + a.lx;
-            const float a0 = blend4(a.sm, r00, r01, r10, r11, x0, w00, w01, w10, w11);
-            const float a1 = blend4(a.sm, r00, r01, r10, r11, x0 + 1, w00, w01, w10, w11);
-            v = __fmaf_rn(__fsub_rn(a1, a0), fx, a0);
-        } else {
-            v = a.sm[i];
+        float fv = 0.0f;
+        if (in) {
+            float v;
+            if (a.lowres) {
+                long z0 = z >> 1, y0 = y >> 1, x0 = x >> 1;
+                if (z0 > a.lz - 2) z0 = a.lz - 2;
+                if (y0 > a.ly - 2) y0 = a.ly - 2;
+                if (x0 > a.lx - 2) x0 = a.lx - 2;
+                float zf = __fsub_rn(__fmul_rn(0.5f, (float)z), (float)z0);
+                float yf = __fsub_rn(__fmul_rn(0.5f, (float)y), (float)y0);
+                float fx = __fsub_rn(__fmul_rn(0.5f, (float)x), (float)x0);
+                zf = zf > 1.0f ? 1.0f : zf;
+                yf = yf > 1.0f ? 1.0f : yf;
+                fx = fx > 1.0f ? 1.0f : fx;
+                const float w00 = __fmul_rn(1.0f - zf, 1.0f - yf), w01 = __fmul_rn(1.0f - zf, yf);
+                const float w10 = __fmul_rn(zf, 1.0f - yf), w11 = __fmul_rn(zf, yf);
+                const size_t r00 = ((size_t)z0 * a.ly + y0) * a.lx, r01 = r00 + a.lx;
+                const size_t r10 = r00 + (size_t)a.ly * a.lx, r11 = r10 + a.lx;
+                const float a0 = blend4(a.sm, r00, r01, r10, r11, x0, w00, w01, w10, w11);
+                const float a1 = blend4(a.sm, r00, r01, r10, r11, x0 + 1, w00, w01, w10, w11);
+                v = __fmaf_rn(__fsub_rn(a1, a0), fx, a0);
+            } else {
+                v = a.sm[i];
+            }
+            const float o = a.orig[i];
+            const float tex = fabsf(__fsub_rn(o, v));
+            fv = a.f[i];
+            if (v < (tex < 0.03f ? cu : ct)) { fv = 0.0f; a.f[i] = 0.0f; }
         }
-        const float tex = fabsf(__fsub_rn(a.orig[i], v));
-        if (v < (tex < 0.03f ? cu : ct)) a.f[i] = 0.0f;
+        if (a.lab) {               // despeckle on: each material voxel points at its x-run's first voxel
+            const bool mat = in && fv > 0.0f;
+            const unsigned bits = __ballot_sync(0xffffffffu, mat);
+            if (in) {
+                const unsigned gaps = ~bits & ((1u << lane) - 1u);
+                const int start = gaps ? 32 - __clz(gaps) : 0;
+                a.lab[i] = mat ? (int)(i - (size_t)(lane - start)) : -1;
+                if (mat && lane == start) a.info[i] = 0u;   // run heads are the only possible roots
+            }
+        }
     }
 }
 
@@ -356,23 +531,6 @@ struct CcArgs {
     int min_size;
 };
 
-// Labels start as x-runs: each material voxel points at the first voxel of its run within
-// its 32-voxel warp chunk of the row (a forest of depth one); info is cleared.
-__global__ void __launch_bounds__(kTpb) k_cc_init(CcArgs a) {
-    const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    const int lane = threadIdx.x & 31;
-    for (long z = blockIdx.z; z < a.nz; z += gridDim.z) {
-        const size_t i = ((size_t)z * a.ny + y) * a.nx + x;
-        const bool mat = x < a.nx && a.f[i] > 0.0f;
-        const unsigned bits = __ballot_sync(0xffffffffu, mat);
-        if (x >= a.nx) continue;
-        const unsigned gaps = ~bits & ((1u << lane) - 1u);      // non-material lanes below this one
-        const int start = gaps ? 32 - __clz(gaps) : 0;          // first lane of this run in the chunk
-        a.lab[i] = mat ? (int)(i - (size_t)(lane - start)) : -1;
-        a.info[i] = 0u;
-    }
-}
-
 // Join runs: across a chunk boundary in x, and to the -y and -z neighbours where a run
 // overlap starts (if the left neighbours are both material, they already joined the runs).
 __global__ void __launch_bounds__(kTpb) k_cc_union(CcArgs a) {
@@ -391,24 +549,42 @@ __global__ void __launch_bounds__(kTpb) k_cc_union(CcArgs a) {
     }
 }
 
-__global__ void __launch_bounds__(256) k_cc_flatten(CcArgs a, size_t n) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        if (a.lab[i] >= 0) a.lab[i] = uf_root(a.lab, (int)i, a.err);
-}
-
-// Component sizes and face contact, one atomic per distinct root per warp.
+// Roots by read-only walks from the x-run heads (a run's voxels share its head's root;
+// each thread then stores its voxel's root for the zero pass), component sizes and face
+// contact with one atomic per run of equal roots in a warp. A count stops growing once it
+// reaches min_size and a face-touching root takes no count: both leave the zero test
+// (no face contact and fewer than min_size voxels) unchanged.
 __global__ void __launch_bounds__(kTpb) k_cc_count(CcArgs a) {
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     const int lane = threadIdx.x & 31;
+    const bool in = x < a.nx;
     for (long z = blockIdx.z; z < a.nz; z += gridDim.z) {
         const size_t i = ((size_t)z * a.ny + y) * a.nx + x;
-        const int root = x < a.nx ? a.lab[i] : -1;
+        const int l = in ? __ldcg(a.lab + i) : -1;
+        // the voxel's x-run (within its warp chunk) shares one root: the run head walks
+        const unsigned bits = __ballot_sync(0xffffffffu, l >= 0);
+        const unsigned gaps = ~bits & ((1u << lane) - 1u);
+        const int head = gaps ? 32 - __clz(gaps) : 0;
+        int root = (l >= 0 && lane == head) ? uf_root(a.lab, l, a.err) : -1;
+        root = __shfl_sync(0xffffffffu, root, head);
+        if (l < 0) root = -1;
+        if (root >= 0) a.lab[i] = root;
         const bool edge = root >= 0 && (z == 0 || z == a.nz - 1 || y == 0 || y == a.ny - 1 || x == 0 || x == a.nx - 1);
-        const unsigned peers = __match_any_sync(0xffffffffu, root);
-        const unsigned epeers = __ballot_sync(0xffffffffu, edge) & peers;
-        if (root >= 0 && lane == __ffs(peers) - 1) {
-            atomicAdd(&a.info[root], (unsigned)__popc(peers));
-            if (epeers) atomicOr(&a.info[root], kEdge);
+        const int prev = __shfl_up_sync(0xffffffffu, root, 1);
+        const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != root);
+        const unsigned edges = __ballot_sync(0xffffffffu, edge);
+        if (root >= 0 && (lane == 0 || prev != root)) {
+            const unsigned after = heads & ~((2u << lane) - 1u);      // run heads above this lane
+            const int end = after ? __ffs(after) - 1 : 32;
+            const unsigned seg = (end == 32 ? 0xffffffffu : (1u << end) - 1u) & ~((1u << lane) - 1u);
+            // Only "touches a face" and "has at least min_size voxels" decide the zero pass, so
+            // a root already known to be either takes no more atomics (the giant components
+            // would otherwise serialise on one address).
+            const unsigned v = __ldcg(a.info + root);
+            if (!(v & kEdge)) {
+                if (edges & seg) atomicOr(&a.info[root], kEdge);
+                else if ((long)(v & ~kEdge) < a.min_size) atomicAdd(&a.info[root], (unsigned)(end - lane));
+            }
         }
     }
 }
@@ -460,7 +636,7 @@ __global__ void __launch_bounds__(kTpb) k_tile_quant(QuantArgs a) {
 // ---------------------------------------------------------------- host side
 struct TileWs {
     fy::DevBuf u8, orig, work, alt, t1, t2, sm, lab, info, tab, ctl, out;
-    fy::HostBuf pin;
+    fy::HostBuf pin, hin, hout;   // control and tables; host-API staging of the u8 tile in/out
     bool have_state = false;
     long hist[256];
     int cuts[3];
@@ -492,7 +668,14 @@ cudaError_t box_pass(const float* in, float* out, int L, int r, long A, long B, 
                      long ob, long ol, cudaStream_t st) {
     LineArgs a{in, out, L, r, A, B, ia, ib, il, oa, ob, ol};
     const long lines = A * B;
-    k_box_line<<<(unsigned)((lines + kTpb - 1) / kTpb), kTpb, 0, st>>>(a);
+    const size_t smem = (size_t)2 * L * kLp * sizeof(float);
+    if (smem <= 200 * 1024) {
+        cudaError_t e = fy_smem_optin(k_box_line_smem, smem);
+        if (e != cudaSuccess) return e;
+        k_box_line_smem<<<(unsigned)((lines + kLines - 1) / kLines), kLines, smem, st>>>(a, ib != 1 ? 1 : 0);
+    } else {
+        k_box_line<<<(unsigned)((lines + kTpb - 1) / kTpb), kTpb, 0, st>>>(a);
+    }
     return cudaGetLastError();
 }
 
@@ -555,17 +738,22 @@ int tile_chain(const fy_pipeline_cfg* c, const uint8_t* d_u8, long rz0, long ry0
         if (zdrift) d_zd = w.tab.as<float>() + ring_floats;
     }
 
+    // Buffers: orig (the pre-deconvolution copy) always; the working field is orig itself
+    // until a stage writes a new one (deconvolution in place on `work`, guided into `alt`),
+    // since the air cut reads orig and writes f one voxel at a time.
     TRY(w.orig.ensure(hn * sizeof(float)));
-    TRY(w.work.ensure(hn * sizeof(float)));
     float* orig = w.orig.as<float>();
-    float* f = w.work.as<float>();
+    float* f = orig;
+    if (c->do_deconv) {
+        TRY(w.work.ensure(hn * sizeof(float)));
+        f = w.work.as<float>();
+    }
     const bool windowed = c->window_hi > c->window_lo;
     const float wlo = (float)c->window_lo, wspan = (float)(c->window_hi - c->window_lo);
     {
         PrepArgs a{};
-        a.u8 = d_u8; a.orig = orig; a.work = f;
+        a.u8 = d_u8; a.orig = orig; a.work = c->do_deconv ? f : nullptr;
         a.hz = hz; a.hy = hy; a.hx = hx;
-        a.zc = std::max<long>(1, (hz + 31) / 32);
         a.ring = d_ring;
         if (rings) {
             a.s0 = s0; a.nslab = dr->nslab; a.slab_z = dr->slab_z; a.nr = dr->nr; a.cy = dr->cy; a.cx = dr->cx;
@@ -577,8 +765,7 @@ int tile_chain(const fy_pipeline_cfg* c, const uint8_t* d_u8, long rz0, long ry0
         a.zdrift = d_zd;
         a.windowed = c->do_deconv && windowed;
         a.wlo = wlo; a.wspan = wspan;
-        dim3 g((unsigned)((hx + kTpb - 1) / kTpb), (unsigned)hy, (unsigned)((hz + a.zc - 1) / a.zc));
-        k_tile_prep<<<g, kTpb, 0, st>>>(a);
+        k_tile_prep<<<grid1((hn + 3) / 4, 256, cx.sms), 256, 0, st>>>(a);
         TRY(cudaGetLastError());
         launches++;
         fy_prof_mark(st, "tile.prep");
@@ -612,7 +799,6 @@ int tile_chain(const fy_pipeline_cfg* c, const uint8_t* d_u8, long rz0, long ry0
         TRY(w.alt.ensure(hn * sizeof(float)));
         float* g = w.alt.as<float>();
         if ((rc = fy_gpu_guided(f, g, (int)hz, (int)hy, (int)hx, 2, eps, gs, st))) return rc;
-        std::swap(w.work, w.alt);
         f = g;
         fy_prof_mark(st, "tile.guided");
     }
@@ -637,29 +823,29 @@ int tile_chain(const fy_pipeline_cfg* c, const uint8_t* d_u8, long rz0, long ry0
         fy_prof_mark(st, "tile.scratch_box");
         k_air_hist<<<grid1(m, 256, cx.sms), 256, 0, st>>>(sm, m, ctl);
         TRY(cudaGetLastError());
-        k_air_cut<<<1, 1, 0, st>>>(ctl, c->air_cut_u8, c->air_cut_band, c->air_thresh, c->air_cut_aggr);
+        k_air_cut<<<1, 256, 0, st>>>(ctl, c->air_cut_u8, c->air_cut_band, c->air_thresh, c->air_cut_aggr);
         TRY(cudaGetLastError());
         fy_prof_mark(st, "tile.air_cut");
-        AirArgs aa{f, orig, sm, ctl, hz, hy, hx, lz, ly, lx, lowres ? 1 : 0};
+        const bool cc = c->air_min_component > 0;
+        if (cc) {
+            TRY(w.lab.ensure(hn * sizeof(int)));
+            TRY(w.info.ensure(hn * sizeof(unsigned)));
+        }
+        AirArgs aa{f, orig, sm, ctl, hz, hy, hx, lz, ly, lx, lowres ? 1 : 0, cc ? w.lab.as<int>() : nullptr,
+                   cc ? w.info.as<unsigned>() : nullptr};
         k_air_apply<<<grid_rows(hx, hy, hz), kTpb, 0, st>>>(aa);
         TRY(cudaGetLastError());
         launches += 6;
         fy_prof_mark(st, "tile.air_apply");
-        if (c->air_min_component > 0) {
-            TRY(w.lab.ensure(hn * sizeof(int)));
-            TRY(w.info.ensure(hn * sizeof(unsigned)));
+        if (cc) {
             CcArgs ca{f, w.lab.as<int>(), w.info.as<unsigned>(), &ctl->err, hz, hy, hx, c->air_min_component};
-            k_cc_init<<<grid_rows(hx, hy, hz), kTpb, 0, st>>>(ca);
-            fy_prof_mark(st, "tile.cc_init");
             k_cc_union<<<grid_rows(hx, hy, hz), kTpb, 0, st>>>(ca);
             fy_prof_mark(st, "tile.cc_union");
-            k_cc_flatten<<<grid1(hn, 256, cx.sms), 256, 0, st>>>(ca, hn);
-            fy_prof_mark(st, "tile.cc_flatten");
             k_cc_count<<<grid_rows(hx, hy, hz), kTpb, 0, st>>>(ca);
             fy_prof_mark(st, "tile.cc_count");
             k_cc_zero<<<grid1(hn, 256, cx.sms), 256, 0, st>>>(ca, hn);
             TRY(cudaGetLastError());
-            launches += 5;
+            launches += 3;
             fy_prof_mark(st, "tile.cc_zero");
         }
     }
@@ -747,16 +933,41 @@ extern "C" int fy_process_buffer(const fy_pipeline_cfg* cfg, const unsigned char
     cudaError_t e;
     if ((e = w.u8.ensure(hn)) != cudaSuccess || (e = w.out.ensure(tn ? tn : 1)) != cudaSuccess)
         return fail_cuda(e, what);
-    if ((e = cudaMemcpyAsync(w.u8.p, u8buf, hn, cudaMemcpyHostToDevice, st)) != cudaSuccess) return fail_cuda(e, what);
+    // Pageable host buffers go through this thread's pinned staging, so that the copies are
+    // plain DMA and the threads of a worker pool do not serialise on the driver's staging.
+    const bool pin_in = fy::is_pinned(u8buf), pin_out = fy::is_pinned(out);
+    const void* src = u8buf;
+    if (!pin_in) {
+        if ((e = w.hin.ensure(hn)) != cudaSuccess) return fail_cuda(e, what);
+        memcpy(w.hin.p, u8buf, hn);
+        src = w.hin.p;
+    }
+    if ((e = cudaMemcpyAsync(w.u8.p, src, hn, cudaMemcpyHostToDevice, st)) != cudaSuccess) return fail_cuda(e, what);
     rc = tile_chain(cfg, w.u8.as<uint8_t>(), rz0, ry0, rx0, hz, hy, hx, z0, y0, x0, tz, ty, tx, vol_y, vol_x,
                     w.out.as<uint8_t>(), all_air, st, what);
     if (rc) return rc;
     if (tn) {
-        if ((e = cudaMemcpyAsync(out, w.out.p, tn, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return fail_cuda(e, what);
+        void* dst = out;
+        if (!pin_out) {
+            if ((e = w.hout.ensure(tn)) != cudaSuccess) return fail_cuda(e, what);
+            dst = w.hout.p;
+        }
+        if ((e = cudaMemcpyAsync(dst, w.out.p, tn, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return fail_cuda(e, what);
         if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, what);
+        if (!pin_out) memcpy(out, w.hout.p, tn);
     }
     fy::ws_release(st);
     return FY_OK;
+}
+
+void fy_tile_release() {
+    TileWs& w = tws;
+    for (fy::DevBuf* b : {&w.u8, &w.orig, &w.work, &w.alt, &w.t1, &w.t2, &w.sm, &w.lab, &w.info, &w.tab, &w.ctl, &w.out})
+        b->release();
+    w.pin.release();
+    w.hin.release();
+    w.hout.release();
+    w.have_state = false;
 }
 
 extern "C" int fy_process_buffer_air_state(long hist[256], int cuts[3]) {

@@ -106,3 +106,34 @@ CONFIG1 = dict(shape=(128, 128, 128), delta_beta=500.0, energy_kev=110.0, distan
                unsharp_sigma=0.8, unsharp_coeff=0.5, g=0.002, b=1e-4)
 CONFIG2 = dict(shape=(512, 512, 512), delta_beta=500.0, energy_kev=110.0, distance_mm=1200.0, pixel_um=2.4,
                unsharp_sigma=0.8, unsharp_coeff=0.5, g=0.002, b=1e-4, sigma_ratio=1.17, rings=40)
+
+
+def scroll_volume(shape, seed=0, specks_per_mvox=400, masked=True):
+    """u8 volume for the per-tile export chain: noisy air (u8 ~ 22) around a cylindrical
+    body of spiral papyrus wraps (sheets ~ 150, gaps ~ 70, thickness ~3 voxels), small
+    bright specks in the air (1-27 voxels; the islands the despeckle removes) and an
+    exactly-zero masked slab (the first tenth of y), so that the air-cut histogram has two
+    modes and a valley. Generated plane by plane (numpy, seeded)."""
+    nz, ny, nx = shape
+    rng = np.random.default_rng(seed)
+    cy, cx = (ny - 1) / 2 + rng.uniform(-3, 3), (nx - 1) / 2 + rng.uniform(-3, 3)
+    y, x = np.mgrid[0:ny, 0:nx]
+    r = np.hypot(y - cy, x - cx)
+    turn = r / 4.5 + np.arctan2(y - cy, x - cx) / (2 * np.pi)
+    body = r < 0.42 * min(ny, nx)
+    out = np.empty(shape, np.uint8)
+    for z in range(nz):
+        sheet = np.cos(2 * np.pi * (turn + 0.15 * np.sin(z / 11.0))) > 0.2
+        air = rng.normal(22, 6, (ny, nx))
+        mat = np.where(sheet, rng.normal(150, 12, (ny, nx)), rng.normal(70, 10, (ny, nx)))
+        out[z] = np.clip(np.rint(np.where(body, mat, air)), 0, 255).astype(np.uint8)
+    for _ in range(int(specks_per_mvox * nz * ny * nx / 1e6)):
+        c = rng.integers([0, 0, 0], [nz, ny, nx])
+        if body[c[1], c[2]]:
+            continue
+        e = rng.integers(0, 3, 3)
+        out[c[0]:c[0] + e[0] + 1, c[1]:c[1] + e[1] + 1, c[2]:c[2] + e[2] + 1] = np.uint8(
+            np.clip(np.rint(rng.normal(150, 10)), 0, 255))
+    if masked:
+        out[:, : max(1, ny // 10), :] = 0
+    return out

@@ -1,9 +1,9 @@
 """Seeded haloed tiles and settings for the per-tile chain (fy_process_buffer).
 
-A synthetic scroll volume: noisy air (u8 ~ 22) around a cylindrical body of papyrus sheets
-(u8 ~ 90-170), small bright specks in the air (the islands the connected-component
-despeckle removes) and an exactly-zero masked slab, so the air-cut histogram has two
-modes and a valley, as on the volumes the export tool processes.
+The volumes are fysics_b200.phantom.scroll_volume: noisy air around a cylindrical body of
+papyrus wraps, bright specks in the air (the islands the connected-component despeckle
+removes) and an exactly-zero masked slab, so the air-cut histogram has two modes and a
+valley, as on the volumes the export tool processes.
 """
 from __future__ import annotations
 
@@ -11,29 +11,7 @@ import ctypes as C
 
 import numpy as np
 
-
-def scroll_volume(shape, seed=0, specks=300, masked=True):
-    nz, ny, nx = shape
-    rng = np.random.default_rng(seed)
-    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
-    cy, cx = (ny - 1) / 2 + rng.uniform(-3, 3), (nx - 1) / 2 + rng.uniform(-3, 3)
-    r = np.hypot(y - cy, x - cx)
-    body = r < 0.42 * min(ny, nx)
-    # sheets: a spiral-like wrap, thickness ~3 voxels
-    phase = r / 4.5 + np.arctan2(y - cy, x - cx) / (2 * np.pi) + 0.15 * np.sin(z / 11.0)
-    sheet = np.cos(2 * np.pi * phase) > 0.2
-    v = rng.normal(22, 6, shape)
-    v = np.where(body, np.where(sheet, rng.normal(150, 12, shape), rng.normal(70, 10, shape)), v)
-    for _ in range(specks):                          # islands of 1..~30 voxels in the air
-        c = rng.integers([0, 0, 0], [nz, ny, nx])
-        if body[tuple(c)]:
-            continue
-        e = rng.integers(0, 3, 3)
-        v[c[0]:c[0] + e[0] + 1, c[1]:c[1] + e[1] + 1, c[2]:c[2] + e[2] + 1] = rng.normal(150, 10)
-    u8 = np.clip(np.rint(v), 0, 255).astype(np.uint8)
-    if masked:
-        u8[:, : max(1, ny // 10), :] = 0                # a masked slab (exact zeros)
-    return u8
+from fysics_b200.phantom import scroll_volume  # noqa: F401  (re-exported for the tests)
 
 
 def halo_box(vol_shape, tile0, tsize, halo):

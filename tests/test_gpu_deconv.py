@@ -142,3 +142,22 @@ def test_oversize_axis_rejected(gpu):
     dummy = np.zeros(8, np.float32)
     rc = lib.fy_deconvolve(dummy.ctypes.data, dummy.ctypes.data, 1, 1, 5000, C.byref(gpu.physics()), 0.015)
     assert rc == gpu.FY_EUNSUPPORTED
+
+
+def test_viewer_slab(gpu):
+    """The viewer path (README.md:109-118, :190): fy_kernel_halo, then fy_deconvolve on an
+    8x512x512 slab -- a thin z axis (pz = 8) under full 512^2 planes."""
+    ph = gpu.physics(delta_beta=1000.0, energy_kev=78.0, distance_mm=220.0, pixel_um=2.4,
+                     unsharp_sigma=1.2, unsharp_coeff=4.0)
+    r = rphys(ph)
+    halo = gpu.kernel_halo(ph)
+    if oracle.have_ref():
+        assert halo == oracle.ref().fy_kernel_halo(C.byref(r))
+    rng = np.random.default_rng(190)
+    slab = rng.uniform(0, 1, (8, 512, 512)).astype(np.float32)
+    got = gpu.deconvolve(slab, ph, -1.0)
+    o64 = oracle.o64_deconvolve(slab, r, -1.0, kind=0)
+    assert np.abs(got - o64).max() < TOL
+    if oracle.have_ref():
+        ref = oracle.ref_deconvolve(slab, r, -1.0)
+        assert np.abs(got - ref).max() < TOL
