@@ -239,23 +239,28 @@ __global__ void __launch_bounds__(kTpb) k_box_line(LineArgs a) {
 // contiguous, across lines otherwise), walks its line in shared memory and stores the
 // means back the same way. Shared memory: 2 * L * (kLines + 1) floats.
 constexpr int kLines = 32;               // lines per CTA: ~5000 lines per pass at 144^3 -> 160 CTAs
+constexpr int kLineThreads = 128;        // the load and store phases use four warps
 constexpr int kLp = kLines + 1;
-__global__ void __launch_bounds__(kLines) k_box_line_smem(LineArgs a, int along) {
+__global__ void __launch_bounds__(kLineThreads) k_box_line_smem(LineArgs a, int along) {
     extern __shared__ float sl[];
     float* so = sl + (size_t)a.L * kLp;
+    __shared__ long ibase[kLines], obase[kLines];
     const long lines = a.A * a.B, t0 = (long)blockIdx.x * kLines;
     const int tid = threadIdx.x;
     const int nl = (int)(lines - t0 < kLines ? lines - t0 : kLines);
-    if (along) {                        // contiguous lines: the CTA reads each line in turn
-        for (int j = 0; j < nl; ++j) {
-            const long t = t0 + j, ai = t / a.B, bi = t - ai * a.B;
-            const float* in = a.in + ai * a.ia + bi * a.ib;
-            for (int e = tid; e < a.L; e += kLines) sl[e * kLp + j] = in[e * a.il];
-        }
-    } else if (tid < nl) {              // neighbouring lines are neighbouring addresses
+    if (tid < nl) {
         const long t = t0 + tid, ai = t / a.B, bi = t - ai * a.B;
-        const float* in = a.in + ai * a.ia + bi * a.ib;
-        for (int e = 0; e < a.L; ++e) sl[e * kLp + tid] = in[e * a.il];
+        ibase[tid] = ai * a.ia + bi * a.ib;
+        obase[tid] = ai * a.oa + bi * a.ob;
+    }
+    __syncthreads();
+    // contiguous lines: consecutive threads walk along a line (k = j*L + e); otherwise they
+    // walk across lines (k = e*kLines + j), skipping the missing lines of the last CTA
+    const unsigned L = (unsigned)a.L, total = along ? (unsigned)nl * L : (unsigned)kLines * L;
+#pragma unroll 4
+    for (unsigned k = tid; k < total; k += kLineThreads) {
+        const unsigned j = along ? k / L : k % kLines, e = along ? k - (k / L) * L : k / kLines;
+        if ((int)j < nl) sl[e * kLp + j] = a.in[ibase[j] + (long)e * a.il];
     }
     __syncthreads();
     if (tid < nl) {
@@ -273,16 +278,10 @@ __global__ void __launch_bounds__(kLines) k_box_line_smem(LineArgs a, int along)
         }
     }
     __syncthreads();
-    if (along) {
-        for (int j = 0; j < nl; ++j) {
-            const long t = t0 + j, ai = t / a.B, bi = t - ai * a.B;
-            float* out = a.out + ai * a.oa + bi * a.ob;
-            for (int e = tid; e < a.L; e += kLines) out[e * a.ol] = so[e * kLp + j];
-        }
-    } else if (tid < nl) {
-        const long t = t0 + tid, ai = t / a.B, bi = t - ai * a.B;
-        float* out = a.out + ai * a.oa + bi * a.ob;
-        for (int e = 0; e < a.L; ++e) out[e * a.ol] = so[e * kLp + tid];
+#pragma unroll 4
+    for (unsigned k = tid; k < total; k += kLineThreads) {
+        const unsigned j = along ? k / L : k % kLines, e = along ? k - (k / L) * L : k / kLines;
+        if ((int)j < nl) a.out[obase[j] + (long)e * a.ol] = so[e * kLp + j];
     }
 }
 
@@ -435,7 +434,7 @@ __device__ __forceinline__ float blend4(const float* s, size_t r00, size_t r01, 
 
 // zero f where the scratch smooth (trilinear from the decimated grid) is below the cut,
 // the cut chosen by the local texture |orig - smooth| (pipeline.c:355-399)
-__global__ void __launch_bounds__(kTpb) k_air_apply(AirArgs a) {
+__global__ void __launch_bounds__(1024) k_air_apply(AirArgs a) {
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     const int lane = threadIdx.x & 31;
     const bool in = x < a.nx;
@@ -533,7 +532,7 @@ struct CcArgs {
 
 // Join runs: across a chunk boundary in x, and to the -y and -z neighbours where a run
 // overlap starts (if the left neighbours are both material, they already joined the runs).
-__global__ void __launch_bounds__(kTpb) k_cc_union(CcArgs a) {
+__global__ void __launch_bounds__(1024) k_cc_union(CcArgs a) {
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= a.nx) return;
     const long plane = a.ny * a.nx;
@@ -554,7 +553,7 @@ __global__ void __launch_bounds__(kTpb) k_cc_union(CcArgs a) {
 // contact with one atomic per run of equal roots in a warp. A count stops growing once it
 // reaches min_size and a face-touching root takes no count: both leave the zero test
 // (no face contact and fewer than min_size voxels) unchanged.
-__global__ void __launch_bounds__(kTpb) k_cc_count(CcArgs a) {
+__global__ void __launch_bounds__(1024) k_cc_count(CcArgs a) {
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     const int lane = threadIdx.x & 31;
     const bool in = x < a.nx;
@@ -610,7 +609,7 @@ struct QuantArgs {
     float midf, k;
 };
 
-__global__ void __launch_bounds__(kTpb) k_tile_quant(QuantArgs a) {
+__global__ void __launch_bounds__(1024) k_tile_quant(QuantArgs a) {
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= a.tx) return;
     for (long z = blockIdx.z; z < a.tz; z += gridDim.z) {
@@ -648,8 +647,12 @@ unsigned grid1(size_t n, int tpb, int sms) {
     return (unsigned)std::max<size_t>(1, std::min(g, cap));
 }
 
+// Row kernels: a CTA spans a row (x) in whole warps, up to 1024 threads; grid (x, y, z).
+// Warp lanes stay aligned with x % 32, which the run labels rely on.
+int row_threads(long nx) { return (int)std::min<long>(1024, (nx + 31) / 32 * 32); }
 dim3 grid_rows(long nx, long ny, long nz) {
-    return dim3((unsigned)((nx + kTpb - 1) / kTpb), (unsigned)ny, (unsigned)std::min<long>(nz, 65535));
+    const long t = row_threads(nx);
+    return dim3((unsigned)((nx + t - 1) / t), (unsigned)ny, (unsigned)std::min<long>(nz, 65535));
 }
 
 // eps_for_tile, pipeline.c:447-456
@@ -672,7 +675,7 @@ cudaError_t box_pass(const float* in, float* out, int L, int r, long A, long B, 
     if (smem <= 200 * 1024) {
         cudaError_t e = fy_smem_optin(k_box_line_smem, smem);
         if (e != cudaSuccess) return e;
-        k_box_line_smem<<<(unsigned)((lines + kLines - 1) / kLines), kLines, smem, st>>>(a, ib != 1 ? 1 : 0);
+        k_box_line_smem<<<(unsigned)((lines + kLines - 1) / kLines), kLineThreads, smem, st>>>(a, ib != 1 ? 1 : 0);
     } else {
         k_box_line<<<(unsigned)((lines + kTpb - 1) / kTpb), kTpb, 0, st>>>(a);
     }
@@ -833,15 +836,15 @@ int tile_chain(const fy_pipeline_cfg* c, const uint8_t* d_u8, long rz0, long ry0
         }
         AirArgs aa{f, orig, sm, ctl, hz, hy, hx, lz, ly, lx, lowres ? 1 : 0, cc ? w.lab.as<int>() : nullptr,
                    cc ? w.info.as<unsigned>() : nullptr};
-        k_air_apply<<<grid_rows(hx, hy, hz), kTpb, 0, st>>>(aa);
+        k_air_apply<<<grid_rows(hx, hy, hz), row_threads(hx), 0, st>>>(aa);
         TRY(cudaGetLastError());
         launches += 6;
         fy_prof_mark(st, "tile.air_apply");
         if (cc) {
             CcArgs ca{f, w.lab.as<int>(), w.info.as<unsigned>(), &ctl->err, hz, hy, hx, c->air_min_component};
-            k_cc_union<<<grid_rows(hx, hy, hz), kTpb, 0, st>>>(ca);
+            k_cc_union<<<grid_rows(hx, hy, hz), row_threads(hx), 0, st>>>(ca);
             fy_prof_mark(st, "tile.cc_union");
-            k_cc_count<<<grid_rows(hx, hy, hz), kTpb, 0, st>>>(ca);
+            k_cc_count<<<grid_rows(hx, hy, hz), row_threads(hx), 0, st>>>(ca);
             fy_prof_mark(st, "tile.cc_count");
             k_cc_zero<<<grid1(hn, 256, cx.sms), 256, 0, st>>>(ca, hn);
             TRY(cudaGetLastError());
@@ -861,7 +864,7 @@ int tile_chain(const fy_pipeline_cfg* c, const uint8_t* d_u8, long rz0, long ry0
         q.midf = 0.5f * (float)(c->norm_lo + c->norm_hi) * (1.0f / 255.0f);
         q.k = q.norm ? (2.0f * 0.375f) * 255.0f / (float)(c->norm_hi - c->norm_lo) : 0.0f;
         if (tn) {
-            k_tile_quant<<<grid_rows(tx, ty, tz), kTpb, 0, st>>>(q);
+            k_tile_quant<<<grid_rows(tx, ty, tz), row_threads(tx), 0, st>>>(q);
             TRY(cudaGetLastError());
             launches++;
         }
