@@ -138,3 +138,14 @@ def test_export_tile_size(gpu):
     assert rc == 0, gpu.load().fy_gpu_last_error()
     o, _ = oracle.ot_process_buffer(d, buf, org, inner, (160, 160))
     assert np.array_equal(g, o), np.count_nonzero(g != o)
+
+
+def test_wide_thin_buffer(gpu):
+    """A thin buffer with wide planes: rows of 212 voxels end in a partial warp."""
+    v = scroll_volume((24, 210, 212), seed=33)
+    d = oracle.pipeline_defaults(air_min_component=40, have_norm=1, norm_lo=40, norm_hi=200)
+    inner = (4, 4, 4, 16, 202, 204)
+    rc, g, _ = gpu_process_buffer(gpu, d, v, (0, 0, 0), inner, (210, 212))
+    assert rc == 0, gpu.load().fy_gpu_last_error()
+    o, _ = oracle.ot_process_buffer(d, v, (0, 0, 0), inner, (210, 212))
+    assert np.array_equal(g, o), np.count_nonzero(g != o)
