@@ -13,7 +13,8 @@
 //                   pipeline.c:330-364), k_air_apply (the texture split, :355-399), which
 //                   also writes the despeckle's x-run labels
 //   despeckle       union-find over 6-connected material (:223-250, :400-405): k_cc_union,
-//                   k_cc_count (roots, sizes, face contact), k_cc_zero
+//                   k_cc_count (roots, sizes, face contact); the zeroing of small interior
+//                   components is applied by the quantiser
 //   k_tile_quant    recenter (:407-421) and the dithered quantiser (:53-65, :501-506) over
 //                   the inner tile
 //
@@ -588,15 +589,6 @@ __global__ void __launch_bounds__(1024) k_cc_count(CcArgs a) {
     }
 }
 
-__global__ void __launch_bounds__(256) k_cc_zero(CcArgs a, size_t n) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int root = a.lab[i];
-        if (root < 0) continue;
-        const unsigned v = a.info[root];
-        if (!(v & kEdge) && (long)(v & ~kEdge) < a.min_size) a.f[i] = 0.0f;
-    }
-}
-
 // ---------------------------------------------------------------- recenter + quantise
 struct QuantArgs {
     const float* f;
@@ -607,13 +599,24 @@ struct QuantArgs {
     long gz0, gy0, gx0;       // inner tile origin in the volume
     int no_dither, norm;
     float midf, k;
+    const int* lab;           // despeckle on: voxel -> component root (k_cc_count), else nullptr
+    const unsigned* info;
+    int min_size;
 };
 
 __global__ void __launch_bounds__(1024) k_tile_quant(QuantArgs a) {
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= a.tx) return;
     for (long z = blockIdx.z; z < a.tz; z += gridDim.z) {
-        float v = a.f[((size_t)(a.iz0 + z) * a.hy + (a.iy0 + y)) * a.hx + (a.ix0 + x)];
+        const size_t j = ((size_t)(a.iz0 + z) * a.hy + (a.iy0 + y)) * a.hx + (a.ix0 + x);
+        float v = a.f[j];
+        if (a.lab) {                        // the despeckle's zeroing, for the voxels kept
+            const int root = a.lab[j];
+            if (root >= 0) {
+                const unsigned c = a.info[root];
+                if (!(c & kEdge) && (long)(c & ~kEdge) < a.min_size) v = 0.0f;
+            }
+        }
         if (a.norm) {
             if (v <= 0.0f) {
                 v = 0.0f;
@@ -845,11 +848,11 @@ int tile_chain(const fy_pipeline_cfg* c, const uint8_t* d_u8, long rz0, long ry0
             k_cc_union<<<grid_rows(hx, hy, hz), row_threads(hx), 0, st>>>(ca);
             fy_prof_mark(st, "tile.cc_union");
             k_cc_count<<<grid_rows(hx, hy, hz), row_threads(hx), 0, st>>>(ca);
-            fy_prof_mark(st, "tile.cc_count");
-            k_cc_zero<<<grid1(hn, 256, cx.sms), 256, 0, st>>>(ca, hn);
             TRY(cudaGetLastError());
-            launches += 3;
-            fy_prof_mark(st, "tile.cc_zero");
+            launches += 2;
+            fy_prof_mark(st, "tile.cc_count");
+            // the zeroing of small interior components happens in the quantiser, which
+            // reads the inner tile only
         }
     }
 
@@ -863,6 +866,10 @@ int tile_chain(const fy_pipeline_cfg* c, const uint8_t* d_u8, long rz0, long ry0
         q.norm = c->have_norm && c->norm_hi > c->norm_lo;
         q.midf = 0.5f * (float)(c->norm_lo + c->norm_hi) * (1.0f / 255.0f);
         q.k = q.norm ? (2.0f * 0.375f) * 255.0f / (float)(c->norm_hi - c->norm_lo) : 0.0f;
+        const bool cc = c->do_air_zero && c->air_min_component > 0;
+        q.lab = cc ? w.lab.as<int>() : nullptr;
+        q.info = cc ? w.info.as<unsigned>() : nullptr;
+        q.min_size = c->air_min_component;
         if (tn) {
             k_tile_quant<<<grid_rows(tx, ty, tz), row_threads(tx), 0, st>>>(q);
             TRY(cudaGetLastError());
