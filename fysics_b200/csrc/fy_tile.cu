@@ -415,6 +415,28 @@ __global__ void __launch_bounds__(256) k_air_cut(TileCtl* ctl, int air_cut_u8, i
     ctl->cutf_tex = __fmul_rn((float)ct, 1.0f / 255.0f);
 }
 
+// The x of the first voxel of this voxel's material run within the CTA's row segment
+// (threads = consecutive x, whole warps): the warp's own ballot, then the earlier warps'
+// ballots in shared memory. Every thread of the CTA must call it (two barriers).
+__device__ __forceinline__ int run_head(bool mat, unsigned* wbits) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned bits = __ballot_sync(0xffffffffu, mat);
+    if (lane == 0) wbits[warp] = bits;
+    __syncthreads();
+    int head = 0;
+    const unsigned gaps = ~bits & ((1u << lane) - 1u);
+    if (gaps) {
+        head = warp * 32 + 32 - __clz(gaps);
+    } else {
+        for (int w = warp - 1; w >= 0; --w) {
+            const unsigned g = ~wbits[w];
+            if (g) { head = w * 32 + 32 - __clz(g); break; }
+        }
+    }
+    __syncthreads();                         // wbits is rewritten by the next row
+    return head;
+}
+
 struct AirArgs {
     float* f;                 // may alias orig: each voxel reads orig and writes f at itself
     const float* orig;
@@ -436,8 +458,8 @@ __device__ __forceinline__ float blend4(const float* s, size_t r00, size_t r01, 
 // zero f where the scratch smooth (trilinear from the decimated grid) is below the cut,
 // the cut chosen by the local texture |orig - smooth| (pipeline.c:355-399)
 __global__ void __launch_bounds__(1024) k_air_apply(AirArgs a) {
+    __shared__ unsigned wbits[32];
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    const int lane = threadIdx.x & 31;
     const bool in = x < a.nx;
     const float cu = a.ctl->cutf_uni, ct = a.ctl->cutf_tex;
     for (long z = blockIdx.z; z < a.nz; z += gridDim.z) {
@@ -473,12 +495,11 @@ __global__ void __launch_bounds__(1024) k_air_apply(AirArgs a) {
         }
         if (a.lab) {               // despeckle on: each material voxel points at its x-run's first voxel
             const bool mat = in && fv > 0.0f;
-            const unsigned bits = __ballot_sync(0xffffffffu, mat);
+            const int head = run_head(mat, wbits);
             if (in) {
-                const unsigned gaps = ~bits & ((1u << lane) - 1u);
-                const int start = gaps ? 32 - __clz(gaps) : 0;
-                a.lab[i] = mat ? (int)(i - (size_t)(lane - start)) : -1;
-                if (mat && lane == start) a.info[i] = 0u;   // run heads are the only possible roots
+                const int t = (int)threadIdx.x;
+                a.lab[i] = mat ? (int)(i - (size_t)(t - head)) : -1;
+                if (mat && t == head) a.info[i] = 0u;       // run heads are the only possible roots
             }
         }
     }
@@ -531,8 +552,9 @@ struct CcArgs {
     int min_size;
 };
 
-// Join runs: across a chunk boundary in x, and to the -y and -z neighbours where a run
-// overlap starts (if the left neighbours are both material, they already joined the runs).
+// Join runs: across a row-segment (CTA) boundary in x, and to the -y and -z neighbours where
+// a run overlap starts (if the left neighbours are both material, they already joined the
+// runs). Launched with the air pass's CTA width, so the segments are the same.
 __global__ void __launch_bounds__(1024) k_cc_union(CcArgs a) {
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= a.nx) return;
@@ -541,7 +563,7 @@ __global__ void __launch_bounds__(1024) k_cc_union(CcArgs a) {
         const int i = (int)(((size_t)z * a.ny + y) * a.nx + x);
         if (a.lab[i] < 0) continue;
         const bool left = x > 0 && a.lab[i - 1] >= 0;
-        if (left && (x & 31) == 0) uf_union(a.lab, i, i - 1, a.err);
+        if (left && x % blockDim.x == 0) uf_union(a.lab, i, i - 1, a.err);   // across row segments
         if (y > 0 && a.lab[i - a.nx] >= 0 && !(left && a.lab[i - 1 - a.nx] >= 0))
             uf_union(a.lab, i, i - (int)a.nx, a.err);
         if (z > 0 && a.lab[i - plane] >= 0 && !(left && a.lab[i - 1 - plane] >= 0))
@@ -555,19 +577,21 @@ __global__ void __launch_bounds__(1024) k_cc_union(CcArgs a) {
 // reaches min_size and a face-touching root takes no count: both leave the zero test
 // (no face contact and fewer than min_size voxels) unchanged.
 __global__ void __launch_bounds__(1024) k_cc_count(CcArgs a) {
+    __shared__ unsigned wbits[32];
+    __shared__ int sroot[1024];
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     const int lane = threadIdx.x & 31;
     const bool in = x < a.nx;
     for (long z = blockIdx.z; z < a.nz; z += gridDim.z) {
         const size_t i = ((size_t)z * a.ny + y) * a.nx + x;
         const int l = in ? __ldcg(a.lab + i) : -1;
-        // the voxel's x-run (within its warp chunk) shares one root: the run head walks
-        const unsigned bits = __ballot_sync(0xffffffffu, l >= 0);
-        const unsigned gaps = ~bits & ((1u << lane) - 1u);
-        const int head = gaps ? 32 - __clz(gaps) : 0;
-        int root = (l >= 0 && lane == head) ? uf_root(a.lab, l, a.err) : -1;
-        root = __shfl_sync(0xffffffffu, root, head);
-        if (l < 0) root = -1;
+        // the voxel's x-run (within the CTA's row segment) shares one root: the head walks
+        const int head = run_head(l >= 0, wbits);
+        const int t = (int)threadIdx.x;
+        if (l >= 0 && t == head) sroot[t] = uf_root(a.lab, l, a.err);
+        __syncthreads();
+        const int root = l >= 0 ? sroot[head] : -1;
+        __syncthreads();                     // sroot is rewritten by the next row
         if (root >= 0) a.lab[i] = root;
         const bool edge = root >= 0 && (z == 0 || z == a.nz - 1 || y == 0 || y == a.ny - 1 || x == 0 || x == a.nx - 1);
         const int prev = __shfl_up_sync(0xffffffffu, root, 1);
