@@ -9,7 +9,7 @@
 //   k_tile_unwin    re-window, dec-range rescale, clamp to [0, 1] (:277-288)
 //   guided filter   fy_gpu_guided, r = 2, subsampled coefficients by default (:290-297)
 //   air zero        k_box_line_smem x3 over the 2x-decimated orig (the sliding sums of
-//                   guided.c:34-98), k_air_hist, k_air_cut (stream.c:138-168 and
+//                   guided.c:34-98; the last pass also bins the means), k_air_cut (stream.c:138-168 and
 //                   pipeline.c:330-364), k_air_apply (the texture split, :355-399), which
 //                   also writes the despeckle's x-run labels
 //   despeckle       union-find over 6-connected material (:223-250, :400-405): k_cc_union,
@@ -217,6 +217,7 @@ struct LineArgs {
     long A, B;                // lines = A x B
     long ia, ib, il;          // input strides: outer, inner, along the line
     long oa, ob, ol;
+    unsigned* hist;           // staged kernel only: histogram of the means (the air cut's bins)
 };
 
 __global__ void __launch_bounds__(kTpb) k_box_line(LineArgs a) {
@@ -246,6 +247,9 @@ __global__ void __launch_bounds__(kLineThreads) k_box_line_smem(LineArgs a, int 
     extern __shared__ float sl[];
     float* so = sl + (size_t)a.L * kLp;
     __shared__ long ibase[kLines], obase[kLines];
+    __shared__ unsigned shist[256];
+    if (a.hist)
+        for (int k = threadIdx.x; k < 256; k += kLineThreads) shist[k] = 0;
     const long lines = a.A * a.B, t0 = (long)blockIdx.x * kLines;
     const int tid = threadIdx.x;
     const int nl = (int)(lines - t0 < kLines ? lines - t0 : kLines);
@@ -282,7 +286,20 @@ __global__ void __launch_bounds__(kLineThreads) k_box_line_smem(LineArgs a, int 
 #pragma unroll 4
     for (unsigned k = tid; k < total; k += kLineThreads) {
         const unsigned j = along ? k / L : k % kLines, e = along ? k - (k / L) * L : k / kLines;
-        if ((int)j < nl) a.out[obase[j] + (long)e * a.ol] = so[e * kLp + j];
+        if ((int)j < nl) {
+            const float v = so[e * kLp + j];
+            a.out[obase[j] + (long)e * a.ol] = v;
+            if (a.hist) {                   // pipeline.c:318-321: (int)(v*255 + 0.5), clamped
+                int bin = (int)__fmaf_rn(v, 255.0f, 0.5f);
+                bin = bin < 0 ? 0 : (bin > 255 ? 255 : bin);
+                atomicAdd(&shist[bin], 1u);
+            }
+        }
+    }
+    if (a.hist) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < 256; k += kLineThreads)
+            if (shist[k]) atomicAdd(&a.hist[k], shist[k]);
     }
 }
 
@@ -558,16 +575,22 @@ struct CcArgs {
 __global__ void __launch_bounds__(1024) k_cc_union(CcArgs a) {
     const long x = (long)blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= a.nx) return;
-    const long plane = a.ny * a.nx;
+    const int nx = (int)a.nx, plane = (int)(a.ny * a.nx);
     for (long z = blockIdx.z; z < a.nz; z += gridDim.z) {
         const int i = (int)(((size_t)z * a.ny + y) * a.nx + x);
-        if (a.lab[i] < 0) continue;
-        const bool left = x > 0 && a.lab[i - 1] >= 0;
+        // Only the signs (material or not) are read here, and those never change; issuing
+        // all six loads before any test keeps them to one memory round trip.
+        const int c = a.lab[i];
+        const int l = x > 0 ? a.lab[i - 1] : -1;
+        const int u = y > 0 ? a.lab[i - nx] : -1;
+        const int ul = (x > 0 && y > 0) ? a.lab[i - 1 - nx] : -1;
+        const int d = z > 0 ? a.lab[i - plane] : -1;
+        const int dl = (x > 0 && z > 0) ? a.lab[i - 1 - plane] : -1;
+        if (c < 0) continue;
+        const bool left = l >= 0;
         if (left && x % blockDim.x == 0) uf_union(a.lab, i, i - 1, a.err);   // across row segments
-        if (y > 0 && a.lab[i - a.nx] >= 0 && !(left && a.lab[i - 1 - a.nx] >= 0))
-            uf_union(a.lab, i, i - (int)a.nx, a.err);
-        if (z > 0 && a.lab[i - plane] >= 0 && !(left && a.lab[i - 1 - plane] >= 0))
-            uf_union(a.lab, i, i - (int)plane, a.err);
+        if (u >= 0 && !(left && ul >= 0)) uf_union(a.lab, i, i - nx, a.err);
+        if (d >= 0 && !(left && dl >= 0)) uf_union(a.lab, i, i - plane, a.err);
     }
 }
 
@@ -694,17 +717,24 @@ double tile_eps(const fy_pipeline_cfg* c, double ecy, double ecx, long y0, long 
     return c->guided_eps * s2;
 }
 
+// One pass of line sums; with ctl set (the last pass) the histogram of the means is added
+// to ctl->hist as they are stored (or by k_air_hist after the unstaged kernel).
 cudaError_t box_pass(const float* in, float* out, int L, int r, long A, long B, long ia, long ib, long il, long oa,
-                     long ob, long ol, cudaStream_t st) {
-    LineArgs a{in, out, L, r, A, B, ia, ib, il, oa, ob, ol};
+                     long ob, long ol, cudaStream_t st, TileCtl* ctl = nullptr, int sms = 148) {
+    LineArgs a{in, out, L, r, A, B, ia, ib, il, oa, ob, ol, nullptr};
     const long lines = A * B;
     const size_t smem = (size_t)2 * L * kLp * sizeof(float);
     if (smem <= 200 * 1024) {
         cudaError_t e = fy_smem_optin(k_box_line_smem, smem);
         if (e != cudaSuccess) return e;
+        a.hist = ctl ? ctl->hist : nullptr;
         k_box_line_smem<<<(unsigned)((lines + kLines - 1) / kLines), kLineThreads, smem, st>>>(a, ib != 1 ? 1 : 0);
     } else {
         k_box_line<<<(unsigned)((lines + kTpb - 1) / kTpb), kTpb, 0, st>>>(a);
+        if (ctl) {
+            const size_t m = (size_t)A * B * L;
+            k_air_hist<<<grid1(m, 256, sms), 256, 0, st>>>(out, m, ctl);
+        }
     }
     return cudaGetLastError();
 }
@@ -849,10 +879,8 @@ int tile_chain(const fy_pipeline_cfg* c, const uint8_t* d_u8, long rz0, long ry0
         // x lines (decimated read of orig), then y lines, then z lines
         TRY(box_pass(orig, t1, (int)mx, r, mz, my, d * hy * hx, d * hx, d, mp, mx, 1, st));
         TRY(box_pass(t1, t2, (int)my, r, mz, mx, mp, 1, mx, mp, 1, mx, st));
-        TRY(box_pass(t2, sm, (int)mz, r, my, mx, mx, 1, mp, mx, 1, mp, st));
+        TRY(box_pass(t2, sm, (int)mz, r, my, mx, mx, 1, mp, mx, 1, mp, st, ctl, cx.sms));   // + histogram
         fy_prof_mark(st, "tile.scratch_box");
-        k_air_hist<<<grid1(m, 256, cx.sms), 256, 0, st>>>(sm, m, ctl);
-        TRY(cudaGetLastError());
         k_air_cut<<<1, 256, 0, st>>>(ctl, c->air_cut_u8, c->air_cut_band, c->air_thresh, c->air_cut_aggr);
         TRY(cudaGetLastError());
         fy_prof_mark(st, "tile.air_cut");
@@ -865,7 +893,7 @@ int tile_chain(const fy_pipeline_cfg* c, const uint8_t* d_u8, long rz0, long ry0
                    cc ? w.info.as<unsigned>() : nullptr};
         k_air_apply<<<grid_rows(hx, hy, hz), row_threads(hx), 0, st>>>(aa);
         TRY(cudaGetLastError());
-        launches += 6;
+        launches += 5;
         fy_prof_mark(st, "tile.air_apply");
         if (cc) {
             CcArgs ca{f, w.lab.as<int>(), w.info.as<unsigned>(), &ctl->err, hz, hy, hx, c->air_min_component};
