@@ -21,7 +21,7 @@ def declared():
 
 def test_header_declares_the_drop_in_set():
     names = set(declared())
-    # the fysics.h entry points on the restoration path (survey scope rows a1-a19)
+    # the fysics.h entry points on the restoration path
     required = {
         "fy_u8_to_phys", "fy_phys_to_u8", "fy_float_to_u8", "fy_u8_to_float", "fy_phys_to_u8_level",
         "fy_fft1d", "fy_fft3d", "fy_fft3d_normalize", "fy_next_fft_size", "fy_is_pow2",
@@ -32,7 +32,7 @@ def test_header_declares_the_drop_in_set():
         "fy_estimate_noise", "fy_guided_eps_for_noise", "fy_dering_init", "fy_dering_free",
         "fy_dering_tile_init", "fy_dering_tile_reset", "fy_dering_accumulate_u8",
         "fy_dering_merge_tile", "fy_dering_finalize", "fy_dering_apply", "fy_phase_correlate",
-        # the per-tile chain and pass-1 helpers (survey rows f1, f2)
+        # the per-tile export chain and the pass-1 calibration helpers
         "fy_process_buffer", "fy_valley_depth", "fy_hist_accumulate_u8", "fy_flat_noise", "fy_noise_aniso",
     }
     assert required <= names, sorted(required - names)
