@@ -172,6 +172,8 @@ SIGNATURES = {
     "fy_gpu_flat_noise": (_i, [_P, _i, _i, _i, _i, _P, _P, _P]),
     "fy_gpu_noise_aniso": (_i, [_P, _i, _i, _i, _P, _P, _P]),
     "fy_valley_depth": (_d, [_P, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
+    "fy_measure_psf_sigma": (_d, [_P, _i, _i, _i, C.POINTER(_i)]),
+    "fy_gpu_measure_psf_sigma": (_i, [_P, _i, _i, _i, _P, _P]),
     "fy_process_buffer": (_i, [C.POINTER(PipelineCfg), _P, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l,
                                _P, C.POINTER(_i)]),
     "fy_gpu_process_buffer": (_i, [C.POINTER(PipelineCfg), _P, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l,

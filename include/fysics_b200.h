@@ -134,6 +134,13 @@ int    fy_hist_percentile_u8_inner(const fy_hist_state *s, double pct);
 double fy_flat_noise(const float *v, int nz, int ny, int nx, int blk);
 int    fy_noise_aniso(const float *v, int nz, int ny, int nx, double *rho_z, double *rho_xy);
 
+/* PSF edge fit of pass-1 calibration (pipeline.c:107-196, static there and called by
+ * fy_calibrate): sigma in voxels of the effective PSF from up to 400 air/papyrus edge
+ * profiles of a u8 tile, or -1 with fewer than 30 (or a fit outside (0.3, 5)). *nprof (may
+ * be NULL) receives the number of profiles used. Returns NaN when it cannot run (reason in
+ * fy_gpu_last_error). */
+double fy_measure_psf_sigma(const unsigned char *vol, int Z, int Y, int X, int *nprof);
+
 /* histogram valley (fysics.h:92, stream.c:138-168): O(256) host arithmetic on counts */
 double fy_valley_depth(const long hist[256], int *dark_out, int *light_out, int *valley_out);
 
@@ -381,6 +388,9 @@ int    fy_gpu_process_buffer(const fy_pipeline_cfg *cfg, const unsigned char *d_
                              long rz0, long ry0, long rx0, long hz, long hy, long hx,
                              long z0, long y0, long x0, long tz, long ty, long tx,
                              long vol_y, long vol_x, unsigned char *d_out, int *all_air, void *stream);
+/* fy_measure_psf_sigma on a device u8 tile; d_out (16 bytes of device memory) receives
+ * { double sigma; int nprof; }. Enqueued on `stream`, no synchronisation. */
+int    fy_gpu_measure_psf_sigma(const unsigned char *d_vol, int Z, int Y, int X, void *d_out, void *stream);
 /* Air-cut state of the calling thread's last fy_process_buffer / fy_gpu_process_buffer:
  * the 256-bin histogram of the scratch smooth and (cut, uniform cut, textured cut) in u8
  * levels. Returns 0, or 1 when that call ran no air cut. */

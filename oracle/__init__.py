@@ -163,6 +163,7 @@ O64_SIGS = {
     "ot_dither01": (C.c_float, [_l, _l, _l]),
     "ot_quant_u8": (C.c_uint8, [C.c_float, _l, _l, _l, _i]),
     "ot_air_cuts": (None, [_P, _i, _i, _d, _d, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
+    "ot_measure_psf_sigma": (_d, [_P, _i, _i, _i, C.POINTER(_i)]),
     "ot_process_buffer": (_i, [C.POINTER(OtTileCfg), _P, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _P,
                                C.POINTER(_i), _P, _P]),
     "o64_radial_tile_eps": (C.c_double, [_i, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
@@ -333,3 +334,18 @@ def ot_process_buffer(d: dict, u8, org, inner, vol_yx, ring=None, ring_geo=None,
                                  C.byref(air), p(hist), p(cuts))
     assert rc == 0, rc
     return (out, air.value, hist, cuts) if state else (out, air.value)
+
+
+PSF_SO = HERE / "_ref" / "libref_psf.so"
+_psf = None
+
+
+def ref_psf():
+    """The reference's static measure_tile_psf_sigma (pipeline.c:107-196) through the shim
+    oracle/ref_psf_shim.c; None where the reference was not built."""
+    global _psf
+    if _psf is None and PSF_SO.exists():
+        _psf = C.CDLL(str(PSF_SO), mode=C.RTLD_LOCAL)
+        _psf.ref_measure_tile_psf_sigma.restype = C.c_double
+        _psf.ref_measure_tile_psf_sigma.argtypes = [_P, _i, _i, _i]
+    return _psf

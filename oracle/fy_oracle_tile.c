@@ -377,3 +377,111 @@ int ot_process_buffer(const ot_tile_cfg *c, const uint8_t *u8buf, long rz0, long
     free(orig);
     return 0;
 }
+
+/* ---------------------------------------------------------------- PSF edge fit
+ * measure_tile_psf_sigma (pipeline.c:107-196): effective PSF sigma (voxels) from air/papyrus
+ * edge profiles of a u8 tile. Candidate lines come from the reference's LCG, reseeded to 1
+ * per call (:111-112, :124); up to 2500 candidates per axis (y lines, then x lines), the
+ * first 400 accepted edges kept in candidate order. The edge normalisation is a true
+ * division (a reciprocal there flipped an edge decision against the compiled reference);
+ * acc / nprof and lsf / lsum are multiplications by the reciprocal, and
+ * e[i]*(1-f) + e[i+1]*f is fused. The final reductions (lsum, mu, var) are sequential
+ * here; the reference build vectorises them, so sigma agrees to rounding (1e-15 measured),
+ * and nprof and the accepted set exactly.
+ * Returns sigma or -1; *nprof_out receives the number of profiles. */
+static unsigned ot_psf_rand(unsigned *s) {
+    *s = *s * 1103515245u + 12345u;
+    return (*s >> 16) & 0x7fff;
+}
+
+/* one candidate: returns 1 and fills e[15], *cross when the line is an accepted edge */
+static int ot_psf_candidate(const uint8_t *vol, int Z, int Y, int X, int ax, unsigned *rng, double *e,
+                            double *cross) {
+    const int half = 7, plen = 15, min_c = 40;
+    int line[15];
+    if (ax == 1) {
+        const int z = (int)(ot_psf_rand(rng) % (unsigned)Z);
+        const int y = half + (int)(ot_psf_rand(rng) % (unsigned)(Y - 2 * half));
+        const int x = (int)(ot_psf_rand(rng) % (unsigned)X);
+        for (int i = 0; i < plen; i++) line[i] = vol[((size_t)z * Y + (y - half + i)) * X + x];
+    } else {
+        const int z = (int)(ot_psf_rand(rng) % (unsigned)Z);
+        const int y = (int)(ot_psf_rand(rng) % (unsigned)Y);
+        const int x = half + (int)(ot_psf_rand(rng) % (unsigned)(X - 2 * half));
+        for (int i = 0; i < plen; i++) line[i] = vol[((size_t)z * Y + y) * X + (x - half + i)];
+    }
+    const double lo = 0.5 * (line[0] + line[1]), hi = 0.5 * (line[plen - 1] + line[plen - 2]);
+    if (fabs(hi - lo) < min_c) return 0;
+    int s[15];
+    for (int i = 0; i < plen; i++) s[i] = hi > lo ? line[i] : line[plen - 1 - i];
+    double dmin = 1e9, dmax = -1e9;
+    int amax = 0;
+    for (int i = 0; i < plen - 1; i++) {
+        const double d = (double)s[i + 1] - s[i];
+        if (d < dmin) dmin = d;
+        if (d > dmax) { dmax = d; amax = i; }
+    }
+    if (dmin < -8) return 0;
+    if (!(amax == half - 1 || amax == half || amax == half + 1)) return 0;
+    int smin = s[0];
+    for (int i = 1; i < plen; i++) smin = s[i] < smin ? s[i] : smin;
+    double emax = 0;
+    for (int i = 0; i < plen; i++) { e[i] = s[i] - smin; emax = e[i] > emax ? e[i] : emax; }
+    if (emax <= 0) return 0;
+    for (int i = 0; i < plen; i++) e[i] /= emax;
+    int idx0 = -1;
+    for (int i = 0; i < plen; i++)
+        if (e[i] >= 0.5) { idx0 = i; break; }
+    if (idx0 <= 0) return 0;
+    const double frac = (0.5 - e[idx0 - 1]) / (e[idx0] - e[idx0 - 1] + 1e-9);
+    *cross = idx0 - 1 + frac;
+    return 1;
+}
+
+double ot_measure_psf_sigma(const uint8_t *vol, int Z, int Y, int X, int *nprof_out) {
+    enum { HALF = 7, SUP = 8, PLEN = 15, GLEN = 2 * HALF * SUP + 1, MAXE = 400 };
+    static double esf_p[MAXE][PLEN], cross_p[MAXE];
+    double grid[GLEN], acc[GLEN], esf[GLEN], lsf[GLEN];
+    for (int i = 0; i < GLEN; i++) { grid[i] = -HALF + (double)i * (2.0 * HALF) / (GLEN - 1); acc[i] = 0; }
+    unsigned rng = 1u;
+    int nprof = 0;
+    for (int ax = 1; ax <= 2 && nprof < MAXE; ax++) {
+        if ((ax == 1 ? Y : X) - 2 * HALF <= 0) continue;      /* the reference breaks before any draw */
+        for (int it = 0; it < 2500 && nprof < MAXE; it++)
+            if (ot_psf_candidate(vol, Z, Y, X, ax, &rng, esf_p[nprof], &cross_p[nprof])) nprof++;
+    }
+    if (nprof_out) *nprof_out = nprof;
+    if (nprof < 30) return -1.0;
+    for (int p = 0; p < nprof; p++)
+        for (int gi = 0; gi < GLEN; gi++) {
+            const double xs = grid[gi] + cross_p[p];
+            double v;
+            if (xs <= 0) v = 0.0;
+            else if (xs >= PLEN - 1) v = 1.0;
+            else {
+                const int i = (int)xs;
+                const double f = xs - i;
+                v = fma(esf_p[p][i + 1], f, esf_p[p][i] * (1.0 - f));
+            }
+            acc[gi] += v;
+        }
+    const double rn = 1.0 / nprof;
+    for (int gi = 0; gi < GLEN; gi++) esf[gi] = acc[gi] * rn;
+    double lsum = 0;
+    for (int gi = 0; gi < GLEN; gi++) {
+        double d;
+        if (gi == 0) d = esf[1] - esf[0];
+        else if (gi == GLEN - 1) d = esf[GLEN - 1] - esf[GLEN - 2];
+        else d = 0.5 * (esf[gi + 1] - esf[gi - 1]);
+        if (d < 0) d = 0;
+        lsf[gi] = d;
+        lsum += d;
+    }
+    if (!(lsum > 0)) return -1.0;
+    const double rl = 1.0 / lsum;
+    double mu = 0, var = 0;
+    for (int gi = 0; gi < GLEN; gi++) { lsf[gi] *= rl; mu = fma(grid[gi], lsf[gi], mu); }
+    for (int gi = 0; gi < GLEN; gi++) { const double g = grid[gi] - mu; var = fma(g * g, lsf[gi], var); }
+    const double sig = sqrt(var);
+    return (sig > 0.3 && sig < 5.0) ? sig : -1.0;
+}

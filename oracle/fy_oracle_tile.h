@@ -47,6 +47,9 @@ int     ot_process_buffer(const ot_tile_cfg *c, const uint8_t *u8buf, long rz0, 
                           long hz, long hy, long hx, long z0, long y0, long x0, long tz, long ty,
                           long tx, uint8_t *out, int *all_air, long *hist_out, int *cuts_out);
 
+/* measure_tile_psf_sigma (pipeline.c:107-196): sigma or -1; *nprof_out = edge profiles used */
+double  ot_measure_psf_sigma(const uint8_t *vol, int Z, int Y, int X, int *nprof_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,3 +71,26 @@ def gpu_process_buffer(fb, d: dict, u8, org, inner, vol_yx, dering=None, zdrift=
     rc = lib.fy_process_buffer(C.byref(cfg), u8.ctypes.data, *org, *u8.shape, z0, y0, x0, tz, ty, tx, *vol_yx,
                                out.ctypes.data, C.byref(air))
     return rc, out, air.value
+
+
+def psf_volume(shape, sigma, orient, noise, seed):
+    """u8 tile of blurred two-level steps (35 / 185) for the PSF edge fit: the steps vary
+    along y ("y"), x ("x") or both ("xy"), blurred by a Gaussian of `sigma` voxels, plus
+    Gaussian noise of `noise` levels."""
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid(*[np.arange(s) for s in shape], indexing="ij")
+    if orient == "y":
+        f = np.sin(y / 6.0 + 0.3 * np.sin(x / 17.0))
+    elif orient == "x":
+        f = np.sin(x / 6.0 + 0.3 * np.sin(z / 13.0))
+    else:
+        f = np.sin(x / 5.0) + np.cos(y / 7.0)
+    step = (f > 0).astype(float) * 150 + 35
+    v = gaussian_filter(step, sigma) + rng.normal(0, noise, shape)
+    return np.clip(np.rint(v), 0, 255).astype(np.uint8)
+
+
+PSF_CASES = [((32, 64, 64), 0.7, "y", 0.5), ((32, 64, 64), 2.0, "xy", 2.0), ((40, 96, 80), 1.2, "x", 2.0),
+             ((40, 96, 80), 3.0, "xy", 0.5), ((16, 30, 200), 2.0, "x", 0.5), ((16, 30, 200), 0.7, "y", 2.0),
+             ((24, 12, 90), 1.2, "x", 0.5), ((24, 90, 12), 1.2, "y", 0.5), ((8, 10, 10), 1.0, "xy", 0.5)]

@@ -80,3 +80,25 @@ def test_hist_host_bookkeeping_matches_reference(fy):
             assert lib.fy_hist_percentile_u8(C.byref(h), pct) == oracle.ref().fy_hist_percentile_u8(C.byref(r), pct)
             assert (lib.fy_hist_percentile_u8_inner(C.byref(h), pct)
                     == oracle.ref().fy_hist_percentile_u8_inner(C.byref(r), pct))
+
+
+@pytest.mark.parametrize("case", range(9))
+def test_psf_sigma_oracle_vs_reference(case):
+    """measure_tile_psf_sigma (pipeline.c:107-196), static in the reference, through the shim:
+    the profile count exactly, sigma within 1e-12 relative (the reference build vectorises
+    the final sums). Covers y-only, x-only and mixed edges, and tiles too thin for one axis
+    (12 voxels) or both."""
+    from tests._tiles import PSF_CASES, psf_volume
+    shape, sigma, orient, noise = PSF_CASES[case]
+    R = oracle.ref_psf()
+    if R is None:
+        pytest.skip("needs the compiled reference")
+    v = psf_volume(shape, sigma, orient, noise, 7)
+    n = C.c_int(-1)
+    got = oracle.o64().ot_measure_psf_sigma(oracle.p(v), *shape, C.byref(n))
+    want = R.ref_measure_tile_psf_sigma(oracle.p(v), *shape)
+    assert abs(got - want) <= 1e-12 * max(abs(want), 1.0), (got, want, n.value)
+    if shape[1] > 14 or shape[2] > 14:
+        assert n.value > 0
+    else:
+        assert n.value == 0 and got == -1.0

@@ -121,3 +121,39 @@ def test_device_forms(gpu):
     oz, ox = C.c_double(), C.c_double()
     assert r.status == o64().o64_noise_aniso(p(v), *shape, C.byref(oz), C.byref(ox)) == 0
     assert rel_close(r.rho_z, oz.value) and rel_close(r.rho_xy, ox.value)
+
+
+@pytest.mark.parametrize("case", range(9))
+def test_psf_sigma_gpu(gpu, case):
+    """The GPU PSF edge fit equals the oracle bit for bit (same draws, same accepted edges,
+    same FP64 operations in the same order) and the reference within 1e-12."""
+    from tests._tiles import PSF_CASES, psf_volume
+    shape, sigma, orient, noise = PSF_CASES[case]
+    v = psf_volume(shape, sigma, orient, noise, 7)
+    lib = gpu.load()
+    n = C.c_int(-1)
+    got = lib.fy_measure_psf_sigma(v.ctypes.data, *shape, C.byref(n))
+    on = C.c_int(-1)
+    want = o64().ot_measure_psf_sigma(p(v), *shape, C.byref(on))
+    assert n.value == on.value and got == want, (got, want, n.value, on.value)
+    if oracle.ref_psf() is not None:
+        ref = oracle.ref_psf().ref_measure_tile_psf_sigma(p(v), *shape)
+        assert abs(got - ref) <= 1e-12 * max(abs(ref), 1.0)
+
+
+def test_psf_sigma_device_form(gpu):
+    import torch
+    from tests._tiles import psf_volume
+    v = psf_volume((32, 64, 64), 1.2, "xy", 1.0, 3)
+    lib = gpu.load()
+    d = torch.from_numpy(v).cuda()
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")       # { double sigma; int nprof; }
+    torch.cuda.synchronize()
+    assert lib.fy_gpu_measure_psf_sigma(C.c_void_p(d.data_ptr()), *v.shape, C.c_void_p(out.data_ptr()), None) == 0
+    torch.cuda.synchronize()
+    h = out.cpu().numpy()
+    sigma, nprof = h[0], int(h[1:].view(np.int32)[0])
+    n = C.c_int()
+    assert sigma == lib.fy_measure_psf_sigma(v.ctypes.data, *v.shape, C.byref(n)) and nprof == n.value
+    assert np.isnan(lib.fy_measure_psf_sigma(v.ctypes.data, 0, 64, 64, None))      # bad dims: NaN + status
+    assert lib.fy_gpu_last_status() == gpu.FY_EINVAL
