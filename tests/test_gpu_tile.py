@@ -149,3 +149,15 @@ def test_wide_thin_buffer(gpu):
     assert rc == 0, gpu.load().fy_gpu_last_error()
     o, _ = oracle.ot_process_buffer(d, v, (0, 0, 0), inner, (210, 212))
     assert np.array_equal(g, o), np.count_nonzero(g != o)
+
+
+def test_rows_over_one_cta(gpu):
+    """Rows longer than 1024 voxels span several CTAs: run heads are per row segment and the
+    union joins runs across the segment boundaries."""
+    v = scroll_volume((8, 24, 1100), seed=44, specks_per_mvox=4000)
+    d = oracle.pipeline_defaults(air_min_component=30, have_norm=1, norm_lo=40, norm_hi=200)
+    inner = (2, 2, 2, 4, 20, 1096)
+    rc, g, _ = gpu_process_buffer(gpu, d, v, (0, 0, 0), inner, (24, 1100))
+    assert rc == 0, gpu.load().fy_gpu_last_error()
+    o, _ = oracle.ot_process_buffer(d, v, (0, 0, 0), inner, (24, 1100))
+    assert np.array_equal(g, o), np.count_nonzero(g != o)
