@@ -200,8 +200,9 @@ cudaError_t fy_launch_guided_fast(const float* in, float* out, float* ws, int nz
     k_decimate<<<grid_1d(nl), 256, 0, st>>>(in, il, ny, nx, lz, ly, lx, s);
     cudaError_t e = fy_launch_guided_fused(il, ma, mb, ab, lz, ly, lx, rl, eps, 1, sms, st, eps_ptr);
     if (e != cudaSuccess) return e;
-    dim3 grid(ceil_div_i(nx, 128), ny, nz);
-    k_upsample_apply<<<grid, 128, 0, st>>>(in, out, ma, mb, nz, ny, nx, lz, ly, lx, s);
+    const int tpb = nx < 256 ? (nx + 31) / 32 * 32 : 256;     // whole warps across a row
+    dim3 grid(ceil_div_i(nx, tpb), ny, nz);
+    k_upsample_apply<<<grid, tpb, 0, st>>>(in, out, ma, mb, nz, ny, nx, lz, ly, lx, s);
     launches += 4;
     return cudaGetLastError();
 }
