@@ -567,15 +567,19 @@ struct WarpCands {
 
 // The counting pass: mean keys against the windows of targets 0 and 1. The counts below each
 // window stay in registers until one warp reduction at the end; the keys inside a window go
-// to the candidate list.
+// to the candidate list (order is irrelevant to the selection). Per step a thread marks its
+// 4*SU keys' window hits in two bit masks; one warp scan of the hit counts places them in the
+// warp's shared-memory buffer, which is appended to the list (one atomic) when nearly full.
+constexpr int kCountBuf = 1152;          // >= one step's worst case (32 lanes x 4*SU keys x 2); 45 KB static smem
 __global__ void __launch_bounds__(256) k_win_count(const float* __restrict__ mean, NoiseCtl* __restrict__ ctl,
                                                    float* __restrict__ cval, uint8_t* __restrict__ clab,
                                                    long long cap) {
-    __shared__ float bufv[256 / 32][kWarpBuf];
-    __shared__ uint8_t bufl[256 / 32][kWarpBuf];
+    static_assert(32 * 4 * SU * 2 <= kCountBuf, "one step must fit the warp buffer");
+    __shared__ float bufv[256 / 32][kCountBuf];
+    __shared__ uint8_t bufl[256 / 32][kCountBuf];
     if (ctl->mode != kModeWin0) return;
     const unsigned full = 0xffffffffu;
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, lane = t & 31;
     WarpCands wc;
     wc.v = bufv[t >> 5];
     wc.l = bufl[t >> 5];
@@ -588,21 +592,39 @@ __global__ void __launch_bounds__(256) k_win_count(const float* __restrict__ mea
         float4 x[SU];
 #pragma unroll
         for (int u = 0; u < SU; ++u) x[u] = __ldg(reinterpret_cast<const float4*>(mean) + base + t + (long long)u * 256);
+        float mv[4 * SU];
+        unsigned m0 = 0, m1 = 0;
 #pragma unroll
         for (int u = 0; u < SU; ++u) {
-            const float mv[4] = {x[u].x, x[u].y, x[u].z, x[u].w};
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const uint32_t k = fkey(mv[j]);
-                bel0 += k < lo0;
-                bel1 += k < lo1;
-                const bool in0 = k >= lo0 && k <= hi0, in1 = k >= lo1 && k <= hi1;
-                if (__any_sync(full, in0 || in1)) {
-                    wc.add(in0, mv[j], 0, cval, clab, &ctl->ncand, cap);
-                    wc.add(in1, mv[j], 1, cval, clab, &ctl->ncand, cap);
-                }
-            }
+            mv[4 * u] = x[u].x; mv[4 * u + 1] = x[u].y; mv[4 * u + 2] = x[u].z; mv[4 * u + 3] = x[u].w;
         }
+#pragma unroll
+        for (int q = 0; q < 4 * SU; ++q) {
+            const uint32_t k = fkey(mv[q]);
+            bel0 += k < lo0;
+            bel1 += k < lo1;
+            m0 |= (unsigned)(k >= lo0 && k <= hi0) << q;
+            m1 |= (unsigned)(k >= lo1 && k <= hi1) << q;
+        }
+        const int c = __popc(m0) + __popc(m1);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(full, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int tot = __shfl_sync(full, incl, 31);
+        if (tot == 0) continue;
+        if (wc.cnt + tot > kCountBuf) wc.flush(cval, clab, &ctl->ncand, cap);     // warp-uniform
+        int pos = wc.cnt + incl - c;
+#pragma unroll
+        for (int q = 0; q < 4 * SU; ++q)          // unrolled, so mv stays in registers
+            if ((m0 >> q) & 1u) { wc.v[pos] = mv[q]; wc.l[pos] = 0; ++pos; }
+#pragma unroll
+        for (int q = 0; q < 4 * SU; ++q)
+            if ((m1 >> q) & 1u) { wc.v[pos] = mv[q]; wc.l[pos] = 1; ++pos; }
+        wc.cnt += tot;
+        __syncwarp();
     }
     if (base < n4) {                                     // the grid's partial chunk
         for (int u = 0; u < SU; ++u)
