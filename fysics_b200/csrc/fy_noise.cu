@@ -28,6 +28,7 @@ constexpr int NT_MAX = 64;             // selection targets: 2 per bin + spare
 // variance fallback, 3 done; kModeWin0: the mean percentiles through the sample-guided
 // window (section 2w), which falls back to mode 0 when the window misses.
 constexpr int kModeWin0 = 4;
+constexpr int kModeBinCand = 6;        // the bins' last digit runs on a candidate list (cc)
 
 FY_D uint32_t fkey(float f) {
     const uint32_t u = __float_as_uint(f);
@@ -123,6 +124,40 @@ struct RunAcc {
     }
 };
 
+constexpr int kWarpBuf = 256;
+struct WarpCands {
+    float* v;                          // this warp's kWarpBuf values in shared memory
+    uint8_t* l;                        // and labels
+    int cnt = 0;                       // warp-uniform fill
+    FY_D void flush(float* __restrict__ cval, uint8_t* __restrict__ clab, unsigned long long* ncand, long long cap) {
+        const unsigned full = 0xffffffffu;
+        __syncwarp();
+        if (cnt) {
+            unsigned long long base = 0;
+            if ((threadIdx.x & 31) == 0) base = atomicAdd(ncand, (unsigned long long)cnt);
+            base = __shfl_sync(full, base, 0);
+            for (int i = threadIdx.x & 31; i < cnt; i += 32)
+                if ((long long)(base + i) < cap) { cval[base + i] = v[i]; clab[base + i] = l[i]; }
+        }
+        cnt = 0;
+        __syncwarp();
+    }
+    // every lane of the warp calls
+    FY_D void add(bool take, float val, uint8_t label, float* __restrict__ cval, uint8_t* __restrict__ clab,
+                  unsigned long long* ncand, long long cap) {
+        const unsigned bal = __ballot_sync(0xffffffffu, take);
+        if (!bal) return;
+        const int lane = threadIdx.x & 31;
+        if (take) {
+            const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+            v[pos] = val;
+            l[pos] = label;
+        }
+        cnt += __popc(bal);
+        if (cnt > kWarpBuf - 32) flush(cval, clab, ncand, cap);
+    }
+};
+
 // Streaming passes read SU float4 (and uchar4 bin labels) per thread before using any, so
 // enough bytes are in flight per SM to cover HBM latency. Full chunks of the grid-stride
 // loop run without per-element range checks; the one partial chunk is checked.
@@ -137,10 +172,15 @@ constexpr int SU = 4;
 // which no key's high part (< 2^(32 - shift - DB)) can equal.
 // LABEL (the first variance pass only): the bin of each voxel is computed from its mean here
 // and its u8 label written for the later passes, so no separate labelling pass runs.
-template <int DB, int MODE, bool LABEL = false>
+// COMPACT (a MODE 1 digit pass): each voxel whose key matches its bin target's prefix is also
+// appended, with its bin, to the candidate list (cval, clab; counter ctl->ncand): every key of
+// the prefixes that the following digits narrow is then in the list.
+constexpr int kCompactBuf = 1152;        // per warp: one step's worst case (32 x 4*SU) + slack
+template <int DB, int MODE, bool LABEL = false, bool COMPACT = false>
 __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean, const float* __restrict__ var,
                                                   uint8_t* __restrict__ bin, NoiseCtl* __restrict__ ctl,
-                                                  int shift) {
+                                                  int shift, float* __restrict__ cval = nullptr,
+                                                  uint8_t* __restrict__ clab = nullptr, long long cap = 0) {
     extern __shared__ unsigned int h[];
     __shared__ uint32_t sp[256];
     __shared__ float fe[NB + 1];
@@ -178,6 +218,12 @@ __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean
         if (MODE == 1) return sp[g] == hb ? g * NBK + dig : -1;
         return hb == p0 ? dig : (hb == p1 ? NBK + dig : -1);
     };
+    WarpCands wc;
+    if (COMPACT) {
+        float* bv = reinterpret_cast<float*>(h + ngroup * NBK);
+        wc.v = bv + (threadIdx.x >> 5) * kCompactBuf;
+        wc.l = reinterpret_cast<uint8_t*>(bv + (blockDim.x >> 5) * kCompactBuf) + (threadIdx.x >> 5) * kCompactBuf;
+    }
     long long base = (long long)blockIdx.x * chunk;
     for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
         float4 x[SU];
@@ -197,12 +243,48 @@ __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean
                 reinterpret_cast<uchar4*>(bin)[base + threadIdx.x + (long long)u * step] = bb[u];
             }
         }
+        if (!COMPACT) {
 #pragma unroll
-        for (int u = 0; u < SU; ++u) {
-            acc.add(h, code_of(x[u].x, MODE == 1 ? bb[u].x : 0));
-            acc.add(h, code_of(x[u].y, MODE == 1 ? bb[u].y : 0));
-            acc.add(h, code_of(x[u].z, MODE == 1 ? bb[u].z : 0));
-            acc.add(h, code_of(x[u].w, MODE == 1 ? bb[u].w : 0));
+            for (int u = 0; u < SU; ++u) {
+                acc.add(h, code_of(x[u].x, MODE == 1 ? bb[u].x : 0));
+                acc.add(h, code_of(x[u].y, MODE == 1 ? bb[u].y : 0));
+                acc.add(h, code_of(x[u].z, MODE == 1 ? bb[u].z : 0));
+                acc.add(h, code_of(x[u].w, MODE == 1 ? bb[u].w : 0));
+            }
+        } else {
+            float xv[4 * SU];
+            unsigned xl[4 * SU];
+            unsigned hit = 0;
+#pragma unroll
+            for (int u = 0; u < SU; ++u) {
+                xv[4 * u] = x[u].x; xv[4 * u + 1] = x[u].y; xv[4 * u + 2] = x[u].z; xv[4 * u + 3] = x[u].w;
+                xl[4 * u] = bb[u].x; xl[4 * u + 1] = bb[u].y; xl[4 * u + 2] = bb[u].z; xl[4 * u + 3] = bb[u].w;
+            }
+#pragma unroll
+            for (int q = 0; q < 4 * SU; ++q) {
+                const int code = code_of(xv[q], (int)xl[q]);
+                acc.add(h, code);
+                hit |= (unsigned)(code >= 0) << q;
+            }
+            // place this step's hits in the warp's buffer (one scan), append it when nearly full
+            const unsigned full = 0xffffffffu;
+            const int lane = threadIdx.x & 31, c = __popc(hit);
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(full, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int tot = __shfl_sync(full, incl, 31);
+            if (tot) {
+                if (wc.cnt + tot > kCompactBuf) wc.flush(cval, clab, &ctl->ncand, cap);
+                int pos = wc.cnt + incl - c;
+#pragma unroll
+                for (int q = 0; q < 4 * SU; ++q)
+                    if ((hit >> q) & 1u) { wc.v[pos] = xv[q]; wc.l[pos] = (uint8_t)xl[q]; ++pos; }
+                wc.cnt += tot;
+                __syncwarp();
+            }
         }
     }
     if (base < n4) {                                     // the grid's partial chunk
@@ -213,9 +295,16 @@ __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean
                 int g = 0;
                 if (LABEL) { g = (int)lab(__ldg(mean + i)); bin[i] = (uint8_t)g; }
                 else if (MODE == 1) g = (int)__ldg(bin + i);
-                acc.add(h, code_of(__ldg(src + i), g));
+                const float v = __ldg(src + i);
+                const int code = code_of(v, g);
+                acc.add(h, code);
+                if (COMPACT && code >= 0) {
+                    const unsigned long long pos = atomicAdd(&ctl->ncand, 1ull);
+                    if ((long long)pos < cap) { cval[pos] = v; clab[pos] = (uint8_t)g; }
+                }
             }
     }
+    if (COMPACT) wc.flush(cval, clab, &ctl->ncand, cap);
     acc.flush(h);
     __syncthreads();
     if (MODE == 1) {
@@ -531,39 +620,6 @@ __global__ void __launch_bounds__(kBoundThreads) k_win_bounds(const float* __res
 // Candidate appends go through a per-warp shared buffer; a full buffer is copied out with one
 // global atomic for its whole run, so the list's counter sees one atomic per ~kWarpBuf
 // candidates instead of one per warp and element.
-constexpr int kWarpBuf = 256;
-struct WarpCands {
-    float* v;                          // this warp's kWarpBuf values in shared memory
-    uint8_t* l;                        // and labels
-    int cnt = 0;                       // warp-uniform fill
-    FY_D void flush(float* __restrict__ cval, uint8_t* __restrict__ clab, unsigned long long* ncand, long long cap) {
-        const unsigned full = 0xffffffffu;
-        __syncwarp();
-        if (cnt) {
-            unsigned long long base = 0;
-            if ((threadIdx.x & 31) == 0) base = atomicAdd(ncand, (unsigned long long)cnt);
-            base = __shfl_sync(full, base, 0);
-            for (int i = threadIdx.x & 31; i < cnt; i += 32)
-                if ((long long)(base + i) < cap) { cval[base + i] = v[i]; clab[base + i] = l[i]; }
-        }
-        cnt = 0;
-        __syncwarp();
-    }
-    // every lane of the warp calls
-    FY_D void add(bool take, float val, uint8_t label, float* __restrict__ cval, uint8_t* __restrict__ clab,
-                  unsigned long long* ncand, long long cap) {
-        const unsigned bal = __ballot_sync(0xffffffffu, take);
-        if (!bal) return;
-        const int lane = threadIdx.x & 31;
-        if (take) {
-            const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
-            v[pos] = val;
-            l[pos] = label;
-        }
-        cnt += __popc(bal);
-        if (cnt > kWarpBuf - 32) flush(cval, clab, ncand, cap);
-    }
-};
 
 // The counting pass: mean keys against the windows of targets 0 and 1. The counts below each
 // window stay in registers until one warp reduction at the end; the keys inside a window go
@@ -693,6 +749,53 @@ __global__ void __launch_bounds__(256) k_win_targets(NoiseCtl* __restrict__ ctl,
         target_init(cc, t, ok ? r : 0, in, ok);
         if (!ok) atomicExch(&ctl->wfail, 1);
     }
+}
+
+// The bins' candidate list (section 2b). Reset before the compacting pass.
+__global__ void k_bin_cand_reset(NoiseCtl* __restrict__ ctl) {
+    if (ctl->mode == 1) ctl->ncand = 0;
+}
+// After the compacting pass and its scan: when the list fits, the bins' targets move to the
+// candidate block for the last digit and the whole-field pass stands aside; otherwise the
+// candidate pass stands aside.
+__global__ void __launch_bounds__(256) k_bin_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc, long long cap) {
+    __shared__ int s_go;
+    if (threadIdx.x == 0) s_go = ctl->mode == 1 && (long long)ctl->ncand <= cap;
+    __syncthreads();
+    if (!s_go) {
+        if (threadIdx.x == 0) cc->mode = 3;
+        return;
+    }
+    for (int i = threadIdx.x; i < NB * 256; i += blockDim.x) cc->hist[i] = 0;
+    for (int t = threadIdx.x; t < NT_MAX; t += blockDim.x) {
+        cc->tk[t] = ctl->tk[t];
+        cc->trank[t] = ctl->trank[t];
+        cc->tgroup_n[t] = ctl->tgroup_n[t];
+        cc->tprefix[t] = ctl->tprefix[t];
+        cc->tactive[t] = ctl->tactive[t];
+        cc->teq[t] = 0;
+        cc->tneed_next[t] = 0;
+        cc->tnext[t] = 0xffffffffu;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cc->n = (long long)ctl->ncand;
+        cc->ntarget = ctl->ntarget;
+        cc->mode = 1;
+        ctl->mode = kModeBinCand;
+    }
+}
+// After the candidates' last digit: the selected keys back into the main block.
+__global__ void k_bin_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restrict__ cc) {
+    if (ctl->mode != kModeBinCand) return;
+    for (int t = 0; t < NT_MAX; ++t) {
+        ctl->tprefix[t] = cc->tprefix[t];
+        ctl->trank[t] = cc->trank[t];
+        ctl->teq[t] = cc->teq[t];
+        ctl->tneed_next[t] = cc->tneed_next[t];
+        ctl->tnext[t] = cc->tnext[t];
+    }
+    ctl->mode = 1;
 }
 
 // One thread: a failed window sends the selection to the radix passes over the whole field.
@@ -879,6 +982,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     const float inv_wc = (float)(1.0 / ((double)win * win * win));
     const unsigned g = grid_sel(n, sms), gc = grid_sel(L.cap, sms);
     const size_t smem_all = 2 * 2048 * sizeof(unsigned int), smem_bin = NB * 256 * sizeof(unsigned int);
+    const size_t smem_bin_c = smem_bin + (size_t)(256 / 32) * kCompactBuf * (sizeof(float) + 1);
     const size_t smem_keys = kSampleMax * sizeof(uint32_t) + 256 * kBoundThreads;   // keys + private digit counts
     const long long m = n < kSampleMax ? n : kSampleMax;
     const unsigned long long wa = weyl_step((unsigned long long)n), wb = (unsigned long long)n / 3;
@@ -924,13 +1028,24 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     k_noise_bins_setup<<<1, 1, 0, st>>>(ctl);
     fy_prof_mark(st, "noise.lohi");
     // 2b. per-bin flat_pct percentile of the variance: 4 x 8 bits, then the k+1 neighbours;
-    // the first pass also labels the voxels with their bins and yields the bin counts
-    for (int sh = 24; sh >= 0; sh -= 8) {
-        if (sh == 24) k_sel_hist<8, 1, true><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, sh);
-        else k_sel_hist<8, 1><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, sh);
-        if (sh == 24) k_bin_targets<<<NB, 256, 0, st>>>(ctl);
-        k_sel_scan<<<NB, 256, 0, st>>>(ctl, 8, 1, sh == 0);
-    }
+    // the first pass also labels the voxels with their bins and yields the bin counts. The
+    // third pass also lists the voxels that match their bin's 16-bit prefix (~1% of them),
+    // and the last digit runs over that list (falling back to the whole field if it overflows).
+    k_sel_hist<8, 1, true><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, 24);
+    k_bin_targets<<<NB, 256, 0, st>>>(ctl);
+    k_sel_scan<<<NB, 256, 0, st>>>(ctl, 8, 1, 0);
+    k_sel_hist<8, 1><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, 16);
+    k_sel_scan<<<NB, 256, 0, st>>>(ctl, 8, 1, 0);
+    k_bin_cand_reset<<<1, 1, 0, st>>>(ctl);
+    if ((e = fy_smem_optin(k_sel_hist<8, 1, false, true>, smem_bin_c)) != cudaSuccess) return e;
+    k_sel_hist<8, 1, false, true><<<g, 256, smem_bin_c, st>>>(mean, var, bin, ctl, 8, cval, clab, L.cap);
+    k_sel_scan<<<NB, 256, 0, st>>>(ctl, 8, 1, 0);
+    k_bin_arm<<<1, 256, 0, st>>>(ctl, cc, L.cap);
+    k_sel_hist<8, 1><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, 0);        // overflow only
+    k_sel_scan<<<NB, 256, 0, st>>>(ctl, 8, 1, 1);
+    k_sel_hist<8, 1><<<gc, 256, smem_bin, st>>>(nullptr, cval, clab, cc, 0);   // the list
+    k_sel_scan<<<NB, 256, 0, st>>>(cc, 8, 1, 1);
+    k_bin_finish<<<1, 1, 0, st>>>(ctl, cc);
     k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 1);
     k_noise_fit<<<1, 1, 0, st>>>(ctl, 0);
     fy_prof_mark(st, "noise.bin_select");
@@ -942,7 +1057,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     }
     k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 2);
     k_noise_fit<<<1, 1, 0, st>>>(ctl, 1);
-    launches += 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 7 + 1 + 10 + 1 + 1 + 7 + 1;
+    launches += 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 7 + 1 + 15 + 1 + 1 + 7 + 1;
     return cudaGetLastError();
 }
 
