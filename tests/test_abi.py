@@ -107,3 +107,22 @@ def test_server_refuses_without_gpu(fy):
     assert cfg.workers == 8 and cfg.small_workers == 2 and cfg.hbm_budget_bytes == 150 << 30
     assert lib.fy_server_create(C.byref(h), C.byref(cfg)) == fy.FY_ENODEV
     assert h.value is None                                  # no handle, no worker threads
+
+
+@pytest.mark.skipif(has_cuda(), reason="a GPU is present: the no-device contract is not observable")
+def test_tile_chain_and_psf_refuse_without_gpu(fy):
+    """The per-tile chain and the PSF edge fit have no CPU fallback either."""
+    lib = fy.load()
+    cfg = fy.PipelineCfg()
+    cfg.do_air_zero = 1
+    buf = np.full((12, 12, 12), 90, np.uint8)
+    out = np.full((8, 8, 8), 0xCD, np.uint8)
+    air = C.c_int(-7)
+    rc = lib.fy_process_buffer(C.byref(cfg), buf.ctypes.data, 0, 0, 0, 12, 12, 12, 2, 2, 2, 8, 8, 8, 12, 12,
+                               out.ctypes.data, C.byref(air))
+    assert rc == fy.FY_ENODEV and (out == 0xCD).all() and air.value == -7
+    assert lib.fy_process_buffer(C.byref(cfg), buf.ctypes.data, 0, 0, 0, 12, 12, 12, 2, 2, 2, 8, 8, 11, 12, 12,
+                                 out.ctypes.data, C.byref(air)) == fy.FY_EINVAL   # geometry is checked first
+    n = C.c_int(-3)
+    assert np.isnan(lib.fy_measure_psf_sigma(buf.ctypes.data, 12, 12, 12, C.byref(n)))
+    assert lib.fy_gpu_last_status() == fy.FY_ENODEV and n.value == -3
