@@ -952,6 +952,9 @@ def main():
         except Exception as exc:       # the baseline is reported, never required
             cpu = {"value": None, "error": str(exc)[:200]}
 
+    # the legs' CPU reference samples use every host core: rank 0 of a one-GPU run only, as
+    # the cpu_baseline leg
+    cpu_legs = rank == 0 and world == 1 and not args.no_cpu
     served = batched = None
     if not args.no_serve:
         try:
@@ -963,21 +966,21 @@ def main():
     if not args.no_phasecorr:
         try:
             phasecorr = phasecorr_sample(fb, lib, dev, args.seed + 31 * rank, db_scale,
-                                         cpu_budget_s=0.0 if args.no_cpu else 10.0)
+                                         cpu_budget_s=10.0 if cpu_legs else 0.0)
         except Exception as exc:      # reported, never required
             phasecorr = {"error": str(exc)[:300]}
 
     tiles = None
     if not args.no_tiles:
         try:
-            tiles = tiles_sample(fb, lib, dev, args.seed + 43 * rank, cpu_budget_s=0.0 if args.no_cpu else 10.0)
+            tiles = tiles_sample(fb, lib, dev, args.seed + 43 * rank, cpu_budget_s=10.0 if cpu_legs else 0.0)
         except Exception as exc:      # reported, never required
             tiles = {"error": str(exc)[:300]}
 
     viewer = None
     if not args.no_viewer:
         try:
-            viewer = viewer_slab_sample(fb, lib, dev, args.seed + 59 * rank, cpu_budget_s=0.0 if args.no_cpu else 5.0)
+            viewer = viewer_slab_sample(fb, lib, dev, args.seed + 59 * rank, cpu_budget_s=5.0 if cpu_legs else 0.0)
         except Exception as exc:      # reported, never required
             viewer = {"error": str(exc)[:300]}
 
