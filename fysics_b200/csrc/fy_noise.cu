@@ -837,17 +837,24 @@ FY_D double pct_small(double* v, int n, double pct) {       // percentile() on <
 
 // stage 0: bin floors; arm the whole-volume fallback when no bin qualifies (mode 2).
 // stage 1: IRLS fit (FP64) and outputs.
-__global__ void k_noise_fit(NoiseCtl* ctl, int stage) {
+// One warp: lane b handles bin b's reads, so the bins' loads are in flight together; the
+// sequential fit then runs on lane 0 from shared memory.
+__global__ void __launch_bounds__(32) k_noise_fit(NoiseCtl* ctl, int stage) {
+    static_assert(NB <= 32, "one lane per bin");
+    const int lane = threadIdx.x;
     if (stage == 0) {
-        int used = 0;
-        for (int b = 0; b < NB; ++b) {
-            const long long c = (long long)ctl->bcount[b];
-            if (c < 200) continue;
-            const double idx = ctl->flat_pct / 100.0 * (double)(c - 1);
-            const long long k = (long long)idx;
-            ctl->bfloor[b] = interp(ctl, b, idx - (double)k, k + 1 < c);
-            ++used;
+        bool use = false;
+        if (lane < NB) {
+            const long long c = (long long)ctl->bcount[lane];
+            if (c >= 200) {
+                const double idx = ctl->flat_pct / 100.0 * (double)(c - 1);
+                const long long k = (long long)idx;
+                ctl->bfloor[lane] = interp(ctl, lane, idx - (double)k, k + 1 < c);
+                use = true;
+            }
         }
+        const int used = __popc(__ballot_sync(0xffffffffu, use));
+        if (lane != 0) return;
         ctl->out_used = used;
         if (used == 0) {                                  // noise.c:166-171
             const long long n = ctl->n;
@@ -861,14 +868,23 @@ __global__ void k_noise_fit(NoiseCtl* ctl, int stage) {
         }
         return;
     }
+    __shared__ double s_i[NB], s_f[NB];
+    __shared__ long long s_c[NB];
+    if (lane < NB) {
+        s_c[lane] = (long long)ctl->bcount[lane];
+        s_i[lane] = 0.5 * (ctl->edge[lane] + ctl->edge[lane + 1]);
+        s_f[lane] = ctl->bfloor[lane];
+    }
+    __syncwarp();
+    if (lane != 0) return;
     double bin_i[NB], bin_f[NB], wv[NB];
     long long bin_c[NB];
     int used = 0;
     for (int b = 0; b < NB; ++b) {
-        if (ctl->bcount[b] < 200) continue;
-        bin_i[used] = 0.5 * (ctl->edge[b] + ctl->edge[b + 1]);
-        bin_f[used] = ctl->bfloor[b];
-        bin_c[used] = (long long)ctl->bcount[b];
+        if (s_c[b] < 200) continue;
+        bin_i[used] = s_i[b];
+        bin_f[used] = s_f[b];
+        bin_c[used] = s_c[b];
         ++used;
     }
     double g = 0, bb = 0;
@@ -1047,7 +1063,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     k_sel_scan<<<NB, 256, 0, st>>>(cc, 8, 1, 1);
     k_bin_finish<<<1, 1, 0, st>>>(ctl, cc);
     k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 1);
-    k_noise_fit<<<1, 1, 0, st>>>(ctl, 0);
+    k_noise_fit<<<1, 32, 0, st>>>(ctl, 0);
     fy_prof_mark(st, "noise.bin_select");
     // 2c. fallback (mode 2 only): flat_pct percentile over all voxels' variance
     for (int i = 0; i < 3; ++i) {
@@ -1056,7 +1072,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
         k_sel_scan<<<1, 256, 0, st>>>(ctl, all_digits[i][1], 2, i == 2);
     }
     k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 2);
-    k_noise_fit<<<1, 1, 0, st>>>(ctl, 1);
+    k_noise_fit<<<1, 32, 0, st>>>(ctl, 1);
     launches += 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 7 + 1 + 15 + 1 + 1 + 7 + 1;
     return cudaGetLastError();
 }
