@@ -12,6 +12,9 @@
 //           sums of both quantities, two float4 stores.
 //   Y phase one thread = one output column x 4 output rows. Its (2R+1)-plane z ring of
 //           XY sums stays in registers and gives the box of plane zi - R to the epilogue.
+// With TMA staging a plane takes one CTA barrier, between the X and Y phases: the X sums
+// alternate between two arrays, and each thread waits on the plane's mbarrier itself.
+// cp.async staging adds a barrier before the X phase (the copies of other threads).
 // The two quantities travel as one float2 through all three window sums, so each tap is
 // one paired FP32 add (__fadd2_rn: two IEEE round-to-nearest adds, the same results as two
 // scalar adds in the same order) and the XY sums are stored and read as pairs.
@@ -73,7 +76,8 @@ struct Geo {
     static constexpr int RW = C * SXW;                           // floats per staged row
     static constexpr int STAGE = (SY * RW + 31) / 32 * 32;      // floats per staged plane (128 B multiple)
     static constexpr int XS = SY * TX;                          // float2 per X-sum array
-    static constexpr size_t bytes = (size_t)(NS * STAGE + 2 * XS + TX + TY) * sizeof(float) + 128;   // + alignment
+    // two X-sum arrays (alternate planes), the reciprocal counts, 128 B for alignment
+    static constexpr size_t bytes = (size_t)(NS * STAGE + 4 * XS + TX + TY) * sizeof(float) + 128;
 };
 
 FY_D float recip_count(int p, int L, int r) {
@@ -197,8 +201,8 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     extern __shared__ float4 zb_smem4[];
     __shared__ __align__(8) unsigned long long bars[NS];
     float* stage = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(zb_smem4) + 127) & ~(uintptr_t)127);
-    float2* xs = reinterpret_cast<float2*>(stage + NS * G::STAGE);   // X sums of both quantities, [SY][TX]
-    float* rx = reinterpret_cast<float*>(xs + G::XS);
+    float2* xs = reinterpret_cast<float2*>(stage + NS * G::STAGE);   // X sums of both quantities, 2 x [SY][TX]
+    float* rx = reinterpret_cast<float*>(xs + 2 * G::XS);
     float* ry = rx + TX;
     const int t = threadIdx.x;
     const int nz = p.nz, ny = p.ny, nx = p.nx;
@@ -213,6 +217,7 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     if (t < TY) ry[t] = y0 + t < ny ? recip_count(y0 + t, ny, R) : 0.f;
     const bool cols_in = x0 - 4 >= 0 && x0 + TX + 4 <= nx;       // no column of the staged rows is outside
     const int zfirst = zs - R, zend = ze + R;
+    int zissued = min(zfirst + NS - 2, zend - 1);                // thread 0: last plane whose copy it issued
     if (TMA) {
         if (t == 0) {
             for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
@@ -267,22 +272,20 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
             const int zi = zi0 + ph;
             if (zi >= zend) break;
             const int slot = (zi - zfirst) & (NS - 1);
+            // TMA: no barrier before the X phase. Every thread passed the previous plane's
+            // barrier, so plane zi - 1's slot is read out (thread 0 refills it) and the X sums
+            // of plane zi - 2, which share this plane's array, are read out.
+            bool ok = true;
+            float2* xcur = xs;
             if (TMA) {
-                const bool ok = mbar_wait_bounded(&bars[slot], (unsigned)(((zi - zfirst) / NS) & 1));
-                if (__syncthreads_or(!ok)) {      // plane zi never landed: flag, drain, return
-                    if (t == 0) {
-                        atomicExch(&zb_timeout, 1);
-                        const int zlast = min(zi + NS - 2, zend - 1);   // loads issued so far
-                        for (int zq = zi; zq <= zlast; ++zq)
-                            mbar_wait_bounded(&bars[(zq - zfirst) & (NS - 1)], (unsigned)(((zq - zfirst) / NS) & 1));
-                    }
-                    __syncthreads();
-                    return;
-                }
-                const int zn = zi + NS - 1;       // plane zi landed for every thread; xs free again
-                if (t == 0 && zn < zend)
+                ok = mbar_wait_bounded(&bars[slot], (unsigned)(((zi - zfirst) / NS) & 1));
+                xcur = xs + ((zi - zfirst) & 1) * G::XS;
+                const int zn = zi + NS - 1;
+                if (t == 0 && ok && zn < zend) {
                     tma_stage<R, C>(stage + ((zn - zfirst) & (NS - 1)) * G::STAGE, tm, &bars[(zn - zfirst) & (NS - 1)],
                                     zn, x0, y0);
+                    zissued = zn;
+                }
             } else {
                 cp_wait<NS - 2>();
                 __syncthreads();             // plane zi landed for every thread; xs free again
@@ -350,16 +353,28 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                     if (out_kind(KIND)) sm = mul2(sm, rx[x4 + k]);
                     o[k] = sm;
                 }
-                float4* dst = reinterpret_cast<float4*>(xs + yy * TX + x4);
+                float4* dst = reinterpret_cast<float4*>(xcur + yy * TX + x4);
                 dst[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
                 dst[1] = make_float4(o[2].x, o[2].y, o[3].x, o[3].y);
             }
-            __syncthreads();
+            if (TMA) {
+                if (__syncthreads_or(!ok)) {      // plane zi never landed: flag, drain, return
+                    if (t == 0) {
+                        atomicExch(&zb_timeout, 1);
+                        for (int zq = zi; zq <= zissued; ++zq)          // loads issued so far
+                            mbar_wait_bounded(&bars[(zq - zfirst) & (NS - 1)], (unsigned)(((zq - zfirst) / NS) & 1));
+                    }
+                    __syncthreads();
+                    return;
+                }
+            } else {
+                __syncthreads();
+            }
             // Y phase -> ring slot ph
             {
                 float2 a[4 + 2 * R];
 #pragma unroll
-                for (int j = 0; j < 4 + 2 * R; ++j) a[j] = xs[(4 * rg + j) * TX + xc];
+                for (int j = 0; j < 4 + 2 * R; ++j) a[j] = xcur[(4 * rg + j) * TX + xc];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     float2 sm = a[k];
