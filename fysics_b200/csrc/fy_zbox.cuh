@@ -9,7 +9,8 @@
 //           copy (TMA) per plane, completing on the slot's mbarrier. Other shapes: cp.async
 //           by all threads.
 //   X phase one item = 4 output columns of one staged row: the row's values, the window
-//           sums of both quantities, two float4 stores.
+//           sums of both quantities, two float4 stores; TY x TX/4 = 256 items, one per
+//           thread. The 2R halo rows go as one-column items, spread over all threads.
 //   Y phase one thread = one output column x 4 output rows. Its (2R+1)-plane z ring of
 //           XY sums stays in registers and gives the box of plane zi - R to the epilogue.
 // With TMA staging a plane takes one CTA barrier, between the X and Y phases: the X sums
@@ -304,8 +305,8 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
             }
             const float* sp = stage + slot * G::STAGE;
             const bool zin = zi >= 0 && zi < nz;
-            // X phase: P[j] = both quantities of staged column x0 - 4 + x4 + j
-            for (int it = t; it < G::SY * (TX / 4); it += NT) {
+            // X phase, output rows 0 .. TY-1: P[j] = both quantities of staged column x0 - 4 + x4 + j
+            for (int it = t; it < TY * (TX / 4); it += NT) {
                 const int yy = it >> 4, x4 = (it & 15) << 2;
                 float2 P[12];
                 if (C == 2) {                    // interleaved pairs: float4 = two columns
@@ -356,6 +357,33 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                 float4* dst = reinterpret_cast<float4*>(xcur + yy * TX + x4);
                 dst[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
                 dst[1] = make_float4(o[2].x, o[2].y, o[3].x, o[3].y);
+            }
+            // X phase, the 2R halo rows: one output column per item, spread over the whole CTA
+            // (one item per thread at R = 2), with the same taps in the same order as above
+            for (int q = t; q < 2 * R * TX; q += NT) {
+                const int yy = TY + (q >> 6), xo = q & (TX - 1);
+                const int gy = y0 - R + yy;
+                const bool rin = zin && gy >= 0 && gy < ny;
+                auto tap = [&](int m) {                  // staged column xo + 4 - R + m
+                    const int col = xo + 4 - R + m;
+                    if (C == 2) {
+                        const float2 v = *reinterpret_cast<const float2*>(sp + yy * G::RW + 2 * col);
+                        return KIND == ZB_GUIDED_OUT_MV ? guided_ab(v, eps) : v;
+                    }
+                    float q1 = sp[yy * G::RW + col];
+                    if (cols_in) {
+                        q1 = q1 - (rin ? c : 0.f);
+                    } else {
+                        const int gxj = x0 - 4 + col;
+                        q1 = (rin && gxj >= 0 && gxj < nx) ? q1 - c : 0.f;
+                    }
+                    return make_float2(q1, q1 * q1);
+                };
+                float2 sm = tap(0);
+#pragma unroll
+                for (int m = 1; m <= 2 * R; ++m) sm = add2(sm, tap(m));
+                if (out_kind(KIND)) sm = mul2(sm, rx[xo]);
+                xcur[yy * TX + xo] = sm;
             }
             if (TMA) {
                 if (__syncthreads_or(!ok)) {      // plane zi never landed: flag, drain, return
