@@ -142,20 +142,6 @@ struct WarpCands {
         cnt = 0;
         __syncwarp();
     }
-    // every lane of the warp calls
-    FY_D void add(bool take, float val, uint8_t label, float* __restrict__ cval, uint8_t* __restrict__ clab,
-                  unsigned long long* ncand, long long cap) {
-        const unsigned bal = __ballot_sync(0xffffffffu, take);
-        if (!bal) return;
-        const int lane = threadIdx.x & 31;
-        if (take) {
-            const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
-            v[pos] = val;
-            l[pos] = label;
-        }
-        cnt += __popc(bal);
-        if (cnt > kWarpBuf - 32) flush(cval, clab, ncand, cap);
-    }
 };
 
 // Streaming passes read SU float4 (and uchar4 bin labels) per thread before using any, so
