@@ -157,8 +157,9 @@ def algorithmic_bytes(name: str, n: int, geo: dict) -> float | None:
     return table.get(name)
 
 
-# DRAM bytes per voxel of each instrumented span, from a one-pass ncu capture of the 512^3
-# chain (dram__bytes_read.sum + dram__bytes_write.sum per launch; profiles/dram_restore_512.md).
+# DRAM bytes per voxel of each instrumented span: dram__bytes_read.sum + dram__bytes_write.sum
+# per launch from a one-pass ncu capture of this chain, divided by the voxels of the captured
+# cube (the spans' traffic grows with the voxel count).
 DRAM_BYTES_PER_VOXEL = {
     "deconv.x_fwd": 4.653, "deconv.y_fwd": 8.031, "deconv.z_weight": 8.290, "deconv.y_inv": 8.031,
     "deconv.x_inv": 7.880, "noise.stats": 19.647, "noise.lohi": 4.402, "noise.bin_select": 23.931,
@@ -178,55 +179,118 @@ def read_profile(lib):
 
 
 # ------------------------------------------------------------------------------ CPU legs
-def cpu_reference_sample(u8_host: np.ndarray, steps: int = 1, crop: int = 128, budget_s: float = 20.0):
-    """The reference CPU chain on crops of the benchmark cube, one crop per host thread
-    (the reference's own tile parallelism, pipeline.c:1008-1020); returns Mvox/s."""
-    import oracle
+def chain_spec(db_scale: float):
+    """The benchmark chain's settings for the CPU chain runner (oracle.chain): the same
+    physics, deconvolution, noise, guided and ring settings as restore_cfg()."""
+    from oracle.chain import ChainSpec
+    phys = dict(delta_beta=500.0 * db_scale, energy_kev=110.0, distance_mm=1200.0, pixel_um=2.4, unsharp_sigma=0.8,
+                unsharp_coeff=0.5, psf_sigma_vox=1.0, psf_sigma_z_vox=1.17)
+    return ChainSpec(phys=phys, matched=True, deconv_param=0.05, noise_win=5, noise_pct=10.0, noise_ref=0.4,
+                     guided_r=2, dering=dict(ss=2, hp_win=15, min_cnt=100, min_amp=0.5, max_amp=6.0, slab_z=512,
+                                             ns=8))
+
+
+def host_memory_bytes() -> int | None:
+    """Memory this process may still use on the host: MemAvailable, capped by a cgroup limit."""
+    avail = None
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemAvailable:"):
+                avail = int(ln.split()[1]) * 1024
+    except OSError:
+        pass
+    try:
+        lim = open("/sys/fs/cgroup/memory.max").read().strip()
+        if lim != "max":
+            used = int(open("/sys/fs/cgroup/memory.current").read().strip())
+            room = int(lim) - used
+            avail = room if avail is None else min(avail, room)
+    except (OSError, ValueError):
+        pass
+    return avail
+
+
+# Peak host memory of one reference chain per voxel: the noise model's three double fields,
+# its float squares, the sorted copy of the means and qsort's merge buffer (44 B), plus the
+# chain's float volumes (dewindowed, deconvolved, output) alive meanwhile; rounded up.
+REF_CHAIN_BYTES_PER_VOXEL = 64
+
+
+def cpu_reference_chain(u8_host: np.ndarray, spec, threads: int | None = None, warmup: int = 3,
+                        keep_output: bool = True) -> dict:
+    """The reference's chain (oracle/_ref, compiled from its own sources) on the WHOLE
+    benchmark cube: one chain per host thread, each thread restoring its own copy of the
+    same cube -- the reference's own parallelism, one tile or cube chain per worker
+    (pipeline.c:1008-1020); its entry points are single-threaded per call. The thread count
+    is the host's cores, or fewer where host memory holds fewer chains at once. Warm-up: the
+    same chain on a 128^3 corner crop, `warmup` times per thread. Returns Mvox/s over the
+    timed cubes, their count (the steps) and one thread's output for the error check."""
     from concurrent.futures import ThreadPoolExecutor
-    L = oracle.ref()
+    from oracle.chain import ref_restore
+    n = u8_host.size
     cores = os.cpu_count() or 1
-    phys = oracle.ref_physics(delta_beta=500.0 * 0.35, energy_kev=110.0, distance_mm=1200.0, pixel_um=2.4,
-                              unsharp_sigma=0.8, unsharp_coeff=0.5, psf_sigma_vox=1.0, psf_sigma_z_vox=1.17)
-    nz = u8_host.shape[0] // crop
-    crops = [(z, y, x) for z in range(nz) for y in range(u8_host.shape[1] // crop) for x in range(u8_host.shape[2] // crop)]
+    mem = host_memory_bytes()
+    by_mem = max(1, int(0.8 * mem) // (REF_CHAIN_BYTES_PER_VOXEL * n)) if mem else 1
+    nthr = threads or max(1, min(cores, by_mem))
+    crop = np.ascontiguousarray(u8_host[:128, :128, :128])
+    with ThreadPoolExecutor(max_workers=nthr) as ex:
+        for _ in range(warmup):
+            list(ex.map(lambda i: ref_restore(crop, spec, keep_stages=False), range(nthr)))
+    kept = {}
+    per = [0.0] * nthr
+
+    def one(i):
+        t0 = time.perf_counter()
+        r = ref_restore(u8_host, spec, keep_stages=False)
+        per[i] = time.perf_counter() - t0
+        if i == 0 and keep_output:
+            kept.update(out=r["out"], noise_ref=r["noise"].noise_ref, detected=r["detected"])
+        return r["detected"]
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=nthr) as ex:
+        detected = list(ex.map(one, range(nthr)))
+    wall = time.perf_counter() - t0
+    shape = "x".join(map(str, u8_host.shape))
+    res = {"value": nthr * n / wall / 1e6, "unit": "Mvoxel/s", "cores": nthr, "kind": "reference",
+           "cubes": nthr, "wall_s": wall, "ms_per_cube_single_thread": 1e3 * min(per),
+           "sample": f"{nthr} full {shape} chains of the benchmark cube, one per host thread ({cores} cores, "
+                     f"{nthr} threads, host memory {mem / 2**30:.0f} GiB free)" if mem else
+                     f"{nthr} full {shape} chains of the benchmark cube, one per host thread ({cores} cores)",
+           "warmup": f"{warmup} chains on a 128^3 corner crop per thread",
+           "detected_rings": detected[0]}
+    if keep_output:
+        res["_out"] = kept
+    return res
+
+
+def cpu_reference_crops(u8_host: np.ndarray, spec, crop: int = 128, budget_s: float = 10.0) -> dict:
+    """Secondary figure: the reference chain on 128^3 crops of the cube, one crop per host
+    thread. Each crop votes its own rings about its own centre and runs crop-sized FFTs and
+    sorts, so this is not the benchmark's configuration."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle.chain import ref_restore
+    cores = os.cpu_count() or 1
+    crops = [(z, y, x) for z in range(u8_host.shape[0] // crop) for y in range(u8_host.shape[1] // crop)
+             for x in range(u8_host.shape[2] // crop)]
 
     def one(i):
         z, y, x = crops[i % len(crops)]
         sub = np.ascontiguousarray(u8_host[z * crop:(z + 1) * crop, y * crop:(y + 1) * crop, x * crop:(x + 1) * crop])
-        n = sub.size
-        f = np.empty(sub.shape, np.float32)
-        L.fy_u8_to_phys(oracle.p(sub), oracle.p(f), n, 0.0, 1.0)
-        d = np.empty_like(f)
-        L.fy_deconvolve_matched(oracle.p(f), oracle.p(d), crop, crop, crop, C.byref(phys), 0.05)
-        nm = oracle.RefNoise()
-        L.fy_estimate_noise(oracle.p(d), crop, crop, crop, 5, 10.0, 0.4, C.byref(nm))
-        eps = L.fy_guided_eps_for_noise(nm.noise_ref)
-        ws = np.empty(4 * n, np.float32)
-        out = np.empty_like(f)
-        L.fy_guided_denoise_ws(oracle.p(d), oracle.p(out), crop, crop, crop, 2, eps, oracle.p(ws))
-        dr, dt = oracle.RefDering(), oracle.RefDering()
-        L.fy_dering_init(C.byref(dr), crop, crop, crop, -1, -1, 512, 8)
-        L.fy_dering_tile_init(C.byref(dt), C.byref(dr))
-        L.fy_dering_accumulate_u8(C.byref(dt), oracle.p(sub), 0, 0, crop, crop, crop, 2)
-        L.fy_dering_merge_tile(C.byref(dr), 0, C.byref(dt))
-        L.fy_dering_finalize(C.byref(dr), 15, 100, 0.5, 6.0)
-        L.fy_dering_apply(C.byref(dr), oracle.p(out), 0, 0, 0, crop, crop, crop, 1.0 / 255.0)
-        L.fy_dering_free(C.byref(dt)); L.fy_dering_free(C.byref(dr))
-        return n
+        ref_restore(sub, spec, keep_stages=False)
+        return sub.size
 
     t0 = time.perf_counter()
-    one(0)                                                  # calibrate one crop, 1 thread
+    one(0)
     t_one = time.perf_counter() - t0
-    per_thread = max(1, int(budget_s / max(t_one, 1e-3)))
-    jobs = cores * max(1, min(per_thread, 4)) * steps
+    jobs = cores * max(1, min(int(budget_s / max(t_one, 1e-3)), 4))
     t0 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=cores) as ex:
         vox = sum(ex.map(one, range(jobs)))
     dt = time.perf_counter() - t0
-    return {"value": vox / dt / 1e6, "unit": "Mvoxel/s", "cores": cores, "kind": "reference",
-            "sample": f"{jobs} crops of {crop}^3 from the benchmark cube, one per host thread "
-                      f"({cores} threads), reference compiled from its sources; {dt:.1f} s wall; "
-                      f"single-thread latency {t_one * 1e3:.0f} ms per {crop}^3 crop"}
+    return {"value": vox / dt / 1e6, "unit": "Mvoxel/s", "cores": cores,
+            "sample": f"{jobs} crops of {crop}^3, one per host thread; not the benchmark configuration (each crop "
+                      f"votes its own rings, crop-sized FFTs and sorts); single-thread {t_one * 1e3:.0f} ms per crop"}
 
 
 # ------------------------------------------------------------------------------ serving
@@ -508,6 +572,40 @@ def tiles_sample(fb, lib, dev, seed, threads=8, passes=3, cpu_budget_s=10.0):
                                          *vyx, C.c_void_p(d_outs[wid].data_ptr()), C.byref(air),
                                          C.c_void_p(streams[wid].cuda_stream))
 
+    # the same band as a local zarr v2 tree of 128^3 chunks (the export's chunking), read through
+    # fy_process_chunk: chunk files -> pinned -> device chunk cache -> GPU assembly -> tile chain
+    import shutil
+    import tempfile
+    zdir = tempfile.mkdtemp(prefix="fy_band_")
+    zroot = Path(zdir) / "band.zarr"
+    (zroot / "0").mkdir(parents=True)
+    (zroot / "0" / ".zarray").write_text(
+        '{"chunks":[128,128,128],"compressor":null,"dtype":"|u1","fill_value":0,"order":"C",'
+        f'"shape":[{vol.shape[0]},{vol.shape[1]},{vol.shape[2]}],"zarr_format":2,"dimension_separator":"/"}}')
+    for cz in range(-(-vol.shape[0] // 128)):
+        for cy in range(-(-vol.shape[1] // 128)):
+            for cx in range(-(-vol.shape[2] // 128)):
+                d = zroot / "0" / str(cz) / str(cy)
+                d.mkdir(parents=True, exist_ok=True)
+                (d / str(cx)).write_bytes(np.ascontiguousarray(
+                    vol[cz * 128:(cz + 1) * 128, cy * 128:(cy + 1) * 128, cx * 128:(cx + 1) * 128]).tobytes())
+    zin = fb.Zarr()
+    fb.check(lib.fy_zarr_open(C.byref(zin), str(zroot).encode()), "fy_zarr_open")
+    zouts = [np.empty((T, T, T), np.uint8) for _ in range(len(tiles))]
+
+    def zarr_work(wid, k):
+        k = k % len(tiles)
+        z0, y0, x0 = tiles[k][2][:3]
+        dims = [C.c_int() for _ in range(3)]
+        air = C.c_int()
+        return lib.fy_process_chunk(C.byref(zin), C.byref(cfg), z0, y0, x0, T, zouts[k].ctypes.data,
+                                    *[C.byref(v) for v in dims], C.byref(air))
+
+    def cache_stats():
+        v = [C.c_ulonglong() for _ in range(3)]
+        lib.fy_gpu_zarr_cache_stats(*[C.byref(x) for x in v])
+        return [x.value for x in v]
+
     n_items = passes * len(tiles)
     pool = WorkerPool(threads, lib)
     try:
@@ -517,8 +615,15 @@ def tiles_sample(fb, lib, dev, seed, threads=8, passes=3, cpu_budget_s=10.0):
         pool.run_each(dev_work)
         pool.run(dev_work, len(tiles))
         t_dev = pool.run(dev_work, n_items)
+        s0 = cache_stats()
+        t_zcold = pool.run(zarr_work, len(tiles))      # first pass: every chunk file read once
+        s1 = cache_stats()
+        pool.run_each(zarr_work)
+        t_zarr = pool.run(zarr_work, n_items)
+        s2 = cache_stats()
     finally:
         pool.close()
+        shutil.rmtree(zdir, ignore_errors=True)
     res = {"workload": "16 tiles of 128^3 (8-voxel halo, 144^3 u8 buffers) from a synthetic 144x528x528 scroll "
                        "band; export settings: no deconvolution, guided eps 8e-4 subsample 2, air cut, despeckle "
                        "< 64 voxels, recenter [40, 200], dithered u8",
@@ -526,7 +631,16 @@ def tiles_sample(fb, lib, dev, seed, threads=8, passes=3, cpu_budget_s=10.0):
            "e2e": {"tiles_per_s": n_items / t_host, "mvox_per_s": n_items * inner_vox / t_host / 1e6,
                    "ms_per_tile": t_host * 1e3 / n_items, "api": "fy_process_buffer, pageable host buffers"},
            "resident": {"tiles_per_s": n_items / t_dev, "mvox_per_s": n_items * inner_vox / t_dev / 1e6,
-                        "ms_per_tile": t_dev * 1e3 / n_items, "api": "fy_gpu_process_buffer, one stream per thread"}}
+                        "ms_per_tile": t_dev * 1e3 / n_items, "api": "fy_gpu_process_buffer, one stream per thread"},
+           "zarr": {"tiles_per_s": n_items / t_zarr, "mvox_per_s": n_items * inner_vox / t_zarr / 1e6,
+                    "ms_per_tile": t_zarr * 1e3 / n_items, "first_pass_ms_per_tile": t_zcold * 1e3 / len(tiles),
+                    "chunk_files_read_first_pass": s1[1] - s0[1], "bytes_read_first_pass": s1[2] - s0[2],
+                    "chunk_cache_hits_timed": s2[0] - s1[0], "chunk_files_read_timed": s2[1] - s1[1],
+                    "haloed_bytes_assembled_per_tile": int(np.prod(tiles[0][0].shape)),
+                    "outputs_equal_fy_process_buffer": all(np.array_equal(zouts[k], outs[k]) for k in range(len(tiles))),
+                    "api": "fy_process_chunk on a local zarr v2 tree of 128^3 chunk files (same band): chunk files "
+                           "read whole into pinned memory, kept in the device chunk cache, haloed tile assembled on "
+                           "the GPU, then the tile chain; the first pass reads every chunk file once"}}
     try:
         import oracle
         from concurrent.futures import ThreadPoolExecutor
@@ -737,28 +851,50 @@ def job_mvox_per_s(world: int, vox_per_rank: int, steps: int, total_ms: float) -
     return world * vox_per_rank * steps / (total_ms * 1e-3) / 1e6
 
 
+def bench_config(db_scale: float, world: int) -> dict:
+    """The workload's description; both arms print the same one."""
+    return {"workload": WORKLOAD, "cube": f"{SHAPE[0]}^3 u8", "deltabeta_scale": db_scale,
+            "l2": "inputs and working set (~3 GB) larger than the 126 MB L2",
+            "parallelism": f"replicas x{world} (one cube per GPU, no collective)"}
+
+
+def benchmark_cube(args, rank: int, delta_beta: float, device: str):
+    """The benchmark's seeded phantom cube (the same in both arms: same seed, recipe, device)."""
+    import fysics_b200.phantom as ph
+    return ph.phantom(SHAPE, seed=args.seed + rank, delta_beta=delta_beta, energy_kev=110.0, distance_mm=1200.0,
+                      pixel_um=2.4, unsharp_sigma=0.8, unsharp_coeff=0.5, fz2_scale=1.17 ** 2, rings=40,
+                      device=device)
+
+
 def run_reference(args, rank, world):
+    """The reference's own CPU chain on the benchmark cube (rank 0 only; the other ranks exit)."""
     if rank != 0:
         return
-    import fysics_b200.phantom as ph
     import oracle
     if not oracle.have_ref():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfysics_ref.so not built"}))
         return
-    u8 = ph.phantom(SHAPE, seed=args.seed, delta_beta=500.0 * 0.35, pixel_um=2.4, fz2_scale=1.17 ** 2,
-                    rings=40, device="cpu") if args.cpu_phantom else None
-    if u8 is None:
-        import torch
-        dev = "cuda" if torch.cuda.is_available() else "cpu"
-        u8 = ph.phantom(SHAPE, seed=args.seed, delta_beta=500.0 * 0.35, pixel_um=2.4, fz2_scale=1.17 ** 2,
-                        rings=40, device=dev).cpu().numpy()
-    res = cpu_reference_sample(u8, steps=1, budget_s=args.cpu_budget)
-    n = int(np.prod(SHAPE))
+    rph = oracle.ref_physics(delta_beta=500.0, energy_kev=110.0, distance_mm=1200.0, pixel_um=2.4, unsharp_sigma=0.8,
+                             unsharp_coeff=0.5, psf_sigma_vox=1.0, psf_sigma_z_vox=1.17)
+    db_scale = oracle.ref().fy_auto_deltabeta_scale(C.byref(rph))
+    import torch
+    dev = "cuda" if torch.cuda.is_available() and not args.cpu_phantom else "cpu"
+    u8 = benchmark_cube(args, 0, 500.0 * db_scale, dev)
+    u8 = u8.cpu().numpy() if hasattr(u8, "cpu") else u8
+    spec = chain_spec(db_scale)
+    res = cpu_reference_chain(u8, spec, threads=args.cpu_threads, warmup=args.warmup, keep_output=False)
+    try:
+        res["crops_128"] = cpu_reference_crops(u8, spec, budget_s=10.0)
+    except Exception as exc:          # secondary figure, reported only
+        res["crops_128"] = {"error": str(exc)[:200]}
     line = {"metric": METRIC, "value": res["value"], "unit": "Mvoxel/s", "impl": "reference",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": n / (res["value"] * 1e6) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "n_gpus": world, "steps": res["cubes"], "warmup": args.warmup,
+            "ms_per_step": res["wall_s"] * 1e3 / res["cubes"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cube": "512^3", "l2": "working set > L2"},
+            "config": bench_config(db_scale, world),
+            "timing": f"{res['cubes']} cubes restored concurrently, one per host thread, in {res['wall_s']:.1f} s "
+                      "wall (steps = cubes timed, ms_per_step = wall / cubes); warm-up: "
+                      f"{args.warmup} chains of a 128^3 crop per thread",
             "cpu_baseline": res,
             "e2e": {"value": res["value"], "unit": "Mvoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -772,7 +908,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
-    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cpu-threads", type=int, default=None,
+                    help="host threads of the reference chain (default: cores, bounded by host memory)")
     ap.add_argument("--cpu-phantom", action="store_true")
     ap.add_argument("--size", type=int, default=512, help="cube edge (512 = the benchmark workload)")
     ap.add_argument("--no-serve", action="store_true", help="skip the served / batched samples")
@@ -800,9 +937,7 @@ def main():
     fb.check(lib.fy_gpu_init(dev), "fy_gpu_init")
     torch.cuda.set_device(dev)
     p, db_scale = physics_for(fb)
-    u8 = ph.phantom(SHAPE, seed=args.seed + rank, delta_beta=p.delta_beta, energy_kev=p.energy_kev,
-                    distance_mm=p.distance_mm, pixel_um=p.pixel_um, unsharp_sigma=p.unsharp_sigma,
-                    unsharp_coeff=p.unsharp_coeff, fz2_scale=1.17 ** 2, rings=40, device=f"cuda:{dev}")
+    u8 = benchmark_cube(args, rank, p.delta_beta, f"cuda:{dev}")
     nz, ny, nx = SHAPE
     n = nz * ny * nx
     out = torch.empty(SHAPE, dtype=torch.float32, device=f"cuda:{dev}")
@@ -939,16 +1074,27 @@ def main():
         tpv = DRAM_BYTES_PER_VOXEL.get(dom)
         roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                 "frac": ach / hbm_peak, "traffic": tpv * n if tpv is not None and SHAPE == (512, 512, 512) else None,
-                "traffic_source": "ncu one-pass capture of the 512^3 chain (profiles/dram_restore_512.md)",
+                "traffic_source": "ncu one-pass DRAM capture of the chain, bytes per voxel x voxels",
                 "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": algorithmic_bytes(dom, n, geo)}
 
-    cpu = None
+    # ---- the reference's chain on the same cube (host cores), and the benchmark output's
+    # error against it: `out` holds the last timed step's result (the chain is deterministic)
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             import oracle
             if oracle.have_ref():
-                cpu = cpu_reference_sample(u8.cpu().numpy(), budget_s=args.cpu_budget)
+                cpu = cpu_reference_chain(u8.cpu().numpy(), chain_spec(db_scale), threads=args.cpu_threads,
+                                          warmup=args.warmup)
+                ref_out = cpu.pop("_out")
+                got = out.cpu().numpy()
+                err = np.abs(got - ref_out["out"])
+                parity = {"against": "the reference's chain on the same cube (oracle/_ref)",
+                          "max_abs_err": float(err.max()), "mean_abs_err": float(err.mean()),
+                          "window_range": 1.0, "bar": 1e-4, "within_bar": bool(err.max() <= 1e-4),
+                          "detected_rings_ref": ref_out["detected"], "noise_ref_ref": ref_out["noise_ref"]}
+                del got, err, ref_out
         except Exception as exc:       # the baseline is reported, never required
             cpu = {"value": None, "error": str(exc)[:200]}
 
@@ -989,9 +1135,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "Mvoxel/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "cube": f"{SHAPE[0]}^3 u8", "deltabeta_scale": db_scale,
-                   "l2": "inputs and working set (~3 GB) larger than the 126 MB L2",
-                   "parallelism": f"replicas x{world} (one cube per GPU, no collective)"},
+        "config": bench_config(db_scale, world),
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "e2e_p50": float(np.percentile(e2e_steps_ms, 50)),
                        "e2e_p99": float(np.percentile(e2e_steps_ms, 99))},
@@ -1001,6 +1145,7 @@ def main():
         "kernels": kernels,
         "clocks": clock,
         "cpu_baseline": cpu,
+        "parity": parity,
         "served": served,
         "batched": batched,
         "phasecorr": phasecorr,

@@ -14,7 +14,7 @@ PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libfysics_b200.so"
 
 FY_OK, FY_EINVAL, FY_ENOMEM, FY_ECUDA, FY_ENODEV = 0, 1, 2, 3, 4
-FY_EUNSUPPORTED, FY_ETIMEDOUT, FY_EBUSY, FY_EDEGENERATE = 5, 6, 7, 8
+FY_EUNSUPPORTED, FY_ETIMEDOUT, FY_EBUSY, FY_EDEGENERATE, FY_EIO = 5, 6, 7, 8, 9
 
 
 class Physics(C.Structure):
@@ -116,6 +116,11 @@ class Dering(C.Structure):
                 ("ring", C.POINTER(C.c_float)), ("have_rings", C.c_int)]
 
 
+class Zarr(C.Structure):
+    """fy_zarr (fysics.h:376-381)."""
+    _fields_ = [("root", C.c_char * 1024), ("shape", C.c_long * 3), ("chunk", C.c_long * 3), ("fill", C.c_ubyte)]
+
+
 _P = C.c_void_p
 _i, _l, _d, _f, _sz = C.c_int, C.c_long, C.c_double, C.c_float, C.c_size_t
 _PP = C.POINTER(Physics)
@@ -179,6 +184,14 @@ SIGNATURES = {
     "fy_gpu_process_buffer": (_i, [C.POINTER(PipelineCfg), _P, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l,
                                    _l, _P, C.POINTER(_i), _P]),
     "fy_process_buffer_air_state": (_i, [_P, _P]),
+    "fy_zarr_open": (_i, [C.POINTER(Zarr), C.c_char_p]),
+    "fy_zarr_read": (_i, [C.POINTER(Zarr), _l, _l, _l, _l, _l, _l, _P]),
+    "fy_process_chunk": (_i, [C.POINTER(Zarr), C.POINTER(PipelineCfg), _l, _l, _l, _i, _P, C.POINTER(_i),
+                              C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
+    "fy_gpu_zarr_read": (_i, [C.POINTER(Zarr), _l, _l, _l, _l, _l, _l, _P, _P]),
+    "fy_gpu_zarr_cache_limit": (_i, [_sz]),
+    "fy_gpu_zarr_cache_stats": (None, [C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong),
+                                       C.POINTER(C.c_ulonglong)]),
     # ---- fy_gpu_* extension
     "fy_gpu_init": (_i, [_i]),
     "fy_gpu_last_status": (_i, []),
@@ -186,6 +199,7 @@ SIGNATURES = {
     "fy_gpu_release": (None, []),
     "fy_gpu_kernel_launches": (C.c_ulonglong, []),
     "fy_gpu_kernel_timeouts": (_i, []),
+    "fy_gpu_test_box_first_wait": (_i, [_i]),
     "fy_gpu_u8_to_phys": (_i, [_P, _P, _sz, _d, _d, _P]),
     "fy_gpu_phys_to_u8": (_i, [_P, _P, _sz, _d, _d, _P]),
     "fy_gpu_deconvolve_ex": (_i, [_P, _i, _d, _d, _P, _i, _i, _i, _PP, _d, _i, _d, _P]),

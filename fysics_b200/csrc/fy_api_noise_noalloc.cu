@@ -36,25 +36,37 @@ constexpr size_t kFieldFloats = 2 * round64(kMaxVoxels) + round64((kMaxVoxels + 
 constexpr size_t kScratchBytes = kCtlBytes + kFieldFloats * sizeof(float);
 static_assert(kCtlBytes % 256 == 0, "fields must start 256-byte aligned");
 
+static_assert(kScratchBytes == FY_NOISE_NOALLOC_SCRATCH_BYTES, "the header states the array's exact size");
+
 static __device__ __align__(256) unsigned char g_noise_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-void* g_addr[kMaxDevices];   // device address of g_noise_scratch, per device
+void* g_addr[kMaxDevices];   // last resolved device address of g_noise_scratch, per device
 
-// Set-up, once per device with that device current: the host-side name g_noise_scratch
-// is only a handle, so the device address comes from cudaGetSymbolAddress.
-int scratch_on(int dev, void** out, const char* what) {
+// The host-side name g_noise_scratch is only a handle, so the device address comes from
+// cudaGetSymbolAddress, with the device current. It is resolved again on every call that is
+// not being captured: a device reset or a new primary context reloads the module, and the
+// array can then sit at another address. A call made while `st` is capturing cannot resolve
+// (module loading is not a stream operation), so it uses the address of the latest
+// uncaptured call on this device, and fails if there was none.
+int scratch_on(int dev, cudaStream_t st, void** out, const char* what) {
     if (dev < 0 || dev >= kMaxDevices) return fail(FY_EUNSUPPORTED, "%s: device %d out of range", what, dev);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) return fail_cuda(e, what);
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noise_scratch);
-        if (e != cudaSuccess) return fail_cuda(e, what);
-        if (!p || ((uintptr_t)p & 255)) return fail(FY_ECUDA, "%s: scratch address %p not 256-byte aligned", what, p);
-        g_addr[dev] = p;
+    if (cap != cudaStreamCaptureStatusNone) {
+        if (!g_addr[dev])
+            return fail(FY_EINVAL, "%s: the first call on device %d must come before any stream capture", what, dev);
+        *out = g_addr[dev];
+        return FY_OK;
     }
-    *out = g_addr[dev];
+    void* p = nullptr;
+    if ((e = cudaGetSymbolAddress(&p, g_noise_scratch)) != cudaSuccess) return fail_cuda(e, what);
+    if (!p || ((uintptr_t)p & 255)) return fail(FY_ECUDA, "%s: scratch address %p not 256-byte aligned", what, p);
+    g_addr[dev] = p;
+    *out = p;
     return FY_OK;
 }
 
@@ -66,6 +78,9 @@ extern "C" int fy_gpu_estimate_noise_noalloc(const float* d_in, int nz, int ny, 
     fy::enter();
     const char* what = "fy_gpu_estimate_noise_noalloc";
     if (!d_in || !d_model) return fail(FY_EINVAL, "%s: null pointer", what);
+    // the model is written as doubles, eps as one float: misaligned pointers would fault
+    if (((uintptr_t)d_model & 7) || ((uintptr_t)d_eps & 3))
+        return fail(FY_EINVAL, "%s: d_model must be 8-byte and d_eps 4-byte aligned", what);
     if (nz < 1 || ny < 1 || nx < 1) return fail(FY_EINVAL, "%s: bad dims", what);
     if (win < 3) win = 5;                                         // noise.c:79-80
     if (flat_pct <= 0) flat_pct = 10.0;
@@ -81,11 +96,11 @@ extern "C" int fy_gpu_estimate_noise_noalloc(const float* d_in, int nz, int ny, 
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) { cudaGetLastError(); return fail(FY_ENODEV, "%s: no CUDA device (%s)", what, cudaGetErrorString(e)); }
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return fail_cuda(e, what);
+    cudaStream_t st = (cudaStream_t)stream;
     void* base = nullptr;
-    int rc = scratch_on(dev, &base, what);
+    int rc = scratch_on(dev, st, &base, what);
     if (rc) return rc;
 
-    cudaStream_t st = (cudaStream_t)stream;
     void* ctl = base;
     float* fields = (float*)((char*)base + kCtlBytes);
     if ((e = cudaMemsetAsync(ctl, 0, fy_noise_ctl_bytes(), st)) != cudaSuccess) return fail_cuda(e, what);

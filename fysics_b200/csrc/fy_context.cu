@@ -203,6 +203,14 @@ int fy_gpu_kernel_timeouts(void) {
     const int a = fy_guided_wait_timeouts(), b = fy_noise_wait_timeouts();
     return a < 0 || b < 0 ? -1 : a + b;
 }
+int fy_gpu_test_box_first_wait(int polls) {
+    fy::enter();
+    int rc = fy::ensure_ctx();
+    if (rc) return rc;
+    cudaError_t e = fy_guided_set_first_wait_polls(polls);
+    if (e == cudaSuccess) e = fy_noise_set_first_wait_polls(polls);
+    return e == cudaSuccess ? FY_OK : fy::fail_cuda(e, "fy_gpu_test_box_first_wait");
+}
 void fy_gpu_release(void) {
     fy::ThreadCtx& c = fy::ctx();
     if (c.st) cudaStreamSynchronize(c.st);

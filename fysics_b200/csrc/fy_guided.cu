@@ -232,3 +232,4 @@ cudaError_t fy_launch_box_mean(const float* in, float* out, float* tmp, int nz, 
 
 // Bounded waits of this unit's box passes that expired (see fy_zbox.cuh); 0 expected.
 int fy_guided_wait_timeouts() { return fyzb::timeouts(); }
+cudaError_t fy_guided_set_first_wait_polls(int polls) { return fyzb::set_first_wait_polls(polls); }

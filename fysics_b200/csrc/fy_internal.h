@@ -152,3 +152,5 @@ int fy_restore_reserve(int nz, int ny, int nx);
 void fy_tile_release();
 int fy_guided_wait_timeouts();
 int fy_noise_wait_timeouts();
+cudaError_t fy_guided_set_first_wait_polls(int polls);
+cudaError_t fy_noise_set_first_wait_polls(int polls);

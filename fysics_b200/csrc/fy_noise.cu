@@ -1098,3 +1098,4 @@ cudaError_t fy_noise_store(const void* ctl_mem, void* d_model, float* d_eps, cud
 
 // Bounded waits of this unit's box passes that expired (see fy_zbox.cuh); 0 expected.
 int fy_noise_wait_timeouts() { return fyzb::timeouts(); }
+cudaError_t fy_noise_set_first_wait_polls(int polls) { return fyzb::set_first_wait_polls(polls); }

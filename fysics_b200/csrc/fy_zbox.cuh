@@ -128,6 +128,10 @@ struct TmaMaps {
 };
 static __device__ int zb_timeout;      // set when a bounded wait expires (never expected)
 constexpr int kWaitSpins = 1 << 20;
+// Polls allowed for each CTA's first wait on its staged plane. Always kWaitSpins, except
+// when a failure-detection test sets it lower to make that wait expire on purpose (the drain
+// that follows keeps the full bound, so every copy issued still lands before the CTA exits).
+static __device__ int zb_first_wait_polls = kWaitSpins;
 
 FY_D unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 FY_D void mbar_init(unsigned long long* bar, unsigned count) {
@@ -146,8 +150,8 @@ FY_D bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
-FY_D bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    for (int i = 0; i < kWaitSpins; ++i)
+FY_D bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, int polls = kWaitSpins) {
+    for (int i = 0; i < polls; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -219,6 +223,7 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     const bool cols_in = x0 - 4 >= 0 && x0 + TX + 4 <= nx;       // no column of the staged rows is outside
     const int zfirst = zs - R, zend = ze + R;
     int zissued = min(zfirst + NS - 2, zend - 1);                // thread 0: last plane whose copy it issued
+    const int first_polls = TMA ? zb_first_wait_polls : 0;
     if (TMA) {
         if (t == 0) {
             for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
@@ -279,7 +284,8 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
             bool ok = true;
             float2* xcur = xs;
             if (TMA) {
-                ok = mbar_wait_bounded(&bars[slot], (unsigned)(((zi - zfirst) / NS) & 1));
+                ok = mbar_wait_bounded(&bars[slot], (unsigned)(((zi - zfirst) / NS) & 1),
+                                       zi == zfirst ? first_polls : kWaitSpins);
                 xcur = xs + ((zi - zfirst) & 1) * G::XS;
                 const int zn = zi + NS - 1;
                 if (t == 0 && ok && zn < zend) {
@@ -539,6 +545,15 @@ static inline int timeouts() {
     int v = 0;
     if (cudaMemcpyFromSymbol(&v, zb_timeout, sizeof v) != cudaSuccess) { cudaGetLastError(); return -1; }
     return v;
+}
+
+// Failure-detection tests: the polls allowed for each CTA's first wait (< 0: the normal
+// bound); clears this translation unit's expiry flag. Synchronous.
+static inline cudaError_t set_first_wait_polls(int polls) {
+    const int v = polls < 0 ? kWaitSpins : polls, zero = 0;
+    cudaError_t e = cudaMemcpyToSymbol(zb_first_wait_polls, &v, sizeof v);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(zb_timeout, &zero, sizeof zero);
+    return e;
 }
 
 // Enqueue one z-sliding box pass, radius r in [1, 4].

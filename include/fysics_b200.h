@@ -194,6 +194,33 @@ int    fy_process_buffer(const fy_pipeline_cfg *cfg, const unsigned char *u8buf,
                          long z0, long y0, long x0, long tz, long ty, long tx,
                          long vol_y, long vol_x, unsigned char *out, int *all_air);
 
+/* ---- local zarr v2 raw-u8 input (fysics.h:375-386, zarr_io.c:133-331), staged into the GPU.
+ * fy_zarr is layout-identical to the reference's. fy_zarr_open reads <root>/0/.zarray with the
+ * reference's header grammar; returns 0, or 1 for a missing or bad header or an "s3://" root
+ * (S3 is not supported). fy_zarr_read assembles the region [z0,z0+dz) x [y0,..) x [x0,..) into
+ * out (dz*dy*dx, C order) with the reference's semantics: chunk files hold their true extent,
+ * a missing or empty chunk reads as fill_value, a short file's tail as fill_value, voxels
+ * outside the volume are left untouched. The chunk files are read whole into pinned memory,
+ * kept in a device chunk cache and assembled on the GPU; thread-safe. Returns 0, or FY_EINVAL
+ * (negative origin or size), FY_EIO (unreadable chunk file), FY_ENOMEM (the chunk cache cannot
+ * hold the region's chunks). */
+typedef struct {
+    char root[1024];
+    long shape[3];
+    long chunk[3];
+    unsigned char fill;
+} fy_zarr;
+int    fy_zarr_open(fy_zarr *z, const char *root);
+int    fy_zarr_read(const fy_zarr *z, long z0, long y0, long x0, long dz, long dy, long dx,
+                    unsigned char *out);
+/* One inner tile of `tile`^3 at (z0,y0,x0) straight from the zarr (fysics.h:500-502,
+ * pipeline.c:512-537): the haloed region (halo = cfg->halo, or 8) is assembled on the GPU from
+ * the chunk cache and fed to the per-tile chain without a host round trip; writes the inner
+ * tile (*out_tz x *out_ty x *out_tx u8) to out and sets *all_air. Thread-safe. */
+int    fy_process_chunk(const fy_zarr *zin, const fy_pipeline_cfg *cfg, long z0, long y0, long x0,
+                        int tile, unsigned char *out, int *out_tz, int *out_ty, int *out_tx,
+                        int *all_air);
+
 /* ================================================================== part 2: fy_gpu_* */
 
 /* status codes (0 = success; 1 is the reference's generic failure) */
@@ -206,6 +233,7 @@ int    fy_process_buffer(const fy_pipeline_cfg *cfg, const unsigned char *u8buf,
 #define FY_ETIMEDOUT 6
 #define FY_EBUSY 7
 #define FY_EDEGENERATE 8
+#define FY_EIO 9          /* a chunk file could not be read */
 
 /* Select the CUDA device for the calling thread (default 0). No reference counterpart. */
 int         fy_gpu_init(int device);
@@ -220,6 +248,12 @@ unsigned long long fy_gpu_kernel_launches(void);
  * up since the library loaded on this device; the kernel then returned without finishing.
  * 0 in normal operation; -1 without a device. */
 int fy_gpu_kernel_timeouts(void);
+/* Failure-detection hook for tests; no reference counterpart. Sets the polls that each box
+ * pass CTA may spend on its FIRST tensor-copy wait (0 makes that wait expire at once, so the
+ * CTA raises the timeout flag, drains its copies under the normal bound and returns with its
+ * output unfinished); polls < 0 restores the normal bound. Also clears the timeout count.
+ * Synchronous; call it only while no kernel of this library is in flight. */
+int fy_gpu_test_box_first_wait(int polls);
 
 /* Device-pointer forms of the drop-in calls, enqueued on `stream` (a cudaStream_t, NULL =
  * legacy default stream) and NOT synchronised: results are valid once the stream reaches
@@ -261,16 +295,21 @@ const float *fy_gpu_noise_eps(const void *d_scratch, int nz, int ny, int nx);
  * callers that may not allocate device memory while they run, e.g. a serving loop whose
  * HBM is already committed to its own pool, where a cudaMalloc can fail or stall the
  * device. Scratch is one static device array inside the library, sized for
- * FY_NOISE_NOALLOC_MAX_VOXELS voxels (128^3, about 18 MB). Every GPU that loads the
- * library holds it until the process exits. Larger volumes return FY_EUNSUPPORTED.
+ * FY_NOISE_NOALLOC_MAX_VOXELS voxels (128^3): FY_NOISE_NOALLOC_SCRATCH_BYTES =
+ * 20,533,248 bytes (19.6 MiB). Every GPU that loads the library holds it until the
+ * process exits. Larger volumes return FY_EUNSUPPORTED.
  * Runs on the calling thread's current device and enqueues on `stream`. The model goes to
- * d_model, caller device memory laid out as fy_noise_model. d_eps, which may be NULL,
- * receives the float fy_guided_eps_for_noise(noise_ref).
- * The first call on each device resolves the array's device address. Make that first
- * call before any stream capture. All calls on a device share the array, which keeps
+ * d_model, caller device memory laid out as fy_noise_model (8-byte aligned). d_eps, which
+ * may be NULL, receives the float fy_guided_eps_for_noise(noise_ref) (4-byte aligned).
+ * Misaligned pointers return FY_EINVAL before anything is enqueued.
+ * Every call that is not being captured resolves the array's device address afresh, so a
+ * device reset between calls is harmless. The first call on each device must come before
+ * any stream capture: a call made while `stream` captures reuses the address that the
+ * latest uncaptured call resolved. All calls on a device share the array, which keeps
  * the previous call's contents. Calls whose GPU work can overlap race on it, e.g. calls
  * on unordered streams or from several host threads, so serialise them. */
 #define FY_NOISE_NOALLOC_MAX_VOXELS 2097152
+#define FY_NOISE_NOALLOC_SCRATCH_BYTES 20533248
 int    fy_gpu_estimate_noise_noalloc(const float *d_in, int nz, int ny, int nx, int win,
                                      double flat_pct, double ref_intensity,
                                      fy_noise_model *d_model, float *d_eps, void *stream);
@@ -310,6 +349,18 @@ int  fy_gpu_dering_finalize(fy_gpu_dering *h, int hp_win, unsigned int min_cnt, 
 int  fy_gpu_dering_apply(const fy_gpu_dering *h, float *d_f, long z0, long y0, long x0, long dz,
                          long dy, long dx, double scale, void *stream);
 int  fy_gpu_dering_download(const fy_gpu_dering *h, fy_dering *d, long *detected, void *stream);
+
+/* Device form of fy_zarr_read (no reference counterpart): assembles the region into d_out
+ * (device memory, dz*dy*dx) on `stream`, with the same semantics; returns once the copies and
+ * the gather are enqueued. The chunks it reads stay in the device chunk cache until that work
+ * has run. fy_gpu_zarr_cache_limit sets the cache's device-memory limit per GPU (default
+ * 4 GiB, at least 16 MiB); fy_gpu_zarr_cache_stats reports chunk hits, chunk loads and the
+ * bytes loaded from chunk files since the library loaded. */
+int    fy_gpu_zarr_read(const fy_zarr *z, long z0, long y0, long x0, long dz, long dy, long dx,
+                        unsigned char *d_out, void *stream);
+int    fy_gpu_zarr_cache_limit(size_t bytes);
+void   fy_gpu_zarr_cache_stats(unsigned long long *hits, unsigned long long *loads,
+                               unsigned long long *bytes_loaded);
 
 /* Phase correlation of `npairs` device volume pairs (fixed[i], moving[i] at a stride of
  * nz*ny*nx floats) with fy_phase_correlate's semantics (fysics.h:311-313). d_scratch holds

@@ -46,6 +46,11 @@ class RefHist(C.Structure):
     _fields_ = [("hist", C.c_long * 256), ("total", C.c_long)]
 
 
+class RefZarr(C.Structure):
+    """fy_zarr (fysics.h:376-381)."""
+    _fields_ = [("root", C.c_char * 1024), ("shape", C.c_long * 3), ("chunk", C.c_long * 3), ("fill", C.c_ubyte)]
+
+
 class RefPipelineCfg(C.Structure):
     """fy_pipeline_cfg (fysics.h:436-491), field for field."""
     _fields_ = ([(n, C.c_double) for n in ("delta_beta", "energy_kev", "distance_mm", "pixel_um", "unsharp_sigma",
@@ -130,6 +135,13 @@ REF_SIGS = {
     "fy_noise_aniso": (_i, [_P, _i, _i, _i, _PDB, _PDB]),
     "fy_valley_depth": (_d, [_P, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
     "fy_box_smooth": (None, [_P, _P, _P, _i, _i, _i, _i]),
+    "fy_zarr_open": (_i, [C.POINTER(RefZarr), C.c_char_p]),
+    "fy_zarr_read": (_i, [C.POINTER(RefZarr), _l, _l, _l, _l, _l, _l, _P]),
+    "fy_zarr_create": (_i, [C.POINTER(RefZarr), C.c_char_p, C.POINTER(_l), C.POINTER(_l)]),
+    "fy_zarr_write_chunk": (_i, [C.POINTER(RefZarr), _l, _l, _l, _P, _l, _l, _l]),
+    "fy_calibrate": (_i, [C.c_char_p, C.POINTER(RefPipelineCfg), _i, _i]),
+    "fy_process_chunk": (_i, [C.POINTER(RefZarr), C.POINTER(RefPipelineCfg), _l, _l, _l, _i, _P, C.POINTER(_i),
+                              C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
     "fy_process_buffer": (_i, [C.POINTER(RefPipelineCfg), _P, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l, _l,
                                _l, _l, _P, C.POINTER(_i)]),
 }
@@ -146,6 +158,7 @@ O64_SIGS = {
     "o64_guided": (_i, [_P, _P, _i, _i, _i, _i, _d]),
     "o64_guided_fast": (_i, [_P, _P, _i, _i, _i, _i, _d, _i]),
     "o64_estimate_noise": (_i, [_P, _i, _i, _i, _i, _d, _d, C.POINTER(RefNoise)]),
+    "o64_estimate_noise64": (_i, [_P, _i, _i, _i, _i, _d, _d, C.POINTER(RefNoise)]),
     "o64_guided_eps_for_noise": (_d, [_d]),
     "o64_dering_nr": (_i, [_l, _l, _d, _d]),
     "o64_dering_accumulate_u8": (None, [_P, _l, _l, _l, _l, _l, _i, _d, _d, _i, _i, _P, _P]),

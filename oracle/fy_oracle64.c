@@ -380,8 +380,10 @@ static double pct_sorted(double *v, long n, double pct) {
     return v[lo];
 }
 
-int o64_estimate_noise(const float *in, int nz, int ny, int nx, int win, double flat_pct,
-                       double ref_intensity, o64_noise_model *out) {
+/* The float input of the reference's API (inf), or a double volume (ind) for the FP64
+ * chain, whose stages pass double data from one to the next. */
+static int noise_impl(const float *inf, const double *ind, int nz, int ny, int nx, int win, double flat_pct,
+                      double ref_intensity, o64_noise_model *out) {
     if (!out) return 1;
     if (win < 3) win = 5;
     if (flat_pct <= 0) flat_pct = 10.0;
@@ -390,9 +392,9 @@ int o64_estimate_noise(const float *in, int nz, int ny, int nx, int win, double 
     double *x = malloc(sizeof(double) * n), *s1 = malloc(sizeof(double) * n);
     double *s2 = malloc(sizeof(double) * n), *t = malloc(sizeof(double) * n);
     if (!x || !s1 || !s2 || !t) { free(x); free(s1); free(s2); free(t); return 1; }
-    for (size_t i = 0; i < n; i++) x[i] = in[i];
+    for (size_t i = 0; i < n; i++) x[i] = inf ? (double)inf[i] : ind[i];
     box_sum3(x, s1, t, nz, ny, nx, r);
-    for (size_t i = 0; i < n; i++) x[i] = (double)in[i] * (double)in[i];
+    for (size_t i = 0; i < n; i++) x[i] = x[i] * x[i];
     box_sum3(x, s2, t, nz, ny, nx, r);
     double wc = (double)win * win * win;                 /* fixed divisor, noise.c:92 */
     double *mean = t, *var = s2;
@@ -456,6 +458,16 @@ int o64_estimate_noise(const float *in, int nz, int ny, int nx, int win, double 
     out->ref_intensity = ref_intensity;
     free(x); free(s1); free(s2); free(t);
     return 0;
+}
+
+int o64_estimate_noise(const float *in, int nz, int ny, int nx, int win, double flat_pct,
+                       double ref_intensity, o64_noise_model *out) {
+    return noise_impl(in, NULL, nz, ny, nx, win, flat_pct, ref_intensity, out);
+}
+
+int o64_estimate_noise64(const double *in, int nz, int ny, int nx, int win, double flat_pct,
+                         double ref_intensity, o64_noise_model *out) {
+    return noise_impl(NULL, in, nz, ny, nx, win, flat_pct, ref_intensity, out);
 }
 
 /* noise.c:197-202 */

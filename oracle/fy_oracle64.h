@@ -53,6 +53,9 @@ int    o64_guided_fast(const double *in, double *out, int nz, int ny, int nx,
 typedef struct { double g, b, noise_ref, ref_intensity; int n_bins_used; } o64_noise_model;
 int    o64_estimate_noise(const float *in, int nz, int ny, int nx, int win, double flat_pct,
                           double ref_intensity, o64_noise_model *out);
+/* the same on a double volume (the FP64 chain's deconvolved output) */
+int    o64_estimate_noise64(const double *in, int nz, int ny, int nx, int win, double flat_pct,
+                            double ref_intensity, o64_noise_model *out);
 double o64_guided_eps_for_noise(double noise_ref);
 
 /* dering: exact 64-bit integer sums; geometry identical to fy_dering_init. */

@@ -161,3 +161,26 @@ def test_viewer_slab(gpu):
     if oracle.have_ref():
         ref = oracle.ref_deconvolve(slab, r, -1.0)
         assert np.abs(got - ref).max() < TOL
+
+
+@pytest.mark.parametrize("shape,matched", [((16, 40, 320), False), ((320, 24, 20), True),
+                                           ((96, 200, 320), False), ((96, 200, 320), True)])
+def test_deconv_384_pad_vs_reference(gpu, shape, matched):
+    """An axis of 320 pads to 384 = 3*2^7 (fy_next_fft_size, fft.c:34-38; paganin.c:155):
+    the reflect padding, the radix-3 plans and the LUT range at that size against the
+    reference and the FP64 oracle. (96, 200, 320) is one of the uneven-cube shapes of the
+    batched configuration (pads 96 / 256 / 384)."""
+    assert gpu.load().fy_next_fft_size(320) == 384
+    rng = np.random.default_rng(sum(shape) + matched)
+    vol = rng.uniform(0, 1, shape).astype(np.float32)
+    if matched:
+        ph = gpu.physics(psf_sigma_vox=1.0, psf_sigma_z_vox=1.17)
+        got = gpu.deconvolve_matched(vol, ph, 0.05)
+    else:
+        ph = gpu.physics()
+        got = gpu.deconvolve(vol, ph, 0.015)
+    o64 = oracle.o64_deconvolve(vol, rphys(ph), 0.05 if matched else 0.015, kind=1 if matched else 0)
+    assert np.abs(got - o64).max() < TOL
+    if oracle.have_ref():
+        ref = oracle.ref_deconvolve(vol, rphys(ph), 0.05 if matched else 0.015, matched=matched)
+        assert np.abs(got - ref).max() < TOL

@@ -114,3 +114,41 @@ def test_batch_device_api(gpu):
         assert st[i] == 0 and np.array_equal(np.array(sh[3 * i:3 * i + 3]), s1) and pk[i] == p1
         assert idx[i] == o64_pc(f, m, 0)[3]                      # bit-exact integer peak
     assert np.array_equal(integer_part(np.array(sh[9:12])), [3, -5, 7])
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="reference library not built")
+@pytest.mark.parametrize("window,seed", [(0, 41), (1, 42)])
+def test_config4_pair_256_vs_reference(gpu, window, seed):
+    """A registration pair at the batched-registration configuration's size: 256^3 phantom
+    (u8/255), the moving volume an FP64 Fourier shift by an integer U[-40,40] plus a
+    subvoxel U[-0.5,0.5] per axis, independent noise var = 0.002*I + 1e-4 on each. The
+    integer peak must equal the reference's fy_phase_correlate (phasecorr.c:121-131) and
+    the subvoxel shift be within 0.01 vox of it; without the window the shift is also held
+    to the reference test's 0.15 L1 of the truth."""
+    import torch
+    import fysics_b200.phantom as ph
+    n = 256
+    rng = np.random.default_rng(seed)
+    u = ph.phantom((n, n, n), seed=seed, delta_beta=175.0, pixel_um=2.4, device="cuda")
+    f = u.to(torch.float64) / 255.0
+    k = torch.fft.fftfreq(n, device="cuda", dtype=torch.float64) * n
+    k[n // 2] = n // 2
+    s = rng.integers(-40, 41, 3) + rng.uniform(-0.5, 0.5, 3)
+    phase = -2 * np.pi * (k[:, None, None] * s[0] + k[None, :, None] * s[1] + k[None, None, :] * s[2]) / n
+    m = torch.fft.ifftn(torch.fft.fftn(f) * torch.exp(1j * phase)).real
+    g = torch.Generator(device="cuda").manual_seed(seed)
+
+    def noisy(v):
+        return (v + torch.sqrt(0.002 * v.clamp(min=0) + 1e-4) *
+                torch.randn(v.shape, generator=g, device="cuda", dtype=torch.float64)).float().cpu().numpy()
+
+    fixed, moving = noisy(f), noisy(m)
+    del f, m, phase
+    rc, got, pk = gpu_pc(gpu, fixed, moving, window)
+    assert rc == 0
+    rr = ref_pc(fixed, moving, window)
+    assert rr[0] == 0
+    assert np.array_equal(integer_part(got), integer_part(rr[1]))
+    assert np.abs(got - rr[1]).max() < 1e-2
+    if window == 0:
+        assert np.abs(got - s).sum() < 0.15
