@@ -204,8 +204,8 @@ def ref() -> C.CDLL:
     global _ref
     if _ref is None:
         if not REF_SO.exists():
-            raise FileNotFoundError(f"{REF_SO} missing: run `make -C oracle ref` where the "
-                                    "reference sources are available")
+            raise FileNotFoundError(f"{REF_SO} missing: run `make -C oracle ref REF_DIR=<reference checkout>` "
+                                    "where the reference sources are available")
         _ref = _bind(REF_SO, REF_SIGS)
     return _ref
 
