@@ -937,6 +937,14 @@ def main():
     fb.check(lib.fy_gpu_init(dev), "fy_gpu_init")
     torch.cuda.set_device(dev)
     p, db_scale = physics_for(fb)
+    # launch shapes measured for this cube shape on this GPU (cached; set-up, not timed)
+    t_tune = time.perf_counter()
+    rc_tune = lib.fy_gpu_autotune(*SHAPE, 0)
+    t_tune = time.perf_counter() - t_tune
+    px = lib.fy_next_fft_size(SHAPE[2])
+    tune_knobs = [f"x1.{px}", f"x5.{px}", "box0.r2.{}x{}x{}".format(*SHAPE), "box3.r2.{}x{}x{}".format(*SHAPE)]
+    tuning = {"rc": rc_tune, "seconds": round(t_tune, 2),
+              "values": {k: lib.fy_gpu_tune_value(k.encode()) for k in tune_knobs}}
     u8 = benchmark_cube(args, rank, p.delta_beta, f"cuda:{dev}")
     nz, ny, nx = SHAPE
     n = nz * ny * nx
@@ -1136,6 +1144,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": bench_config(db_scale, world),
+        "tuning": tuning,
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "e2e_p50": float(np.percentile(e2e_steps_ms, 50)),
                        "e2e_p99": float(np.percentile(e2e_steps_ms, 99))},

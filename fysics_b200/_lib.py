@@ -189,6 +189,9 @@ SIGNATURES = {
     "fy_process_chunk": (_i, [C.POINTER(Zarr), C.POINTER(PipelineCfg), _l, _l, _l, _i, _P, C.POINTER(_i),
                               C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
     "fy_gpu_zarr_read": (_i, [C.POINTER(Zarr), _l, _l, _l, _l, _l, _l, _P, _P]),
+    "fy_gpu_autotune": (_i, [_i, _i, _i, _i]),
+    "fy_gpu_tune_load": (_i, [C.c_char_p]),
+    "fy_gpu_tune_value": (_i, [C.c_char_p]),
     "fy_gpu_zarr_cache_limit": (_i, [_sz]),
     "fy_gpu_zarr_cache_stats": (None, [C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong),
                                        C.POINTER(C.c_ulonglong)]),

@@ -291,7 +291,7 @@ cudaError_t fy_deconv_pass(int pass, const DeconvLaunch& d, cudaStream_t st) {
     };
     switch (pass) {
     case 1: {   // X forward, rows paired two per line (line-major staging)
-        const TileShape t = fy_tile_shape(g.px);
+        const TileShape t = fy_x_tile_shape(1, g.px);
         const size_t smem = (size_t)t.W * (g.px + 1) * sizeof(float2) + (size_t)g.px * sizeof(float2);
         const unsigned grid = (unsigned)((Q + 2 * t.W - 1) / (2 * t.W));
         const int esz = d.src_u8 ? 1 : 4;
@@ -348,7 +348,7 @@ cudaError_t fy_deconv_pass(int pass, const DeconvLaunch& d, cudaStream_t st) {
         });
     }
     case 5: {   // X C2R, crop, 1/N (line-major staging, vector stores when rows are 16-byte aligned)
-        const TileShape t = fy_tile_shape(g.px);
+        const TileShape t = fy_x_tile_shape(5, g.px);
         const size_t smem = (size_t)t.W * (g.px + 1) * sizeof(float2) + (size_t)g.px * sizeof(float2);
         const unsigned grid = (unsigned)((Q + 2 * t.W - 1) / (2 * t.W));
         const float invN = 1.0f / ((float)g.pz * (float)g.py * (float)g.px);   // paganin.c:263

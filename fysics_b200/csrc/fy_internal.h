@@ -141,6 +141,49 @@ inline TileShape fy_tile_shape(int n) {
     return t;
 }
 
+// Autotuned launch shapes (fy_autotune.cu), per device. A lookup returns 0 when nothing is
+// tuned for the key (the caller keeps its default). Tuned shapes change how work is split
+// over CTAs, never the arithmetic, so results are bit-identical to the defaults.
+//   fy_tuned_x_wlog   log2 of the lines per CTA of a deconvolution X pass (pass 1 or 5) of
+//                     axis length n (line-major tiles: any W <= the default fits)
+//   fy_tuned_box_chunks  z chunks of a box pass (fy_zbox.cuh kind, radius) on a volume
+int fy_tuned_x_wlog(int pass, int n);
+int fy_tuned_box_chunks(int kind, int r, int nz, int ny, int nx);
+// Default z-chunk count of a box pass (64 x 16 column tiles, two CTAs resident per SM, so a
+// launch runs in waves of 2*sms CTAs): among chunk counts with chunks of >= 8r planes and at
+// least ~3 waves of work, the one whose CTAs best fill their last wave, net of the 2r-plane
+// warm-up each chunk repeats: score = (waves / ceil(waves)) * zchunk / (zchunk + 2r).
+inline int fy_box_default_chunks(int nz, int ny, int nx, int r, int sms) {
+    const long txy = (long)((nx + 63) / 64) * ((ny + 15) / 16), slots = 2L * sms;
+    int hi = nz / (8 * r);
+    if (hi < 1) hi = 1;
+    int lo = (int)((3 * slots + txy - 1) / txy);
+    if (lo > hi) lo = hi;
+    if (lo < 1) lo = 1;
+    int best = lo;
+    double best_score = -1.0;
+    for (int nc = lo; nc <= hi && nc <= 4 * lo; ++nc) {
+        const int zc = (nz + nc - 1) / nc;
+        const long ctas = txy * ((nz + zc - 1) / zc);
+        const double waves = (double)ctas / (double)slots;
+        const long whole = (long)waves + ((double)(long)waves < waves ? 1 : 0);
+        const double score = waves / (double)whole * (double)zc / (double)(zc + 2 * r);
+        if (score > best_score + 1e-9) { best_score = score; best = nc; }
+    }
+    return best;
+}
+// TileShape of an X pass: the tuned lines per CTA when there is one, else the default.
+inline TileShape fy_x_tile_shape(int pass, int n) {
+    TileShape t = fy_tile_shape(n);
+    const int wl = fy_tuned_x_wlog(pass, n);
+    if (wl > 0 && wl < t.wlog && (n << wl) / t.E >= 32) {
+        t.wlog = wl;
+        t.W = 1 << wl;
+        t.NT = t.W * n / t.E;
+    }
+    return t;
+}
+
 // Radial guided-eps model (fy_radial.cu): cube eps = base * radial scale, on the device.
 cudaError_t fy_launch_radial_tile_eps(const fy_radial_eps* d_fit, const float* base_dev, float base_host, double ecy,
                                       double ecx, long y0, long x0, long ty, long tx, float* d_out, cudaStream_t st);

@@ -507,47 +507,51 @@ constexpr int kBoundThreads = 512;
 constexpr double kWinSigmas = 5.0;
 
 // Block radix select over keys in shared memory: the rank-th smallest (0-based) of keys[0, c),
-// c <= kSampleMax, by kBoundThreads threads. Four 8-bit digit passes; each thread counts its
-// own keys (<= 32) in a private byte column of hist8 ([256 digits][kBoundThreads]), so no
-// atomics are needed; two threads then sum each digit's row.
-FY_D uint32_t block_select(const uint32_t* keys, int c, long long rank, unsigned char* hist8,
+// c <= kSampleMax, by kBoundThreads threads. Four 8-bit digit passes. Each warp counts into a
+// private 256-bin histogram (wh, [warps][256]); the lanes of a warp that hold the same digit
+// are merged with __match_any_sync, so one shared atomic counts them all (the high digits of
+// a sample are nearly all equal). Then one thread per digit sums the warps' counts and a
+// warp-shuffle scan over the 256 digit totals finds the bucket of the rank.
+FY_D uint32_t block_select(const uint32_t* keys, int c, long long rank, unsigned int* wh,
                            unsigned long long* part, uint32_t* s_sel) {
-    constexpr int NTB = kBoundThreads, RW = NTB / 4;    // threads, words per digit row
-    const int t = threadIdx.x;
+    constexpr int NTB = kBoundThreads, NW = NTB / 32;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const unsigned full = 0xffffffffu;
     uint32_t prefix = 0, pmask = 0;
-    uint32_t* h32 = reinterpret_cast<uint32_t*>(hist8);
+    unsigned int* mine_h = wh + w * 256;
     for (int sh = 24; sh >= 0; sh -= 8) {
-        for (int i = t; i < 256 * RW; i += NTB) h32[i] = 0;
+        for (int i = t; i < NW * 256; i += NTB) wh[i] = 0;
         __syncthreads();
-        for (int i = t; i < c; i += NTB) {
-            const uint32_t k = keys[i];
-            if ((k & pmask) == prefix) ++hist8[((k >> sh) & 255u) * NTB + t];
+        for (int i0 = 0; i0 < c; i0 += NTB) {             // warp-uniform trip count
+            const int i = i0 + t;
+            const uint32_t k = i < c ? keys[i] : 0u;
+            const bool ok = i < c && (k & pmask) == prefix;
+            const unsigned act = __ballot_sync(full, ok);
+            if (ok) {
+                const unsigned d = (k >> sh) & 255u;
+                const unsigned same = __match_any_sync(act, d);
+                if (lane == __ffs(same) - 1) atomicAdd(&mine_h[d], (unsigned)__popc(same));
+            }
         }
         __syncthreads();
-        unsigned long long mine = 0;                   // half of digit t/2's row
-        const uint32_t* row = h32 + (t >> 1) * RW + (t & 1) * (RW / 2);
-        for (int w = 0; w < RW / 2; ++w) {
-            const uint32_t v = row[w];
-            mine += (v & 255u) + ((v >> 8) & 255u) + ((v >> 16) & 255u) + (v >> 24);
+        unsigned long long tot = 0;                     // digit t's count over the warps
+        if (t < 256)
+            for (int ww = 0; ww < NW; ++ww) tot += wh[ww * 256 + t];
+        // inclusive scan of the 256 digit totals: within warps by shuffles, then warp sums
+        unsigned long long incl = tot;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(full, incl, o);
+            if (lane >= o) incl += y;
         }
-        part[t] = mine;
+        if (t < 256 && lane == 31) part[w] = incl;
         __syncthreads();
-        unsigned long long dsum = 0;
-        if (t < 256) dsum = part[2 * t] + part[2 * t + 1];
-        __syncthreads();
-        if (t < 256) part[t] = dsum;
-        __syncthreads();
-        for (int off = 1; off < 256; off <<= 1) {      // inclusive scan over digits
-            const unsigned long long add = (t < 256 && t >= off) ? part[t - off] : 0ull;
-            __syncthreads();
-            if (t < 256) part[t] += add;
-            __syncthreads();
-        }
         if (t < 256) {
-            const unsigned long long before = t ? part[t - 1] : 0ull;
-            if ((unsigned long long)rank >= before && (unsigned long long)rank < part[t]) {
+            unsigned long long off = 0;
+            for (int ww = 0; ww < w; ++ww) off += part[ww];
+            const unsigned long long hi = off + incl, lo = hi - tot;
+            if ((unsigned long long)rank >= lo && (unsigned long long)rank < hi) {
                 s_sel[0] = (uint32_t)t;
-                s_sel[1] = (uint32_t)(rank - (long long)before);
+                s_sel[1] = (uint32_t)(rank - (long long)lo);
             }
         }
         __syncthreads();
@@ -569,12 +573,12 @@ __global__ void __launch_bounds__(256) k_win_sample(const float* __restrict__ me
 }
 
 // One CTA (kBoundThreads threads) per target (blockIdx.x 0/1: 1st/99th percentile) and window
-// end (blockIdx.y 0: wlo, 1: whi). Dynamic shared memory: kSampleMax keys, then the private
-// digit counts (256 x kBoundThreads bytes).
+// end (blockIdx.y 0: wlo, 1: whi). Dynamic shared memory: kSampleMax keys, then the warps'
+// digit histograms (kBoundThreads/32 x 256 counters).
 __global__ void __launch_bounds__(kBoundThreads) k_win_bounds(const float* __restrict__ sm,
                                                               NoiseCtl* __restrict__ ctl, long long m) {
     extern __shared__ uint32_t wkeys[];
-    unsigned char* hist8 = reinterpret_cast<unsigned char*>(wkeys + kSampleMax);
+    unsigned int* wh = wkeys + kSampleMax;
     __shared__ unsigned long long part[kBoundThreads];
     __shared__ uint32_t s_sel[2];
     if (ctl->mode != kModeWin0) return;
@@ -589,8 +593,8 @@ __global__ void __launch_bounds__(kBoundThreads) k_win_bounds(const float* __res
         const double qc = q < 1.0 / c ? 1.0 / c : (q > 1.0 - 1.0 / c ? 1.0 - 1.0 / c : q);
         const long long ks = (long long)(q * (double)(c - 1));
         const long long d = (long long)ceil(kWinSigmas * sqrt((double)c * qc * (1.0 - qc))) + 4;
-        if (!upper && ks - d >= 0) w = block_select(wkeys, c, ks - d, hist8, part, s_sel);
-        if (upper && ks + d + 1 < c) w = block_select(wkeys, c, ks + d + 1, hist8, part, s_sel);
+        if (!upper && ks - d >= 0) w = block_select(wkeys, c, ks - d, wh, part, s_sel);
+        if (upper && ks + d + 1 < c) w = block_select(wkeys, c, ks + d + 1, wh, part, s_sel);
     }
     if (threadIdx.x == 0) {
         if (upper) {
@@ -985,7 +989,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     const unsigned g = grid_sel(n, sms), gc = grid_sel(L.cap, sms);
     const size_t smem_all = 2 * 2048 * sizeof(unsigned int), smem_bin = NB * 256 * sizeof(unsigned int);
     const size_t smem_bin_c = smem_bin + (size_t)(256 / 32) * kCompactBuf * (sizeof(float) + 1);
-    const size_t smem_keys = kSampleMax * sizeof(uint32_t) + 256 * kBoundThreads;   // keys + private digit counts
+    const size_t smem_keys = (kSampleMax + 256 * (kBoundThreads / 32)) * sizeof(uint32_t);   // keys + warp digit counts
     const long long m = n < kSampleMax ? n : kSampleMax;
     const unsigned long long wa = weyl_step((unsigned long long)n), wb = (unsigned long long)n / 3;
     cudaError_t e;

@@ -77,8 +77,10 @@ struct Geo {
     static constexpr int RW = C * SXW;                           // floats per staged row
     static constexpr int STAGE = (SY * RW + 31) / 32 * 32;      // floats per staged plane (128 B multiple)
     static constexpr int XS = SY * TX;                          // float2 per X-sum array
-    // two X-sum arrays (alternate planes), the reciprocal counts, 128 B for alignment
-    static constexpr size_t bytes = (size_t)(NS * STAGE + 4 * XS + TX + TY) * sizeof(float) + 128;
+    static constexpr int GUIDE = C == 2 ? TX * TY : 0;           // floats per staged guide tile
+    // the staged planes, the guide tiles (output passes), two X-sum arrays (alternate planes),
+    // the reciprocal counts, 128 B for alignment
+    static constexpr size_t bytes = (size_t)(NS * (STAGE + GUIDE) + 4 * XS + TX + TY) * sizeof(float) + 128;
 };
 
 FY_D float recip_count(int p, int L, int r) {
@@ -125,6 +127,8 @@ FY_D void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memor
 // zb_timeout, waits (bounded) for its own copies in flight and returns.
 struct TmaMaps {
     CUtensorMap m0;                    // the staged field; 64-byte aligned type
+    CUtensorMap m1;                    // output passes: the guide I, one TX x TY tile per plane
+    int guide;                         // m1 is valid: the guide is staged with the planes
 };
 static __device__ int zb_timeout;      // set when a bounded wait expires (never expected)
 constexpr int kWaitSpins = 1 << 20;
@@ -165,12 +169,15 @@ FY_D void tma_load_3d(float* dst, const CUtensorMap* map, int x, int y, int z, u
 // Issue plane zi into slot `dst` (thread 0 only). The innermost coordinate C*(x0 - 4) is a
 // multiple of 4 floats (16 bytes) as the tensor copy requires; rows and planes outside the
 // volume, negative ones included, are zero-filled by the copy.
+// gdst, when not null, receives the guide tile of output plane zi - R (x0 a multiple of TX:
+// 16-byte aligned), completing on the same barrier.
 template <int R, int C>
-FY_D void tma_stage(float* dst, const TmaMaps& tm, unsigned long long* bar, int zi, int x0, int y0) {
+FY_D void tma_stage(float* dst, float* gdst, const TmaMaps& tm, unsigned long long* bar, int zi, int x0, int y0) {
     using G = Geo<R, C>;
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // prior generic reads of the slot
-    mbar_expect_tx(bar, (unsigned)(G::SY * G::RW * sizeof(float)));
+    mbar_expect_tx(bar, (unsigned)((G::SY * G::RW + (gdst ? TX * TY : 0)) * sizeof(float)));
     tma_load_3d(dst, &tm.m0, C * (x0 - 4), y0 - R, zi, bar);
+    if (gdst) tma_load_3d(gdst, &tm.m1, x0, y0, zi - R, bar);
 }
 
 // Stage plane zi into dst with cp.async; zero fill outside the volume. VEC: 16-byte copies
@@ -206,7 +213,8 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     extern __shared__ float4 zb_smem4[];
     __shared__ __align__(8) unsigned long long bars[NS];
     float* stage = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(zb_smem4) + 127) & ~(uintptr_t)127);
-    float2* xs = reinterpret_cast<float2*>(stage + NS * G::STAGE);   // X sums of both quantities, 2 x [SY][TX]
+    float* sguide = stage + NS * G::STAGE;                         // NS guide tiles (output passes)
+    float2* xs = reinterpret_cast<float2*>(sguide + NS * G::GUIDE);  // X sums of both quantities, 2 x [SY][TX]
     float* rx = reinterpret_cast<float*>(xs + 2 * G::XS);
     float* ry = rx + TX;
     const int t = threadIdx.x;
@@ -224,6 +232,12 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     const int zfirst = zs - R, zend = ze + R;
     int zissued = min(zfirst + NS - 2, zend - 1);                // thread 0: last plane whose copy it issued
     const int first_polls = TMA ? zb_first_wait_polls : 0;
+    // the guide tile of output plane zi - R rides with staged plane zi when that output plane
+    // is this CTA's (TMA output passes with an aligned guide)
+    const bool gstage = TMA && out_kind(KIND) && p.out_mode == 0 && tm.guide;
+    auto guide_slot = [&](int slot, int zi) -> float* {
+        return gstage && zi - R >= zs && zi - R < ze ? sguide + slot * G::GUIDE : nullptr;
+    };
     if (TMA) {
         if (t == 0) {
             for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
@@ -232,7 +246,8 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
         __syncthreads();
         if (t == 0)
             for (int s = 0; s < NS - 1; ++s)
-                if (zfirst + s < zend) tma_stage<R, C>(stage + s * G::STAGE, tm, &bars[s], zfirst + s, x0, y0);
+                if (zfirst + s < zend)
+                    tma_stage<R, C>(stage + s * G::STAGE, guide_slot(s, zfirst + s), tm, &bars[s], zfirst + s, x0, y0);
     } else {
 #pragma unroll
         for (int s = 0; s < NS - 1; ++s) {
@@ -287,12 +302,6 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                 ok = mbar_wait_bounded(&bars[slot], (unsigned)(((zi - zfirst) / NS) & 1),
                                        zi == zfirst ? first_polls : kWaitSpins);
                 xcur = xs + ((zi - zfirst) & 1) * G::XS;
-                const int zn = zi + NS - 1;
-                if (t == 0 && ok && zn < zend) {
-                    tma_stage<R, C>(stage + ((zn - zfirst) & (NS - 1)) * G::STAGE, tm, &bars[(zn - zfirst) & (NS - 1)],
-                                    zn, x0, y0);
-                    zissued = zn;
-                }
             } else {
                 cp_wait<NS - 2>();
                 __syncthreads();             // plane zi landed for every thread; xs free again
@@ -304,7 +313,7 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
             const bool emit = zo >= zs && zo < ze && gx < nx;
             const size_t obase = (size_t)(emit ? zo : 0) * plane + (size_t)(y0 + 4 * rg) * nx + gx;
             float gv[4] = {0.f, 0.f, 0.f, 0.f};
-            if (out_kind(KIND) && p.out_mode == 0 && emit) {   // issued early, used after the Y phase
+            if (out_kind(KIND) && p.out_mode == 0 && emit && !gstage) {   // issued early, used after the Y phase
 #pragma unroll
                 for (int k = 0; k < 4; ++k)
                     if (y0 + 4 * rg + k < ny) gv[k] = __ldg(p.guide + obase + (size_t)k * nx);
@@ -401,6 +410,14 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                     __syncthreads();
                     return;
                 }
+                // Refill the slot of plane zi - 1: past this barrier every thread has finished
+                // plane zi - 1, its staged rows and its guide tile alike.
+                const int zn = zi + NS - 1;
+                if (t == 0 && zn < zend) {
+                    const int sn = (zn - zfirst) & (NS - 1);
+                    tma_stage<R, C>(stage + sn * G::STAGE, guide_slot(sn, zn), tm, &bars[sn], zn, x0, y0);
+                    zissued = zn;
+                }
             } else {
                 __syncthreads();
             }
@@ -462,7 +479,8 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
                 } else {
                     const float2 mab = mul2(sm, rz);
                     if (p.out_mode == 0) {
-                        float w = mab.x * gv[k] + mab.y;
+                        const float g = gstage ? sguide[slot * G::GUIDE + (4 * rg + k) * TX + xc] : gv[k];
+                        float w = mab.x * g + mab.y;
                         if (rings && w > 0.f && ri[k] < p.ra.nr) {     // masked voxels untouched
                             const float w2 = w - p.ra.sc * rv[k];
                             w = w2 > 0.f ? w2 : 0.f;
@@ -478,24 +496,22 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     if (!TMA) cp_wait<0>();
 }
 
-// Tiles and z chunks: ~6 CTAs per SM, chunks of >= 8R planes so the 2R-plane warm-up stays
-// a small fraction.
-inline dim3 grid_for(int nz, int ny, int nx, int r, int sms, int& zchunk) {
+// Tiles and z chunks: the autotuned chunk count when there is one, else the default of
+// fy_box_default_chunks (fy_internal.h).
+inline dim3 grid_for(int kind, int nz, int ny, int nx, int r, int sms, int& zchunk) {
     const int tx = (nx + TX - 1) / TX, ty = (ny + TY - 1) / TY;
-    const long txy = (long)tx * ty;
-    int nchunk = (int)((6L * sms + txy - 1) / txy);
-    const int min_chunk = 8 * r;
-    if (nchunk > nz / min_chunk) nchunk = nz / min_chunk;
-    if (nchunk < 1) nchunk = 1;
-    zchunk = (nz + nchunk - 1) / nchunk;
+    int nc = fy_tuned_box_chunks(kind, r, nz, ny, nx);
+    if (nc <= 0) nc = fy_box_default_chunks(nz, ny, nx, r, sms);
+    zchunk = (nz + nc - 1) / nc;
     return dim3(tx, ty, (nz + zchunk - 1) / zchunk);
 }
 
-// Tensor map of one f32 volume field of C floats per voxel for the TMA staging: box
-// (C*(x0-4) .. C*(x0+TX+4), SY rows, 1 plane), zero fill outside. The encoder comes from the
+// Tensor map of one f32 volume field of c floats per voxel for the TMA staging: a box of
+// bx voxels x by rows x 1 plane (the staged rows: SXW x SY; the guide: TX x TY), zero fill
+// outside. The encoder comes from the
 // driver through the runtime, so the library needs no link-time driver dependency. Returns
 // false when unavailable.
-inline bool make_tma_map(CUtensorMap* m, const float* base, int nz, int ny, int nx, int c, int sy) {
+inline bool make_tma_map(CUtensorMap* m, const float* base, int nz, int ny, int nx, int c, int bx, int by) {
     using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -513,7 +529,7 @@ inline bool make_tma_map(CUtensorMap* m, const float* base, int nz, int ny, int 
     if (!fn || ((uintptr_t)base & 15) || (nx % 4)) return false;
     const cuuint64_t dims[3] = {(cuuint64_t)nx * c, (cuuint64_t)ny, (cuuint64_t)nz};
     const cuuint64_t strides[2] = {(cuuint64_t)nx * c * 4, (cuuint64_t)nx * ny * c * 4};
-    const cuuint32_t box[3] = {(cuuint32_t)(SXW * c), (cuuint32_t)sy, 1};
+    const cuuint32_t box[3] = {(cuuint32_t)(bx * c), (cuuint32_t)by, 1};
     const cuuint32_t es[3] = {1, 1, 1};
     return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -526,7 +542,9 @@ inline cudaError_t launch_r(const Params& p, dim3 grid, cudaStream_t st) {
     const size_t smem = Geo<R, C>::bytes;
     TmaMaps tm;
     memset(&tm, 0, sizeof tm);
-    const bool tma = VEC && make_tma_map(&tm.m0, p.f0, p.nz, p.ny, p.nx, C, Geo<R, C>::SY);
+    const bool tma = VEC && make_tma_map(&tm.m0, p.f0, p.nz, p.ny, p.nx, C, SXW, Geo<R, C>::SY);
+    if (tma && out_kind(KIND) && p.out_mode == 0 && p.guide)
+        tm.guide = make_tma_map(&tm.m1, p.guide, p.nz, p.ny, p.nx, 1, TX, TY) ? 1 : 0;
     cudaError_t e;
     if (tma) {
         auto k = k_zbox<R, KIND, true, true>;
@@ -559,7 +577,7 @@ static inline cudaError_t set_first_wait_polls(int polls) {
 // Enqueue one z-sliding box pass, radius r in [1, 4].
 template <int KIND>
 inline cudaError_t launch(Params p, int r, int sms, cudaStream_t st) {
-    const dim3 grid = grid_for(p.nz, p.ny, p.nx, r, sms, p.zchunk);
+    const dim3 grid = grid_for(KIND, p.nz, p.ny, p.nx, r, sms, p.zchunk);
     auto al = [](const void* q) { return ((uintptr_t)q & 15) == 0; };
     const bool vec = p.nx % 4 == 0 && al(p.f0);
     switch (r * 2 + (vec ? 1 : 0)) {
