@@ -431,6 +431,9 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
         "plain_mvox_per_s": plain,
         "plain": "the first 120 requests one at a time: pinned H2D, fy_gpu_restore_u8, D2H, synchronise",
     }
+    if n_batch <= 0:
+        lib.fy_server_destroy(srv)
+        return served, None
     # ---- config-3 sample: uneven cubes submitted at once
     dims = [96, 128, 160, 200, 240, 256, 320]
     bre = []
@@ -900,6 +903,32 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+SWEEP_RATES = (200.0, 400.0, 700.0, 1000.0, 1400.0, 2000.0)
+
+
+def run_serve_sweep(args, rank, local):
+    """The serving configuration at its stated scale: `--sweep-requests` requests (sizes
+    64^3:128^3:256^3:512^3 = 40:30:25:5, Poisson arrivals) through the request loop at each
+    rate of SWEEP_RATES; per rate the throughput and p50/p99 latency overall and per size, and
+    the highest rate whose 256^3 p99 stays under 10 ms."""
+    if rank != 0:
+        return
+    import fysics_b200 as fb
+    lib = fb.load()
+    fb.check(lib.fy_gpu_init(local), "fy_gpu_init")
+    import torch
+    torch.cuda.set_device(local)
+    _, db_scale = physics_for(fb)
+    served, _ = served_and_batched(fb, lib, local, args.seed, db_scale, n_requests=args.sweep_requests,
+                                   rates=SWEEP_RATES, n_batch=0)
+    ok = [pt["arrival_rps"] for pt in served["points"] if pt["p99_ms_by_size"].get("256^3", 1e9) < 10.0]
+    line = {"mode": "serve_sweep", "metric": METRIC, "unit": "Mvoxel/s", "requests_per_rate": args.sweep_requests,
+            "rates_rps": list(SWEEP_RATES),
+            "max_rate_rps_256_p99_under_10ms": max(ok) if ok else None,
+            "served": served}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -916,6 +945,10 @@ def main():
     ap.add_argument("--no-phasecorr", action="store_true", help="skip the registration sample")
     ap.add_argument("--no-tiles", action="store_true", help="skip the per-tile export chain sample")
     ap.add_argument("--no-viewer", action="store_true", help="skip the viewer slab sample")
+    ap.add_argument("--serve-sweep", action="store_true",
+                    help="the serving configuration at its stated scale instead of the benchmark: 20,000 "
+                         "requests per arrival rate over a sweep of 200-2000 req/s (one JSON line)")
+    ap.add_argument("--sweep-requests", type=int, default=20000)
     args = ap.parse_args()
     global SHAPE, WORKLOAD
     if args.size != 512:
@@ -923,6 +956,11 @@ def main():
         WORKLOAD = WORKLOAD.replace("512^3", f"{args.size}^3")
     args.warmup = max(args.warmup, 3)
     rank, world, local, dist = dist_setup(args.gpus)
+    if args.serve_sweep:
+        run_serve_sweep(args, rank, local)
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         if dist:
