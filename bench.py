@@ -336,7 +336,7 @@ def _plain(fb, lib, reqs, dev):
     return vox / (time.perf_counter() - t0) / 1e6
 
 
-def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.0, 2000.0), n_batch=24):
+def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.0, 2000.0), n_batch=96):
     """Config-5 sample (Poisson arrivals, 64:128:256:512 = 40:30:25:5) through the request
     loop, and a config-3 sample (uneven cubes, dims per axis from {96..320}) submitted at
     once; each next to the same requests on the plain per-cube path."""
@@ -434,24 +434,54 @@ def served_and_batched(fb, lib, dev, seed, db_scale, n_requests=400, rates=(500.
     if n_batch <= 0:
         lib.fy_server_destroy(srv)
         return served, None
-    # ---- config-3 sample: uneven cubes submitted at once
+    # ---- config-3: uneven cubes submitted at once, device-resident and through host buffers
     dims = [96, 128, 160, 200, 240, 256, 320]
-    bre = []
+    bre, dre = [], []
     keep = []
     for i in range(n_batch):
         shape = tuple(int(d) for d in rng.choice(dims, 3))
-        h = pinned_phantom(shape, seed + 1000 + i)
+        u = ph.phantom(shape, seed=seed + 1000 + i, delta_beta=500.0 * db_scale, pixel_um=2.4, fz2_scale=1.17 ** 2,
+                       device=f"cuda:{dev}")
+        h = torch.empty(shape, dtype=torch.uint8, pin_memory=True)
+        h.copy_(u.cpu())
         o = torch.empty(shape, dtype=torch.float32, pin_memory=True)
-        keep += [h, o]
-        bre.append(_req(fb, h, o, rng.uniform(200, 1000), 1.0, db_scale))
+        do = torch.empty(shape, dtype=torch.float32, device=f"cuda:{dev}")
+        keep += [h, o, u, do]
+        db = rng.uniform(200, 1000)
+        bre.append(_req(fb, h, o, db, 1.0, db_scale))
+        r = _req(fb, h, o, db, 1.0, db_scale)
+        r.u8, r.out = u.data_ptr(), do.data_ptr()
+        dre.append(r)
+    bvox = sum(r.nz * r.ny * r.nx for r in bre)
+    torch.cuda.synchronize()
+    run_all(dre[:8])                                                                       # warm-up
+    _, dwall, _, _ = run_all(dre)
+    # the plain per-cube path on device buffers: one fy_gpu_restore_u8 after another, one stream
+    st = torch.cuda.Stream(device=dev)
+    spp = C.c_void_p(st.cuda_stream)
+
+    def plain_device():
+        for r in dre:
+            fb.check(lib.fy_gpu_restore_u8(C.c_void_p(r.u8), C.c_void_p(r.out), r.nz, r.ny, r.nx, r.f32_min,
+                                           r.f32_max, C.byref(r.phys), C.byref(r.cfg), spp), "fy_gpu_restore_u8")
+        st.synchronize()
+
+    plain_device()
+    t0 = time.perf_counter()
+    plain_device()
+    pdev = bvox / (time.perf_counter() - t0) / 1e6
     run_all(bre[:4])                                                                       # warm-up
     _, bwall, _, _ = run_all(bre)
-    bvox = sum(r.nz * r.ny * r.nx for r in bre)
     batched = {
-        "workload": f"{n_batch} cubes, dims per axis from {dims}, per-cube delta_beta U[200,1000], submitted "
-                    "at once to the request loop; host pinned buffers",
-        "mvox_per_s": bvox / bwall / 1e6,
-        "plain_mvox_per_s": _plain(fb, lib, bre, dev),
+        "workload": f"{n_batch} cubes, dims per axis from {dims} ({bvox / 1e6:.0f} Mvoxel), per-cube delta_beta "
+                    "U[200,1000], submitted at once to the request loop",
+        "resident": {"mvox_per_s": bvox / dwall / 1e6, "plain_mvox_per_s": pdev,
+                     "api": "request loop on device-resident cubes (no link copies) vs the plain per-cube "
+                            "fy_gpu_restore_u8 one after another on one stream"},
+        "host": {"mvox_per_s": bvox / bwall / 1e6, "plain_mvox_per_s": _plain(fb, lib, bre, dev),
+                 "api": "host pinned buffers: request loop vs plain per-cube H2D + chain + D2H"},
+        "mvox_per_s": bvox / dwall / 1e6,
+        "plain_mvox_per_s": pdev,
     }
     lib.fy_server_destroy(srv)
     return served, batched

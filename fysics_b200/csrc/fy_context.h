@@ -69,5 +69,7 @@ inline void count_launch(int k = 1) { ctx().launches += k; }
 inline void enter() { ThreadCtx& c = ctx(); c.status = 0; if (!c.err.empty()) c.err.clear(); }
 // Is `p` host memory that the GPU can DMA directly (pinned / registered)?
 bool is_pinned(const void* p);
+// Is `p` device memory (or managed memory)?
+bool is_device(const void* p);
 
 }  // namespace fy

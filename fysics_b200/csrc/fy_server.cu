@@ -260,7 +260,13 @@ void run_one(fy_server* s, Ticket* t, WorkerBufs& wb) {
     int rc = FY_OK;
     const bool in_pinned = fy::is_pinned(r.u8), out_pinned = fy::is_pinned(r.out);
     const bool timed = wb.ev[1] != nullptr;
-    do {
+    if (fy::is_device(r.u8) && fy::is_device(r.out)) {   // device-resident request: no link copies
+        if (timed) cudaEventRecord(wb.ev[0], st);
+        rc = fy_gpu_restore_u8(r.u8, r.out, r.nz, r.ny, r.nx, r.f32_min, r.f32_max, &r.phys, &r.cfg, st);
+        if (!rc && timed) cudaEventRecord(wb.ev[1], st);
+        if (!rc && (e = cudaStreamSynchronize(st)) != cudaSuccess) rc = fail_cuda(e, "fy_server");
+        if (!rc && timed && cudaEventElapsedTime(&t->chain_ms, wb.ev[0], wb.ev[1]) != cudaSuccess) cudaGetLastError();
+    } else do {
         if ((e = wb.d_in.ensure(n)) != cudaSuccess || (e = wb.d_out.ensure(4 * n)) != cudaSuccess) {
             rc = fail_cuda(e, "fy_server");
             break;

@@ -490,8 +490,9 @@ typedef struct {
                                     free synchronises the device); 0: grow on demand */
 } fy_server_cfg;
 typedef struct {
-    const unsigned char *u8;     /* host input, nz*ny*nx (pinned memory avoids a staging copy) */
-    float *out;                  /* host output, nz*ny*nx floats */
+    const unsigned char *u8;     /* input, nz*ny*nx: host (pinned avoids a staging copy) or, together
+                                    with out, device memory (the chain then runs in place, no copies) */
+    float *out;                  /* output, nz*ny*nx floats: host, or device when u8 is */
     int    nz, ny, nx;
     double f32_min, f32_max;     /* dewindow range (fy_u8_to_phys) */
     fy_physics phys;

@@ -120,3 +120,34 @@ def test_budget_admits_one_at_a_time_and_refuses_oversize(gpu):
     lib.fy_server_destroy(srv)
     for r, o in zip(reqs, outs):
         assert np.array_equal(o, alone(gpu, r))
+
+
+def test_device_resident_requests_equal_alone(gpu):
+    """Requests whose input and output are device memory run the chain in place (no link
+    copies); results equal the single-cube call, several requests at once."""
+    import torch
+    lib = gpu.load()
+    shapes = SHAPES[:6]
+    ins = [torch.from_numpy(phantom(s, 20 + i)).cuda() for i, s in enumerate(shapes)]
+    outs = [torch.full(s, float("nan"), dtype=torch.float32, device="cuda") for s in shapes]
+    reqs = []
+    for i, (u, o) in enumerate(zip(ins, outs)):
+        r = request(gpu, np.zeros(shapes[i], np.uint8), np.zeros(1, np.float32), 20 + i)
+        r.u8, r.out = u.data_ptr(), o.data_ptr()
+        reqs.append(r)
+    torch.cuda.synchronize()
+    srv = make_server(gpu)
+    ts = []
+    for r in reqs:
+        t = C.c_longlong()
+        assert lib.fy_server_submit(srv, C.byref(r), C.byref(t)) == 0
+        ts.append(t.value)
+    for t in ts:
+        res = gpu.RequestResult()
+        assert lib.fy_server_wait(srv, t, -1.0, C.byref(res)) == 0, lib.fy_gpu_last_error()
+        assert res.status == 0 and res.h2d_ms == 0 and res.d2h_ms == 0
+    lib.fy_server_destroy(srv)
+    for i, r in enumerate(reqs):
+        host = ins[i].cpu().numpy()
+        r.u8 = host.ctypes.data
+        assert np.array_equal(outs[i].cpu().numpy(), alone(gpu, r))
