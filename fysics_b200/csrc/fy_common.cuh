@@ -61,3 +61,10 @@ struct FastDiv {
         return (uint32_t)(((uint64_t)__umulhi(n, m) + n) >> s);
     }
 };
+
+// Programmatic dependent launch. A kernel launched with fy_launch_pdl (fy_internal.h) may be
+// scheduled while the previous kernel on its stream is finishing; fy_pdl_wait(), its first
+// statement, then waits until that kernel has completed and its memory is visible (and is a
+// no-op for a normal launch). Nothing before it may touch global memory.
+FY_D void fy_pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+

@@ -112,6 +112,25 @@ inline cudaError_t fy_smem_optin(K kernel, size_t bytes) {
     return fy_smem_optin_raw((const void*)kernel, bytes);
 }
 
+// Launch with programmatic stream serialization: the kernel (which starts with fy_pdl_wait())
+// may be scheduled before the previous kernel on `st` has finished, hiding the launch gap
+// between a chain of small dependent kernels.
+template <class... KArgs, class... Args>
+inline cudaError_t fy_launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                                 Args... args) {
+    cudaLaunchConfig_t c = {};
+    c.gridDim = grid;
+    c.blockDim = block;
+    c.dynamicSmemBytes = smem;
+    c.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    c.attrs = at;
+    c.numAttrs = 1;
+    return cudaLaunchKernelEx(&c, k, ((KArgs)args)...);
+}
+
 // Runtime elements-per-thread (fy_fft_e) -> compile-time E for kernel instantiation.
 template <class F>
 inline cudaError_t fy_with_e(int e, F&& f) {

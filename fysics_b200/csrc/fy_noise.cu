@@ -167,6 +167,7 @@ __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean
                                                   uint8_t* __restrict__ bin, NoiseCtl* __restrict__ ctl,
                                                   int shift, float* __restrict__ cval = nullptr,
                                                   uint8_t* __restrict__ clab = nullptr, long long cap = 0) {
+    fy_pdl_wait();
     extern __shared__ unsigned int h[];
     __shared__ uint32_t sp[256];
     __shared__ float fe[NB + 1];
@@ -310,6 +311,7 @@ __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean
 // After the last digit, the next non-empty bucket of that digit is the smallest key above
 // the selected one within the prefix; k_sel_next scans only when there is none.
 __global__ void __launch_bounds__(256) k_sel_scan(NoiseCtl* __restrict__ ctl, int db, int want_mode, int last) {
+    fy_pdl_wait();
     __shared__ unsigned long long part[256];
     __shared__ int s_sel;
     __shared__ unsigned int s_nextb;
@@ -364,6 +366,7 @@ __global__ void __launch_bounds__(256) k_sel_scan(NoiseCtl* __restrict__ ctl, in
 __global__ void __launch_bounds__(256) k_sel_next(const float* __restrict__ mean, const float* __restrict__ var,
                                                   const uint8_t* __restrict__ bin, NoiseCtl* __restrict__ ctl,
                                                   int want_mode) {
+    fy_pdl_wait();
     __shared__ uint32_t sp[NT_MAX];
     __shared__ int sn[NT_MAX];
     __shared__ unsigned int smin[NT_MAX];
@@ -420,6 +423,7 @@ FY_D void target_init(NoiseCtl* ctl, int t, long long k, long long group_n, bool
 }
 
 __global__ void k_noise_setup(NoiseCtl* ctl, long long n, double flat_pct, double ref_intensity) {
+    fy_pdl_wait();
     ctl->n = n;
     ctl->flat_pct = flat_pct;
     ctl->ref_intensity = ref_intensity;
@@ -434,6 +438,7 @@ __global__ void k_noise_setup(NoiseCtl* ctl, long long n, double flat_pct, doubl
 
 // lo/hi from the selected means; bin edges (noise.c:106-119)
 __global__ void k_noise_bins_setup(NoiseCtl* ctl) {
+    fy_pdl_wait();
     const long long n = ctl->n;
     const double i1 = 1.0 / 100.0 * (double)(n - 1), i99 = 99.0 / 100.0 * (double)(n - 1);
     const long long k1 = (long long)i1, k99 = (long long)i99;
@@ -460,6 +465,7 @@ __global__ void k_noise_bins_setup(NoiseCtl* ctl) {
 // histogram; targets of the flat_pct percentile for bins with >= 200 voxels (noise.c:123).
 // Bins below that drop out and their histogram is cleared.
 __global__ void __launch_bounds__(256) k_bin_targets(NoiseCtl* ctl) {
+    fy_pdl_wait();
     __shared__ unsigned long long part[256];
     if (ctl->mode != 1) return;
     const int b = blockIdx.x;
@@ -566,6 +572,7 @@ FY_D uint32_t block_select(const uint32_t* keys, int c, long long rank, unsigned
 __global__ void __launch_bounds__(256) k_win_sample(const float* __restrict__ mean, const NoiseCtl* __restrict__ ctl,
                                                     float* __restrict__ sm, long long m, unsigned long long A,
                                                     unsigned long long B) {
+    fy_pdl_wait();
     if (ctl->mode != kModeWin0) return;
     const unsigned long long n = (unsigned long long)ctl->n;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
@@ -577,6 +584,7 @@ __global__ void __launch_bounds__(256) k_win_sample(const float* __restrict__ me
 // digit histograms (kBoundThreads/32 x 256 counters).
 __global__ void __launch_bounds__(kBoundThreads) k_win_bounds(const float* __restrict__ sm,
                                                               NoiseCtl* __restrict__ ctl, long long m) {
+    fy_pdl_wait();
     extern __shared__ uint32_t wkeys[];
     unsigned int* wh = wkeys + kSampleMax;
     __shared__ unsigned long long part[kBoundThreads];
@@ -620,6 +628,7 @@ constexpr int kCountBuf = 1152;          // >= one step's worst case (32 lanes x
 __global__ void __launch_bounds__(256) k_win_count(const float* __restrict__ mean, NoiseCtl* __restrict__ ctl,
                                                    float* __restrict__ cval, uint8_t* __restrict__ clab,
                                                    long long cap) {
+    fy_pdl_wait();
     static_assert(32 * 4 * SU * 2 <= kCountBuf, "one step must fit the warp buffer");
     __shared__ float bufv[256 / 32][kCountBuf];
     __shared__ uint8_t bufl[256 / 32][kCountBuf];
@@ -700,6 +709,7 @@ __global__ void __launch_bounds__(256) k_win_count(const float* __restrict__ mea
 // (both targets active with the empty prefix, like the bin selection's labelling pass), or,
 // when the candidate list overflowed, sends the selection to the radix passes.
 __global__ void k_win_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc, long long cap) {
+    fy_pdl_wait();
     if (ctl->mode != kModeWin0) { cc->mode = 3; return; }
     for (int t = 0; t < NT_MAX; ++t) target_init(cc, t, 0, 0, t < 2);
     cc->ntarget = 2;
@@ -717,6 +727,7 @@ __global__ void k_win_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc,
 // is the sum of its histogram; its rank among the candidates is r = k - below, which must
 // leave k and (when it exists) k+1 inside. Otherwise the selection fails (k_win_check).
 __global__ void __launch_bounds__(256) k_win_targets(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) {
+    fy_pdl_wait();
     __shared__ unsigned long long part[256];
     if (cc->mode != 1) return;
     const int t = blockIdx.x;
@@ -743,12 +754,14 @@ __global__ void __launch_bounds__(256) k_win_targets(NoiseCtl* __restrict__ ctl,
 
 // The bins' candidate list (section 2b). Reset before the compacting pass.
 __global__ void k_bin_cand_reset(NoiseCtl* __restrict__ ctl) {
+    fy_pdl_wait();
     if (ctl->mode == 1) ctl->ncand = 0;
 }
 // After the compacting pass and its scan: when the list fits, the bins' targets move to the
 // candidate block for the last digit and the whole-field pass stands aside; otherwise the
 // candidate pass stands aside.
 __global__ void __launch_bounds__(256) k_bin_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc, long long cap) {
+    fy_pdl_wait();
     __shared__ int s_go;
     if (threadIdx.x == 0) s_go = ctl->mode == 1 && (long long)ctl->ncand <= cap;
     __syncthreads();
@@ -777,6 +790,7 @@ __global__ void __launch_bounds__(256) k_bin_arm(NoiseCtl* __restrict__ ctl, Noi
 }
 // After the candidates' last digit: the selected keys back into the main block.
 __global__ void k_bin_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restrict__ cc) {
+    fy_pdl_wait();
     if (ctl->mode != kModeBinCand) return;
     for (int t = 0; t < NT_MAX; ++t) {
         ctl->tprefix[t] = cc->tprefix[t];
@@ -790,6 +804,7 @@ __global__ void k_bin_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restr
 
 // One thread: a failed window sends the selection to the radix passes over the whole field.
 __global__ void k_win_check(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) {
+    fy_pdl_wait();
     if (ctl->mode != kModeWin0 || !ctl->wfail) return;
     cc->mode = 3;
     ctl->mode = 0;
@@ -798,6 +813,7 @@ __global__ void k_win_check(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ c
 // Keys of order statistics k and k+1 into the main block's targets 0/1 (interp / next_value
 // form); the radix passes of mode 0 then stand aside.
 __global__ void k_win_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restrict__ cc) {
+    fy_pdl_wait();
     if (ctl->mode != kModeWin0) return;
     for (int t = 0; t < 2; ++t) {
         ctl->tprefix[t] = cc->tprefix[t];
@@ -830,6 +846,7 @@ FY_D double pct_small(double* v, int n, double pct) {       // percentile() on <
 // One warp: lane b handles bin b's reads, so the bins' loads are in flight together; the
 // sequential fit then runs on lane 0 from shared memory.
 __global__ void __launch_bounds__(32) k_noise_fit(NoiseCtl* ctl, int stage) {
+    fy_pdl_wait();
     static_assert(NB <= 32, "one lane per bin");
     const int lane = threadIdx.x;
     if (stage == 0) {
@@ -971,6 +988,13 @@ size_t fy_noise_scratch_floats(size_t n) { return noise_layout(n).total; }
 // fy_noise_ctl_bytes(). Supports win in {3..9} (r = win/2 <= 4). guided_mv (optional,
 // 2n floats): the statistics pass also writes the guided filter's (mean, var) pairs of the
 // same window, for fy_launch_guided_apply_mv with r = win/2.
+// Every selection kernel runs as a programmatic dependent launch; the first failed launch
+// is returned.
+#define PDL(k, ...)                                                            \
+    do {                                                                       \
+        const cudaError_t pe_ = fy_launch_pdl(k, __VA_ARGS__);                 \
+        if (pe_ != cudaSuccess) return pe_;                                    \
+    } while (0)
 cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, int win, double flat_pct,
                                      double ref_intensity, float* scratch, void* ctl_mem, int sms,
                                      cudaStream_t st, int& launches, float* guided_mv) {
@@ -996,7 +1020,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     if ((e = fy_smem_optin(k_win_bounds, smem_keys)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(ctl->hist, 0, sizeof(ctl->hist), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(cc->hist, 0, sizeof(cc->hist), st)) != cudaSuccess) return e;
-    k_noise_setup<<<1, 1, 0, st>>>(ctl, n, flat_pct, ref_intensity);
+    PDL(k_noise_setup, 1, 1, 0, st, ctl, n, flat_pct, ref_intensity);
     {   // 1. stats
         fyzb::Params sp{};
         sp.nz = nz; sp.ny = ny; sp.nx = nx;
@@ -1010,59 +1034,59 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     // of mode 1 over the candidates (control block cc, targets = labels); the radix passes
     // over the whole field (11 + 11 + 10 bits, then the k+1 neighbours) run only if the
     // window misses
-    k_win_sample<<<64, 256, 0, st>>>(mean, ctl, sm, m, wa, wb);
-    k_win_bounds<<<dim3(2, 2), kBoundThreads, smem_keys, st>>>(sm, ctl, m);
-    k_win_count<<<g, 256, 0, st>>>(mean, ctl, cval, clab, L.cap);
-    k_win_arm<<<1, 1, 0, st>>>(ctl, cc, L.cap);
+    PDL(k_win_sample, 64, 256, 0, st, mean, ctl, sm, m, wa, wb);
+    PDL(k_win_bounds, dim3(2, 2), kBoundThreads, smem_keys, st, sm, ctl, m);
+    PDL(k_win_count, g, 256, 0, st, mean, ctl, cval, clab, L.cap);
+    PDL(k_win_arm, 1, 1, 0, st, ctl, cc, L.cap);
     for (int sh = 24; sh >= 0; sh -= 8) {
-        k_sel_hist<8, 1><<<gc, 256, smem_bin, st>>>(nullptr, cval, clab, cc, sh);
+        PDL((k_sel_hist<8, 1>), gc, 256, smem_bin, st, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL);
         if (sh == 24) {
-            k_win_targets<<<2, 256, 0, st>>>(ctl, cc);
-            k_win_check<<<1, 1, 0, st>>>(ctl, cc);
+            PDL(k_win_targets, 2, 256, 0, st, ctl, cc);
+            PDL(k_win_check, 1, 1, 0, st, ctl, cc);
         }
-        k_sel_scan<<<2, 256, 0, st>>>(cc, 8, 1, sh == 0);
+        PDL(k_sel_scan, 2, 256, 0, st, cc, 8, 1, sh == 0);
     }
-    k_sel_next<<<gc, 256, 0, st>>>(nullptr, cval, clab, cc, 1);
-    k_win_finish<<<1, 1, 0, st>>>(ctl, cc);
+    PDL(k_sel_next, gc, 256, 0, st, nullptr, cval, clab, cc, 1);
+    PDL(k_win_finish, 1, 1, 0, st, ctl, cc);
     const int all_digits[3][2] = {{21, 11}, {10, 11}, {0, 10}};
     for (int i = 0; i < 3; ++i) {
-        if (all_digits[i][1] == 11) k_sel_hist<11, 0><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0]);
-        else k_sel_hist<10, 0><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0]);
-        k_sel_scan<<<2, 256, 0, st>>>(ctl, all_digits[i][1], 0, i == 2);
+        if (all_digits[i][1] == 11) PDL((k_sel_hist<11, 0>), g, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
+        else PDL((k_sel_hist<10, 0>), g, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
+        PDL(k_sel_scan, 2, 256, 0, st, ctl, all_digits[i][1], 0, i == 2);
     }
-    k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 0);
-    k_noise_bins_setup<<<1, 1, 0, st>>>(ctl);
+    PDL(k_sel_next, g, 256, 0, st, mean, var, bin, ctl, 0);
+    PDL(k_noise_bins_setup, 1, 1, 0, st, ctl);
     fy_prof_mark(st, "noise.lohi");
     // 2b. per-bin flat_pct percentile of the variance: 4 x 8 bits, then the k+1 neighbours;
     // the first pass also labels the voxels with their bins and yields the bin counts. The
     // third pass also lists the voxels that match their bin's 16-bit prefix (~1% of them),
     // and the last digit runs over that list (falling back to the whole field if it overflows).
-    k_sel_hist<8, 1, true><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, 24);
-    k_bin_targets<<<NB, 256, 0, st>>>(ctl);
-    k_sel_scan<<<NB, 256, 0, st>>>(ctl, 8, 1, 0);
-    k_sel_hist<8, 1><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, 16);
-    k_sel_scan<<<NB, 256, 0, st>>>(ctl, 8, 1, 0);
-    k_bin_cand_reset<<<1, 1, 0, st>>>(ctl);
+    PDL((k_sel_hist<8, 1, true>), g, 256, smem_bin, st, mean, var, bin, ctl, 24, nullptr, nullptr, 0LL);
+    PDL(k_bin_targets, NB, 256, 0, st, ctl);
+    PDL(k_sel_scan, NB, 256, 0, st, ctl, 8, 1, 0);
+    PDL((k_sel_hist<8, 1>), g, 256, smem_bin, st, mean, var, bin, ctl, 16, nullptr, nullptr, 0LL);
+    PDL(k_sel_scan, NB, 256, 0, st, ctl, 8, 1, 0);
+    PDL(k_bin_cand_reset, 1, 1, 0, st, ctl);
     if ((e = fy_smem_optin(k_sel_hist<8, 1, false, true>, smem_bin_c)) != cudaSuccess) return e;
-    k_sel_hist<8, 1, false, true><<<g, 256, smem_bin_c, st>>>(mean, var, bin, ctl, 8, cval, clab, L.cap);
-    k_sel_scan<<<NB, 256, 0, st>>>(ctl, 8, 1, 0);
-    k_bin_arm<<<1, 256, 0, st>>>(ctl, cc, L.cap);
-    k_sel_hist<8, 1><<<g, 256, smem_bin, st>>>(mean, var, bin, ctl, 0);        // overflow only
-    k_sel_scan<<<NB, 256, 0, st>>>(ctl, 8, 1, 1);
-    k_sel_hist<8, 1><<<gc, 256, smem_bin, st>>>(nullptr, cval, clab, cc, 0);   // the list
-    k_sel_scan<<<NB, 256, 0, st>>>(cc, 8, 1, 1);
-    k_bin_finish<<<1, 1, 0, st>>>(ctl, cc);
-    k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 1);
-    k_noise_fit<<<1, 32, 0, st>>>(ctl, 0);
+    PDL((k_sel_hist<8, 1, false, true>), g, 256, smem_bin_c, st, mean, var, bin, ctl, 8, cval, clab, L.cap);
+    PDL(k_sel_scan, NB, 256, 0, st, ctl, 8, 1, 0);
+    PDL(k_bin_arm, 1, 256, 0, st, ctl, cc, L.cap);
+    PDL((k_sel_hist<8, 1>), g, 256, smem_bin, st, mean, var, bin, ctl, 0, nullptr, nullptr, 0LL);        // overflow only
+    PDL(k_sel_scan, NB, 256, 0, st, ctl, 8, 1, 1);
+    PDL((k_sel_hist<8, 1>), gc, 256, smem_bin, st, nullptr, cval, clab, cc, 0, nullptr, nullptr, 0LL);   // the list
+    PDL(k_sel_scan, NB, 256, 0, st, cc, 8, 1, 1);
+    PDL(k_bin_finish, 1, 1, 0, st, ctl, cc);
+    PDL(k_sel_next, g, 256, 0, st, mean, var, bin, ctl, 1);
+    PDL(k_noise_fit, 1, 32, 0, st, ctl, 0);
     fy_prof_mark(st, "noise.bin_select");
     // 2c. fallback (mode 2 only): flat_pct percentile over all voxels' variance
     for (int i = 0; i < 3; ++i) {
-        if (all_digits[i][1] == 11) k_sel_hist<11, 2><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0]);
-        else k_sel_hist<10, 2><<<g, 256, smem_all, st>>>(mean, var, bin, ctl, all_digits[i][0]);
-        k_sel_scan<<<1, 256, 0, st>>>(ctl, all_digits[i][1], 2, i == 2);
+        if (all_digits[i][1] == 11) PDL((k_sel_hist<11, 2>), g, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
+        else PDL((k_sel_hist<10, 2>), g, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
+        PDL(k_sel_scan, 1, 256, 0, st, ctl, all_digits[i][1], 2, i == 2);
     }
-    k_sel_next<<<g, 256, 0, st>>>(mean, var, bin, ctl, 2);
-    k_noise_fit<<<1, 32, 0, st>>>(ctl, 1);
+    PDL(k_sel_next, g, 256, 0, st, mean, var, bin, ctl, 2);
+    PDL(k_noise_fit, 1, 32, 0, st, ctl, 1);
     launches += 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 7 + 1 + 15 + 1 + 1 + 7 + 1;
     return cudaGetLastError();
 }
