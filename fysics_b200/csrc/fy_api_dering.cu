@@ -253,6 +253,7 @@ struct fy_gpu_dering {
 
 namespace {
 __global__ void k_u64_to_f32(const unsigned long long* s, float* f, size_t n) {
+    fy_pdl_wait();
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         f[i] = (float)s[i];
 }
@@ -336,8 +337,10 @@ extern "C" int fy_gpu_dering_finalize(fy_gpu_dering* h, int hp_win, unsigned int
     finalize_defaults(hp_win, min_amp, max_amp);
     cudaStream_t st = (cudaStream_t)stream;
     const size_t nb = (size_t)h->geo.nslab * h->geo.ns * h->geo.nr;
-    k_u64_to_f32<<<(unsigned)((nb + 255) / 256 < 1024 ? (nb + 255) / 256 : 1024), 256, 0, st>>>(h->dsum, h->dsumf, nb);
-    cudaError_t e = fy_launch_dering_finalize(h->dsumf, h->dcnt, h->dring, h->dscr, h->ddet, h->dhave, h->geo.nslab,
+    cudaError_t e = fy_launch_pdl(k_u64_to_f32, dim3((unsigned)((nb + 255) / 256 < 1024 ? (nb + 255) / 256 : 1024)),
+                                  dim3(256), 0, st, (const unsigned long long*)h->dsum, h->dsumf, nb);
+    if (e != cudaSuccess) return fail_cuda(e, "fy_gpu_dering_finalize");
+    e = fy_launch_dering_finalize(h->dsumf, h->dcnt, h->dring, h->dscr, h->ddet, h->dhave, h->geo.nslab,
                                               h->geo.ns, h->geo.nr, hp_win, min_cnt, min_amp, max_amp, st);
     if (e != cudaSuccess) return fail_cuda(e, "fy_gpu_dering_finalize");
     fy::count_launch(4);

@@ -79,6 +79,7 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(const T* __restrict__ sr
                                                         const __grid_constant__ FftPlan pl,
                                                         const float2* __restrict__ tw, int wlog, FastDiv dchunk,
                                                         FastDiv dhx, FastDiv dpad) {
+    fy_pdl_wait();
     extern __shared__ float4 smem4[];
     const int W = 1 << wlog, LPX = g.px + 1;
     float2* s = reinterpret_cast<float2*>(smem4);
@@ -142,6 +143,7 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(const T* __restrict__ sr
 template <int N, int E>
 __global__ void __launch_bounds__(KB<E>::nt, 2) k_y_fwd(float2* __restrict__ spec, SpecGeom g, const __grid_constant__ FftPlan pl,
                                                  const float2* __restrict__ tw, int wlog) {
+    fy_pdl_wait();
     extern __shared__ float4 smem4[];
     const int W = 1 << wlog;
     float2* s = reinterpret_cast<float2*>(smem4);
@@ -169,6 +171,7 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_z_weight(float2* __restrict__ 
                                                        const double* __restrict__ fz2,
                                                        const double* __restrict__ fy2,
                                                        const double* __restrict__ fx2, double us, int wlog) {
+    fy_pdl_wait();
     extern __shared__ float4 smem4[];
     const int W = 1 << wlog;
     float2* s = reinterpret_cast<float2*>(smem4);
@@ -213,6 +216,7 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_z_weight(float2* __restrict__ 
 template <int N, int E>
 __global__ void __launch_bounds__(KB<E>::nt, 2) k_y_inv(float2* __restrict__ spec, SpecGeom g, const __grid_constant__ FftPlan pl,
                                                  const float2* __restrict__ tw, int keep_rows, int wlog) {
+    fy_pdl_wait();
     extern __shared__ float4 smem4[];
     const int W = 1 << wlog;
     float2* s = reinterpret_cast<float2*>(smem4);
@@ -233,6 +237,7 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_inv(const float2* __restrict
                                                         SpecGeom g, const __grid_constant__ FftPlan pl,
                                                         const float2* __restrict__ tw, float invN, int wlog,
                                                         FastDiv dchunk, FastDiv dhx) {
+    fy_pdl_wait();
     extern __shared__ float4 smem4[];
     const int W = 1 << wlog, LPX = g.px + 1;
     float2* s = reinterpret_cast<float2*>(smem4);
@@ -304,8 +309,9 @@ cudaError_t fy_deconv_pass(int pass, const DeconvLaunch& d, cudaStream_t st) {
 #define FY_P1(T, V)                                                                                   \
             { auto k = k_x_fwd<N, E, T, V>;                                                           \
               if ((e2 = fy_smem_optin(k, smem)) != cudaSuccess) return e2;                            \
-              k<<<grid, t.NT, smem, st>>>((const T*)d.src, d.lo, d.scale, d.src_u8, d.spec, g, d.plx, d.twx, \
-                                          t.wlog, dch, dhx, dpad); }
+              if ((e2 = fy_launch_pdl(k, dim3(grid), dim3(t.NT), smem, st, (const T*)d.src, d.lo, d.scale,      \
+                                      d.src_u8, d.spec, g, d.plx, d.twx, t.wlog, dch, dhx, dpad)) != cudaSuccess) \
+                  return e2; }
             if (d.src_u8) { if (vec) FY_P1(uint8_t, 4) else FY_P1(uint8_t, 1) }
             else { if (vec) FY_P1(float, 4) else FY_P1(float, 1) }
 #undef FY_P1
@@ -323,12 +329,15 @@ cudaError_t fy_deconv_pass(int pass, const DeconvLaunch& d, cudaStream_t st) {
                 auto k = k_y_fwd<N, E>;
                 cudaError_t e2 = fy_smem_optin(k, smem);
                 if (e2 != cudaSuccess) return e2;
-                k<<<grid, t.NT, smem, st>>>(d.spec, g, d.ply, d.twy, t.wlog);
+                if ((e2 = fy_launch_pdl(k, grid, dim3(t.NT), smem, st, d.spec, g, d.ply, d.twy, t.wlog)) != cudaSuccess)
+                    return e2;
             } else {
                 auto k = k_y_inv<N, E>;
                 cudaError_t e2 = fy_smem_optin(k, smem);
                 if (e2 != cudaSuccess) return e2;
-                k<<<grid, t.NT, smem, st>>>(d.spec, g, d.ply, d.twy, g.ny, t.wlog);
+                if ((e2 = fy_launch_pdl(k, grid, dim3(t.NT), smem, st, d.spec, g, d.ply, d.twy, g.ny, t.wlog)) !=
+                    cudaSuccess)
+                    return e2;
             }
             return cudaGetLastError();
         });
@@ -343,7 +352,9 @@ cudaError_t fy_deconv_pass(int pass, const DeconvLaunch& d, cudaStream_t st) {
             auto k = k_z_weight<N, E>;
             cudaError_t e2 = fy_smem_optin(k, smem);
             if (e2 != cudaSuccess) return e2;
-            k<<<grid, t.NT, smem, st>>>(d.spec, g, d.plz, d.twz, d.lut, d.fz2, d.fy2, d.fx2, d.us, t.wlog);
+            if ((e2 = fy_launch_pdl(k, grid, dim3(t.NT), smem, st, d.spec, g, d.plz, d.twz, d.lut, d.fz2, d.fy2, d.fx2,
+                                    d.us, t.wlog)) != cudaSuccess)
+                return e2;
             return cudaGetLastError();
         });
     }
@@ -360,11 +371,15 @@ cudaError_t fy_deconv_pass(int pass, const DeconvLaunch& d, cudaStream_t st) {
             if (vec) {
                 auto k = k_x_inv<N, E, 4>;
                 if ((e2 = fy_smem_optin(k, smem)) != cudaSuccess) return e2;
-                k<<<grid, t.NT, smem, st>>>(d.spec, d.dst, g, d.plx, d.twx, invN, t.wlog, dch, dhx);
+                if ((e2 = fy_launch_pdl(k, dim3(grid), dim3(t.NT), smem, st, (const float2*)d.spec, d.dst, g, d.plx,
+                                        d.twx, invN, t.wlog, dch, dhx)) != cudaSuccess)
+                    return e2;
             } else {
                 auto k = k_x_inv<N, E, 1>;
                 if ((e2 = fy_smem_optin(k, smem)) != cudaSuccess) return e2;
-                k<<<grid, t.NT, smem, st>>>(d.spec, d.dst, g, d.plx, d.twx, invN, t.wlog, dch, dhx);
+                if ((e2 = fy_launch_pdl(k, dim3(grid), dim3(t.NT), smem, st, (const float2*)d.spec, d.dst, g, d.plx,
+                                        d.twx, invN, t.wlog, dch, dhx)) != cudaSuccess)
+                    return e2;
             }
             return cudaGetLastError();
         });

@@ -74,7 +74,9 @@ __global__ void __launch_bounds__(256) k_dering_smooth(const float* __restrict__
                                                        const unsigned int* __restrict__ cnt,
                                                        float* __restrict__ p, float* __restrict__ hp,
                                                        unsigned char* __restrict__ vd, int ns, int nr, int hw,
-                                                       unsigned min_cnt) {
+                                                       unsigned min_cnt, unsigned long long* __restrict__ detected) {
+    fy_pdl_wait();
+    if (blockIdx.x == 0 && threadIdx.x == 0) *detected = 0;   // the vote counts after this kernel
     extern __shared__ float sm_f[];
     float* sp = sm_f;                                  // p, hp and validity of this row in smem
     float* shp = sp + nr;
@@ -122,6 +124,7 @@ __global__ void __launch_bounds__(256) k_dering_smooth(const float* __restrict__
 __global__ void k_dering_vote(const float* __restrict__ hp, const unsigned char* __restrict__ vd,
                               float* __restrict__ ring, int nslab, int ns, int nr, float min_amp, float max_amp,
                               unsigned long long* __restrict__ detected) {
+    fy_pdl_wait();
     const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (slab, radius)
     if (id >= (long)nslab * nr) return;
     const int s = (int)(id / nr), r = (int)(id % nr);
@@ -155,6 +158,7 @@ __global__ void k_dering_vote(const float* __restrict__ hp, const unsigned char*
 
 // detected -> have_rings (dering.c:192)
 __global__ void k_dering_flag(const unsigned long long* detected, int* have_rings) {
+    fy_pdl_wait();
     *have_rings = *detected >= 2;
 }
 
@@ -218,18 +222,20 @@ cudaError_t fy_launch_dering_finalize(const float* sum_f, const unsigned int* cn
     float* p = (float*)scratch;
     float* hp = p + nb;
     unsigned char* vd = (unsigned char*)(hp + nb);
-    cudaError_t e = cudaMemsetAsync(detected, 0, sizeof(unsigned long long), st);
-    if (e != cudaSuccess) return e;
     const int hw = hp_win / 2;
     const size_t smem = (size_t)nr * (2 * sizeof(float) + 2);
-    e = fy_smem_optin(k_dering_smooth, smem);
+    cudaError_t e = fy_smem_optin(k_dering_smooth, smem);
     if (e != cudaSuccess) return e;
-    k_dering_smooth<<<nslab * ns, 256, smem, st>>>(sum_f, cnt, p, hp, vd, ns, nr, hw, min_cnt);
+    // the smoothing also zeroes the detected count (block 0), which the vote then adds to;
+    // the three run as programmatic dependent launches
+    if ((e = fy_launch_pdl(k_dering_smooth, dim3(nslab * ns), dim3(256), smem, st, sum_f, cnt, p, hp, vd, ns, nr, hw,
+                           min_cnt, detected)) != cudaSuccess)
+        return e;
     const long nv = (long)nslab * nr;
-    k_dering_vote<<<(unsigned)((nv + 127) / 128), 128, 0, st>>>(hp, vd, ring, nslab, ns, nr, (float)min_amp,
-                                                                (float)max_amp, detected);
-    k_dering_flag<<<1, 1, 0, st>>>(detected, have_rings);
-    return cudaGetLastError();
+    if ((e = fy_launch_pdl(k_dering_vote, dim3((unsigned)((nv + 127) / 128)), dim3(128), 0, st, hp, vd, ring, nslab, ns,
+                           nr, (float)min_amp, (float)max_amp, detected)) != cudaSuccess)
+        return e;
+    return fy_launch_pdl(k_dering_flag, dim3(1), dim3(1), 0, st, detected, have_rings);
 }
 
 size_t fy_dering_finalize_scratch(int nslab, int ns, int nr) {

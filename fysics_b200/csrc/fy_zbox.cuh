@@ -207,6 +207,7 @@ FY_D void stage_plane(float* dst, const Params& p, int zi, int x0, int y0) {
 
 template <int R, int KIND, bool VEC, bool TMA>
 __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p, const __grid_constant__ TmaMaps tm) {
+    fy_pdl_wait();
     constexpr int C = out_kind(KIND) ? 2 : 1;
     using G = Geo<R, C>;
     constexpr int NR = G::NR;
@@ -549,13 +550,11 @@ inline cudaError_t launch_r(const Params& p, dim3 grid, cudaStream_t st) {
     if (tma) {
         auto k = k_zbox<R, KIND, true, true>;
         if ((e = fy_smem_optin(k, smem)) != cudaSuccess) return e;
-        k<<<grid, NT, smem, st>>>(p, tm);
-    } else {
-        auto k = k_zbox<R, KIND, VEC, false>;
-        if ((e = fy_smem_optin(k, smem)) != cudaSuccess) return e;
-        k<<<grid, NT, smem, st>>>(p, tm);
+        return fy_launch_pdl(k, grid, dim3(NT), smem, st, p, tm);
     }
-    return cudaGetLastError();
+    auto k = k_zbox<R, KIND, VEC, false>;
+    if ((e = fy_smem_optin(k, smem)) != cudaSuccess) return e;
+    return fy_launch_pdl(k, grid, dim3(NT), smem, st, p, tm);
 }
 
 // Number of bounded waits that expired in this translation unit's box passes (0 expected).

@@ -35,7 +35,8 @@ def chain(fb, u8):
 
 def cube():
     import fysics_b200.phantom as ph
-    return ph.phantom(SHAPE, seed=4, delta_beta=175.0, pixel_um=2.4, fz2_scale=1.17 ** 2, device="cpu")
+    u = ph.phantom(SHAPE, seed=4, delta_beta=175.0, pixel_um=2.4, fz2_scale=1.17 ** 2, device="cpu")
+    return np.ascontiguousarray(u.numpy() if hasattr(u, "numpy") else u)
 
 
 def test_forced_shapes_are_bit_identical(gpu, tmp_path, monkeypatch):
