@@ -270,6 +270,8 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     int ri[4] = {0, 0, 0, 0};
     float rv[4] = {0.f, 0.f, 0.f, 0.f};                           // ring values of the cached slab
     long rslab = -1;
+    long rlo = 1, rhi = 0;                                        // global z range of the cached ring slab
+    const float rz_in = recip_count(R, 2 * R + 1, R);             // 1/(2R+1): interior planes
     if (out_kind(KIND) && p.out_mode == 0 && p.ra.ring) {
         rings = p.ra.have ? (*p.ra.have != 0) : true;
         const double gxd = (double)(p.ra.x0 + gx) - p.ra.cx;
@@ -438,18 +440,25 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
             }
             if (!emit) continue;
             if (out_kind(KIND) && rings) {                        // this plane's ring slab (dering.c:212-215)
-                long sl = (p.ra.z0 + zo) / p.ra.slab_z;
-                if (sl < 0) sl = 0;
-                if (sl >= p.ra.nslab) sl = p.ra.nslab - 1;
-                if (sl != rslab) {
-                    rslab = sl;
+                const long zg = p.ra.z0 + zo;
+                if (!(zg >= rlo && zg < rhi)) {                   // left the cached slab's planes: divide once
+                    const long q = zg / p.ra.slab_z;
+                    rlo = q * p.ra.slab_z;
+                    rhi = rlo + p.ra.slab_z;
+                    long sl = q;
+                    if (sl < 0) sl = 0;
+                    if (sl >= p.ra.nslab) sl = p.ra.nslab - 1;
+                    if (sl != rslab) {
+                        rslab = sl;
 #pragma unroll
-                    for (int k = 0; k < 4; ++k)
-                        rv[k] = ri[k] < p.ra.nr ? __ldg(p.ra.ring + (size_t)sl * p.ra.nr + ri[k]) : 0.f;
+                        for (int k = 0; k < 4; ++k)
+                            rv[k] = ri[k] < p.ra.nr ? __ldg(p.ra.ring + (size_t)sl * p.ra.nr + ri[k]) : 0.f;
+                    }
                 }
             }
-            const float rz = recip_count(zo, nz, R);
-            const int cz = min(zo + R, nz - 1) - max(zo - R, 0) + 1;
+            const bool zint = zo >= R && zo + R <= nz - 1;        // the window's planes all inside
+            const float rz = zint ? rz_in : recip_count(zo, nz, R);
+            const int cz = zint ? 2 * R + 1 : min(zo + R, nz - 1) - max(zo - R, 0) + 1;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 if (y0 + 4 * rg + k >= ny) continue;
