@@ -67,6 +67,9 @@ static int init_device(int device) {
     if (c.st && c.dev != device) {          // switching devices: drop the old state
         cudaStreamDestroy(c.st); c.st = nullptr;
         if (c.ws_done) { cudaEventDestroy(c.ws_done); c.ws_done = nullptr; }
+        if (c.side) { cudaStreamDestroy(c.side); c.side = nullptr; }
+        if (c.fork_ev) { cudaEventDestroy(c.fork_ev); c.fork_ev = nullptr; }
+        if (c.join_ev) { cudaEventDestroy(c.join_ev); c.join_ev = nullptr; }
     }
     c.dev = device;
     cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, device);
@@ -88,6 +91,18 @@ int ensure_ctx() {
     int dev = 0;
     if (const char* s = getenv("FY_DEVICE")) dev = atoi(s);
     return init_device(dev);
+}
+
+int ensure_side() {
+    ThreadCtx& c = t_ctx;
+    cudaError_t e = cudaSuccess;
+    if (!c.side && (e = cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail_cuda(e, "cudaStreamCreate");
+    if (!c.fork_ev && (e = cudaEventCreateWithFlags(&c.fork_ev, cudaEventDisableTiming)) != cudaSuccess)
+        return fail_cuda(e, "cudaEventCreate");
+    if (!c.join_ev && (e = cudaEventCreateWithFlags(&c.join_ev, cudaEventDisableTiming)) != cudaSuccess)
+        return fail_cuda(e, "cudaEventCreate");
+    return FY_OK;
 }
 
 void ws_acquire(cudaStream_t s) {

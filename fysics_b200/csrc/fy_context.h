@@ -38,6 +38,8 @@ struct ThreadCtx {
     cudaStream_t st = nullptr;
     cudaEvent_t ws_done = nullptr;     // last enqueue that used this thread's workspaces
     bool ws_pending = false;
+    cudaStream_t side = nullptr;       // second stream for work that overlaps the chain
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     int status = 0;
     std::string err;
     unsigned long long launches = 0;
@@ -58,6 +60,8 @@ int ensure_ctx();
 // Record a failure for fy_gpu_last_error(); returns code.
 int fail(int code, const char* fmt, ...);
 int fail_cuda(cudaError_t e, const char* what);
+// The thread's side stream and its fork/join events, created on first use.
+int ensure_side();
 // Make `s` wait for the previous user of this thread's workspaces; call before reuse.
 void ws_acquire(cudaStream_t s);
 // Mark the workspaces as used by work enqueued on `s`.

@@ -58,15 +58,24 @@ extern "C" int fy_gpu_restore_u8(const unsigned char* d_u8, float* d_out, int nz
     fy::ThreadCtx& c = ctx();
     cudaStream_t st = (cudaStream_t)stream;
     const size_t n = (size_t)nz * ny * nx;
-    // 1. ring statistics from the raw u8 input (the pipeline accumulates u8 in pass 1)
+    // 1. ring statistics from the raw u8 input (the pipeline accumulates u8 in pass 1). They
+    // need only the input and only the guided output pass reads them, so they run on the
+    // thread's side stream, overlapping the deconvolution and the noise model.
+    bool ring_join = false;
     if (cfg->dering && cfg->dering_accumulate) {
+        if ((rc = fy::ensure_side())) return rc;
+        cudaError_t e0;
+        if ((e0 = cudaEventRecord(c.fork_ev, st)) != cudaSuccess || (e0 = cudaStreamWaitEvent(c.side, c.fork_ev, 0)) !=
+            cudaSuccess)
+            return fail_cuda(e0, what);
         if ((rc = fy_gpu_dering_accumulate_u8(cfg->dering, d_u8, cfg->z0, cfg->y0, cfg->x0, nz, ny, nx,
-                                              cfg->dering_ss, stream)))
+                                              cfg->dering_ss, c.side)))
             return rc;
         if ((rc = fy_gpu_dering_finalize(cfg->dering, cfg->dering_hp_win, cfg->dering_min_cnt, cfg->dering_min_amp,
-                                         cfg->dering_max_amp, stream)))
+                                         cfg->dering_max_amp, c.side)))
             return rc;
-        fy_prof_mark(st, "dering.accumulate+vote");
+        if ((e0 = cudaEventRecord(c.join_ev, c.side)) != cudaSuccess) return fail_cuda(e0, what);
+        ring_join = true;
     }
     fy::ws_acquire(st);
     cudaError_t e;
@@ -109,7 +118,8 @@ extern "C" int fy_gpu_restore_u8(const unsigned char* d_u8, float* d_out, int nz
         launches += 1;
         eps_ptr = d_eps;
     }
-    // 4. guided filter dec -> d_out
+    // 4. guided filter dec -> d_out (after the ring statistics, when they ran on the side stream)
+    if (ring_join && (e = cudaStreamWaitEvent(st, c.join_ev, 0)) != cudaSuccess) return fail_cuda(e, what);
     bool rings_done = false;
     if (cfg->guided_s > 1) {
         const int s = cfg->guided_s;
