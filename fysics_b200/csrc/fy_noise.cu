@@ -1011,6 +1011,12 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     const int r = win / 2;
     const float inv_wc = (float)(1.0 / ((double)win * win * win));
     const unsigned g = grid_sel(n, sms), gc = grid_sel(L.cap, sms);
+    // passes that usually exit at once (the fallbacks, the k+1 scans): one CTA per SM, so the
+    // common case schedules few empty CTAs; when they do run, their grid-stride loops cover
+    // every voxel
+    const unsigned gs = (unsigned)(g < (unsigned)sms ? g : (unsigned)sms);
+    // candidate lists hold ~1-2% of the voxels (their capacity is n/8): two CTAs per SM
+    const unsigned gcl = (unsigned)(gc < 2u * (unsigned)sms ? gc : 2u * (unsigned)sms);
     const size_t smem_all = 2 * 2048 * sizeof(unsigned int), smem_bin = NB * 256 * sizeof(unsigned int);
     const size_t smem_bin_c = smem_bin + (size_t)(256 / 32) * kCompactBuf * (sizeof(float) + 1);
     const size_t smem_keys = (kSampleMax + 256 * (kBoundThreads / 32)) * sizeof(uint32_t);   // keys + warp digit counts
@@ -1039,22 +1045,22 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     PDL(k_win_count, g, 256, 0, st, mean, ctl, cval, clab, L.cap);
     PDL(k_win_arm, 1, 1, 0, st, ctl, cc, L.cap);
     for (int sh = 24; sh >= 0; sh -= 8) {
-        PDL((k_sel_hist<8, 1>), gc, 256, smem_bin, st, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL);
+        PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL);
         if (sh == 24) {
             PDL(k_win_targets, 2, 256, 0, st, ctl, cc);
             PDL(k_win_check, 1, 1, 0, st, ctl, cc);
         }
         PDL(k_sel_scan, 2, 256, 0, st, cc, 8, 1, sh == 0);
     }
-    PDL(k_sel_next, gc, 256, 0, st, nullptr, cval, clab, cc, 1);
+    PDL(k_sel_next, gs, 256, 0, st, nullptr, cval, clab, cc, 1);
     PDL(k_win_finish, 1, 1, 0, st, ctl, cc);
     const int all_digits[3][2] = {{21, 11}, {10, 11}, {0, 10}};
     for (int i = 0; i < 3; ++i) {
-        if (all_digits[i][1] == 11) PDL((k_sel_hist<11, 0>), g, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
-        else PDL((k_sel_hist<10, 0>), g, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
+        if (all_digits[i][1] == 11) PDL((k_sel_hist<11, 0>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
+        else PDL((k_sel_hist<10, 0>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
         PDL(k_sel_scan, 2, 256, 0, st, ctl, all_digits[i][1], 0, i == 2);
     }
-    PDL(k_sel_next, g, 256, 0, st, mean, var, bin, ctl, 0);
+    PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 0);
     PDL(k_noise_bins_setup, 1, 1, 0, st, ctl);
     fy_prof_mark(st, "noise.lohi");
     // 2b. per-bin flat_pct percentile of the variance: 4 x 8 bits, then the k+1 neighbours;
@@ -1071,21 +1077,21 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     PDL((k_sel_hist<8, 1, false, true>), g, 256, smem_bin_c, st, mean, var, bin, ctl, 8, cval, clab, L.cap);
     PDL(k_sel_scan, NB, 256, 0, st, ctl, 8, 1, 0);
     PDL(k_bin_arm, 1, 256, 0, st, ctl, cc, L.cap);
-    PDL((k_sel_hist<8, 1>), g, 256, smem_bin, st, mean, var, bin, ctl, 0, nullptr, nullptr, 0LL);        // overflow only
+    PDL((k_sel_hist<8, 1>), gs, 256, smem_bin, st, mean, var, bin, ctl, 0, nullptr, nullptr, 0LL);       // overflow only
     PDL(k_sel_scan, NB, 256, 0, st, ctl, 8, 1, 1);
-    PDL((k_sel_hist<8, 1>), gc, 256, smem_bin, st, nullptr, cval, clab, cc, 0, nullptr, nullptr, 0LL);   // the list
+    PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, 0, nullptr, nullptr, 0LL);  // the list
     PDL(k_sel_scan, NB, 256, 0, st, cc, 8, 1, 1);
     PDL(k_bin_finish, 1, 1, 0, st, ctl, cc);
-    PDL(k_sel_next, g, 256, 0, st, mean, var, bin, ctl, 1);
+    PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 1);
     PDL(k_noise_fit, 1, 32, 0, st, ctl, 0);
     fy_prof_mark(st, "noise.bin_select");
     // 2c. fallback (mode 2 only): flat_pct percentile over all voxels' variance
     for (int i = 0; i < 3; ++i) {
-        if (all_digits[i][1] == 11) PDL((k_sel_hist<11, 2>), g, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
-        else PDL((k_sel_hist<10, 2>), g, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
+        if (all_digits[i][1] == 11) PDL((k_sel_hist<11, 2>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
+        else PDL((k_sel_hist<10, 2>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
         PDL(k_sel_scan, 1, 256, 0, st, ctl, all_digits[i][1], 2, i == 2);
     }
-    PDL(k_sel_next, g, 256, 0, st, mean, var, bin, ctl, 2);
+    PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 2);
     PDL(k_noise_fit, 1, 32, 0, st, ctl, 1);
     launches += 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 7 + 1 + 15 + 1 + 1 + 7 + 1;
     return cudaGetLastError();
