@@ -875,56 +875,86 @@ __global__ void __launch_bounds__(32) k_noise_fit(NoiseCtl* ctl, int stage) {
         }
         return;
     }
-    __shared__ double s_i[NB], s_f[NB];
+    // stage 1: the used bins compacted in bin order; the weights, residuals and the median
+    // of the residuals are formed by one lane per bin, the five weighted sums by lane 0 in the
+    // reference's order (noise.c:141-147), so every value equals the sequential fit's
+    __shared__ double s_i[NB], s_f[NB], s_w[NB], s_r[NB];
     __shared__ long long s_c[NB];
-    if (lane < NB) {
-        s_c[lane] = (long long)ctl->bcount[lane];
-        s_i[lane] = 0.5 * (ctl->edge[lane] + ctl->edge[lane + 1]);
-        s_f[lane] = ctl->bfloor[lane];
+    __shared__ double s_g, s_b;
+    __shared__ int s_brk;
+    const unsigned full = 0xffffffffu;
+    const bool in_use = lane < NB && (long long)ctl->bcount[lane] >= 200;
+    const unsigned um = __ballot_sync(full, in_use);
+    const int used = __popc(um);
+    if (in_use) {
+        const int pos = __popc(um & ((1u << lane) - 1u));
+        s_c[pos] = (long long)ctl->bcount[lane];
+        s_i[pos] = 0.5 * (ctl->edge[lane] + ctl->edge[lane + 1]);
+        s_f[pos] = ctl->bfloor[lane];
     }
     __syncwarp();
-    if (lane != 0) return;
-    double bin_i[NB], bin_f[NB], wv[NB];
-    long long bin_c[NB];
-    int used = 0;
-    for (int b = 0; b < NB; ++b) {
-        if (s_c[b] < 200) continue;
-        bin_i[used] = s_i[b];
-        bin_f[used] = s_f[b];
-        bin_c[used] = s_c[b];
-        ++used;
-    }
     double g = 0, bb = 0;
     if (ctl->mode == 2) {
-        const long long n = ctl->n;
-        const double idx = ctl->flat_pct / 100.0 * (double)(n - 1);
-        const long long k = (long long)idx;
-        bb = interp(ctl, 0, idx - (double)k, k + 1 < n);
+        if (lane == 0) {
+            const long long n = ctl->n;
+            const double idx = ctl->flat_pct / 100.0 * (double)(n - 1);
+            const long long k = (long long)idx;
+            bb = interp(ctl, 0, idx - (double)k, k + 1 < n);
+        }
     } else if (used >= 3) {                               // IRLS, noise.c:139-161
-        for (int i = 0; i < used; i++) wv[i] = sqrt((double)bin_c[i]);
+        if (lane < used) s_w[lane] = sqrt((double)s_c[lane]);
+        __syncwarp();
         for (int it = 0; it < 4; it++) {
-            double Sw = 0, Swx = 0, Swy = 0, Swxx = 0, Swxy = 0;
-            for (int i = 0; i < used; i++) {
-                const double wi = wv[i], xi = bin_i[i], yi = bin_f[i];
-                Sw += wi; Swx += wi * xi; Swy += wi * yi; Swxx += wi * xi * xi; Swxy += wi * xi * yi;
+            if (lane == 0) {
+                double Sw = 0, Swx = 0, Swy = 0, Swxx = 0, Swxy = 0;
+                for (int i = 0; i < used; i++) {
+                    const double wi = s_w[i], xi = s_i[i], yi = s_f[i];
+                    Sw += wi; Swx += wi * xi; Swy += wi * yi; Swxx += wi * xi * xi; Swxy += wi * xi * yi;
+                }
+                const double det = Sw * Swxx - Swx * Swx;
+                s_brk = fabs(det) < 1e-20;
+                if (!s_brk) {
+                    s_g = (Sw * Swxy - Swx * Swy) / det;
+                    s_b = (Swxx * Swy - Swx * Swxy) / det;
+                }
             }
-            const double det = Sw * Swxx - Swx * Swx;
-            if (fabs(det) < 1e-20) break;
-            g = (Sw * Swxy - Swx * Swy) / det;
-            bb = (Swxx * Swy - Swx * Swxy) / det;
-            double resid[NB], rc[NB];
-            for (int i = 0; i < used; i++) { resid[i] = fabs(bin_f[i] - (g * bin_i[i] + bb)); rc[i] = resid[i]; }
-            const double med = pct_small(rc, used, 50.0) + 1e-9;
-            for (int i = 0; i < used; i++) {
-                const double rr = resid[i] / (2.0 * med);
-                wv[i] = sqrt((double)bin_c[i]) / (1.0 + rr * rr);
+            __syncwarp();
+            if (s_brk) break;
+            g = s_g;
+            bb = s_b;
+            double res = 0.0;
+            if (lane < used) {
+                res = fabs(s_f[lane] - (g * s_i[lane] + bb));
+                s_r[lane] = res;
             }
+            __syncwarp();
+            // percentile(resid, used, 50) (noise.c:66-73): the values at sorted positions lo and
+            // lo + 1, found by ranking each residual (ties by index)
+            const double pidx = 50.0 / 100.0 * (used - 1);
+            const int plo = (int)pidx;
+            const double pf = pidx - plo;
+            int rank = 0;
+            if (lane < used)
+                for (int j = 0; j < used; ++j) rank += s_r[j] < res || (s_r[j] == res && j < lane);
+            const unsigned mlo = __ballot_sync(full, lane < used && rank == plo);
+            const unsigned mhi = __ballot_sync(full, lane < used && rank == plo + 1);
+            const double vlo = __shfl_sync(full, res, mlo ? __ffs(mlo) - 1 : 0);    // (no rank: NaN residuals)
+            const double vhi = __shfl_sync(full, res, mhi ? __ffs(mhi) - 1 : (mlo ? __ffs(mlo) - 1 : 0));
+            const double med = (plo + 1 < used ? vlo * (1 - pf) + vhi * pf : vlo) + 1e-9;
+            if (lane < used) {
+                const double rr = res / (2.0 * med);
+                s_w[lane] = sqrt((double)s_c[lane]) / (1.0 + rr * rr);
+            }
+            __syncwarp();
         }
     } else if (used > 0) {                                // noise.c:162-165
-        double sum = 0;
-        for (int i = 0; i < used; i++) sum += bin_f[i];
-        bb = sum / used;
+        if (lane == 0) {
+            double sum = 0;
+            for (int i = 0; i < used; i++) sum += s_f[i];
+            bb = sum / used;
+        }
     }
+    if (lane != 0) return;
     if (!isfinite(g)) g = 0;
     if (!isfinite(bb)) bb = 0;
     double var_ref = g * ctl->ref_intensity + bb;
@@ -1081,6 +1111,11 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     PDL(k_sel_scan, NB, 256, 0, st, ctl, 8, 1, 1);
     PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, 0, nullptr, nullptr, 0LL);  // the list
     PDL(k_sel_scan, NB, 256, 0, st, cc, 8, 1, 1);
+    // k+1 past the selected key's 24-bit prefix: the list holds every key of the bin that shares
+    // its 16-bit prefix, so when it holds a larger key, its smallest larger key is the next one
+    // (a key in between would share the prefix and be listed too). Only targets whose next key
+    // leaves the 16-bit prefix are left to the whole-field scan below.
+    PDL(k_sel_next, gcl, 256, 0, st, nullptr, cval, clab, cc, 1);
     PDL(k_bin_finish, 1, 1, 0, st, ctl, cc);
     PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 1);
     PDL(k_noise_fit, 1, 32, 0, st, ctl, 0);
@@ -1093,7 +1128,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     }
     PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 2);
     PDL(k_noise_fit, 1, 32, 0, st, ctl, 1);
-    launches += 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 7 + 1 + 15 + 1 + 1 + 7 + 1;
+    launches += 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 7 + 1 + 16 + 1 + 1 + 7 + 1;
     return cudaGetLastError();
 }
 
