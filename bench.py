@@ -1010,7 +1010,7 @@ def main():
     rc_tune = lib.fy_gpu_autotune(*SHAPE, 0)
     t_tune = time.perf_counter() - t_tune
     px = lib.fy_next_fft_size(SHAPE[2])
-    tune_knobs = [f"x1.{px}", f"x5.{px}", "box0.r2.{}x{}x{}".format(*SHAPE), "box3.r2.{}x{}x{}".format(*SHAPE)]
+    tune_knobs = [f"x1.{px}", f"x5.{px}"]
     tuning = {"rc": rc_tune, "seconds": round(t_tune, 2),
               "values": {k: lib.fy_gpu_tune_value(k.encode()) for k in tune_knobs}}
     u8 = benchmark_cube(args, rank, p.delta_beta, f"cuda:{dev}")

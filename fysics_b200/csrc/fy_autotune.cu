@@ -5,8 +5,8 @@
 //   x1.<n>, x5.<n>        lines per CTA (log2) of the deconvolution X passes (forward, inverse)
 //                         of axis length n. Their tiles are line-major, so any power of two up
 //                         to the default fits: fewer lines, more CTAs per SM.
-//   box<K>.r<R>.<nz>x<ny>x<nx>  z chunks of a z-sliding box pass of kind K (0 the noise
-//                         statistics, 3 the guided output from (mean, var)), radius R.
+// The z chunk count of the z-sliding box passes is not a knob: each chunk takes its variance
+// shift from its own first plane, so the chunking changes the float rounding of the sums.
 // fy_gpu_autotune measures candidates of each knob by timing the whole chain on a scratch
 // cube of the given shape (coordinate descent, median of repeated CUDA-event timings) and
 // writes the winners to a JSON cache, one entry per line:
@@ -170,10 +170,6 @@ int save_locked() {
 }
 
 std::string x_knob(int pass, int n) { return "x" + std::to_string(pass) + "." + std::to_string(n); }
-std::string box_knob(int kind, int r, int nz, int ny, int nx) {
-    return "box" + std::to_string(kind) + ".r" + std::to_string(r) + "." + std::to_string(nz) + "x" +
-           std::to_string(ny) + "x" + std::to_string(nx);
-}
 
 __global__ void k_tune_fill(unsigned char* p, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -186,7 +182,6 @@ __global__ void k_tune_fill(unsigned char* p, size_t n) {
 }  // namespace
 
 int fy_tuned_x_wlog(int pass, int n) { return lookup(x_knob(pass, n)); }
-int fy_tuned_box_chunks(int kind, int r, int nz, int ny, int nx) { return lookup(box_knob(kind, r, nz, ny, nx)); }
 
 extern "C" int fy_gpu_tune_load(const char* path) {
     fy::enter();
@@ -212,9 +207,7 @@ extern "C" int fy_gpu_autotune(int nz, int ny, int nx, int flags) {
     const std::string dk = device_key(c.dev);
     if (dk.empty()) return fail(FY_ECUDA, "%s: device properties", what);
     const int px = fy_next_fft_size(nx);
-    const int r = 2;                                       // the chain's guided radius (noise window 5)
-    const std::vector<std::string> knobs = {x_knob(1, px), x_knob(5, px), box_knob(0, r, nz, ny, nx),
-                                            box_knob(3, r, nz, ny, nx)};
+    const std::vector<std::string> knobs = {x_knob(1, px), x_knob(5, px)};
     {
         std::lock_guard<std::mutex> lk(g_mu);
         ensure_loaded();
@@ -269,15 +262,11 @@ extern "C" int fy_gpu_autotune(int nz, int ny, int nx, int flags) {
     std::vector<int> xc = {0};
     for (int wl = tx.wlog - 1; wl >= 1 && wl >= tx.wlog - 2; --wl)
         if ((px << wl) / tx.E >= 32) xc.push_back(wl);
-    const int h = fy_box_default_chunks(nz, ny, nx, r, c.sms), hi = std::max(1, nz / (8 * r));
-    std::vector<int> bc = {0};
-    for (int cand : {h / 2, (3 * h) / 4, (3 * h) / 2, 2 * h})
-        if (cand >= 1 && cand <= hi && cand != h && std::find(bc.begin(), bc.end(), cand) == bc.end()) bc.push_back(cand);
     for (const auto& k : knobs) set(k, 0);
     double best_ms = 0.0;
     rc = chain_ms(best_ms);
     for (size_t ki = 0; ki < knobs.size() && !rc; ++ki) {
-        const std::vector<int>& cands = ki < 2 ? xc : bc;
+        const std::vector<int>& cands = xc;
         int best = 0;
         for (size_t i = 1; i < cands.size() && !rc; ++i) {
             set(knobs[ki], cands[i]);
@@ -290,9 +279,8 @@ extern "C" int fy_gpu_autotune(int nz, int ny, int nx, int flags) {
         }
         set(knobs[ki], best);
         if (!best) {                                       // the default won: record it explicitly
-            const int dv = ki < 2 ? tx.wlog : h;
             std::lock_guard<std::mutex> lk(g_mu);
-            g_table[dk + "#" + knobs[ki]] = dv;
+            g_table[dk + "#" + knobs[ki]] = tx.wlog;
         }
     }
     cudaEventDestroy(e0);

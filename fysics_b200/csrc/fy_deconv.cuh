@@ -90,23 +90,42 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(const T* __restrict__ sr
     load_twiddles(stw, tw, pl.n);
     row_offsets(soff, q0, W, Q, g);
     const int nch = g.nx / VEC;
-    for (int it = threadIdx.x; it < W * nch; it += blockDim.x) {
-        const int l = dchunk.div(it), x = (it - l * nch) * VEC;
-        const long qa = q0 + 2 * l, qb = qa + 1;
-        float va[VEC], vb[VEC];
+    // kU chunks per thread are loaded before any is dewindowed and stored (loads in flight)
+    constexpr int kU = VEC == 1 ? 8 : 4;
+    const int total = W * nch, step = blockDim.x;
+    for (int base = threadIdx.x; base < total; base += kU * step) {
+        float va[kU][VEC], vb[kU][VEC];
+        int L[kU], X[kU];
 #pragma unroll
-        for (int j = 0; j < VEC; ++j) va[j] = vb[j] = 0.f;
-        if (qa < Q) VecLoad<T, VEC>::run(src + qa * g.nx + x, va);
-        if (qb < Q) VecLoad<T, VEC>::run(src + qb * g.nx + x, vb);
-        float2* dst = s + l * LPX + x;
+        for (int u = 0; u < kU; ++u) {
+            const int it = base + u * step;
 #pragma unroll
-        for (int j = 0; j < VEC; ++j) {
-            float a = va[j], b = vb[j];
-            if (is_u8) {                                   // fy_u8_to_phys, FMA as the reference build
-                a = qa < Q ? __fmaf_rn(a, scale, lo) : 0.f;
-                b = qb < Q ? __fmaf_rn(b, scale, lo) : 0.f;
+            for (int j = 0; j < VEC; ++j) va[u][j] = vb[u][j] = 0.f;
+            L[u] = -1;
+            X[u] = 0;
+            if (it < total) {
+                const int l = dchunk.div(it), x = (it - l * nch) * VEC;
+                const long qa = q0 + 2 * l, qb = qa + 1;
+                L[u] = l;
+                X[u] = x;
+                if (qa < Q) VecLoad<T, VEC>::run(src + qa * g.nx + x, va[u]);
+                if (qb < Q) VecLoad<T, VEC>::run(src + qb * g.nx + x, vb[u]);
             }
-            dst[j] = make_float2(a, b);
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            if (L[u] < 0) continue;
+            const long qa = q0 + 2 * L[u], qb = qa + 1;
+            float2* dst = s + L[u] * LPX + X[u];
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) {
+                float a = va[u][j], b = vb[u][j];
+                if (is_u8) {                               // fy_u8_to_phys, FMA as the reference build
+                    a = qa < Q ? __fmaf_rn(a, scale, lo) : 0.f;
+                    b = qb < Q ? __fmaf_rn(b, scale, lo) : 0.f;
+                }
+                dst[j] = make_float2(a, b);
+            }
         }
     }
     const int npad = g.px - g.nx;
@@ -184,7 +203,13 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_z_weight(float2* __restrict__ 
     float2* col = spec + (size_t)blockIdx.y * g.hxp + c0 + ln.l;
     load_twiddles(stw, tw, pl.n);
     for (int i = threadIdx.x; i < pl.n; i += blockDim.x) sfz[i] = fz2[i];
-    for (int i = threadIdx.x; i <= FY_LUT_N; i += blockDim.x) slut[i] = lut[i];
+    // the table as 16-byte loads (the device table holds FY_LUT_N + 4 floats)
+    if ((reinterpret_cast<uintptr_t>(slut) & 15) == 0) {
+        for (int i = threadIdx.x; i < (FY_LUT_N + 4) / 4; i += blockDim.x)
+            reinterpret_cast<float4*>(slut)[i] = __ldg(reinterpret_cast<const float4*>(lut) + i);
+    } else {
+        for (int i = threadIdx.x; i <= FY_LUT_N; i += blockDim.x) slut[i] = lut[i];
+    }
     __syncthreads();
     fft_line<N, E, ct_pitch(N), -1>(s + ln.l, W, ln.tl, pl, stw,
                 [&](int i) {
@@ -249,13 +274,35 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_inv(const float2* __restrict
     row_offsets(soff, q0, W, Q, g);
     __syncthreads();
     const int hi_max = g.px - g.hx;                 // m in [1, px-hx] mirrors to px-m
-    for (int idx = threadIdx.x; idx < W * g.hx; idx += blockDim.x) {
-        const int l = dhx.div(idx), k = idx - l * g.hx;
-        const long long oa = soff[2 * l], ob = soff[2 * l + 1];
-        const float2 A = oa >= 0 ? spec[oa + k] : make_float2(0.f, 0.f);
-        const float2 B = ob >= 0 ? spec[ob + k] : make_float2(0.f, 0.f);
-        s[l * LPX + k] = pack_lo(A, B);
-        if (k >= 1 && k <= hi_max) s[l * LPX + g.px - k] = pack_hi(A, B);
+    // kU rows' elements per thread are loaded before any is stored, so that many loads are in
+    // flight per thread while the CTA waits for its tile
+    constexpr int kU = 4;
+    const int total = W * g.hx, step = blockDim.x;
+    for (int base = threadIdx.x; base < total; base += kU * step) {
+        float2 A[kU], B[kU];
+        int L[kU], K[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int idx = base + u * step;
+            A[u] = B[u] = make_float2(0.f, 0.f);
+            L[u] = -1;
+            K[u] = 0;
+            if (idx < total) {
+                const int l = dhx.div(idx), k = idx - l * g.hx;
+                const long long oa = soff[2 * l], ob = soff[2 * l + 1];
+                L[u] = l;
+                K[u] = k;
+                if (oa >= 0) A[u] = __ldg(spec + oa + k);
+                if (ob >= 0) B[u] = __ldg(spec + ob + k);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            if (L[u] < 0) continue;
+            const int l = L[u], k = K[u];
+            s[l * LPX + k] = pack_lo(A[u], B[u]);
+            if (k >= 1 && k <= hi_max) s[l * LPX + g.px - k] = pack_hi(A[u], B[u]);
+        }
     }
     __syncthreads();
     const Lane ln(wlog);
@@ -345,7 +392,7 @@ cudaError_t fy_deconv_pass(int pass, const DeconvLaunch& d, cudaStream_t st) {
     case 3: {   // Z forward, weight, Z inverse
         const TileShape t = fy_tile_shape(g.pz);
         const size_t smem = (size_t)g.pz * t.W * sizeof(float2) + (size_t)g.pz * sizeof(float2) +
-                            (size_t)g.pz * sizeof(double) + (FY_LUT_N + 1) * sizeof(float);
+                            (size_t)g.pz * sizeof(double) + (FY_LUT_N + 4) * sizeof(float);
         dim3 grid(ceil_div_i(g.hx, t.W), g.py);
         return with_e(g.pz, [&](auto ec) -> cudaError_t {
             constexpr int E = decltype(ec)::value;

@@ -165,9 +165,7 @@ inline TileShape fy_tile_shape(int n) {
 // over CTAs, never the arithmetic, so results are bit-identical to the defaults.
 //   fy_tuned_x_wlog   log2 of the lines per CTA of a deconvolution X pass (pass 1 or 5) of
 //                     axis length n (line-major tiles: any W <= the default fits)
-//   fy_tuned_box_chunks  z chunks of a box pass (fy_zbox.cuh kind, radius) on a volume
 int fy_tuned_x_wlog(int pass, int n);
-int fy_tuned_box_chunks(int kind, int r, int nz, int ny, int nx);
 // Default z-chunk count of a box pass (64 x 16 column tiles, two CTAs resident per SM, so a
 // launch runs in waves of 2*sms CTAs): among chunk counts with chunks of >= 8r planes and at
 // least ~3 waves of work, the one whose CTAs best fill their last wave, net of the 2r-plane

@@ -506,12 +506,13 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
     if (!TMA) cp_wait<0>();
 }
 
-// Tiles and z chunks: the autotuned chunk count when there is one, else the default of
-// fy_box_default_chunks (fy_internal.h).
+// Tiles and z chunks (fy_box_default_chunks, fy_internal.h). The chunk count is fixed by the
+// shape and SM count alone: each chunk takes its variance shift from its first plane, so
+// another chunking would round the sums differently.
 inline dim3 grid_for(int kind, int nz, int ny, int nx, int r, int sms, int& zchunk) {
+    (void)kind;
     const int tx = (nx + TX - 1) / TX, ty = (ny + TY - 1) / TY;
-    int nc = fy_tuned_box_chunks(kind, r, nz, ny, nx);
-    if (nc <= 0) nc = fy_box_default_chunks(nz, ny, nx, r, sms);
+    const int nc = fy_box_default_chunks(nz, ny, nx, r, sms);
     zchunk = (nz + nc - 1) / nc;
     return dim3(tx, ty, (nz + zchunk - 1) / zchunk);
 }

@@ -365,17 +365,17 @@ void   fy_gpu_zarr_cache_stats(unsigned long long *hits, unsigned long long *loa
 /* Autotuner (no reference counterpart). fy_gpu_autotune times the restoration chain
  * (fy_gpu_restore_u8 with the matched anisotropic deconvolution, noise window 5, exact guided
  * filter r 2) on a scratch cube of this shape on the calling thread's device, varies one
- * launch-shape knob at a time -- the lines per CTA of the deconvolution X passes, the z-chunk
- * count of the box passes -- keeps each change that is faster, and writes the winners to the
- * tuning cache, one JSON object per line, keyed by GPU model, SM count, driver and runtime
- * versions and the knob (axis length or cube shape). Every knob only splits the work
+ * launch-shape knob at a time -- the lines per CTA of the forward and inverse deconvolution X
+ * passes -- keeps each change that is faster, and writes the winners to the tuning cache, one
+ * JSON object per line, keyed by GPU model, SM count, driver and runtime versions and the
+ * knob (pass and padded axis length). Every knob only splits the work
  * differently, so results stay bit-identical. The cache file is $FY_TUNE_CACHE, else
  * $XDG_CACHE_HOME/fysics_b200/tune.json, else ~/.cache/fysics_b200/tune.json; later calls
  * and processes read it on first use. It allocates scratch (about 5 bytes per voxel) and
  * synchronises the device: call it at set-up. flags bit 0 re-measures shapes already in the
  * cache. fy_gpu_tune_load replaces the in-memory table with a cache file's entries (NULL:
  * the default path) and returns how many it read; fy_gpu_tune_value returns the tuned value
- * of a knob on the current device ("x1.512", "box3.r2.512x512x512"), 0 when untuned.
+ * of a knob on the current device ("x1.512", "x5.512"), 0 when untuned.
  * FY_TUNE=0 in the environment makes every lookup use the defaults. */
 int    fy_gpu_autotune(int nz, int ny, int nx, int flags);
 int    fy_gpu_tune_load(const char *path);
