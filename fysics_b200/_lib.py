@@ -203,6 +203,7 @@ SIGNATURES = {
     "fy_gpu_kernel_launches": (C.c_ulonglong, []),
     "fy_gpu_kernel_timeouts": (_i, []),
     "fy_gpu_test_box_first_wait": (_i, [_i]),
+    "fy_gpu_test_noise_paths": (_i, [_i, C.POINTER(C.c_int)]),
     "fy_gpu_u8_to_phys": (_i, [_P, _P, _sz, _d, _d, _P]),
     "fy_gpu_phys_to_u8": (_i, [_P, _P, _sz, _d, _d, _P]),
     "fy_gpu_deconvolve_ex": (_i, [_P, _i, _d, _d, _P, _i, _i, _i, _PP, _d, _i, _d, _P]),

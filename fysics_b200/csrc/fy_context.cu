@@ -231,6 +231,14 @@ int fy_gpu_test_box_first_wait(int polls) {
     if (e == cudaSuccess) e = fy_noise_set_first_wait_polls(polls);
     return e == cudaSuccess ? FY_OK : fy::fail_cuda(e, "fy_gpu_test_box_first_wait");
 }
+int fy_gpu_test_noise_paths(int force_radix, int* window_used) {
+    fy::enter();
+    int rc = fy::ensure_ctx();
+    if (rc) return rc;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = fy_noise_test_paths(force_radix, window_used);
+    return e == cudaSuccess ? FY_OK : fy::fail_cuda(e, "fy_gpu_test_noise_paths");
+}
 void fy_gpu_release(void) {
     fy::ThreadCtx& c = fy::ctx();
     if (c.st) cudaStreamSynchronize(c.st);

@@ -90,42 +90,23 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(const T* __restrict__ sr
     load_twiddles(stw, tw, pl.n);
     row_offsets(soff, q0, W, Q, g);
     const int nch = g.nx / VEC;
-    // kU chunks per thread are loaded before any is dewindowed and stored (loads in flight)
-    constexpr int kU = VEC == 1 ? 8 : 4;
-    const int total = W * nch, step = blockDim.x;
-    for (int base = threadIdx.x; base < total; base += kU * step) {
-        float va[kU][VEC], vb[kU][VEC];
-        int L[kU], X[kU];
+    for (int it = threadIdx.x; it < W * nch; it += blockDim.x) {
+        const int l = dchunk.div(it), x = (it - l * nch) * VEC;
+        const long qa = q0 + 2 * l, qb = qa + 1;
+        float va[VEC], vb[VEC];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int it = base + u * step;
+        for (int j = 0; j < VEC; ++j) va[j] = vb[j] = 0.f;
+        if (qa < Q) VecLoad<T, VEC>::run(src + qa * g.nx + x, va);
+        if (qb < Q) VecLoad<T, VEC>::run(src + qb * g.nx + x, vb);
+        float2* dst = s + l * LPX + x;
 #pragma unroll
-            for (int j = 0; j < VEC; ++j) va[u][j] = vb[u][j] = 0.f;
-            L[u] = -1;
-            X[u] = 0;
-            if (it < total) {
-                const int l = dchunk.div(it), x = (it - l * nch) * VEC;
-                const long qa = q0 + 2 * l, qb = qa + 1;
-                L[u] = l;
-                X[u] = x;
-                if (qa < Q) VecLoad<T, VEC>::run(src + qa * g.nx + x, va[u]);
-                if (qb < Q) VecLoad<T, VEC>::run(src + qb * g.nx + x, vb[u]);
+        for (int j = 0; j < VEC; ++j) {
+            float a = va[j], b = vb[j];
+            if (is_u8) {                                   // fy_u8_to_phys, FMA as the reference build
+                a = qa < Q ? __fmaf_rn(a, scale, lo) : 0.f;
+                b = qb < Q ? __fmaf_rn(b, scale, lo) : 0.f;
             }
-        }
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            if (L[u] < 0) continue;
-            const long qa = q0 + 2 * L[u], qb = qa + 1;
-            float2* dst = s + L[u] * LPX + X[u];
-#pragma unroll
-            for (int j = 0; j < VEC; ++j) {
-                float a = va[u][j], b = vb[u][j];
-                if (is_u8) {                               // fy_u8_to_phys, FMA as the reference build
-                    a = qa < Q ? __fmaf_rn(a, scale, lo) : 0.f;
-                    b = qb < Q ? __fmaf_rn(b, scale, lo) : 0.f;
-                }
-                dst[j] = make_float2(a, b);
-            }
+            dst[j] = make_float2(a, b);
         }
     }
     const int npad = g.px - g.nx;

@@ -214,3 +214,4 @@ int fy_guided_wait_timeouts();
 int fy_noise_wait_timeouts();
 cudaError_t fy_guided_set_first_wait_polls(int polls);
 cudaError_t fy_noise_set_first_wait_polls(int polls);
+cudaError_t fy_noise_test_paths(int force_radix, int* used);

@@ -10,8 +10,9 @@
 //      of m (noise.c:104-108) through a sample-guided window, one pass over m and a radix
 //      select of the window's candidates (falling back to radix passes over m when the
 //      window misses), and, per intensity bin with >= 200 voxels, the flat_pct percentile of
-//      v (noise.c:117-134) by radix passes; each interpolated between order statistics k and
-//      k+1 exactly as percentile() does (noise.c:66-73).
+//      v (noise.c:117-134) through the same scheme over mean and variance (falling back to
+//      radix passes over v); each interpolated between order statistics k and k+1 exactly
+//      as percentile() does (noise.c:66-73).
 //   3. k_noise_fit: one thread, FP64: IRLS line fit var = g*I + b (noise.c:137-172) and
 //      noise_ref = sqrt(max(g*ref + b, ..))*1.15 (noise.c:181-187), plus the guided eps
 //      (3*noise_ref)^2 floored at 1e-8 (noise.c:197-202).
@@ -29,6 +30,8 @@ constexpr int NT_MAX = 64;             // selection targets: 2 per bin + spare
 // window (section 2w), which falls back to mode 0 when the window misses.
 constexpr int kModeWin0 = 4;
 constexpr int kModeBinCand = 6;        // the bins' last digit runs on a candidate list (cc)
+constexpr int kModeBinWin = 7;         // the bins' percentiles through the sample-guided window (2bw)
+constexpr int kModeBinDone = 8;        // the window found them: the bins' radix passes stand aside
 
 FY_D uint32_t fkey(float f) {
     const uint32_t u = __float_as_uint(f);
@@ -82,6 +85,10 @@ struct NoiseCtl {
     unsigned long long wbelow[2];
     unsigned long long ncand;          // candidates appended (may exceed the capacity)
     int wfail;                         // the window missed: the radix passes run instead
+    // The bins' windows (section 2bw): per bin the variance keys [bwlo, bwhi] and the counts
+    // of the bin's keys below, inside and above it.
+    uint32_t bwlo[NB], bwhi[NB];
+    unsigned long long bwc[NB * 3];
 };
 
 namespace {
@@ -458,7 +465,11 @@ __global__ void k_noise_bins_setup(NoiseCtl* ctl) {
     // gives the bin counts; k_bin_targets then sets the ranks)
     for (int t = 0; t < NT_MAX; ++t) target_init(ctl, t, 0, 0, t < NB);
     ctl->ntarget = NB;
-    ctl->mode = 1;
+    // the bins' window runs first (section 2bw); it hands over to these radix passes (mode 1)
+    // when it misses
+    for (int i = 0; i < NB * 3; ++i) ctl->bwc[i] = 0;
+    ctl->ncand = 0;
+    ctl->mode = kModeBinWin;
 }
 
 // After the first variance digit pass (one block per bin): the bin's count is the sum of its
@@ -506,26 +517,31 @@ __global__ void __launch_bounds__(256) k_bin_targets(NoiseCtl* ctl) {
 //            over the whole field (mode 0), which are exact in every case.
 //   finish   the keys of k and k+1 go into the main block in the form the fit reads.
 // The result is the same exact order statistics as the radix path: only which pass finds
-// them changes. (The per-bin variance percentiles keep the radix path: their counting pass
-// must bin every voxel, which costs as much as the radix path's labelling pass.)
+// them changes. The per-bin variance percentiles use the same scheme (section 2bw).
 constexpr int kSampleMax = 16384;
 constexpr int kBoundThreads = 512;
 constexpr double kWinSigmas = 5.0;
+// Test hook: bit 0 forces the mean percentiles, bit 1 the bins, to the radix passes over the
+// whole field; noise_window_used records (bits 0/1) which windows produced their result.
+static __device__ int noise_force_radix;
+static __device__ int noise_window_used;
 
 // Block radix select over keys in shared memory: the rank-th smallest (0-based) of keys[0, c),
-// c <= kSampleMax, by kBoundThreads threads. Four 8-bit digit passes. Each warp counts into a
+// c <= kSampleMax, by kBoundThreads threads. npass 8-bit digit passes from the top: with
+// npass < 4 the result is the selected key's top 8*npass bits with the rest zero (the bucket
+// that holds it, enough for a window bound). Each warp counts into a
 // private 256-bin histogram (wh, [warps][256]); the lanes of a warp that hold the same digit
 // are merged with __match_any_sync, so one shared atomic counts them all (the high digits of
 // a sample are nearly all equal). Then one thread per digit sums the warps' counts and a
 // warp-shuffle scan over the 256 digit totals finds the bucket of the rank.
 FY_D uint32_t block_select(const uint32_t* keys, int c, long long rank, unsigned int* wh,
-                           unsigned long long* part, uint32_t* s_sel) {
+                           unsigned long long* part, uint32_t* s_sel, int npass = 4) {
     constexpr int NTB = kBoundThreads, NW = NTB / 32;
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const unsigned full = 0xffffffffu;
     uint32_t prefix = 0, pmask = 0;
     unsigned int* mine_h = wh + w * 256;
-    for (int sh = 24; sh >= 0; sh -= 8) {
+    for (int sh = 24; sh >= 32 - 8 * npass; sh -= 8) {
         for (int i = t; i < NW * 256; i += NTB) wh[i] = 0;
         __syncthreads();
         for (int i0 = 0; i0 < c; i0 += NTB) {             // warp-uniform trip count
@@ -592,7 +608,19 @@ __global__ void __launch_bounds__(kBoundThreads) k_win_bounds(const float* __res
     if (ctl->mode != kModeWin0) return;
     const int t = blockIdx.x;
     const int c = (int)(m < kSampleMax ? m : kSampleMax);
-    for (int i = threadIdx.x; i < c; i += blockDim.x) wkeys[i] = fkey(sm[i]);
+    for (int i0 = threadIdx.x; i0 < c; i0 += 8 * blockDim.x) {   // eight loads in flight per thread
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + u * blockDim.x;
+            v[u] = i < c ? sm[i] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < c) wkeys[i] = fkey(v[u]);
+        }
+    }
     __syncthreads();
     const double q = (double)ctl->tk[t] / (double)(ctl->n > 1 ? ctl->n - 1 : 1);   // the target's quantile
     const bool upper = blockIdx.y == 1;
@@ -715,7 +743,7 @@ __global__ void k_win_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc,
     cc->ntarget = 2;
     cc->n = (long long)(ctl->ncand < (unsigned long long)cap ? ctl->ncand : (unsigned long long)cap);
     ctl->wfail = 0;
-    if ((long long)ctl->ncand > cap) {
+    if ((long long)ctl->ncand > cap || (noise_force_radix & 1)) {
         cc->mode = 3;
         ctl->wfail = 1;
     } else {
@@ -820,6 +848,292 @@ __global__ void k_win_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restr
         ctl->tnext[t] = cc->tneed_next[t] ? cc->tnext[t] : cc->tprefix[t];
         ctl->tneed_next[t] = 1;
         ctl->tactive[t] = 1;
+    }
+    atomicOr(&noise_window_used, 1);
+}
+
+// ---------------------------------------------------------------- 2bw. the bins' window
+// The flat_pct percentile of the variance per intensity bin by the scheme of section 2w,
+// so the variance field is read once instead of once per digit:
+//   sample   m (<= kBinSampleMax) voxels at positions (A*i + B) mod n: the key of each
+//            variance and the bin of its mean (255: outside every bin).
+//   window   one CTA per bin gathers the bin's sample keys in sample order (at most
+//            kSampleMax) and takes the order statistics kWinSigmas binomial standard
+//            deviations either side of the target's sample rank, each widened to its 16-bit
+//            key bucket (two digit passes): [bwlo, bwhi]. Under 64 samples: every key.
+//   count    one pass over mean and variance: per bin, the keys below, inside and above its
+//            window (their sum is the bin count, noise.c:118-123); the keys inside go to the
+//            candidate list with their bin.
+//   arm      for each bin of >= 200 voxels, k = flat_pct/100*(count - 1) and r = k - below
+//            must leave k and k+1 inside; the four digit passes of mode 1 over the candidates
+//            (control block cc, targets = bins) then select them. A miss or an overfull list
+//            sends the bins to the radix passes over the whole field (mode 1).
+//   finish   the keys of k and k+1 into the main block; mode kModeBinDone makes the radix
+//            passes stand aside.
+constexpr int kBinSampleMax = 65536;
+
+__global__ void __launch_bounds__(256) k_bwin_sample(const float* __restrict__ mean, const float* __restrict__ var,
+                                                     const NoiseCtl* __restrict__ ctl, uint32_t* __restrict__ skey,
+                                                     uint8_t* __restrict__ slab, long long m, unsigned long long A,
+                                                     unsigned long long B) {
+    fy_pdl_wait();
+    __shared__ float fe[NB + 1];
+    if (ctl->mode != kModeBinWin) return;
+    if (threadIdx.x <= NB) fe[threadIdx.x] = ctl->fedge[threadIdx.x];
+    __syncthreads();
+    const float lo_f = fe[0], fscale = ctl->fscale;
+    const unsigned long long n = (unsigned long long)ctl->n;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long q = (A * (unsigned long long)i + B) % n;
+        const float mv = __ldg(mean + q), vv = __ldg(var + q);
+        const int b = bin_of(mv, fe, lo_f, fscale);
+        skey[i] = fkey(vv);
+        slab[i] = (uint8_t)(b < 0 ? 255 : b);
+    }
+}
+
+// One CTA (kBoundThreads threads) per bin. Dynamic shared memory as k_win_bounds. The sample
+// labels are read 16 per thread and chunk (slab 16-byte aligned), the next chunk's while the
+// current one is placed; a block scan of the per-thread hit counts keeps sample order.
+__global__ void __launch_bounds__(kBoundThreads) k_bwin_bounds(const uint32_t* __restrict__ skey,
+                                                               const uint8_t* __restrict__ slab,
+                                                               NoiseCtl* __restrict__ ctl, long long m) {
+    fy_pdl_wait();
+    constexpr int NTB = kBoundThreads, NW = NTB / 32, U = 16;
+    extern __shared__ uint32_t wkeys[];
+    unsigned int* wh = wkeys + kSampleMax;
+    __shared__ unsigned long long part[NTB];
+    __shared__ uint32_t s_sel[2];
+    __shared__ int s_wt[NW];
+    if (ctl->mode != kModeBinWin) return;
+    const int b = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const unsigned full = 0xffffffffu;
+    auto load_labels = [&](long long e0, uint8_t* lab) {
+        if (e0 + U <= m) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4*>(slab + e0));
+            const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int j = 0; j < U; ++j) lab[j] = (uint8_t)(wv[j >> 2] >> (8 * (j & 3)));
+        } else {
+#pragma unroll
+            for (int j = 0; j < U; ++j) lab[j] = e0 + j < m ? slab[e0 + j] : (uint8_t)255;
+        }
+    };
+    int c = 0;                                            // block-uniform
+    uint8_t nxt[U];
+    load_labels((long long)t * U, nxt);
+    for (long long i0 = 0; i0 < m && c < kSampleMax; i0 += (long long)U * NTB) {
+        uint8_t lab[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) lab[j] = nxt[j];
+        const long long e0 = i0 + (long long)t * U;
+        if (i0 + (long long)U * NTB < m) load_labels(e0 + (long long)U * NTB, nxt);
+        unsigned hit = 0;
+#pragma unroll
+        for (int j = 0; j < U; ++j) hit |= (unsigned)(lab[j] == (uint8_t)b) << j;
+        const int cnt = __popc(hit);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(full, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_wt[w] = incl;
+        __syncthreads();
+        int off = 0, tot = 0;
+#pragma unroll
+        for (int ww = 0; ww < NW; ++ww) {
+            const int v = s_wt[ww];
+            off += ww < w ? v : 0;
+            tot += v;
+        }
+        int pos = c + off + incl - cnt;
+#pragma unroll
+        for (int j = 0; j < U; ++j)
+            if ((hit >> j) & 1u) {
+                if (pos < kSampleMax) wkeys[pos] = __ldg(skey + e0 + j);
+                ++pos;
+            }
+        c = c + tot < kSampleMax ? c + tot : kSampleMax;
+        __syncthreads();                                  // s_wt reused
+    }
+    __syncthreads();
+    uint32_t lo = 0u, hi = 0xffffffffu;
+    if (c >= 64) {
+        const double q = ctl->flat_pct / 100.0;
+        const double qc = q < 1.0 / c ? 1.0 / c : (q > 1.0 - 1.0 / c ? 1.0 - 1.0 / c : q);
+        const long long ks = (long long)(q * (double)(c - 1));
+        const long long d = (long long)ceil(kWinSigmas * sqrt((double)c * qc * (1.0 - qc))) + 4;
+        if (ks - d >= 0) lo = block_select(wkeys, c, ks - d, wh, part, s_sel, 2);
+        if (ks + d + 1 < c) hi = block_select(wkeys, c, ks + d + 1, wh, part, s_sel, 2) | 0xffffu;
+    }
+    if (t == 0) {
+        ctl->bwlo[b] = lo;
+        ctl->bwhi[b] = hi;
+    }
+}
+
+// The counting pass of the bins' windows: mean and variance read once (SU float4 of each per
+// thread and step). Per voxel a code bin*3 + {below, inside, above} goes through a run
+// accumulator into shared counters; the inside keys are placed by one warp scan per step in
+// the warp's buffer and appended to the list (one atomic per buffer), as in k_win_count.
+__global__ void __launch_bounds__(256) k_bwin_count(const float* __restrict__ mean, const float* __restrict__ var,
+                                                    NoiseCtl* __restrict__ ctl, float* __restrict__ cval,
+                                                    uint8_t* __restrict__ clab, long long cap) {
+    fy_pdl_wait();
+    __shared__ float bufv[256 / 32][kCountBuf];
+    __shared__ uint8_t bufl[256 / 32][kCountBuf];
+    __shared__ float fe[NB + 1];
+    __shared__ uint32_t swl[NB], swh[NB];
+    __shared__ unsigned int sc[NB * 3];
+    if (ctl->mode != kModeBinWin) return;
+    const unsigned full = 0xffffffffu;
+    const int t = threadIdx.x, lane = t & 31;
+    if (t <= NB) fe[t] = ctl->fedge[t];
+    if (t < NB) {
+        swl[t] = ctl->bwlo[t];
+        swh[t] = ctl->bwhi[t];
+    }
+    for (int i = t; i < NB * 3; i += blockDim.x) sc[i] = 0;
+    __syncthreads();
+    const float lo_f = fe[0], fscale = ctl->fscale;
+    WarpCands wc;
+    wc.v = bufv[t >> 5];
+    wc.l = bufl[t >> 5];
+    RunAcc acc;
+    // class of one voxel: -1 outside every bin, else bin*3 + {0 below, 1 inside, 2 above}
+    auto code_of = [&](float m, float v) -> int {
+        const int b = bin_of(m, fe, lo_f, fscale);
+        if (b < 0) return -1;
+        const uint32_t k = fkey(v);
+        return b * 3 + (k < swl[b] ? 0 : (k <= swh[b] ? 1 : 2));
+    };
+    const long long n = ctl->n, n4 = (n + 3) / 4, n4f = n / 4;
+    const long long chunk = (long long)SU * 256;
+    long long base = (long long)blockIdx.x * chunk;
+    for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
+        float4 xm[SU], xv[SU];
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            const long long q = base + t + (long long)u * 256;
+            xm[u] = __ldg(reinterpret_cast<const float4*>(mean) + q);
+            xv[u] = __ldg(reinterpret_cast<const float4*>(var) + q);
+        }
+        float vv[4 * SU];
+        int cd[4 * SU];
+        unsigned hit = 0;
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            vv[4 * u] = xv[u].x; vv[4 * u + 1] = xv[u].y; vv[4 * u + 2] = xv[u].z; vv[4 * u + 3] = xv[u].w;
+            cd[4 * u] = code_of(xm[u].x, xv[u].x);
+            cd[4 * u + 1] = code_of(xm[u].y, xv[u].y);
+            cd[4 * u + 2] = code_of(xm[u].z, xv[u].z);
+            cd[4 * u + 3] = code_of(xm[u].w, xv[u].w);
+        }
+#pragma unroll
+        for (int q = 0; q < 4 * SU; ++q) {
+            acc.add(sc, cd[q]);
+            hit |= (unsigned)(cd[q] >= 0 && cd[q] % 3 == 1) << q;
+        }
+        const int c = __popc(hit);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(full, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int tot = __shfl_sync(full, incl, 31);
+        if (tot == 0) continue;
+        if (wc.cnt + tot > kCountBuf) wc.flush(cval, clab, &ctl->ncand, cap);     // warp-uniform
+        int pos = wc.cnt + incl - c;
+#pragma unroll
+        for (int q = 0; q < 4 * SU; ++q)
+            if ((hit >> q) & 1u) { wc.v[pos] = vv[q]; wc.l[pos] = (uint8_t)(cd[q] / 3); ++pos; }
+        wc.cnt += tot;
+        __syncwarp();
+    }
+    if (base < n4) {                                     // the grid's partial chunk
+        for (int u = 0; u < SU; ++u)
+            for (int j = 0; j < 4; ++j) {
+                const long long i = 4 * (base + t + (long long)u * 256) + j;
+                if (i >= n) continue;
+                const float v = __ldg(var + i);
+                const int code = code_of(__ldg(mean + i), v);
+                acc.add(sc, code);
+                if (code >= 0 && code % 3 == 1) {
+                    const unsigned long long pos = atomicAdd(&ctl->ncand, 1ull);
+                    if ((long long)pos < cap) { cval[pos] = v; clab[pos] = (uint8_t)(code / 3); }
+                }
+            }
+    }
+    wc.flush(cval, clab, &ctl->ncand, cap);
+    acc.flush(sc);
+    __syncthreads();
+    for (int i = t; i < NB * 3; i += blockDim.x)
+        if (sc[i]) atomicAdd(&ctl->bwc[i], (unsigned long long)sc[i]);
+}
+
+// After the counting pass: bin counts and, when every used bin's k and k+1 are inside its
+// window and the list fits, the candidate block armed for the bins' digit passes; otherwise
+// the radix passes over the whole field (mode 1) run instead.
+__global__ void __launch_bounds__(256) k_bwin_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc, long long cap) {
+    fy_pdl_wait();
+    __shared__ int s_ok;
+    if (ctl->mode != kModeBinWin) {
+        if (threadIdx.x == 0) cc->mode = 3;
+        return;
+    }
+    const int t = threadIdx.x;
+    if (t == 0) s_ok = (long long)ctl->ncand <= cap && !(noise_force_radix & 2);
+    __syncthreads();
+    long long cnt = 0, in = 0, r = 0;
+    bool on = false;
+    if (t < NB) {
+        const long long below = (long long)ctl->bwc[3 * t];
+        in = (long long)ctl->bwc[3 * t + 1];
+        cnt = below + in + (long long)ctl->bwc[3 * t + 2];
+        on = cnt >= 200;                                  // noise.c:123
+        if (on) {
+            const double idx = ctl->flat_pct / 100.0 * (double)(cnt - 1);
+            const long long k = (long long)idx;
+            r = k - below;
+            if (!(r >= 0 && r < in && (k + 1 >= cnt || r + 1 < in))) s_ok = 0;
+        }
+    }
+    __syncthreads();
+    if (!s_ok) {
+        if (t == 0) {
+            cc->mode = 3;
+            ctl->mode = 1;
+        }
+        return;
+    }
+    for (int i = t; i < NB * 256; i += blockDim.x) cc->hist[i] = 0;
+    if (t < NT_MAX) target_init(cc, t, on ? r : 0, t < NB ? in : 0, on);
+    if (t < NB) ctl->bcount[t] = (unsigned long long)cnt;
+    __syncthreads();
+    if (t == 0) {
+        cc->n = (long long)ctl->ncand;
+        cc->ntarget = NB;
+        cc->mode = 1;
+    }
+}
+
+// The bins' selected keys (k and k+1, in the form interp() reads) into the main block.
+__global__ void k_bwin_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restrict__ cc) {
+    fy_pdl_wait();
+    if (ctl->mode != kModeBinWin) return;
+    const int t = threadIdx.x;
+    if (t < NB) {
+        ctl->tprefix[t] = cc->tprefix[t];
+        ctl->tnext[t] = cc->tneed_next[t] ? cc->tnext[t] : cc->tprefix[t];
+        ctl->tneed_next[t] = 1;
+        ctl->tactive[t] = cc->tactive[t];
+    }
+    __syncwarp();
+    if (t == 0) {
+        ctl->mode = kModeBinDone;
+        atomicOr(&noise_window_used, 2);
     }
 }
 
@@ -1093,7 +1407,29 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 0);
     PDL(k_noise_bins_setup, 1, 1, 0, st, ctl);
     fy_prof_mark(st, "noise.lohi");
-    // 2b. per-bin flat_pct percentile of the variance: 4 x 8 bits, then the k+1 neighbours;
+    // 2bw. per-bin flat_pct percentile of the variance through the bins' window: sample,
+    // bounds, one counting pass over mean and variance, then four digit passes over the
+    // candidates. The sample lives in the candidate region until the counting pass refills it.
+    {
+        long long m2 = n < kBinSampleMax ? n : kBinSampleMax;
+        const long long m2cap = (L.cap - 64) * 4 / 5;    // keys, then labels 256-byte aligned
+        if (m2 > m2cap) m2 = m2cap;
+        uint32_t* skey = reinterpret_cast<uint32_t*>(cval);
+        uint8_t* slab = reinterpret_cast<uint8_t*>(cval + round64((size_t)m2));
+        if ((e = fy_smem_optin(k_bwin_bounds, smem_keys)) != cudaSuccess) return e;
+        PDL(k_bwin_sample, 64, 256, 0, st, mean, var, ctl, skey, slab, m2, wa, (unsigned long long)n / 5);
+        PDL(k_bwin_bounds, NB, kBoundThreads, smem_keys, st, skey, slab, ctl, m2);
+        PDL(k_bwin_count, g, 256, 0, st, mean, var, ctl, cval, clab, L.cap);
+        PDL(k_bwin_arm, 1, 256, 0, st, ctl, cc, L.cap);
+        for (int sh = 24; sh >= 0; sh -= 8) {
+            PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL);
+            PDL(k_sel_scan, NB, 256, 0, st, cc, 8, 1, sh == 0);
+        }
+        PDL(k_sel_next, gcl, 256, 0, st, nullptr, cval, clab, cc, 1);
+        PDL(k_bwin_finish, 1, 32, 0, st, ctl, cc);
+    }
+    // 2b. (when the bins' window missed) per-bin flat_pct percentile of the variance by radix
+    // passes over the whole field: 4 x 8 bits, then the k+1 neighbours;
     // the first pass also labels the voxels with their bins and yields the bin counts. The
     // third pass also lists the voxels that match their bin's 16-bit prefix (~1% of them),
     // and the last digit runs over that list (falling back to the whole field if it overflows).
@@ -1128,7 +1464,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     }
     PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 2);
     PDL(k_noise_fit, 1, 32, 0, st, ctl, 1);
-    launches += 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 7 + 1 + 16 + 1 + 1 + 7 + 1;
+    launches += 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 7 + 1 + 14 + 16 + 1 + 1 + 7 + 1;
     return cudaGetLastError();
 }
 
@@ -1163,6 +1499,17 @@ __global__ void k_noise_store(const NoiseCtl* __restrict__ ctl, fy_noise_model* 
 cudaError_t fy_noise_store(const void* ctl_mem, void* d_model, float* d_eps, cudaStream_t st) {
     k_noise_store<<<1, 1, 0, st>>>((const NoiseCtl*)ctl_mem, (fy_noise_model*)d_model, d_eps);
     return cudaGetLastError();
+}
+
+// Test hook of the selection paths (see noise_force_radix): sets the forcing mask and returns
+// the windows used since the previous call in *used. Synchronous.
+cudaError_t fy_noise_test_paths(int force_radix, int* used) {
+    int u = 0, zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&u, noise_window_used, sizeof u);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(noise_window_used, &zero, sizeof zero);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(noise_force_radix, &force_radix, sizeof force_radix);
+    if (e == cudaSuccess && used) *used = u;
+    return e;
 }
 
 // Bounded waits of this unit's box passes that expired (see fy_zbox.cuh); 0 expected.

@@ -254,6 +254,14 @@ int fy_gpu_kernel_timeouts(void);
  * output unfinished); polls < 0 restores the normal bound. Also clears the timeout count.
  * Synchronous; call it only while no kernel of this library is in flight. */
 int fy_gpu_test_box_first_wait(int polls);
+/* Test hook of the noise model's order-statistic paths; no reference counterpart. The 1st/
+ * 99th percentiles of the local means and the per-bin percentiles of the local variances
+ * come from sample-guided key windows over one pass each, with exact radix passes over the
+ * whole field when a window misses. force_radix bit 0 sends the means, bit 1 the bins, to
+ * the radix passes every time (0 restores the windows). *window_used (optional) receives
+ * which windows produced their result (bit 0 means, bit 1 bins) since the previous call.
+ * Both paths give the same exact order statistics. Synchronises the device. */
+int fy_gpu_test_noise_paths(int force_radix, int *window_used);
 
 /* Device-pointer forms of the drop-in calls, enqueued on `stream` (a cudaStream_t, NULL =
  * legacy default stream) and NOT synchronised: results are valid once the stream reaches

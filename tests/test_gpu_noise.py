@@ -137,3 +137,38 @@ def test_noise_window_overflow_falls_back(gpu):
         r = ref_noise(vol, 5, 10.0, 0.4)
         assert g.n_bins_used == r.n_bins_used
         assert close(g.noise_ref, r.noise_ref)
+
+
+def _paths_volume(shape, seed):
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid(*[np.linspace(0, 1, n) for n in shape], indexing="ij")
+    sig = 0.3 + 0.5 * x * (0.5 + 0.5 * np.sin(3 * y + 2 * z))
+    return (sig + rng.standard_normal(shape) * np.sqrt(0.002 * sig + 1e-4)).astype(np.float32)
+
+
+@pytest.mark.parametrize("shape,win,pct", [((96, 96, 96), 5, 10.0), ((64, 80, 72), 3, 25.0),
+                                           ((128, 128, 128), 5, 10.0), ((40, 50, 60), 7, 5.0)])
+def test_noise_windows_equal_radix_paths(gpu, shape, win, pct):
+    """Both order-statistic paths are exact, so the model must be bit-identical whether the
+    sample-guided windows (one pass over the means, one over mean and variance) or the radix
+    passes over the whole field find the 1st/99th mean percentiles and the per-bin variance
+    percentiles; and on such volumes the windows are the path that normally runs."""
+    lib = gpu.load()
+    vol = _paths_volume(shape, sum(shape) + win)
+    used = C.c_int(-1)
+    try:
+        assert lib.fy_gpu_test_noise_paths(0, C.byref(used)) == 0
+        base = gpu_noise(gpu, vol, win, pct, 0.4)
+        assert lib.fy_gpu_test_noise_paths(0, C.byref(used)) == 0
+        assert used.value == 3, used.value                    # both windows held their targets
+        for force in (1, 2, 3):
+            assert lib.fy_gpu_test_noise_paths(force, None) == 0
+            got = gpu_noise(gpu, vol, win, pct, 0.4)
+            assert lib.fy_gpu_test_noise_paths(0, C.byref(used)) == 0
+            assert used.value == 3 & ~force, (force, used.value)
+            assert (got.g, got.b, got.noise_ref, got.n_bins_used) == (base.g, base.b, base.noise_ref,
+                                                                        base.n_bins_used), force
+    finally:
+        lib.fy_gpu_test_noise_paths(0, None)
+    o = o64_noise(vol, win, pct, 0.4)
+    assert base.n_bins_used == o.n_bins_used and close(base.noise_ref, o.noise_ref)
