@@ -148,7 +148,7 @@ def algorithmic_bytes(name: str, n: int, geo: dict) -> float | None:
         # window is the guided window: the chain then skips the guided a/b pass)
         "noise.stats": n * (20 if geo.get("shared_window") else 12),
         "noise.lohi": n * 4,                   # one window pass over mean (candidates ~1%: small)
-        "noise.bin_select": n * 24,            # mean + var read, labels written; 3 passes over var + labels
+        "noise.bin_select": n * 8,             # one pass over mean + var (the bins' window; candidates ~5%)
         # (mean, var) pairs + I -> out (16 B); without the shared window I -> a, b (12 B) first
         "guided": n * (16 if geo.get("shared_window") else 28),
         "dering.accumulate+vote": n * 1,

@@ -166,12 +166,12 @@ inline TileShape fy_tile_shape(int n) {
 //   fy_tuned_x_wlog   log2 of the lines per CTA of a deconvolution X pass (pass 1 or 5) of
 //                     axis length n (line-major tiles: any W <= the default fits)
 int fy_tuned_x_wlog(int pass, int n);
-// Default z-chunk count of a box pass (64 x 16 column tiles, two CTAs resident per SM, so a
-// launch runs in waves of 2*sms CTAs): among chunk counts with chunks of >= 8r planes and at
-// least ~3 waves of work, the one whose CTAs best fill their last wave, net of the 2r-plane
-// warm-up each chunk repeats: score = (waves / ceil(waves)) * zchunk / (zchunk + 2r).
-inline int fy_box_default_chunks(int nz, int ny, int nx, int r, int sms) {
-    const long txy = (long)((nx + 63) / 64) * ((ny + 15) / 16), slots = 2L * sms;
+// Default z-chunk count of a box pass (64 x 16 column tiles, `per_sm` CTAs resident per SM,
+// so a launch runs in waves of per_sm*sms CTAs): among chunk counts with chunks of >= 8r
+// planes and at least ~3 waves of work, the one whose CTAs best fill their last wave, net of
+// the 2r-plane warm-up each chunk repeats: score = (waves / ceil(waves)) * zchunk / (zchunk + 2r).
+inline int fy_box_default_chunks(int nz, int ny, int nx, int r, int sms, int per_sm = 2) {
+    const long txy = (long)((nx + 63) / 64) * ((ny + 15) / 16), slots = (long)per_sm * sms;
     int hi = nz / (8 * r);
     if (hi < 1) hi = 1;
     int lo = (int)((3 * slots + txy - 1) / txy);

@@ -89,6 +89,7 @@ struct NoiseCtl {
     // of the bin's keys below, inside and above it.
     uint32_t bwlo[NB], bwhi[NB];
     unsigned long long bwc[NB * 3];
+    unsigned int done_ctas;            // CTAs of the current digit pass that have flushed (0 between passes)
 };
 
 namespace {
@@ -106,6 +107,19 @@ FY_D int bin_of(float m, const float* __restrict__ fe, float lo_f, float scale) 
     b = b < 0 ? 0 : (b > NB - 1 ? NB - 1 : b);
     while (b > 0 && m < fe[b]) --b;
     while (b < NB - 1 && m >= fe[b + 1]) ++b;
+    return b;
+}
+
+// bin_of with at most one step from the float guess (the guess is within one bin of the
+// exact one unless the range [lo, hi] is degenerate; then the exact walk runs): the common
+// path has no loop. lo_e, hi_e: fe[0], fe[NB].
+FY_D int bin_fast(float m, const float* __restrict__ fe, float lo_e, float hi_e, float lo_f, float scale) {
+    if (!(m >= lo_e && m < hi_e)) return -1;
+    int b = (int)((m - lo_f) * scale);
+    b = b < 0 ? 0 : (b > NB - 1 ? NB - 1 : b);
+    b -= (int)(m < fe[b]);                      // m >= fe[0], so b stays >= 0
+    b += (int)(m >= fe[b + 1]);                 // m < fe[NB], so b stays <= NB - 1
+    if (m < fe[b] || m >= fe[b + 1]) b = bin_of(m, fe, lo_f, scale);
     return b;
 }
 
@@ -168,12 +182,68 @@ constexpr int SU = 4;
 // COMPACT (a MODE 1 digit pass): each voxel whose key matches its bin target's prefix is also
 // appended, with its bin, to the candidate list (cval, clab; counter ctl->ncand): every key of
 // the prefixes that the following digits narrow is then in the list.
+// scan >= 0: the CTA that flushes last (a ticket on ctl->done_ctas) then does every active
+// target's bookkeeping (warp_scan_target; scan 1: after the last digit), so no separate scan
+// launch follows the pass.
 constexpr int kCompactBuf = 1152;        // per warp: one step's worst case (32 x 4*SU) + slack
+
+// The bookkeeping after a digit pass for target t, by one warp: the bucket that holds the
+// target's rank (a warp scan of the lanes' bucket sums), the prefix extended by it, the keys
+// equal to the selected key and, after the last digit, the next non-empty bucket (the
+// smallest key above the selected one within the prefix; k_sel_next scans only when there is
+// none). The histogram is read through L2 (other CTAs' atomics) and cleared.
+FY_D void warp_scan_target(NoiseCtl* ctl, int t, int db, bool last) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int nbk = 1 << db, per = nbk / 32;
+    unsigned int* h = ctl->hist + (size_t)t * nbk;
+    const int b0 = lane * per;
+    unsigned long long mine = 0;
+    for (int b = b0; b < b0 + per; ++b) mine += __ldcg(h + b);
+    unsigned long long incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(full, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const long long r = ctl->trank[t];
+    const unsigned long long before = incl - mine;
+    unsigned int sel = (unsigned)nbk;
+    if ((unsigned long long)r >= before && (unsigned long long)r < incl) {
+        unsigned long long acc = before;
+        for (int b = b0; b < b0 + per; ++b) {
+            const unsigned int hb = __ldcg(h + b);
+            if (acc + hb > (unsigned long long)r) {
+                ctl->trank[t] = r - (long long)acc;
+                ctl->tprefix[t] = (ctl->tprefix[t] << db) | (uint32_t)b;
+                if (last) ctl->teq[t] = hb;
+                sel = (unsigned)b;
+                break;
+            }
+            acc += hb;
+        }
+    }
+    sel = __reduce_min_sync(full, sel);
+    unsigned int nextb = 0xffffffffu;
+    if (last) {
+        for (int b = b0 > (int)sel + 1 ? b0 : (int)sel + 1; b < b0 + per; ++b)
+            if (__ldcg(h + b)) { nextb = (unsigned)b; break; }
+        nextb = __reduce_min_sync(full, nextb);
+    }
+    __syncwarp();
+    for (int b = b0; b < b0 + per; ++b) h[b] = 0;
+    __syncwarp();
+    if (last && lane == 0) {
+        ctl->tneed_next[t] = (ctl->trank[t] + 1 >= (long long)ctl->teq[t]) && (ctl->tk[t] + 1 < ctl->tgroup_n[t]);
+        ctl->tnext[t] = nextb != 0xffffffffu ? ((ctl->tprefix[t] >> db) << db) | nextb : 0xffffffffu;
+    }
+}
 template <int DB, int MODE, bool LABEL = false, bool COMPACT = false>
 __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean, const float* __restrict__ var,
                                                   uint8_t* __restrict__ bin, NoiseCtl* __restrict__ ctl,
                                                   int shift, float* __restrict__ cval = nullptr,
-                                                  uint8_t* __restrict__ clab = nullptr, long long cap = 0) {
+                                                  uint8_t* __restrict__ clab = nullptr, long long cap = 0,
+                                                  int scan = -1) {
     fy_pdl_wait();
     extern __shared__ unsigned int h[];
     __shared__ uint32_t sp[256];
@@ -311,6 +381,17 @@ __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean
             if (cnt) atomicAdd(&ctl->hist[i], cnt);
         }
     }
+    if (scan < 0) return;
+    __shared__ int s_last;
+    __threadfence();                                     // this CTA's counts before its ticket
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&ctl->done_ctas, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int t = threadIdx.x >> 5; t < nt; t += blockDim.x >> 5)
+        if (ctl->tactive[t]) warp_scan_target(ctl, t, DB, scan == 1);
+    if (threadIdx.x == 0) ctl->done_ctas = 0;
 }
 
 // After a digit pass: target t (one block) finds the bucket holding its rank by a block
@@ -392,16 +473,41 @@ __global__ void __launch_bounds__(256) k_sel_next(const float* __restrict__ mean
     if (!s_any) return;
     const long long n = ctl->n;
     const float* src = want_mode == 0 ? mean : var;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const uint32_t key = fkey(__ldg(src + i));
+    auto visit = [&](float v, int g) {
+        const uint32_t key = fkey(v);
         if (want_mode == 1) {            // one target per voxel: its bin
-            const int g = __ldg(bin + i);
             if (g < NB && g < nt && sn[g] && key > sp[g] && key < smin[g]) atomicMin(&smin[g], key);
         } else {
             for (int t = 0; t < nt; ++t)
                 if (sn[t] && key > sp[t] && key < smin[t]) atomicMin(&smin[t], key);
         }
+    };
+    // SU float4 (and uchar4 labels) per thread before any is used, as the streaming passes
+    const long long n4 = (n + 3) / 4, n4f = n / 4, chunk = (long long)SU * blockDim.x;
+    long long base = (long long)blockIdx.x * chunk;
+    for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
+        float4 x[SU];
+        uchar4 bb[SU];
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            const long long q = base + threadIdx.x + (long long)u * blockDim.x;
+            x[u] = __ldg(reinterpret_cast<const float4*>(src) + q);
+            bb[u] = want_mode == 1 ? __ldg(reinterpret_cast<const uchar4*>(bin) + q) : make_uchar4(0, 0, 0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+            visit(x[u].x, bb[u].x);
+            visit(x[u].y, bb[u].y);
+            visit(x[u].z, bb[u].z);
+            visit(x[u].w, bb[u].w);
+        }
     }
+    if (base < n4)                                       // the grid's partial chunk
+        for (int u = 0; u < SU; ++u)
+            for (int j = 0; j < 4; ++j) {
+                const long long i = 4 * (base + threadIdx.x + (long long)u * blockDim.x) + j;
+                if (i < n) visit(__ldg(src + i), want_mode == 1 ? (int)__ldg(bin + i) : 0);
+            }
     __syncthreads();
     for (int i = threadIdx.x; i < nt; i += blockDim.x)
         if (sn[i] && smin[i] != 0xffffffffu) atomicMin(&ctl->tnext[i], smin[i]);
@@ -429,8 +535,10 @@ FY_D void target_init(NoiseCtl* ctl, int t, long long k, long long group_n, bool
     ctl->tnext[t] = 0xffffffffu;
 }
 
-__global__ void k_noise_setup(NoiseCtl* ctl, long long n, double flat_pct, double ref_intensity) {
+__global__ void k_noise_setup(NoiseCtl* ctl, NoiseCtl* cc, long long n, double flat_pct, double ref_intensity) {
     fy_pdl_wait();
+    ctl->done_ctas = 0;
+    cc->done_ctas = 0;
     ctl->n = n;
     ctl->flat_pct = flat_pct;
     ctl->ref_intensity = ref_intensity;
@@ -506,7 +614,7 @@ __global__ void __launch_bounds__(256) k_bin_targets(NoiseCtl* ctl) {
 //            deviations either side of the target's expected sample rank give a key window
 //            [wlo, whi] that holds the target's order statistics k and k+1 with
 //            overwhelming probability (one CTA per target and window end, radix select in
-//            shared memory).
+//            shared memory to the 24-bit key bucket, widened to its ends).
 //   count    one pass over the means counts, per target, the keys below wlo and appends the
 //            keys inside [wlo, whi] with their target label to a candidate list.
 //   select   the radix passes of mode 1 over the candidates with a second control block,
@@ -629,8 +737,9 @@ __global__ void __launch_bounds__(kBoundThreads) k_win_bounds(const float* __res
         const double qc = q < 1.0 / c ? 1.0 / c : (q > 1.0 - 1.0 / c ? 1.0 - 1.0 / c : q);
         const long long ks = (long long)(q * (double)(c - 1));
         const long long d = (long long)ceil(kWinSigmas * sqrt((double)c * qc * (1.0 - qc))) + 4;
-        if (!upper && ks - d >= 0) w = block_select(wkeys, c, ks - d, wh, part, s_sel);
-        if (upper && ks + d + 1 < c) w = block_select(wkeys, c, ks + d + 1, wh, part, s_sel);
+        // three digits: the order statistic's 24-bit key bucket, widened to its ends
+        if (!upper && ks - d >= 0) w = block_select(wkeys, c, ks - d, wh, part, s_sel, 3);
+        if (upper && ks + d + 1 < c) w = block_select(wkeys, c, ks + d + 1, wh, part, s_sel, 3) | 0xffu;
     }
     if (threadIdx.x == 0) {
         if (upper) {
@@ -858,7 +967,7 @@ __global__ void k_win_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restr
 //   sample   m (<= kBinSampleMax) voxels at positions (A*i + B) mod n: the key of each
 //            variance and the bin of its mean (255: outside every bin).
 //   window   one CTA per bin gathers the bin's sample keys in sample order (at most
-//            kSampleMax) and takes the order statistics kWinSigmas binomial standard
+//            kBinKeysMax) and takes the order statistics kWinSigmas binomial standard
 //            deviations either side of the target's sample rank, each widened to its 16-bit
 //            key bucket (two digit passes): [bwlo, bwhi]. Under 64 samples: every key.
 //   count    one pass over mean and variance: per bin, the keys below, inside and above its
@@ -871,6 +980,7 @@ __global__ void k_win_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restr
 //   finish   the keys of k and k+1 into the main block; mode kModeBinDone makes the radix
 //            passes stand aside.
 constexpr int kBinSampleMax = 65536;
+constexpr int kBinKeysMax = 4096;      // per bin: enough for a window of ~5% of a large bin
 
 __global__ void __launch_bounds__(256) k_bwin_sample(const float* __restrict__ mean, const float* __restrict__ var,
                                                      const NoiseCtl* __restrict__ ctl, uint32_t* __restrict__ skey,
@@ -892,19 +1002,23 @@ __global__ void __launch_bounds__(256) k_bwin_sample(const float* __restrict__ m
     }
 }
 
-// One CTA (kBoundThreads threads) per bin. Dynamic shared memory as k_win_bounds. The sample
-// labels are read 16 per thread and chunk (slab 16-byte aligned), the next chunk's while the
-// current one is placed; a block scan of the per-thread hit counts keeps sample order.
+// One CTA (kBoundThreads threads) per bin. Dynamic shared memory as k_win_bounds. Each warp
+// owns a contiguous slice of the sample (whole 512-entry steps, 16 labels per lane and step,
+// read 16 bytes at a time, the next step's while the current one is placed) and compacts its
+// bin's keys in sample order into its own kBinKeysMax/NW slots, with no block barrier; one
+// block pass then concatenates the warps' keys (a deterministic subset in sample order).
 __global__ void __launch_bounds__(kBoundThreads) k_bwin_bounds(const uint32_t* __restrict__ skey,
                                                                const uint8_t* __restrict__ slab,
                                                                NoiseCtl* __restrict__ ctl, long long m) {
     fy_pdl_wait();
-    constexpr int NTB = kBoundThreads, NW = NTB / 32, U = 16;
+    constexpr int NTB = kBoundThreads, NW = NTB / 32, U = 16, STEP = 32 * U, WCAP = kBinKeysMax / NW;
+    static_assert(2 * kBinKeysMax <= kSampleMax, "staging and compacted keys share the key array");
     extern __shared__ uint32_t wkeys[];
     unsigned int* wh = wkeys + kSampleMax;
+    uint32_t* keys = wkeys + kBinKeysMax;                 // the concatenated keys
     __shared__ unsigned long long part[NTB];
     __shared__ uint32_t s_sel[2];
-    __shared__ int s_wt[NW];
+    __shared__ int s_wc[NW];
     if (ctl->mode != kModeBinWin) return;
     const int b = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
     const unsigned full = 0xffffffffu;
@@ -919,18 +1033,22 @@ __global__ void __launch_bounds__(kBoundThreads) k_bwin_bounds(const uint32_t* _
             for (int j = 0; j < U; ++j) lab[j] = e0 + j < m ? slab[e0 + j] : (uint8_t)255;
         }
     };
-    int c = 0;                                            // block-uniform
+    // this warp's slice: whole steps, so every 16-label read is 16-byte aligned
+    const long long steps = (m + STEP - 1) / STEP, per = (steps + NW - 1) / NW;
+    const long long s0 = (long long)w * per * STEP, s1 = s0 + per * STEP < m ? s0 + per * STEP : m;
+    uint32_t* mine = wkeys + w * WCAP;
+    int wc = 0;                                           // warp-uniform
     uint8_t nxt[U];
-    load_labels((long long)t * U, nxt);
-    for (long long i0 = 0; i0 < m && c < kSampleMax; i0 += (long long)U * NTB) {
+    if (s0 < s1) load_labels(s0 + lane * U, nxt);
+    for (long long i0 = s0; i0 < s1 && wc < WCAP; i0 += STEP) {
         uint8_t lab[U];
 #pragma unroll
         for (int j = 0; j < U; ++j) lab[j] = nxt[j];
-        const long long e0 = i0 + (long long)t * U;
-        if (i0 + (long long)U * NTB < m) load_labels(e0 + (long long)U * NTB, nxt);
+        const long long e0 = i0 + lane * U;
+        if (i0 + STEP < s1) load_labels(e0 + STEP, nxt);
         unsigned hit = 0;
 #pragma unroll
-        for (int j = 0; j < U; ++j) hit |= (unsigned)(lab[j] == (uint8_t)b) << j;
+        for (int j = 0; j < U; ++j) hit |= (unsigned)(lab[j] == (uint8_t)b && e0 + j < s1) << j;
         const int cnt = __popc(hit);
         int incl = cnt;
 #pragma unroll
@@ -938,25 +1056,26 @@ __global__ void __launch_bounds__(kBoundThreads) k_bwin_bounds(const uint32_t* _
             const int y = __shfl_up_sync(full, incl, o);
             if (lane >= o) incl += y;
         }
-        if (lane == 31) s_wt[w] = incl;
-        __syncthreads();
-        int off = 0, tot = 0;
-#pragma unroll
-        for (int ww = 0; ww < NW; ++ww) {
-            const int v = s_wt[ww];
-            off += ww < w ? v : 0;
-            tot += v;
-        }
-        int pos = c + off + incl - cnt;
+        int pos = wc + incl - cnt;
 #pragma unroll
         for (int j = 0; j < U; ++j)
             if ((hit >> j) & 1u) {
-                if (pos < kSampleMax) wkeys[pos] = __ldg(skey + e0 + j);
+                if (pos < WCAP) mine[pos] = __ldg(skey + e0 + j);
                 ++pos;
             }
-        c = c + tot < kSampleMax ? c + tot : kSampleMax;
-        __syncthreads();                                  // s_wt reused
+        const int tot = __shfl_sync(full, incl, 31);
+        wc = wc + tot < WCAP ? wc + tot : WCAP;
     }
+    if (lane == 0) s_wc[w] = wc;
+    __syncthreads();
+    int off = 0, c = 0;
+#pragma unroll
+    for (int ww = 0; ww < NW; ++ww) {
+        const int v = s_wc[ww];
+        off += ww < w ? v : 0;
+        c += v;
+    }
+    for (int i = lane; i < wc; i += 32) keys[off + i] = mine[i];
     __syncthreads();
     uint32_t lo = 0u, hi = 0xffffffffu;
     if (c >= 64) {
@@ -964,8 +1083,8 @@ __global__ void __launch_bounds__(kBoundThreads) k_bwin_bounds(const uint32_t* _
         const double qc = q < 1.0 / c ? 1.0 / c : (q > 1.0 - 1.0 / c ? 1.0 - 1.0 / c : q);
         const long long ks = (long long)(q * (double)(c - 1));
         const long long d = (long long)ceil(kWinSigmas * sqrt((double)c * qc * (1.0 - qc))) + 4;
-        if (ks - d >= 0) lo = block_select(wkeys, c, ks - d, wh, part, s_sel, 2);
-        if (ks + d + 1 < c) hi = block_select(wkeys, c, ks + d + 1, wh, part, s_sel, 2) | 0xffffu;
+        if (ks - d >= 0) lo = block_select(keys, c, ks - d, wh, part, s_sel, 2);
+        if (ks + d + 1 < c) hi = block_select(keys, c, ks + d + 1, wh, part, s_sel, 2) | 0xffffu;
     }
     if (t == 0) {
         ctl->bwlo[b] = lo;
@@ -973,11 +1092,39 @@ __global__ void __launch_bounds__(kBoundThreads) k_bwin_bounds(const uint32_t* _
     }
 }
 
-// The counting pass of the bins' windows: mean and variance read once (SU float4 of each per
-// thread and step). Per voxel a code bin*3 + {below, inside, above} goes through a run
-// accumulator into shared counters; the inside keys are placed by one warp scan per step in
-// the warp's buffer and appended to the list (one atomic per buffer), as in k_win_count.
-__global__ void __launch_bounds__(256) k_bwin_count(const float* __restrict__ mean, const float* __restrict__ var,
+// Per-thread run of voxels in one bin with its below / inside counts: neighbouring voxels
+// mostly share a bin, so the shared counters (bin*3 + {below, inside, above}) take a few
+// atomics per run rather than one per change of class.
+struct BinRun {
+    int cur = -1;
+    unsigned int n = 0, below = 0, in = 0;
+    FY_D void flush(unsigned int* h) {
+        if (cur >= 0) {
+            if (below) atomicAdd(&h[3 * cur], below);
+            if (in) atomicAdd(&h[3 * cur + 1], in);
+            if (n - below - in) atomicAdd(&h[3 * cur + 2], n - below - in);
+        }
+        cur = -1;
+        n = below = in = 0;
+    }
+    FY_D void add(unsigned int* h, int b, int cls) {
+        if (b != cur) {                 // also leaves a run for an out-of-range voxel (b = -1)
+            flush(h);
+            cur = b;
+        }
+        n += b >= 0;
+        below += b >= 0 && cls == 0;
+        in += b >= 0 && cls == 1;
+    }
+};
+
+// The counting pass of the bins' windows: mean and variance read once, SU float4 of each per
+// thread and step, consecutive in x (4*SU neighbouring voxels, which mostly share a bin, so
+// the BinRun's runs are long). Each voxel's bin and class (below, inside, above the bin's
+// window) go through the BinRun into shared counters; the inside keys are placed by one warp
+// scan per step in the warp's buffer and appended to the list (one atomic per buffer), as
+// in k_win_count.
+__global__ void __launch_bounds__(256, 4) k_bwin_count(const float* __restrict__ mean, const float* __restrict__ var,
                                                     NoiseCtl* __restrict__ ctl, float* __restrict__ cval,
                                                     uint8_t* __restrict__ clab, long long cap) {
     fy_pdl_wait();
@@ -996,17 +1143,33 @@ __global__ void __launch_bounds__(256) k_bwin_count(const float* __restrict__ me
     }
     for (int i = t; i < NB * 3; i += blockDim.x) sc[i] = 0;
     __syncthreads();
-    const float lo_f = fe[0], fscale = ctl->fscale;
+    const float lo_f = fe[0], hi_e = fe[NB], fscale = ctl->fscale;
     WarpCands wc;
     wc.v = bufv[t >> 5];
     wc.l = bufl[t >> 5];
-    RunAcc acc;
-    // class of one voxel: -1 outside every bin, else bin*3 + {0 below, 1 inside, 2 above}
-    auto code_of = [&](float m, float v) -> int {
-        const int b = bin_of(m, fe, lo_f, fscale);
-        if (b < 0) return -1;
+    BinRun acc;
+    // bin of one voxel (-1 outside every bin) and its class {0 below, 1 inside, 2 above}. The
+    // last bin's edges and window stay in registers: a voxel in the same bin as the thread's
+    // previous one (the common case) reads no shared memory.
+    int cb = -1;
+    float ce0 = 1.f, ce1 = 0.f;                          // empty: matches nothing
+    uint32_t cwl = 0u, cwh = 0u;
+    auto classify = [&](float m, float v, int& b, int& cls) {
+        if (!(m >= ce0 && m < ce1)) {
+            const int nb = bin_fast(m, fe, lo_f, hi_e, lo_f, fscale);
+            if (nb >= 0) {
+                cb = nb;
+                ce0 = fe[nb];
+                ce1 = fe[nb + 1];
+                cwl = swl[nb];
+                cwh = swh[nb];
+            }
+            b = nb;
+        } else {
+            b = cb;
+        }
         const uint32_t k = fkey(v);
-        return b * 3 + (k < swl[b] ? 0 : (k <= swh[b] ? 1 : 2));
+        cls = (int)(k >= cwl) + (int)(k > cwh);
     };
     const long long n = ctl->n, n4 = (n + 3) / 4, n4f = n / 4;
     const long long chunk = (long long)SU * 256;
@@ -1015,25 +1178,25 @@ __global__ void __launch_bounds__(256) k_bwin_count(const float* __restrict__ me
         float4 xm[SU], xv[SU];
 #pragma unroll
         for (int u = 0; u < SU; ++u) {
-            const long long q = base + t + (long long)u * 256;
+            const long long q = base + (long long)t * SU + u;
             xm[u] = __ldg(reinterpret_cast<const float4*>(mean) + q);
             xv[u] = __ldg(reinterpret_cast<const float4*>(var) + q);
         }
         float vv[4 * SU];
-        int cd[4 * SU];
+        int bq[4 * SU];
         unsigned hit = 0;
 #pragma unroll
         for (int u = 0; u < SU; ++u) {
             vv[4 * u] = xv[u].x; vv[4 * u + 1] = xv[u].y; vv[4 * u + 2] = xv[u].z; vv[4 * u + 3] = xv[u].w;
-            cd[4 * u] = code_of(xm[u].x, xv[u].x);
-            cd[4 * u + 1] = code_of(xm[u].y, xv[u].y);
-            cd[4 * u + 2] = code_of(xm[u].z, xv[u].z);
-            cd[4 * u + 3] = code_of(xm[u].w, xv[u].w);
-        }
+            const float mm[4] = {xm[u].x, xm[u].y, xm[u].z, xm[u].w};
 #pragma unroll
-        for (int q = 0; q < 4 * SU; ++q) {
-            acc.add(sc, cd[q]);
-            hit |= (unsigned)(cd[q] >= 0 && cd[q] % 3 == 1) << q;
+            for (int j = 0; j < 4; ++j) {
+                int b, cls;
+                classify(mm[j], vv[4 * u + j], b, cls);
+                bq[4 * u + j] = b;
+                acc.add(sc, b, cls);
+                hit |= (unsigned)(b >= 0 && cls == 1) << (4 * u + j);
+            }
         }
         const int c = __popc(hit);
         int incl = c;
@@ -1048,21 +1211,22 @@ __global__ void __launch_bounds__(256) k_bwin_count(const float* __restrict__ me
         int pos = wc.cnt + incl - c;
 #pragma unroll
         for (int q = 0; q < 4 * SU; ++q)
-            if ((hit >> q) & 1u) { wc.v[pos] = vv[q]; wc.l[pos] = (uint8_t)(cd[q] / 3); ++pos; }
+            if ((hit >> q) & 1u) { wc.v[pos] = vv[q]; wc.l[pos] = (uint8_t)bq[q]; ++pos; }
         wc.cnt += tot;
         __syncwarp();
     }
     if (base < n4) {                                     // the grid's partial chunk
         for (int u = 0; u < SU; ++u)
             for (int j = 0; j < 4; ++j) {
-                const long long i = 4 * (base + t + (long long)u * 256) + j;
+                const long long i = 4 * (base + (long long)t * SU + u) + j;
                 if (i >= n) continue;
                 const float v = __ldg(var + i);
-                const int code = code_of(__ldg(mean + i), v);
-                acc.add(sc, code);
-                if (code >= 0 && code % 3 == 1) {
+                int b, cls;
+                classify(__ldg(mean + i), v, b, cls);
+                acc.add(sc, b, cls);
+                if (b >= 0 && cls == 1) {
                     const unsigned long long pos = atomicAdd(&ctl->ncand, 1ull);
-                    if ((long long)pos < cap) { cval[pos] = v; clab[pos] = (uint8_t)(code / 3); }
+                    if ((long long)pos < cap) { cval[pos] = v; clab[pos] = (uint8_t)b; }
                 }
             }
     }
@@ -1333,11 +1497,12 @@ size_t fy_noise_scratch_floats(size_t n) { return noise_layout(n).total; }
 // 2n floats): the statistics pass also writes the guided filter's (mean, var) pairs of the
 // same window, for fy_launch_guided_apply_mv with r = win/2.
 // Every selection kernel runs as a programmatic dependent launch; the first failed launch
-// is returned.
+// is returned. PDL counts the launches into `launches`.
 #define PDL(k, ...)                                                            \
     do {                                                                       \
         const cudaError_t pe_ = fy_launch_pdl(k, __VA_ARGS__);                 \
         if (pe_ != cudaSuccess) return pe_;                                    \
+        ++launches;                                                            \
     } while (0)
 cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, int win, double flat_pct,
                                      double ref_intensity, float* scratch, void* ctl_mem, int sms,
@@ -1370,7 +1535,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     if ((e = fy_smem_optin(k_win_bounds, smem_keys)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(ctl->hist, 0, sizeof(ctl->hist), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(cc->hist, 0, sizeof(cc->hist), st)) != cudaSuccess) return e;
-    PDL(k_noise_setup, 1, 1, 0, st, ctl, n, flat_pct, ref_intensity);
+    PDL(k_noise_setup, 1, 1, 0, st, ctl, cc, n, flat_pct, ref_intensity);
     {   // 1. stats
         fyzb::Params sp{};
         sp.nz = nz; sp.ny = ny; sp.nx = nx;
@@ -1378,6 +1543,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
         sp.inv_wc = inv_wc; sp.wci = win * win * win;
         cudaError_t e0 = fyzb::launch<fyzb::ZB_NOISE>(sp, r, sms, st);
         if (e0 != cudaSuccess) return e0;
+        ++launches;
         fy_prof_mark(st, "noise.stats");
     }
     // 2a. 1st/99th percentile of the means: sample-guided window pass, then the radix passes
@@ -1389,20 +1555,22 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     PDL(k_win_count, g, 256, 0, st, mean, ctl, cval, clab, L.cap);
     PDL(k_win_arm, 1, 1, 0, st, ctl, cc, L.cap);
     for (int sh = 24; sh >= 0; sh -= 8) {
-        PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL);
+        // the first digit's histogram sets the ranks (k_win_targets) before its scan; the
+        // later digits' scans run in each pass's last CTA
+        PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL,
+            sh == 24 ? -1 : (sh == 0 ? 1 : 0));
         if (sh == 24) {
             PDL(k_win_targets, 2, 256, 0, st, ctl, cc);
             PDL(k_win_check, 1, 1, 0, st, ctl, cc);
+            PDL(k_sel_scan, 2, 256, 0, st, cc, 8, 1, 0);
         }
-        PDL(k_sel_scan, 2, 256, 0, st, cc, 8, 1, sh == 0);
     }
     PDL(k_sel_next, gs, 256, 0, st, nullptr, cval, clab, cc, 1);
     PDL(k_win_finish, 1, 1, 0, st, ctl, cc);
     const int all_digits[3][2] = {{21, 11}, {10, 11}, {0, 10}};
     for (int i = 0; i < 3; ++i) {
-        if (all_digits[i][1] == 11) PDL((k_sel_hist<11, 0>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
-        else PDL((k_sel_hist<10, 0>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
-        PDL(k_sel_scan, 2, 256, 0, st, ctl, all_digits[i][1], 0, i == 2);
+        if (all_digits[i][1] == 11) PDL((k_sel_hist<11, 0>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
+        else PDL((k_sel_hist<10, 0>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
     }
     PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 0);
     PDL(k_noise_bins_setup, 1, 1, 0, st, ctl);
@@ -1421,10 +1589,9 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
         PDL(k_bwin_bounds, NB, kBoundThreads, smem_keys, st, skey, slab, ctl, m2);
         PDL(k_bwin_count, g, 256, 0, st, mean, var, ctl, cval, clab, L.cap);
         PDL(k_bwin_arm, 1, 256, 0, st, ctl, cc, L.cap);
-        for (int sh = 24; sh >= 0; sh -= 8) {
-            PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL);
-            PDL(k_sel_scan, NB, 256, 0, st, cc, 8, 1, sh == 0);
-        }
+        for (int sh = 24; sh >= 0; sh -= 8)
+            PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL,
+                sh == 0 ? 1 : 0);
         PDL(k_sel_next, gcl, 256, 0, st, nullptr, cval, clab, cc, 1);
         PDL(k_bwin_finish, 1, 32, 0, st, ctl, cc);
     }
@@ -1433,20 +1600,16 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     // the first pass also labels the voxels with their bins and yields the bin counts. The
     // third pass also lists the voxels that match their bin's 16-bit prefix (~1% of them),
     // and the last digit runs over that list (falling back to the whole field if it overflows).
-    PDL((k_sel_hist<8, 1, true>), g, 256, smem_bin, st, mean, var, bin, ctl, 24, nullptr, nullptr, 0LL);
+    PDL((k_sel_hist<8, 1, true>), g, 256, smem_bin, st, mean, var, bin, ctl, 24, nullptr, nullptr, 0LL, -1);
     PDL(k_bin_targets, NB, 256, 0, st, ctl);
     PDL(k_sel_scan, NB, 256, 0, st, ctl, 8, 1, 0);
-    PDL((k_sel_hist<8, 1>), g, 256, smem_bin, st, mean, var, bin, ctl, 16, nullptr, nullptr, 0LL);
-    PDL(k_sel_scan, NB, 256, 0, st, ctl, 8, 1, 0);
+    PDL((k_sel_hist<8, 1>), g, 256, smem_bin, st, mean, var, bin, ctl, 16, nullptr, nullptr, 0LL, 0);
     PDL(k_bin_cand_reset, 1, 1, 0, st, ctl);
     if ((e = fy_smem_optin(k_sel_hist<8, 1, false, true>, smem_bin_c)) != cudaSuccess) return e;
-    PDL((k_sel_hist<8, 1, false, true>), g, 256, smem_bin_c, st, mean, var, bin, ctl, 8, cval, clab, L.cap);
-    PDL(k_sel_scan, NB, 256, 0, st, ctl, 8, 1, 0);
+    PDL((k_sel_hist<8, 1, false, true>), g, 256, smem_bin_c, st, mean, var, bin, ctl, 8, cval, clab, L.cap, 0);
     PDL(k_bin_arm, 1, 256, 0, st, ctl, cc, L.cap);
-    PDL((k_sel_hist<8, 1>), gs, 256, smem_bin, st, mean, var, bin, ctl, 0, nullptr, nullptr, 0LL);       // overflow only
-    PDL(k_sel_scan, NB, 256, 0, st, ctl, 8, 1, 1);
-    PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, 0, nullptr, nullptr, 0LL);  // the list
-    PDL(k_sel_scan, NB, 256, 0, st, cc, 8, 1, 1);
+    PDL((k_sel_hist<8, 1>), gs, 256, smem_bin, st, mean, var, bin, ctl, 0, nullptr, nullptr, 0LL, 1);       // overflow only
+    PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, 0, nullptr, nullptr, 0LL, 1);  // the list
     // k+1 past the selected key's 24-bit prefix: the list holds every key of the bin that shares
     // its 16-bit prefix, so when it holds a larger key, its smallest larger key is the next one
     // (a key in between would share the prefix and be listed too). Only targets whose next key
@@ -1458,13 +1621,11 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     fy_prof_mark(st, "noise.bin_select");
     // 2c. fallback (mode 2 only): flat_pct percentile over all voxels' variance
     for (int i = 0; i < 3; ++i) {
-        if (all_digits[i][1] == 11) PDL((k_sel_hist<11, 2>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
-        else PDL((k_sel_hist<10, 2>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL);
-        PDL(k_sel_scan, 1, 256, 0, st, ctl, all_digits[i][1], 2, i == 2);
+        if (all_digits[i][1] == 11) PDL((k_sel_hist<11, 2>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
+        else PDL((k_sel_hist<10, 2>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
     }
     PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 2);
     PDL(k_noise_fit, 1, 32, 0, st, ctl, 1);
-    launches += 1 + 1 + 1 + 1 + 1 + 1 + 1 + 10 + 1 + 1 + 7 + 1 + 14 + 16 + 1 + 1 + 7 + 1;
     return cudaGetLastError();
 }
 

@@ -36,7 +36,9 @@
 //                 (guided.c:181-182). The pairs are staged as one interleaved field.
 //   ZB_GUIDED_OUT_MV  the same from staged (mean, var) pairs, turned into (a, b) as the X
 //                 phase reads them, with ZB_GUIDED_AB's expressions, so the output equals the
-//                 two-pass filter's bit for bit (eps > 0).
+//                 two-pass filter's bit for bit (eps > 0). (Converting each staged pair once,
+//                 in place, a plane ahead measured 19% slower: the extra wait and conversion
+//                 sit before the plane's barrier.)
 // Window sums are direct (2R+1)-tap float sums in ascending order, started from the first
 // tap, so no running-sum chain accumulates error. Each output voxel is written once by one
 // thread, and ZB_GUIDED_OUT reads the guide only at the voxel it writes, so out may alias
@@ -53,6 +55,9 @@ constexpr int TX = 64, TY = 16, NT = 256, NS = 4;
 constexpr int SXW = TX + 8;                 // staged row: x0 - 4 .. x0 + TX + 4 (R <= 4)
 enum { ZB_NOISE = 0, ZB_GUIDED_AB = 1, ZB_GUIDED_OUT = 2, ZB_GUIDED_OUT_MV = 3 };
 __host__ __device__ constexpr bool out_kind(int k) { return k == ZB_GUIDED_OUT || k == ZB_GUIDED_OUT_MV; }
+// Resident CTAs per SM (two: a third CTA of the noise statistics, which fits at R <= 2,
+// measured 45% slower per pass).
+__host__ __device__ constexpr int ctas_per_sm(int r, int kind) { return (void)r, (void)kind, 2; }
 
 struct Params {
     const float* f0;       // I (NOISE, GUIDED_AB) or interleaved (a, b) | (mean, var) pairs (OUT kinds)
@@ -206,7 +211,7 @@ FY_D void stage_plane(float* dst, const Params& p, int zi, int x0, int y0) {
 }
 
 template <int R, int KIND, bool VEC, bool TMA>
-__global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p, const __grid_constant__ TmaMaps tm) {
+__global__ void __launch_bounds__(NT, ctas_per_sm(R, KIND)) k_zbox(const __grid_constant__ Params p, const __grid_constant__ TmaMaps tm) {
     fy_pdl_wait();
     constexpr int C = out_kind(KIND) ? 2 : 1;
     using G = Geo<R, C>;
@@ -507,12 +512,11 @@ __global__ void __launch_bounds__(NT, 2) k_zbox(const __grid_constant__ Params p
 }
 
 // Tiles and z chunks (fy_box_default_chunks, fy_internal.h). The chunk count is fixed by the
-// shape and SM count alone: each chunk takes its variance shift from its first plane, so
-// another chunking would round the sums differently.
+// shape, the kind's residency and the SM count alone: each chunk takes its variance shift
+// from its first plane, so another chunking would round the sums differently.
 inline dim3 grid_for(int kind, int nz, int ny, int nx, int r, int sms, int& zchunk) {
-    (void)kind;
     const int tx = (nx + TX - 1) / TX, ty = (ny + TY - 1) / TY;
-    const int nc = fy_box_default_chunks(nz, ny, nx, r, sms);
+    const int nc = fy_box_default_chunks(nz, ny, nx, r, sms, ctas_per_sm(r, kind));
     zchunk = (nz + nc - 1) / nc;
     return dim3(tx, ty, (nz + zchunk - 1) / zchunk);
 }
