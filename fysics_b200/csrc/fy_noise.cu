@@ -535,49 +535,66 @@ FY_D void target_init(NoiseCtl* ctl, int t, long long k, long long group_n, bool
     ctl->tnext[t] = 0xffffffffu;
 }
 
-__global__ void k_noise_setup(NoiseCtl* ctl, NoiseCtl* cc, long long n, double flat_pct, double ref_intensity) {
+// One block of NT_MAX threads: thread t initialises target t.
+__global__ void __launch_bounds__(NT_MAX) k_noise_setup(NoiseCtl* ctl, NoiseCtl* cc, long long n, double flat_pct,
+                                                       double ref_intensity) {
     fy_pdl_wait();
-    ctl->done_ctas = 0;
-    cc->done_ctas = 0;
-    ctl->n = n;
-    ctl->flat_pct = flat_pct;
-    ctl->ref_intensity = ref_intensity;
-    ctl->mode = kModeWin0;                 // the radix passes run only if the windows fail
-    for (int t = 0; t < NT_MAX; ++t) target_init(ctl, t, 0, 0, false);
+    const int t = threadIdx.x;
     const double i1 = 1.0 / 100.0 * (double)(n - 1), i99 = 99.0 / 100.0 * (double)(n - 1);
-    target_init(ctl, 0, (long long)i1, n, true);              // 1st percentile of the means
-    target_init(ctl, 1, (long long)i99, n, true);             // 99th
-    ctl->ntarget = 2;
-    for (int b = 0; b < NB; ++b) ctl->bcount[b] = 0;
+    if (t == 0) target_init(ctl, 0, (long long)i1, n, true);           // 1st percentile of the means
+    else if (t == 1) target_init(ctl, 1, (long long)i99, n, true);     // 99th
+    else target_init(ctl, t, 0, 0, false);
+    if (t < NB) ctl->bcount[t] = 0;
+    if (t == 0) {
+        ctl->done_ctas = 0;
+        cc->done_ctas = 0;
+        ctl->n = n;
+        ctl->flat_pct = flat_pct;
+        ctl->ref_intensity = ref_intensity;
+        ctl->mode = kModeWin0;             // the radix passes run only if the windows fail
+        ctl->ntarget = 2;
+    }
 }
 
-// lo/hi from the selected means; bin edges (noise.c:106-119)
-__global__ void k_noise_bins_setup(NoiseCtl* ctl) {
+// lo/hi from the selected means; bin edges (noise.c:106-119). One block of NT_MAX threads.
+__global__ void __launch_bounds__(NT_MAX) k_noise_bins_setup(NoiseCtl* ctl) {
     fy_pdl_wait();
-    const long long n = ctl->n;
-    const double i1 = 1.0 / 100.0 * (double)(n - 1), i99 = 99.0 / 100.0 * (double)(n - 1);
-    const long long k1 = (long long)i1, k99 = (long long)i99;
-    double lo = interp(ctl, 0, i1 - (double)k1, k1 + 1 < n);
-    double hi = interp(ctl, 1, i99 - (double)k99, k99 + 1 < n);
-    if (hi <= lo) hi = lo + 1e-6;                       // noise.c:109
-    ctl->lo = lo; ctl->hi = hi;
-    for (int k = 0; k <= NB; ++k) {
-        const double e = lo + (hi - lo) * k / NB;      // noise.c:118-119
-        ctl->edge[k] = e;
+    __shared__ double s_lo, s_hi;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        const long long n = ctl->n;
+        const double i1 = 1.0 / 100.0 * (double)(n - 1), i99 = 99.0 / 100.0 * (double)(n - 1);
+        const long long k1 = (long long)i1, k99 = (long long)i99;
+        const double lo = interp(ctl, 0, i1 - (double)k1, k1 + 1 < n);
+        double hi = interp(ctl, 1, i99 - (double)k99, k99 + 1 < n);
+        if (hi <= lo) hi = lo + 1e-6;                   // noise.c:109
+        s_lo = lo;
+        s_hi = hi;
+    }
+    __syncthreads();                                    // targets 0/1 read before they are reset
+    const double lo = s_lo, hi = s_hi;
+    if (t <= NB) {
+        const double e = lo + (hi - lo) * t / NB;      // noise.c:118-119
+        ctl->edge[t] = e;
         float f = (float)e;
         if ((double)f < e) f = nextafterf(f, INFINITY);
-        ctl->fedge[k] = f;
+        ctl->fedge[t] = f;
     }
-    ctl->fscale = (float)(NB / (hi - lo));
-    // first variance digit pass: every bin active with the empty prefix (its histogram
-    // gives the bin counts; k_bin_targets then sets the ranks)
-    for (int t = 0; t < NT_MAX; ++t) target_init(ctl, t, 0, 0, t < NB);
-    ctl->ntarget = NB;
-    // the bins' window runs first (section 2bw); it hands over to these radix passes (mode 1)
-    // when it misses
-    for (int i = 0; i < NB * 3; ++i) ctl->bwc[i] = 0;
-    ctl->ncand = 0;
-    ctl->mode = kModeBinWin;
+    // the radix passes' first variance digit: every bin active with the empty prefix (its
+    // histogram gives the bin counts; k_bin_targets then sets the ranks)
+    target_init(ctl, t, 0, 0, t < NB);
+    for (int i = t; i < NB * 3; i += blockDim.x) ctl->bwc[i] = 0;
+    if (t == 0) {
+        ctl->lo = lo;
+        ctl->hi = hi;
+        ctl->fscale = (float)(NB / (hi - lo));
+        ctl->ntarget = NB;
+        // the bins' window runs first (section 2bw); it hands over to the radix passes
+        // (mode 1) when it misses
+        ctl->ncand = 0;
+        ctl->wfail = 0;
+        ctl->mode = kModeBinWin;
+    }
 }
 
 // After the first variance digit pass (one block per bin): the bin's count is the sum of its
@@ -855,6 +872,7 @@ __global__ void k_win_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc,
     if ((long long)ctl->ncand > cap || (noise_force_radix & 1)) {
         cc->mode = 3;
         ctl->wfail = 1;
+        ctl->mode = 0;                     // the radix passes over the whole field
     } else {
         cc->mode = 1;
     }
@@ -862,7 +880,9 @@ __global__ void k_win_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc,
 
 // After the candidates' first digit pass (one block per target): the target's inside count
 // is the sum of its histogram; its rank among the candidates is r = k - below, which must
-// leave k and (when it exists) k+1 inside. Otherwise the selection fails (k_win_check).
+// leave k and (when it exists) k+1 inside. Otherwise the window failed: the candidate passes
+// stand aside (cc mode 3) and the radix passes over the whole field run (mode 0). A block
+// that finds cc already failed leaves its histogram, which every later user clears first.
 __global__ void __launch_bounds__(256) k_win_targets(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) {
     fy_pdl_wait();
     __shared__ unsigned long long part[256];
@@ -885,7 +905,11 @@ __global__ void __launch_bounds__(256) k_win_targets(NoiseCtl* __restrict__ ctl,
     if (!ok) h[threadIdx.x] = 0;                         // inactive: its histogram is cleared
     if (threadIdx.x == 0) {
         target_init(cc, t, ok ? r : 0, in, ok);
-        if (!ok) atomicExch(&ctl->wfail, 1);
+        if (!ok) {
+            ctl->wfail = 1;
+            cc->mode = 3;
+            ctl->mode = 0;
+        }
     }
 }
 
@@ -939,14 +963,6 @@ __global__ void k_bin_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restr
     ctl->mode = 1;
 }
 
-// One thread: a failed window sends the selection to the radix passes over the whole field.
-__global__ void k_win_check(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) {
-    fy_pdl_wait();
-    if (ctl->mode != kModeWin0 || !ctl->wfail) return;
-    cc->mode = 3;
-    ctl->mode = 0;
-}
-
 // Keys of order statistics k and k+1 into the main block's targets 0/1 (interp / next_value
 // form); the radix passes of mode 0 then stand aside.
 __global__ void k_win_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restrict__ cc) {
@@ -970,12 +986,13 @@ __global__ void k_win_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restr
 //            kBinKeysMax) and takes the order statistics kWinSigmas binomial standard
 //            deviations either side of the target's sample rank, each widened to its 16-bit
 //            key bucket (two digit passes): [bwlo, bwhi]. Under 64 samples: every key.
-//   count    one pass over mean and variance: per bin, the keys below, inside and above its
-//            window (their sum is the bin count, noise.c:118-123); the keys inside go to the
+//   count    one branch-free pass over mean and variance: per bin its voxels (the bin count,
+//            noise.c:118-123) and the keys below its window; the keys inside go to the
 //            candidate list with their bin.
-//   arm      for each bin of >= 200 voxels, k = flat_pct/100*(count - 1) and r = k - below
-//            must leave k and k+1 inside; the four digit passes of mode 1 over the candidates
-//            (control block cc, targets = bins) then select them. A miss or an overfull list
+//   arm      for each bin of >= 200 voxels, r = k - below with k = flat_pct/100*(count - 1);
+//            the first digit pass over the candidates (control block cc, targets = bins) gives
+//            the inside counts, and k and k+1 must be inside (k_bwin_targets); the other three
+//            digit passes then select them. A miss, an overfull list or a failed bin guess
 //            sends the bins to the radix passes over the whole field (mode 1).
 //   finish   the keys of k and k+1 into the main block; mode kModeBinDone makes the radix
 //            passes stand aside.
@@ -1092,47 +1109,32 @@ __global__ void __launch_bounds__(kBoundThreads) k_bwin_bounds(const uint32_t* _
     }
 }
 
-// Per-thread run of voxels in one bin with its below / inside counts: neighbouring voxels
-// mostly share a bin, so the shared counters (bin*3 + {below, inside, above}) take a few
-// atomics per run rather than one per change of class.
-struct BinRun {
-    int cur = -1;
-    unsigned int n = 0, below = 0, in = 0;
-    FY_D void flush(unsigned int* h) {
-        if (cur >= 0) {
-            if (below) atomicAdd(&h[3 * cur], below);
-            if (in) atomicAdd(&h[3 * cur + 1], in);
-            if (n - below - in) atomicAdd(&h[3 * cur + 2], n - below - in);
-        }
-        cur = -1;
-        n = below = in = 0;
-    }
-    FY_D void add(unsigned int* h, int b, int cls) {
-        if (b != cur) {                 // also leaves a run for an out-of-range voxel (b = -1)
-            flush(h);
-            cur = b;
-        }
-        n += b >= 0;
-        below += b >= 0 && cls == 0;
-        in += b >= 0 && cls == 1;
-    }
-};
-
-// The counting pass of the bins' windows: mean and variance read once, SU float4 of each per
-// thread and step, consecutive in x (4*SU neighbouring voxels, which mostly share a bin, so
-// the BinRun's runs are long). Each voxel's bin and class (below, inside, above the bin's
-// window) go through the BinRun into shared counters; the inside keys are placed by one warp
-// scan per step in the warp's buffer and appended to the list (one atomic per buffer), as
-// in k_win_count.
+// The counting pass of the bins' windows: mean and variance read once, SUB float4 of each
+// per thread and step. Every voxel takes the same branch-free path: its bin from the float
+// guess corrected by one step (exact unless the range [lo, hi] is degenerate; a voxel whose
+// corrected bin fails the exact membership test raises ctl->wfail and the bins fall back to
+// the radix passes), the key of its variance against the bin's window, and one
+// read-modify-write of the lane's own shared-memory counter of its bin (low 16 bits: the
+// bin's voxels, high 16 bits: those below the window; rows of 25 words, so the lanes of a
+// warp hit distinct banks when they share a bin; added into the CTA's totals before a field
+// can pass 65535). The keys inside the window are placed by one warp scan per step in the
+// warp's buffer and appended to the list (one atomic per buffer), as in k_win_count. The
+// inside counts come from the candidates' first digit histogram (k_bwin_targets).
+constexpr int kBCountBuf = 512;          // per warp: two steps' worst case (32 x 8 each)
+constexpr int kLaneRow = 25;             // counter words per lane (NB = 24, odd stride)
 __global__ void __launch_bounds__(256, 4) k_bwin_count(const float* __restrict__ mean, const float* __restrict__ var,
-                                                    NoiseCtl* __restrict__ ctl, float* __restrict__ cval,
-                                                    uint8_t* __restrict__ clab, long long cap) {
+                                                       NoiseCtl* __restrict__ ctl, float* __restrict__ cval,
+                                                       uint8_t* __restrict__ clab, long long cap) {
     fy_pdl_wait();
-    __shared__ float bufv[256 / 32][kCountBuf];
-    __shared__ uint8_t bufl[256 / 32][kCountBuf];
+    constexpr int SUB = 2;                               // float4 of each field per thread and step
+    static_assert(32 * 4 * SUB <= kBCountBuf && NB < kLaneRow, "buffer and counter rows");
+    __shared__ float bufv[256 / 32][kBCountBuf];
+    __shared__ uint8_t bufl[256 / 32][kBCountBuf];
+    __shared__ unsigned int lc[256 * kLaneRow];          // per-lane counters
     __shared__ float fe[NB + 1];
     __shared__ uint32_t swl[NB], swh[NB];
     __shared__ unsigned int sc[NB * 3];
+    __shared__ int s_bad;
     if (ctl->mode != kModeBinWin) return;
     const unsigned full = 0xffffffffu;
     const int t = threadIdx.x, lane = t & 31;
@@ -1142,61 +1144,73 @@ __global__ void __launch_bounds__(256, 4) k_bwin_count(const float* __restrict__
         swh[t] = ctl->bwhi[t];
     }
     for (int i = t; i < NB * 3; i += blockDim.x) sc[i] = 0;
+    for (int i = t; i < 256 * kLaneRow; i += blockDim.x) lc[i] = 0;
+    if (t == 0) s_bad = 0;
     __syncthreads();
-    const float lo_f = fe[0], hi_e = fe[NB], fscale = ctl->fscale;
+    const float lo_e = fe[0], hi_e = fe[NB], fscale = ctl->fscale;
+    unsigned int* row = lc + t * kLaneRow;
     WarpCands wc;
     wc.v = bufv[t >> 5];
     wc.l = bufl[t >> 5];
-    BinRun acc;
-    // bin of one voxel (-1 outside every bin) and its class {0 below, 1 inside, 2 above}. The
-    // last bin's edges and window stay in registers: a voxel in the same bin as the thread's
-    // previous one (the common case) reads no shared memory.
-    int cb = -1;
-    float ce0 = 1.f, ce1 = 0.f;                          // empty: matches nothing
-    uint32_t cwl = 0u, cwh = 0u;
-    auto classify = [&](float m, float v, int& b, int& cls) {
-        if (!(m >= ce0 && m < ce1)) {
-            const int nb = bin_fast(m, fe, lo_f, hi_e, lo_f, fscale);
-            if (nb >= 0) {
-                cb = nb;
-                ce0 = fe[nb];
-                ce1 = fe[nb + 1];
-                cwl = swl[nb];
-                cwh = swh[nb];
-            }
-            b = nb;
-        } else {
-            b = cb;
-        }
+    bool bad = false;
+    // bin (or -1 outside every bin) and whether the key is inside the bin's window
+    auto classify = [&](float m, float v, bool valid, int& bo, bool& inside) {
+        const bool inr = valid && m >= lo_e && m < hi_e;
+        const float mc = inr ? m : lo_e;
+        int b = (int)((mc - lo_e) * fscale);
+        b = b < 0 ? 0 : (b > NB - 1 ? NB - 1 : b);
+        b = b - (int)(mc < fe[b]) + (int)(mc >= fe[b + 1]);
+        bad |= !(mc >= fe[b] && mc < fe[b + 1]);
         const uint32_t k = fkey(v);
-        cls = (int)(k >= cwl) + (int)(k > cwh);
+        const uint32_t wl = swl[b], wh = swh[b];
+        row[b] += inr ? (k < wl ? 0x10001u : 1u) : 0u;
+        inside = inr && k >= wl && k <= wh;
+        bo = b;
+    };
+    auto flush_rows = [&]() {                             // CTA-uniform
+        __syncthreads();
+        for (int i = t; i < NB * 2; i += blockDim.x) {   // one thread per bin and field
+            const int bb = i >> 1, hi = i & 1;
+            unsigned int sum = 0;
+            for (int l = 0; l < 256; ++l) {
+                const unsigned int w = lc[l * kLaneRow + bb];
+                sum += hi ? w >> 16 : w & 0xffffu;
+            }
+            if (sum) atomicAdd(&sc[3 * bb + (hi ? 0 : 2)], sum);
+        }
+        __syncthreads();
+        for (int i = 0; i < NB; ++i) row[i] = 0;
+        __syncthreads();
     };
     const long long n = ctl->n, n4 = (n + 3) / 4, n4f = n / 4;
-    const long long chunk = (long long)SU * 256;
+    const long long chunk = (long long)SUB * 256;
     long long base = (long long)blockIdx.x * chunk;
+    int steps = 0;
     for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
-        float4 xm[SU], xv[SU];
+        float4 xm[SUB], xv[SUB];
 #pragma unroll
-        for (int u = 0; u < SU; ++u) {
-            const long long q = base + (long long)t * SU + u;
+        for (int u = 0; u < SUB; ++u) {
+            const long long q = base + (long long)t * SUB + u;
             xm[u] = __ldg(reinterpret_cast<const float4*>(mean) + q);
             xv[u] = __ldg(reinterpret_cast<const float4*>(var) + q);
         }
-        float vv[4 * SU];
-        int bq[4 * SU];
+        float vv[4 * SUB];
+        int bq[4 * SUB];
         unsigned hit = 0;
 #pragma unroll
-        for (int u = 0; u < SU; ++u) {
-            vv[4 * u] = xv[u].x; vv[4 * u + 1] = xv[u].y; vv[4 * u + 2] = xv[u].z; vv[4 * u + 3] = xv[u].w;
+        for (int u = 0; u < SUB; ++u) {
             const float mm[4] = {xm[u].x, xm[u].y, xm[u].z, xm[u].w};
+            vv[4 * u] = xv[u].x; vv[4 * u + 1] = xv[u].y; vv[4 * u + 2] = xv[u].z; vv[4 * u + 3] = xv[u].w;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                int b, cls;
-                classify(mm[j], vv[4 * u + j], b, cls);
-                bq[4 * u + j] = b;
-                acc.add(sc, b, cls);
-                hit |= (unsigned)(b >= 0 && cls == 1) << (4 * u + j);
+                bool ins;
+                classify(mm[j], vv[4 * u + j], true, bq[4 * u + j], ins);
+                hit |= (unsigned)ins << (4 * u + j);
             }
+        }
+        if (++steps == 65535 / (4 * SUB)) {              // a 16-bit field could pass 65535
+            flush_rows();
+            steps = 0;
         }
         const int c = __popc(hit);
         int incl = c;
@@ -1207,39 +1221,41 @@ __global__ void __launch_bounds__(256, 4) k_bwin_count(const float* __restrict__
         }
         const int tot = __shfl_sync(full, incl, 31);
         if (tot == 0) continue;
-        if (wc.cnt + tot > kCountBuf) wc.flush(cval, clab, &ctl->ncand, cap);     // warp-uniform
+        if (wc.cnt + tot > kBCountBuf) wc.flush(cval, clab, &ctl->ncand, cap);     // warp-uniform
         int pos = wc.cnt + incl - c;
 #pragma unroll
-        for (int q = 0; q < 4 * SU; ++q)
+        for (int q = 0; q < 4 * SUB; ++q)
             if ((hit >> q) & 1u) { wc.v[pos] = vv[q]; wc.l[pos] = (uint8_t)bq[q]; ++pos; }
         wc.cnt += tot;
         __syncwarp();
     }
-    if (base < n4) {                                     // the grid's partial chunk
-        for (int u = 0; u < SU; ++u)
+    if (base < n4) {                                      // the grid's partial chunk (CTA-uniform)
+        for (int u = 0; u < SUB; ++u)
             for (int j = 0; j < 4; ++j) {
-                const long long i = 4 * (base + (long long)t * SU + u) + j;
-                if (i >= n) continue;
-                const float v = __ldg(var + i);
-                int b, cls;
-                classify(__ldg(mean + i), v, b, cls);
-                acc.add(sc, b, cls);
-                if (b >= 0 && cls == 1) {
+                const long long i = 4 * (base + (long long)t * SUB + u) + j;
+                const bool valid = i < n;
+                const float v = valid ? __ldg(var + i) : 0.f;
+                int b;
+                bool ins;
+                classify(valid ? __ldg(mean + i) : 0.f, v, valid, b, ins);
+                if (ins) {
                     const unsigned long long pos = atomicAdd(&ctl->ncand, 1ull);
                     if ((long long)pos < cap) { cval[pos] = v; clab[pos] = (uint8_t)b; }
                 }
             }
     }
     wc.flush(cval, clab, &ctl->ncand, cap);
-    acc.flush(sc);
-    __syncthreads();
+    if (bad) s_bad = 1;
+    flush_rows();
     for (int i = t; i < NB * 3; i += blockDim.x)
         if (sc[i]) atomicAdd(&ctl->bwc[i], (unsigned long long)sc[i]);
+    if (t == 0 && s_bad) atomicExch(&ctl->wfail, 1);
 }
 
-// After the counting pass: bin counts and, when every used bin's k and k+1 are inside its
-// window and the list fits, the candidate block armed for the bins' digit passes; otherwise
-// the radix passes over the whole field (mode 1) run instead.
+// After the counting pass: the bin counts, and, when the list fits and every bin's guess held,
+// the candidate block armed for the bins' digit passes with r = k - below for each bin of
+// >= 200 voxels (noise.c:123); otherwise the radix passes over the whole field (mode 1).
+// ctl->bwc per bin: [0] keys below the window, [2] the bin's voxels.
 __global__ void __launch_bounds__(256) k_bwin_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc, long long cap) {
     fy_pdl_wait();
     __shared__ int s_ok;
@@ -1248,20 +1264,18 @@ __global__ void __launch_bounds__(256) k_bwin_arm(NoiseCtl* __restrict__ ctl, No
         return;
     }
     const int t = threadIdx.x;
-    if (t == 0) s_ok = (long long)ctl->ncand <= cap && !(noise_force_radix & 2);
+    if (t == 0) s_ok = (long long)ctl->ncand <= cap && !ctl->wfail && !(noise_force_radix & 2);
     __syncthreads();
-    long long cnt = 0, in = 0, r = 0;
+    long long cnt = 0, r = 0;
     bool on = false;
     if (t < NB) {
         const long long below = (long long)ctl->bwc[3 * t];
-        in = (long long)ctl->bwc[3 * t + 1];
-        cnt = below + in + (long long)ctl->bwc[3 * t + 2];
-        on = cnt >= 200;                                  // noise.c:123
+        cnt = (long long)ctl->bwc[3 * t + 2];
+        on = cnt >= 200;
         if (on) {
             const double idx = ctl->flat_pct / 100.0 * (double)(cnt - 1);
-            const long long k = (long long)idx;
-            r = k - below;
-            if (!(r >= 0 && r < in && (k + 1 >= cnt || r + 1 < in))) s_ok = 0;
+            r = (long long)idx - below;
+            if (r < 0) s_ok = 0;
         }
     }
     __syncthreads();
@@ -1273,13 +1287,43 @@ __global__ void __launch_bounds__(256) k_bwin_arm(NoiseCtl* __restrict__ ctl, No
         return;
     }
     for (int i = t; i < NB * 256; i += blockDim.x) cc->hist[i] = 0;
-    if (t < NT_MAX) target_init(cc, t, on ? r : 0, t < NB ? in : 0, on);
+    if (t < NT_MAX) target_init(cc, t, on ? r : 0, 0, on);
     if (t < NB) ctl->bcount[t] = (unsigned long long)cnt;
     __syncthreads();
     if (t == 0) {
         cc->n = (long long)ctl->ncand;
         cc->ntarget = NB;
         cc->mode = 1;
+    }
+}
+
+// After the candidates' first digit pass (one block per bin): the bin's inside count is the sum
+// of its histogram; k and (when it exists) k+1 must be inside, else the bins go to the radix
+// passes over the whole field.
+__global__ void __launch_bounds__(256) k_bwin_targets(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) {
+    fy_pdl_wait();
+    __shared__ unsigned long long part[256];
+    if (cc->mode != 1 || ctl->mode != kModeBinWin) return;
+    const int b = blockIdx.x;
+    if (!cc->tactive[b]) return;
+    unsigned int* h = cc->hist + (size_t)b * 256;
+    part[threadIdx.x] = h[threadIdx.x];
+    __syncthreads();
+    for (int off = 128; off > 0; off >>= 1) {
+        if (threadIdx.x < off) part[threadIdx.x] += part[threadIdx.x + off];
+        __syncthreads();
+    }
+    const long long in = (long long)part[0];
+    const long long r = cc->trank[b];
+    const long long k = r + (long long)ctl->bwc[3 * b];
+    const bool has_next = k + 1 < (long long)ctl->bcount[b];
+    if (threadIdx.x == 0) {
+        if (r < in && (!has_next || r + 1 < in)) {
+            target_init(cc, b, r, in, true);
+        } else {
+            cc->mode = 3;
+            ctl->mode = 1;
+        }
     }
 }
 
@@ -1535,7 +1579,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     if ((e = fy_smem_optin(k_win_bounds, smem_keys)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(ctl->hist, 0, sizeof(ctl->hist), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(cc->hist, 0, sizeof(cc->hist), st)) != cudaSuccess) return e;
-    PDL(k_noise_setup, 1, 1, 0, st, ctl, cc, n, flat_pct, ref_intensity);
+    PDL(k_noise_setup, 1, NT_MAX, 0, st, ctl, cc, n, flat_pct, ref_intensity);
     {   // 1. stats
         fyzb::Params sp{};
         sp.nz = nz; sp.ny = ny; sp.nx = nx;
@@ -1561,7 +1605,6 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
             sh == 24 ? -1 : (sh == 0 ? 1 : 0));
         if (sh == 24) {
             PDL(k_win_targets, 2, 256, 0, st, ctl, cc);
-            PDL(k_win_check, 1, 1, 0, st, ctl, cc);
             PDL(k_sel_scan, 2, 256, 0, st, cc, 8, 1, 0);
         }
     }
@@ -1573,7 +1616,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
         else PDL((k_sel_hist<10, 0>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
     }
     PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 0);
-    PDL(k_noise_bins_setup, 1, 1, 0, st, ctl);
+    PDL(k_noise_bins_setup, 1, NT_MAX, 0, st, ctl);
     fy_prof_mark(st, "noise.lohi");
     // 2bw. per-bin flat_pct percentile of the variance through the bins' window: sample,
     // bounds, one counting pass over mean and variance, then four digit passes over the
@@ -1589,9 +1632,16 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
         PDL(k_bwin_bounds, NB, kBoundThreads, smem_keys, st, skey, slab, ctl, m2);
         PDL(k_bwin_count, g, 256, 0, st, mean, var, ctl, cval, clab, L.cap);
         PDL(k_bwin_arm, 1, 256, 0, st, ctl, cc, L.cap);
-        for (int sh = 24; sh >= 0; sh -= 8)
+        for (int sh = 24; sh >= 0; sh -= 8) {
+            // the first digit's histogram gives the inside counts (k_bwin_targets) before its
+            // scan; the later digits' scans run in each pass's last CTA
             PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL,
-                sh == 0 ? 1 : 0);
+                sh == 24 ? -1 : (sh == 0 ? 1 : 0));
+            if (sh == 24) {
+                PDL(k_bwin_targets, NB, 256, 0, st, ctl, cc);
+                PDL(k_sel_scan, NB, 256, 0, st, cc, 8, 1, 0);
+            }
+        }
         PDL(k_sel_next, gcl, 256, 0, st, nullptr, cval, clab, cc, 1);
         PDL(k_bwin_finish, 1, 32, 0, st, ctl, cc);
     }
