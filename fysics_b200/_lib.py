@@ -89,6 +89,12 @@ class Request(C.Structure):
                 ("f32_min", C.c_double), ("f32_max", C.c_double), ("phys", Physics), ("cfg", RestoreCfg)]
 
 
+class BatchCube(C.Structure):
+    """fy_batch_cube (include/fysics_b200.h)."""
+    _fields_ = [("u8", C.c_void_p), ("out", C.c_void_p), ("nz", C.c_int), ("ny", C.c_int), ("nx", C.c_int),
+                ("f32_min", C.c_double), ("f32_max", C.c_double), ("phys", Physics)]
+
+
 class RequestResult(C.Structure):
     """fy_request_result (include/fysics_b200.h)."""
     _fields_ = [("status", C.c_int), ("queue_ms", C.c_double), ("run_ms", C.c_double), ("latency_ms", C.c_double),
@@ -234,6 +240,7 @@ SIGNATURES = {
     "fy_gpu_phase_correlate_scratch_bytes": (_sz, [_i, _i, _i]),
     "fy_restore_cfg_default": (None, [C.c_void_p]),
     "fy_gpu_restore_u8": (_i, [_P, _P, _i, _i, _i, _d, _d, _PP, C.c_void_p, _P]),
+    "fy_gpu_restore_u8_batch": (_i, [C.POINTER(BatchCube), _i, C.c_void_p, _P]),
     "fy_gpu_profile_start": (_i, [_i, _P]),
     "fy_gpu_profile_stop": (_i, []),
     "fy_gpu_profile_read": (_i, [_i, C.POINTER(C.c_char_p), C.POINTER(C.c_float)]),

@@ -188,8 +188,51 @@ struct DeconvKey {
     fy_physics p;
 };
 
-// Plan-time tables of deconv_radial (paganin.c:213-230): fz2/fy2/fx2 in double and the
-// 4097-entry float LUT of the capped weight over u = f^2, uploaded once per parameter set.
+}  // namespace
+
+// Plan-time tables of deconv_radial (paganin.c:213-230) into host memory of
+// fy_deconv_table_bytes(g) bytes: the 4097-entry float LUT of the capped weight over u = f^2
+// (padded to 16 bytes), then fz2, fy2 and fx2 in double. Returns the LUT index scale us.
+size_t fy_deconv_table_bytes(const SpecGeom& g) {
+    const size_t lut_bytes = ((FY_LUT_N + 1) * sizeof(float) + 15) & ~(size_t)15;
+    return lut_bytes + sizeof(double) * ((size_t)g.pz + g.py + g.hx);
+}
+double fy_deconv_fill_tables(const SpecGeom& g, const fy_physics* p, double param, int kind, double fz2s,
+                             void* host) {
+    const size_t lut_bytes = ((FY_LUT_N + 1) * sizeof(float) + 15) & ~(size_t)15;
+    unsigned char* h = (unsigned char*)host;
+    float* lut = (float*)h;
+    double* fz2 = (double*)(h + lut_bytes);
+    double* fy2 = fz2 + g.pz;
+    double* fx2 = fy2 + g.py;
+    double mz = 0, my = 0, mx = 0;
+    for (int i = 0; i < g.pz; i++) {
+        const double f = (i <= g.pz / 2) ? (double)i / g.pz : (double)(i - g.pz) / g.pz;
+        fz2[i] = f * f * fz2s; if (fz2[i] > mz) mz = fz2[i];
+    }
+    for (int i = 0; i < g.py; i++) {
+        const double f = (i <= g.py / 2) ? (double)i / g.py : (double)(i - g.py) / g.py;
+        fy2[i] = f * f; if (fy2[i] > my) my = fy2[i];
+    }
+    for (int i = 0; i < g.hx; i++) {
+        const double f = (double)i / g.px;
+        fx2[i] = f * f; if (fx2[i] > mx) mx = fx2[i];
+    }
+    const double umax = mz + my + mx;
+    // A 1x1x1 volume has umax = 0; every sample then sits at u = 0 (us = 0 -> t = 0).
+    const double us = umax > 0 ? FY_LUT_N / umax : 0.0;
+    const double cap = kind == 1 ? 0.0 : FY_MAX_DECONV_GAIN;
+    for (int i = 0; i <= FY_LUT_N; i++) {
+        const double fr = us > 0 ? sqrt((double)i / us) : 0.0;
+        double w = kind == 1 ? matched_w(fr, p, param) : wiener_w(fr, p, param);
+        if (cap > 0 && w > cap) w = cap;
+        lut[i] = (float)w;
+    }
+    return us;
+}
+
+namespace {
+// The same tables, cached per thread and uploaded once per parameter set.
 int deconv_tables(const SpecGeom& g, const fy_physics* p, double param, int kind, double fz2s,
                   cudaStream_t st, DeconvLaunch& d) {
     fy::ThreadCtx& c = ctx();
@@ -198,36 +241,10 @@ int deconv_tables(const SpecGeom& g, const fy_physics* p, double param, int kind
     key.nz = g.nz; key.ny = g.ny; key.nx = g.nx; key.kind = kind;
     key.param = param; key.fz2s = fz2s; key.p = *p;
     const size_t lut_bytes = ((FY_LUT_N + 1) * sizeof(float) + 15) & ~(size_t)15;
-    const size_t bytes = lut_bytes + sizeof(double) * ((size_t)g.pz + g.py + g.hx);
+    const size_t bytes = fy_deconv_table_bytes(g);
     if (!(c.tab.valid && c.tab.keylen == sizeof key && !memcmp(c.tab.key, &key, sizeof key))) {
         std::vector<unsigned char> h(bytes);
-        float* lut = (float*)h.data();
-        double* fz2 = (double*)(h.data() + lut_bytes);
-        double* fy2 = fz2 + g.pz;
-        double* fx2 = fy2 + g.py;
-        double mz = 0, my = 0, mx = 0;
-        for (int i = 0; i < g.pz; i++) {
-            const double f = (i <= g.pz / 2) ? (double)i / g.pz : (double)(i - g.pz) / g.pz;
-            fz2[i] = f * f * fz2s; if (fz2[i] > mz) mz = fz2[i];
-        }
-        for (int i = 0; i < g.py; i++) {
-            const double f = (i <= g.py / 2) ? (double)i / g.py : (double)(i - g.py) / g.py;
-            fy2[i] = f * f; if (fy2[i] > my) my = fy2[i];
-        }
-        for (int i = 0; i < g.hx; i++) {
-            const double f = (double)i / g.px;
-            fx2[i] = f * f; if (fx2[i] > mx) mx = fx2[i];
-        }
-        const double umax = mz + my + mx;
-        // A 1x1x1 volume has umax = 0; every sample then sits at u = 0 (us = 0 -> t = 0).
-        const double us = umax > 0 ? FY_LUT_N / umax : 0.0;
-        const double cap = kind == 1 ? 0.0 : FY_MAX_DECONV_GAIN;
-        for (int i = 0; i <= FY_LUT_N; i++) {
-            const double fr = us > 0 ? sqrt((double)i / us) : 0.0;
-            double w = kind == 1 ? matched_w(fr, p, param) : wiener_w(fr, p, param);
-            if (cap > 0 && w > cap) w = cap;
-            lut[i] = (float)w;
-        }
+        const double us = fy_deconv_fill_tables(g, p, param, kind, fz2s, h.data());
         cudaError_t e = c.tab.buf.ensure(bytes);
         if (e != cudaSuccess) return fail_cuda(e, "deconv tables");
         // Stage through pinned memory so the upload is an ordinary asynchronous copy (a
@@ -334,6 +351,21 @@ int host_deconv(const float* in, float* out, int nz, int ny, int nx, const fy_ph
     return FY_OK;
 }
 }  // namespace
+
+// Everything of a deconvolution launch but its buffers (spectrum, tables, source, output): the
+// geometry, the kind's defaults (param and fz2 scale, as fy_deconvolve* resolve them), the
+// plans, the twiddle tables and the dewindow scalars.
+int fy_deconv_setup(int nz, int ny, int nx, const fy_physics* p, double& param, int kind, double& fz2s,
+                    double fmin, double fmax, DeconvLaunch& d, const char* what) {
+    int rc = make_geom(nz, ny, nx, d.g, what);
+    if (rc) return rc;
+    deconv_defaults(p, kind, param, fz2s);
+    d.plx = fy_make_plan(d.g.px); d.ply = fy_make_plan(d.g.py); d.plz = fy_make_plan(d.g.pz);
+    d.twx = fy::twiddles(d.g.px); d.twy = fy::twiddles(d.g.py); d.twz = fy::twiddles(d.g.pz);
+    if (!d.twx || !d.twy || !d.twz) return fail(FY_ENOMEM, "%s: twiddle tables", what);
+    dewindow_params(fmin, fmax, d.lo, d.scale);
+    return FY_OK;
+}
 
 // Size the calling thread's deconvolution workspaces (half spectrum, tables) for a cube shape,
 // so later calls up to that shape allocate nothing.

@@ -70,6 +70,13 @@ static int init_device(int device) {
         if (c.side) { cudaStreamDestroy(c.side); c.side = nullptr; }
         if (c.fork_ev) { cudaEventDestroy(c.fork_ev); c.fork_ev = nullptr; }
         if (c.join_ev) { cudaEventDestroy(c.join_ev); c.join_ev = nullptr; }
+        for (int i = 0; i < ThreadCtx::kBatchStreams; ++i) {
+            if (c.bst[i]) { cudaStreamDestroy(c.bst[i]); c.bst[i] = nullptr; }
+            if (c.bev[i]) { cudaEventDestroy(c.bev[i]); c.bev[i] = nullptr; }
+        }
+        if (c.bfork) { cudaEventDestroy(c.bfork); c.bfork = nullptr; }
+        if (c.batch_done) { cudaEventDestroy(c.batch_done); c.batch_done = nullptr; }
+        c.batch_pending = false;
     }
     c.dev = device;
     cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, device);
@@ -101,6 +108,22 @@ int ensure_side() {
     if (!c.fork_ev && (e = cudaEventCreateWithFlags(&c.fork_ev, cudaEventDisableTiming)) != cudaSuccess)
         return fail_cuda(e, "cudaEventCreate");
     if (!c.join_ev && (e = cudaEventCreateWithFlags(&c.join_ev, cudaEventDisableTiming)) != cudaSuccess)
+        return fail_cuda(e, "cudaEventCreate");
+    return FY_OK;
+}
+
+int ensure_batch_streams() {
+    ThreadCtx& c = t_ctx;
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < ThreadCtx::kBatchStreams; ++i) {
+        if (!c.bst[i] && (e = cudaStreamCreateWithFlags(&c.bst[i], cudaStreamNonBlocking)) != cudaSuccess)
+            return fail_cuda(e, "cudaStreamCreate");
+        if (!c.bev[i] && (e = cudaEventCreateWithFlags(&c.bev[i], cudaEventDisableTiming)) != cudaSuccess)
+            return fail_cuda(e, "cudaEventCreate");
+    }
+    if (!c.bfork && (e = cudaEventCreateWithFlags(&c.bfork, cudaEventDisableTiming)) != cudaSuccess)
+        return fail_cuda(e, "cudaEventCreate");
+    if (!c.batch_done && (e = cudaEventCreateWithFlags(&c.batch_done, cudaEventDisableTiming)) != cudaSuccess)
         return fail_cuda(e, "cudaEventCreate");
     return FY_OK;
 }
@@ -220,8 +243,8 @@ int fy_gpu_last_status(void) { return fy::ctx().status; }
 const char* fy_gpu_last_error(void) { return fy::ctx().err.c_str(); }
 unsigned long long fy_gpu_kernel_launches(void) { return fy::ctx().launches; }
 int fy_gpu_kernel_timeouts(void) {
-    const int a = fy_guided_wait_timeouts(), b = fy_noise_wait_timeouts();
-    return a < 0 || b < 0 ? -1 : a + b;
+    const int a = fy_guided_wait_timeouts(), b = fy_noise_wait_timeouts(), d = fy_batch_wait_timeouts();
+    return a < 0 || b < 0 || d < 0 ? -1 : a + b + d;
 }
 int fy_gpu_test_box_first_wait(int polls) {
     fy::enter();
@@ -229,6 +252,7 @@ int fy_gpu_test_box_first_wait(int polls) {
     if (rc) return rc;
     cudaError_t e = fy_guided_set_first_wait_polls(polls);
     if (e == cudaSuccess) e = fy_noise_set_first_wait_polls(polls);
+    if (e == cudaSuccess) e = fy_batch_set_first_wait_polls(polls);
     return e == cudaSuccess ? FY_OK : fy::fail_cuda(e, "fy_gpu_test_box_first_wait");
 }
 int fy_gpu_test_noise_paths(int force_radix, int* window_used) {
@@ -250,5 +274,12 @@ void fy_gpu_release(void) {
     c.tab_pin.release();
     if (c.tab_done) { cudaEventDestroy(c.tab_done); c.tab_done = nullptr; }
     c.tab_pending = false;
+    if (c.batch_pending && c.batch_done) cudaEventSynchronize(c.batch_done);
+    c.batch_pending = false;
+    c.batch.release(); c.batch_up.release(); c.batch_pin.release();
+    for (int i = 0; i < fy::ThreadCtx::kBatchStreams; ++i) {
+        if (c.bst[i]) cudaStreamSynchronize(c.bst[i]);
+        c.bspec[i].release();
+    }
 }
 }

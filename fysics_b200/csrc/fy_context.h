@@ -51,6 +51,18 @@ struct ThreadCtx {
     HostBuf tab_pin;                   // pinned staging of the table upload (asynchronous copy)
     cudaEvent_t tab_done = nullptr;    // the last upload from tab_pin has been read
     bool tab_pending = false;
+    // batches of volumes (fy_batch.cu): the per-volume buffers, the uploaded plan (tables,
+    // box-pass jobs, selection arguments) with its pinned staging and the event after its
+    // copy, and kBatchStreams streams with a half-spectrum workspace each
+    static constexpr int kBatchStreams = 8;
+    DevBuf batch, batch_up;
+    HostBuf batch_pin;
+    cudaEvent_t batch_done = nullptr;
+    bool batch_pending = false;
+    cudaStream_t bst[kBatchStreams] = {};
+    cudaEvent_t bev[kBatchStreams] = {};
+    cudaEvent_t bfork = nullptr;
+    DevBuf bspec[kBatchStreams];
 };
 
 ThreadCtx& ctx();
@@ -62,6 +74,8 @@ int fail(int code, const char* fmt, ...);
 int fail_cuda(cudaError_t e, const char* what);
 // The thread's side stream and its fork/join events, created on first use.
 int ensure_side();
+// The thread's batch streams and events, created on first use.
+int ensure_batch_streams();
 // Make `s` wait for the previous user of this thread's workspaces; call before reuse.
 void ws_acquire(cudaStream_t s);
 // Mark the workspaces as used by work enqueued on `s`.

@@ -30,6 +30,12 @@ cudaError_t fy_deconv_pass_ct_a(int pass, int n, const DeconvLaunch& d, cudaStre
 cudaError_t fy_deconv_pass_ct_b(int pass, int n, const DeconvLaunch& d, cudaStream_t st);
 cudaError_t fy_deconv_pass_ct_c(int pass, int n, const DeconvLaunch& d, cudaStream_t st);
 size_t fy_deconv_spec_elems(const SpecGeom& g);
+// Host side of a deconvolution (fy_api.cu): the plan-time tables into host memory (returns the
+// LUT index scale), their size, and the launch fields other than its buffers.
+size_t fy_deconv_table_bytes(const SpecGeom& g);
+double fy_deconv_fill_tables(const SpecGeom& g, const fy_physics* p, double param, int kind, double fz2s, void* host);
+int fy_deconv_setup(int nz, int ny, int nx, const fy_physics* p, double& param, int kind, double& fz2s,
+                    double fmin, double fmax, DeconvLaunch& d, const char* what);
 cudaError_t fy_launch_spec_y(float2* spec, const SpecGeom& g, const FftPlan& ply, const float2* twy, int nplanes,
                              int sign, int keep_rows, cudaStream_t st);
 cudaError_t fy_launch_cfft3d(float2* c, int nz, int ny, int nx, int nxp, int sign, cudaStream_t st);
@@ -211,6 +217,8 @@ int fy_restore_reserve(int nz, int ny, int nx);
 // Free the calling thread's per-tile chain workspaces (fy_tile.cu); part of fy_gpu_release.
 void fy_tile_release();
 int fy_guided_wait_timeouts();
+int fy_batch_wait_timeouts();
+cudaError_t fy_batch_set_first_wait_polls(int polls);
 int fy_noise_wait_timeouts();
 cudaError_t fy_guided_set_first_wait_polls(int polls);
 cudaError_t fy_noise_set_first_wait_polls(int polls);

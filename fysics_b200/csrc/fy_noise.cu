@@ -17,6 +17,9 @@
 //      noise_ref = sqrt(max(g*ref + b, ..))*1.15 (noise.c:181-187), plus the guided eps
 //      (3*noise_ref)^2 floored at 1e-8 (noise.c:197-202).
 // The launch sequence is fixed (no host decisions), so a chain can keep it on one stream.
+#include <cuda/std/tuple>
+#include <vector>
+
 #include "fy_internal.h"
 #include "fysics_b200.h"
 #include "fy_zbox.cuh"
@@ -78,7 +81,7 @@ struct NoiseCtl {
     double out_g, out_b, out_noise_ref, out_ref_intensity;
     int out_used;
     float eps;                         // fy_guided_eps_for_noise(noise_ref), for a chained guided filter
-    unsigned int hist[NT_MAX * 256];   // per-target histogram (bins: 24 x 256; whole: 2 x 2048)
+    alignas(16) unsigned int hist[NT_MAX * 256];   // per-target histogram (bins: 24 x 256; whole: 2 x 2048)
     // Sample-guided window (section 2w): per target the window keys [wlo, whi] and the count
     // of keys below wlo.
     uint32_t wlo[2], whi[2];
@@ -239,7 +242,7 @@ FY_D void warp_scan_target(NoiseCtl* ctl, int t, int db, bool last) {
     }
 }
 template <int DB, int MODE, bool LABEL = false, bool COMPACT = false>
-__global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean, const float* __restrict__ var,
+FY_D void k_sel_hist(const float* __restrict__ mean, const float* __restrict__ var,
                                                   uint8_t* __restrict__ bin, NoiseCtl* __restrict__ ctl,
                                                   int shift, float* __restrict__ cval = nullptr,
                                                   uint8_t* __restrict__ clab = nullptr, long long cap = 0,
@@ -398,7 +401,7 @@ __global__ void __launch_bounds__(256) k_sel_hist(const float* __restrict__ mean
 // scan of the histogram, extends its prefix, records how many keys share the final key.
 // After the last digit, the next non-empty bucket of that digit is the smallest key above
 // the selected one within the prefix; k_sel_next scans only when there is none.
-__global__ void __launch_bounds__(256) k_sel_scan(NoiseCtl* __restrict__ ctl, int db, int want_mode, int last) {
+FY_D void k_sel_scan(NoiseCtl* __restrict__ ctl, int db, int want_mode, int last) {
     fy_pdl_wait();
     __shared__ unsigned long long part[256];
     __shared__ int s_sel;
@@ -451,7 +454,7 @@ __global__ void __launch_bounds__(256) k_sel_scan(NoiseCtl* __restrict__ ctl, in
 
 // Smallest key greater than the selected key, for targets whose k+1 lies past it and whose
 // last digit histogram held no larger key (k_sel_scan resolves every other target).
-__global__ void __launch_bounds__(256) k_sel_next(const float* __restrict__ mean, const float* __restrict__ var,
+FY_D void k_sel_next(const float* __restrict__ mean, const float* __restrict__ var,
                                                   const uint8_t* __restrict__ bin, NoiseCtl* __restrict__ ctl,
                                                   int want_mode) {
     fy_pdl_wait();
@@ -535,11 +538,17 @@ FY_D void target_init(NoiseCtl* ctl, int t, long long k, long long group_n, bool
     ctl->tnext[t] = 0xffffffffu;
 }
 
-// One block of NT_MAX threads: thread t initialises target t.
-__global__ void __launch_bounds__(NT_MAX) k_noise_setup(NoiseCtl* ctl, NoiseCtl* cc, long long n, double flat_pct,
-                                                       double ref_intensity) {
+// One block of 256 threads: thread t < NT_MAX initialises target t; all clear both blocks'
+// histograms.
+FY_D void k_noise_setup(NoiseCtl* ctl, NoiseCtl* cc, long long n, double flat_pct, double ref_intensity) {
     fy_pdl_wait();
     const int t = threadIdx.x;
+    static_assert(sizeof(ctl->hist) % 16 == 0 && offsetof(NoiseCtl, hist) % 16 == 0, "uint4 clears");
+    for (int i = t; i < (int)(sizeof(ctl->hist) / 16); i += blockDim.x) {
+        reinterpret_cast<uint4*>(ctl->hist)[i] = make_uint4(0u, 0u, 0u, 0u);
+        reinterpret_cast<uint4*>(cc->hist)[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    if (t >= NT_MAX) return;
     const double i1 = 1.0 / 100.0 * (double)(n - 1), i99 = 99.0 / 100.0 * (double)(n - 1);
     if (t == 0) target_init(ctl, 0, (long long)i1, n, true);           // 1st percentile of the means
     else if (t == 1) target_init(ctl, 1, (long long)i99, n, true);     // 99th
@@ -557,7 +566,7 @@ __global__ void __launch_bounds__(NT_MAX) k_noise_setup(NoiseCtl* ctl, NoiseCtl*
 }
 
 // lo/hi from the selected means; bin edges (noise.c:106-119). One block of NT_MAX threads.
-__global__ void __launch_bounds__(NT_MAX) k_noise_bins_setup(NoiseCtl* ctl) {
+FY_D void k_noise_bins_setup(NoiseCtl* ctl) {
     fy_pdl_wait();
     __shared__ double s_lo, s_hi;
     const int t = threadIdx.x;
@@ -600,7 +609,7 @@ __global__ void __launch_bounds__(NT_MAX) k_noise_bins_setup(NoiseCtl* ctl) {
 // After the first variance digit pass (one block per bin): the bin's count is the sum of its
 // histogram; targets of the flat_pct percentile for bins with >= 200 voxels (noise.c:123).
 // Bins below that drop out and their histogram is cleared.
-__global__ void __launch_bounds__(256) k_bin_targets(NoiseCtl* ctl) {
+FY_D void k_bin_targets(NoiseCtl* ctl) {
     fy_pdl_wait();
     __shared__ unsigned long long part[256];
     if (ctl->mode != 1) return;
@@ -710,7 +719,7 @@ FY_D uint32_t block_select(const uint32_t* keys, int c, long long rank, unsigned
     return prefix;
 }
 
-__global__ void __launch_bounds__(256) k_win_sample(const float* __restrict__ mean, const NoiseCtl* __restrict__ ctl,
+FY_D void k_win_sample(const float* __restrict__ mean, const NoiseCtl* __restrict__ ctl,
                                                     float* __restrict__ sm, long long m, unsigned long long A,
                                                     unsigned long long B) {
     fy_pdl_wait();
@@ -723,7 +732,7 @@ __global__ void __launch_bounds__(256) k_win_sample(const float* __restrict__ me
 // One CTA (kBoundThreads threads) per target (blockIdx.x 0/1: 1st/99th percentile) and window
 // end (blockIdx.y 0: wlo, 1: whi). Dynamic shared memory: kSampleMax keys, then the warps'
 // digit histograms (kBoundThreads/32 x 256 counters).
-__global__ void __launch_bounds__(kBoundThreads) k_win_bounds(const float* __restrict__ sm,
+FY_D void k_win_bounds(const float* __restrict__ sm,
                                                               NoiseCtl* __restrict__ ctl, long long m) {
     fy_pdl_wait();
     extern __shared__ uint32_t wkeys[];
@@ -779,7 +788,7 @@ __global__ void __launch_bounds__(kBoundThreads) k_win_bounds(const float* __res
 // 4*SU keys' window hits in two bit masks; one warp scan of the hit counts places them in the
 // warp's shared-memory buffer, which is appended to the list (one atomic) when nearly full.
 constexpr int kCountBuf = 1152;          // >= one step's worst case (32 lanes x 4*SU keys x 2); 45 KB static smem
-__global__ void __launch_bounds__(256) k_win_count(const float* __restrict__ mean, NoiseCtl* __restrict__ ctl,
+FY_D void k_win_count(const float* __restrict__ mean, NoiseCtl* __restrict__ ctl,
                                                    float* __restrict__ cval, uint8_t* __restrict__ clab,
                                                    long long cap) {
     fy_pdl_wait();
@@ -862,7 +871,7 @@ __global__ void __launch_bounds__(256) k_win_count(const float* __restrict__ mea
 // After the counting pass (one thread): arms the candidate block for its first digit pass
 // (both targets active with the empty prefix, like the bin selection's labelling pass), or,
 // when the candidate list overflowed, sends the selection to the radix passes.
-__global__ void k_win_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc, long long cap) {
+FY_D void k_win_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc, long long cap) {
     fy_pdl_wait();
     if (ctl->mode != kModeWin0) { cc->mode = 3; return; }
     for (int t = 0; t < NT_MAX; ++t) target_init(cc, t, 0, 0, t < 2);
@@ -883,7 +892,7 @@ __global__ void k_win_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc,
 // leave k and (when it exists) k+1 inside. Otherwise the window failed: the candidate passes
 // stand aside (cc mode 3) and the radix passes over the whole field run (mode 0). A block
 // that finds cc already failed leaves its histogram, which every later user clears first.
-__global__ void __launch_bounds__(256) k_win_targets(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) {
+FY_D void k_win_targets(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) {
     fy_pdl_wait();
     __shared__ unsigned long long part[256];
     if (cc->mode != 1) return;
@@ -914,14 +923,14 @@ __global__ void __launch_bounds__(256) k_win_targets(NoiseCtl* __restrict__ ctl,
 }
 
 // The bins' candidate list (section 2b). Reset before the compacting pass.
-__global__ void k_bin_cand_reset(NoiseCtl* __restrict__ ctl) {
+FY_D void k_bin_cand_reset(NoiseCtl* __restrict__ ctl) {
     fy_pdl_wait();
     if (ctl->mode == 1) ctl->ncand = 0;
 }
 // After the compacting pass and its scan: when the list fits, the bins' targets move to the
 // candidate block for the last digit and the whole-field pass stands aside; otherwise the
 // candidate pass stands aside.
-__global__ void __launch_bounds__(256) k_bin_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc, long long cap) {
+FY_D void k_bin_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc, long long cap) {
     fy_pdl_wait();
     __shared__ int s_go;
     if (threadIdx.x == 0) s_go = ctl->mode == 1 && (long long)ctl->ncand <= cap;
@@ -950,7 +959,7 @@ __global__ void __launch_bounds__(256) k_bin_arm(NoiseCtl* __restrict__ ctl, Noi
     }
 }
 // After the candidates' last digit: the selected keys back into the main block.
-__global__ void k_bin_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restrict__ cc) {
+FY_D void k_bin_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restrict__ cc) {
     fy_pdl_wait();
     if (ctl->mode != kModeBinCand) return;
     for (int t = 0; t < NT_MAX; ++t) {
@@ -965,7 +974,7 @@ __global__ void k_bin_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restr
 
 // Keys of order statistics k and k+1 into the main block's targets 0/1 (interp / next_value
 // form); the radix passes of mode 0 then stand aside.
-__global__ void k_win_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restrict__ cc) {
+FY_D void k_win_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restrict__ cc) {
     fy_pdl_wait();
     if (ctl->mode != kModeWin0) return;
     for (int t = 0; t < 2; ++t) {
@@ -999,7 +1008,7 @@ __global__ void k_win_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restr
 constexpr int kBinSampleMax = 65536;
 constexpr int kBinKeysMax = 4096;      // per bin: enough for a window of ~5% of a large bin
 
-__global__ void __launch_bounds__(256) k_bwin_sample(const float* __restrict__ mean, const float* __restrict__ var,
+FY_D void k_bwin_sample(const float* __restrict__ mean, const float* __restrict__ var,
                                                      const NoiseCtl* __restrict__ ctl, uint32_t* __restrict__ skey,
                                                      uint8_t* __restrict__ slab, long long m, unsigned long long A,
                                                      unsigned long long B) {
@@ -1024,7 +1033,7 @@ __global__ void __launch_bounds__(256) k_bwin_sample(const float* __restrict__ m
 // read 16 bytes at a time, the next step's while the current one is placed) and compacts its
 // bin's keys in sample order into its own kBinKeysMax/NW slots, with no block barrier; one
 // block pass then concatenates the warps' keys (a deterministic subset in sample order).
-__global__ void __launch_bounds__(kBoundThreads) k_bwin_bounds(const uint32_t* __restrict__ skey,
+FY_D void k_bwin_bounds(const uint32_t* __restrict__ skey,
                                                                const uint8_t* __restrict__ slab,
                                                                NoiseCtl* __restrict__ ctl, long long m) {
     fy_pdl_wait();
@@ -1122,7 +1131,7 @@ __global__ void __launch_bounds__(kBoundThreads) k_bwin_bounds(const uint32_t* _
 // inside counts come from the candidates' first digit histogram (k_bwin_targets).
 constexpr int kBCountBuf = 512;          // per warp: two steps' worst case (32 x 8 each)
 constexpr int kLaneRow = 25;             // counter words per lane (NB = 24, odd stride)
-__global__ void __launch_bounds__(256, 4) k_bwin_count(const float* __restrict__ mean, const float* __restrict__ var,
+FY_D void k_bwin_count(const float* __restrict__ mean, const float* __restrict__ var,
                                                        NoiseCtl* __restrict__ ctl, float* __restrict__ cval,
                                                        uint8_t* __restrict__ clab, long long cap) {
     fy_pdl_wait();
@@ -1256,7 +1265,7 @@ __global__ void __launch_bounds__(256, 4) k_bwin_count(const float* __restrict__
 // the candidate block armed for the bins' digit passes with r = k - below for each bin of
 // >= 200 voxels (noise.c:123); otherwise the radix passes over the whole field (mode 1).
 // ctl->bwc per bin: [0] keys below the window, [2] the bin's voxels.
-__global__ void __launch_bounds__(256) k_bwin_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc, long long cap) {
+FY_D void k_bwin_arm(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc, long long cap) {
     fy_pdl_wait();
     __shared__ int s_ok;
     if (ctl->mode != kModeBinWin) {
@@ -1300,7 +1309,7 @@ __global__ void __launch_bounds__(256) k_bwin_arm(NoiseCtl* __restrict__ ctl, No
 // After the candidates' first digit pass (one block per bin): the bin's inside count is the sum
 // of its histogram; k and (when it exists) k+1 must be inside, else the bins go to the radix
 // passes over the whole field.
-__global__ void __launch_bounds__(256) k_bwin_targets(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) {
+FY_D void k_bwin_targets(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) {
     fy_pdl_wait();
     __shared__ unsigned long long part[256];
     if (cc->mode != 1 || ctl->mode != kModeBinWin) return;
@@ -1328,7 +1337,7 @@ __global__ void __launch_bounds__(256) k_bwin_targets(NoiseCtl* __restrict__ ctl
 }
 
 // The bins' selected keys (k and k+1, in the form interp() reads) into the main block.
-__global__ void k_bwin_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restrict__ cc) {
+FY_D void k_bwin_finish(NoiseCtl* __restrict__ ctl, const NoiseCtl* __restrict__ cc) {
     fy_pdl_wait();
     if (ctl->mode != kModeBinWin) return;
     const int t = threadIdx.x;
@@ -1367,7 +1376,7 @@ FY_D double pct_small(double* v, int n, double pct) {       // percentile() on <
 // stage 1: IRLS fit (FP64) and outputs.
 // One warp: lane b handles bin b's reads, so the bins' loads are in flight together; the
 // sequential fit then runs on lane 0 from shared memory.
-__global__ void __launch_bounds__(32) k_noise_fit(NoiseCtl* ctl, int stage) {
+FY_D void k_noise_fit(NoiseCtl* ctl, int stage) {
     fy_pdl_wait();
     static_assert(NB <= 32, "one lane per bin");
     const int lane = threadIdx.x;
@@ -1536,34 +1545,93 @@ unsigned long long weyl_step(unsigned long long n) {
 
 size_t fy_noise_scratch_floats(size_t n) { return noise_layout(n).total; }
 
-// Enqueue the whole estimate. scratch: fy_noise_scratch_floats(n) floats; ctl:
-// fy_noise_ctl_bytes(). Supports win in {3..9} (r = win/2 <= 4). guided_mv (optional,
-// 2n floats): the statistics pass also writes the guided filter's (mean, var) pairs of the
-// same window, for fy_launch_guided_apply_mv with r = win/2.
-// Every selection kernel runs as a programmatic dependent launch; the first failed launch
-// is returned. PDL counts the launches into `launches`.
-#define PDL(k, ...)                                                            \
+namespace {
+
+// ---------------------------------------------------------------- launching: one cube or a batch
+// Every selection step above is a __device__ body run by one of two wrappers: k_one, one volume,
+// the body's arguments as kernel parameters; k_many, a batch of volumes, blockIdx.z = volume
+// and each volume's arguments read from a device array. NoiseLaunch either launches k_one at
+// once or, in batch mode, records each volume's arguments for every step of the sequence (the
+// same sequence for every volume) and then replays it: one launch per step for all volumes,
+// with the largest grid any volume asked for (the bodies' loops are grid-stride, and the grids
+// that index targets or bins are the same for every volume).
+template <int NTB, int MINB, auto F, class... P>
+__global__ void __launch_bounds__(NTB, MINB) k_one(P... a) { F(a...); }
+template <int NTB, int MINB, auto F, class... P>
+__global__ void __launch_bounds__(NTB, MINB) k_many(const cuda::std::tuple<P...>* __restrict__ packs) {
+    cuda::std::apply([](auto... x) { F(x...); }, packs[blockIdx.z]);
+}
+
+struct NoiseLaunch {
+    cudaStream_t st = nullptr;
+    bool record = false;
+    struct Step {
+        const void* kern;                  // the k_many instance
+        dim3 grid, block;
+        size_t smem, pack;                 // bytes of one volume's arguments
+        std::vector<unsigned char> packs;
+    };
+    std::vector<Step> steps;
+    size_t si = 0;                         // the next step of the volume being recorded
+    int cubes = 0;
+
+    template <int NTB, int MINB, auto F, class... P, class... A>
+    cudaError_t run_sig(void (*)(P...), dim3 grid, dim3 block, size_t smem, A... a) {
+        if (!record) {
+            auto k = k_one<NTB, MINB, F, P...>;
+            cudaError_t e = fy_smem_optin(k, smem);
+            if (e != cudaSuccess) return e;
+            return fy_launch_pdl(k, grid, block, smem, st, (P)a...);
+        }
+        using T = cuda::std::tuple<P...>;
+        const void* k = (const void*)k_many<NTB, MINB, F, P...>;
+        if (si == steps.size()) {
+            if (cubes > 0) return cudaErrorInvalidValue;          // every volume has the same sequence
+            cudaError_t e = fy_smem_optin(k_many<NTB, MINB, F, P...>, smem);
+            if (e != cudaSuccess) return e;
+            steps.push_back(Step{k, grid, block, smem, sizeof(T), {}});
+        }
+        Step& s = steps[si++];
+        if (s.kern != k || s.block.x != block.x || s.smem != smem) return cudaErrorInvalidValue;
+        s.grid.x = s.grid.x > grid.x ? s.grid.x : grid.x;
+        s.grid.y = s.grid.y > grid.y ? s.grid.y : grid.y;
+        const T t((P)a...);
+        const unsigned char* b = reinterpret_cast<const unsigned char*>(&t);
+        s.packs.insert(s.packs.end(), b, b + sizeof(T));
+        return cudaSuccess;
+    }
+    template <int NTB, int MINB, auto F, class... A>
+    cudaError_t run(dim3 grid, dim3 block, size_t smem, A... a) {
+        return run_sig<NTB, MINB, F>(F, grid, block, smem, a...);
+    }
+};
+
+#define RUN(NTB, MINB, F, ...)                                                 \
     do {                                                                       \
-        const cudaError_t pe_ = fy_launch_pdl(k, __VA_ARGS__);                 \
+        const cudaError_t pe_ = L.run<NTB, MINB, F>(__VA_ARGS__);              \
         if (pe_ != cudaSuccess) return pe_;                                    \
         ++launches;                                                            \
     } while (0)
-cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, int win, double flat_pct,
-                                     double ref_intensity, float* scratch, void* ctl_mem, int sms,
-                                     cudaStream_t st, int& launches, float* guided_mv) {
+
+// The estimate's launch sequence for one volume through L. stats: run the statistics pass here
+// (a batch runs it for all volumes at once before the sequence).
+cudaError_t noise_sequence(NoiseLaunch& L, const float* in, int nz, int ny, int nx, int win, double flat_pct,
+                           double ref_intensity, float* scratch, void* ctl_mem, int sms, int& launches,
+                           float* guided_mv, bool stats) {
+    cudaStream_t st = L.st;
     NoiseCtl* ctl = (NoiseCtl*)ctl_mem;
     const long long n = (long long)nz * ny * nx;
-    const NoiseLayout L = noise_layout((size_t)n);
-    float* mean = scratch + L.mean;
-    float* var = scratch + L.var;
-    uint8_t* bin = (uint8_t*)(scratch + L.bin);
-    NoiseCtl* cc = (NoiseCtl*)(scratch + L.cc);
-    float* sm = scratch + L.samp;
-    float* cval = scratch + L.cval;
-    uint8_t* clab = (uint8_t*)(scratch + L.clab);
+    const NoiseLayout Lay = noise_layout((size_t)n);
+    float* mean = scratch + Lay.mean;
+    float* var = scratch + Lay.var;
+    uint8_t* bin = (uint8_t*)(scratch + Lay.bin);
+    NoiseCtl* cc = (NoiseCtl*)(scratch + Lay.cc);
+    float* sm = scratch + Lay.samp;
+    float* cval = scratch + Lay.cval;
+    uint8_t* clab = (uint8_t*)(scratch + Lay.clab);
     const int r = win / 2;
     const float inv_wc = (float)(1.0 / ((double)win * win * win));
-    const unsigned g = grid_sel(n, sms), gc = grid_sel(L.cap, sms);
+    const unsigned g = grid_sel(n, sms), gc = grid_sel(Lay.cap, sms);
     // passes that usually exit at once (the fallbacks, the k+1 scans): one CTA per SM, so the
     // common case schedules few empty CTAs; when they do run, their grid-stride loops cover
     // every voxel
@@ -1575,12 +1643,8 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
     const size_t smem_keys = (kSampleMax + 256 * (kBoundThreads / 32)) * sizeof(uint32_t);   // keys + warp digit counts
     const long long m = n < kSampleMax ? n : kSampleMax;
     const unsigned long long wa = weyl_step((unsigned long long)n), wb = (unsigned long long)n / 3;
-    cudaError_t e;
-    if ((e = fy_smem_optin(k_win_bounds, smem_keys)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(ctl->hist, 0, sizeof(ctl->hist), st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(cc->hist, 0, sizeof(cc->hist), st)) != cudaSuccess) return e;
-    PDL(k_noise_setup, 1, NT_MAX, 0, st, ctl, cc, n, flat_pct, ref_intensity);
-    {   // 1. stats
+    RUN(256, 1, k_noise_setup, 1, 256, 0, ctl, cc, n, flat_pct, ref_intensity);
+    if (stats) {   // 1. stats
         fyzb::Params sp{};
         sp.nz = nz; sp.ny = ny; sp.nx = nx;
         sp.f0 = in; sp.o0 = mean; sp.o1 = var; sp.o2 = guided_mv;
@@ -1588,95 +1652,189 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
         cudaError_t e0 = fyzb::launch<fyzb::ZB_NOISE>(sp, r, sms, st);
         if (e0 != cudaSuccess) return e0;
         ++launches;
-        fy_prof_mark(st, "noise.stats");
+        if (!L.record) fy_prof_mark(st, "noise.stats");
     }
     // 2a. 1st/99th percentile of the means: sample-guided window pass, then the radix passes
     // of mode 1 over the candidates (control block cc, targets = labels); the radix passes
     // over the whole field (11 + 11 + 10 bits, then the k+1 neighbours) run only if the
     // window misses
-    PDL(k_win_sample, 64, 256, 0, st, mean, ctl, sm, m, wa, wb);
-    PDL(k_win_bounds, dim3(2, 2), kBoundThreads, smem_keys, st, sm, ctl, m);
-    PDL(k_win_count, g, 256, 0, st, mean, ctl, cval, clab, L.cap);
-    PDL(k_win_arm, 1, 1, 0, st, ctl, cc, L.cap);
+    RUN(256, 1, k_win_sample, 64, 256, 0, mean, ctl, sm, m, wa, wb);
+    RUN(kBoundThreads, 1, k_win_bounds, dim3(2, 2), kBoundThreads, smem_keys, sm, ctl, m);
+    RUN(256, 1, k_win_count, g, 256, 0, mean, ctl, cval, clab, Lay.cap);
+    RUN(32, 1, k_win_arm, 1, 1, 0, ctl, cc, Lay.cap);
     for (int sh = 24; sh >= 0; sh -= 8) {
         // the first digit's histogram sets the ranks (k_win_targets) before its scan; the
         // later digits' scans run in each pass's last CTA
-        PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL,
+        RUN(256, 1, (k_sel_hist<8, 1>), gcl, 256, smem_bin, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL,
             sh == 24 ? -1 : (sh == 0 ? 1 : 0));
         if (sh == 24) {
-            PDL(k_win_targets, 2, 256, 0, st, ctl, cc);
-            PDL(k_sel_scan, 2, 256, 0, st, cc, 8, 1, 0);
+            RUN(256, 1, k_win_targets, 2, 256, 0, ctl, cc);
+            RUN(256, 1, k_sel_scan, 2, 256, 0, cc, 8, 1, 0);
         }
     }
-    PDL(k_sel_next, gs, 256, 0, st, nullptr, cval, clab, cc, 1);
-    PDL(k_win_finish, 1, 1, 0, st, ctl, cc);
+    RUN(256, 1, k_sel_next, gs, 256, 0, nullptr, cval, clab, cc, 1);
+    RUN(32, 1, k_win_finish, 1, 1, 0, ctl, cc);
     const int all_digits[3][2] = {{21, 11}, {10, 11}, {0, 10}};
     for (int i = 0; i < 3; ++i) {
-        if (all_digits[i][1] == 11) PDL((k_sel_hist<11, 0>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
-        else PDL((k_sel_hist<10, 0>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
+        if (all_digits[i][1] == 11) RUN(256, 1, (k_sel_hist<11, 0>), gs, 256, smem_all, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
+        else RUN(256, 1, (k_sel_hist<10, 0>), gs, 256, smem_all, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
     }
-    PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 0);
-    PDL(k_noise_bins_setup, 1, NT_MAX, 0, st, ctl);
-    fy_prof_mark(st, "noise.lohi");
+    RUN(256, 1, k_sel_next, gs, 256, 0, mean, var, bin, ctl, 0);
+    RUN(NT_MAX, 1, k_noise_bins_setup, 1, NT_MAX, 0, ctl);
+    if (!L.record) fy_prof_mark(st, "noise.lohi");
     // 2bw. per-bin flat_pct percentile of the variance through the bins' window: sample,
     // bounds, one counting pass over mean and variance, then four digit passes over the
     // candidates. The sample lives in the candidate region until the counting pass refills it.
     {
         long long m2 = n < kBinSampleMax ? n : kBinSampleMax;
-        const long long m2cap = (L.cap - 64) * 4 / 5;    // keys, then labels 256-byte aligned
+        const long long m2cap = (Lay.cap - 64) * 4 / 5;    // keys, then labels 256-byte aligned
         if (m2 > m2cap) m2 = m2cap;
         uint32_t* skey = reinterpret_cast<uint32_t*>(cval);
         uint8_t* slab = reinterpret_cast<uint8_t*>(cval + round64((size_t)m2));
-        if ((e = fy_smem_optin(k_bwin_bounds, smem_keys)) != cudaSuccess) return e;
-        PDL(k_bwin_sample, 64, 256, 0, st, mean, var, ctl, skey, slab, m2, wa, (unsigned long long)n / 5);
-        PDL(k_bwin_bounds, NB, kBoundThreads, smem_keys, st, skey, slab, ctl, m2);
-        PDL(k_bwin_count, g, 256, 0, st, mean, var, ctl, cval, clab, L.cap);
-        PDL(k_bwin_arm, 1, 256, 0, st, ctl, cc, L.cap);
+        RUN(256, 1, k_bwin_sample, 64, 256, 0, mean, var, ctl, skey, slab, m2, wa, (unsigned long long)n / 5);
+        RUN(kBoundThreads, 1, k_bwin_bounds, NB, kBoundThreads, smem_keys, skey, slab, ctl, m2);
+        RUN(256, 4, k_bwin_count, g, 256, 0, mean, var, ctl, cval, clab, Lay.cap);
+        RUN(256, 1, k_bwin_arm, 1, 256, 0, ctl, cc, Lay.cap);
         for (int sh = 24; sh >= 0; sh -= 8) {
             // the first digit's histogram gives the inside counts (k_bwin_targets) before its
             // scan; the later digits' scans run in each pass's last CTA
-            PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL,
+            RUN(256, 1, (k_sel_hist<8, 1>), gcl, 256, smem_bin, nullptr, cval, clab, cc, sh, nullptr, nullptr, 0LL,
                 sh == 24 ? -1 : (sh == 0 ? 1 : 0));
             if (sh == 24) {
-                PDL(k_bwin_targets, NB, 256, 0, st, ctl, cc);
-                PDL(k_sel_scan, NB, 256, 0, st, cc, 8, 1, 0);
+                RUN(256, 1, k_bwin_targets, NB, 256, 0, ctl, cc);
+                RUN(256, 1, k_sel_scan, NB, 256, 0, cc, 8, 1, 0);
             }
         }
-        PDL(k_sel_next, gcl, 256, 0, st, nullptr, cval, clab, cc, 1);
-        PDL(k_bwin_finish, 1, 32, 0, st, ctl, cc);
+        RUN(256, 1, k_sel_next, gcl, 256, 0, nullptr, cval, clab, cc, 1);
+        RUN(32, 1, k_bwin_finish, 1, 32, 0, ctl, cc);
     }
     // 2b. (when the bins' window missed) per-bin flat_pct percentile of the variance by radix
     // passes over the whole field: 4 x 8 bits, then the k+1 neighbours;
     // the first pass also labels the voxels with their bins and yields the bin counts. The
     // third pass also lists the voxels that match their bin's 16-bit prefix (~1% of them),
     // and the last digit runs over that list (falling back to the whole field if it overflows).
-    PDL((k_sel_hist<8, 1, true>), g, 256, smem_bin, st, mean, var, bin, ctl, 24, nullptr, nullptr, 0LL, -1);
-    PDL(k_bin_targets, NB, 256, 0, st, ctl);
-    PDL(k_sel_scan, NB, 256, 0, st, ctl, 8, 1, 0);
-    PDL((k_sel_hist<8, 1>), g, 256, smem_bin, st, mean, var, bin, ctl, 16, nullptr, nullptr, 0LL, 0);
-    PDL(k_bin_cand_reset, 1, 1, 0, st, ctl);
-    if ((e = fy_smem_optin(k_sel_hist<8, 1, false, true>, smem_bin_c)) != cudaSuccess) return e;
-    PDL((k_sel_hist<8, 1, false, true>), g, 256, smem_bin_c, st, mean, var, bin, ctl, 8, cval, clab, L.cap, 0);
-    PDL(k_bin_arm, 1, 256, 0, st, ctl, cc, L.cap);
-    PDL((k_sel_hist<8, 1>), gs, 256, smem_bin, st, mean, var, bin, ctl, 0, nullptr, nullptr, 0LL, 1);       // overflow only
-    PDL((k_sel_hist<8, 1>), gcl, 256, smem_bin, st, nullptr, cval, clab, cc, 0, nullptr, nullptr, 0LL, 1);  // the list
+    RUN(256, 1, (k_sel_hist<8, 1, true>), g, 256, smem_bin, mean, var, bin, ctl, 24, nullptr, nullptr, 0LL, -1);
+    RUN(256, 1, k_bin_targets, NB, 256, 0, ctl);
+    RUN(256, 1, k_sel_scan, NB, 256, 0, ctl, 8, 1, 0);
+    RUN(256, 1, (k_sel_hist<8, 1>), g, 256, smem_bin, mean, var, bin, ctl, 16, nullptr, nullptr, 0LL, 0);
+    RUN(32, 1, k_bin_cand_reset, 1, 1, 0, ctl);
+    RUN(256, 1, (k_sel_hist<8, 1, false, true>), g, 256, smem_bin_c, mean, var, bin, ctl, 8, cval, clab, Lay.cap, 0);
+    RUN(256, 1, k_bin_arm, 1, 256, 0, ctl, cc, Lay.cap);
+    RUN(256, 1, (k_sel_hist<8, 1>), gs, 256, smem_bin, mean, var, bin, ctl, 0, nullptr, nullptr, 0LL, 1);       // overflow only
+    RUN(256, 1, (k_sel_hist<8, 1>), gcl, 256, smem_bin, nullptr, cval, clab, cc, 0, nullptr, nullptr, 0LL, 1);  // the list
     // k+1 past the selected key's 24-bit prefix: the list holds every key of the bin that shares
     // its 16-bit prefix, so when it holds a larger key, its smallest larger key is the next one
     // (a key in between would share the prefix and be listed too). Only targets whose next key
     // leaves the 16-bit prefix are left to the whole-field scan below.
-    PDL(k_sel_next, gcl, 256, 0, st, nullptr, cval, clab, cc, 1);
-    PDL(k_bin_finish, 1, 1, 0, st, ctl, cc);
-    PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 1);
-    PDL(k_noise_fit, 1, 32, 0, st, ctl, 0);
-    fy_prof_mark(st, "noise.bin_select");
+    RUN(256, 1, k_sel_next, gcl, 256, 0, nullptr, cval, clab, cc, 1);
+    RUN(32, 1, k_bin_finish, 1, 1, 0, ctl, cc);
+    RUN(256, 1, k_sel_next, gs, 256, 0, mean, var, bin, ctl, 1);
+    RUN(32, 1, k_noise_fit, 1, 32, 0, ctl, 0);
+    if (!L.record) fy_prof_mark(st, "noise.bin_select");
     // 2c. fallback (mode 2 only): flat_pct percentile over all voxels' variance
     for (int i = 0; i < 3; ++i) {
-        if (all_digits[i][1] == 11) PDL((k_sel_hist<11, 2>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
-        else PDL((k_sel_hist<10, 2>), gs, 256, smem_all, st, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
+        if (all_digits[i][1] == 11) RUN(256, 1, (k_sel_hist<11, 2>), gs, 256, smem_all, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
+        else RUN(256, 1, (k_sel_hist<10, 2>), gs, 256, smem_all, mean, var, bin, ctl, all_digits[i][0], nullptr, nullptr, 0LL, i == 2 ? 1 : 0);
     }
-    PDL(k_sel_next, gs, 256, 0, st, mean, var, bin, ctl, 2);
-    PDL(k_noise_fit, 1, 32, 0, st, ctl, 1);
-    return cudaGetLastError();
+    RUN(256, 1, k_sel_next, gs, 256, 0, mean, var, bin, ctl, 2);
+    RUN(32, 1, k_noise_fit, 1, 32, 0, ctl, 1);
+    return cudaSuccess;
+}
+
+}  // namespace
+
+// Enqueue the whole estimate. scratch: fy_noise_scratch_floats(n) floats; ctl:
+// fy_noise_ctl_bytes(). Supports win in {3..9} (r = win/2 <= 4). guided_mv (optional,
+// 2n floats): the statistics pass also writes the guided filter's (mean, var) pairs of the
+// same window, for fy_launch_guided_apply_mv with r = win/2.
+// Every kernel runs as a programmatic dependent launch; the first failed launch is returned.
+cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, int win, double flat_pct,
+                                     double ref_intensity, float* scratch, void* ctl_mem, int sms,
+                                     cudaStream_t st, int& launches, float* guided_mv) {
+    NoiseLaunch L;
+    L.st = st;
+    cudaError_t e = noise_sequence(L, in, nz, ny, nx, win, flat_pct, ref_intensity, scratch, ctl_mem, sms, launches,
+                                   guided_mv, true);
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- a batch of volumes
+// The selection sequences of many volumes, recorded (no launch) for one replay: each step of
+// the sequence becomes one launch over all volumes (blockIdx.z = volume). The statistics pass
+// is not part of it (the caller runs it for every volume first: fy_noise_stats_params).
+struct NoiseBatch {
+    NoiseLaunch L;
+    int launches = 0;                      // per volume
+};
+NoiseBatch* fy_noise_batch_record(const float* const* in, const int* dims, float* const* scratch,
+                                  void* const* ctl_mem, int nvol, int win, double flat_pct, double ref_intensity,
+                                  int sms, cudaError_t* err) {
+    NoiseBatch* b = new NoiseBatch();
+    b->L.record = true;
+    *err = cudaSuccess;
+    for (int i = 0; i < nvol && *err == cudaSuccess; ++i) {
+        int launches = 0;
+        b->L.si = 0;
+        *err = noise_sequence(b->L, in[i], dims[3 * i], dims[3 * i + 1], dims[3 * i + 2], win, flat_pct, ref_intensity,
+                              scratch[i], ctl_mem[i], sms, launches, nullptr, false);
+        if (*err == cudaSuccess && b->L.si != b->L.steps.size()) *err = cudaErrorInvalidValue;
+        b->L.cubes = i + 1;
+        b->launches = launches;
+    }
+    if (*err != cudaSuccess) {
+        delete b;
+        return nullptr;
+    }
+    return b;
+}
+// Bytes of the packed arguments (each step's volumes contiguous, steps 256-byte aligned).
+size_t fy_noise_batch_bytes(const NoiseBatch* b) {
+    size_t t = 0;
+    for (const auto& s : b->L.steps) t += (s.packs.size() + 255) & ~(size_t)255;
+    return t;
+}
+void fy_noise_batch_pack(const NoiseBatch* b, void* host) {
+    unsigned char* h = (unsigned char*)host;
+    for (const auto& s : b->L.steps) {
+        memcpy(h, s.packs.data(), s.packs.size());
+        h += (s.packs.size() + 255) & ~(size_t)255;
+    }
+}
+int fy_noise_batch_steps(const NoiseBatch* b) { return (int)b->L.steps.size(); }
+// One launch per step on st, its volumes' arguments read from dev (fy_noise_batch_pack's
+// layout, already in device memory by stream order).
+cudaError_t fy_noise_batch_launch(const NoiseBatch* b, const void* dev, cudaStream_t st) {
+    const unsigned char* d = (const unsigned char*)dev;
+    for (const auto& s : b->L.steps) {
+        cudaLaunchConfig_t c = {};
+        c.gridDim = dim3(s.grid.x, s.grid.y, (unsigned)b->L.cubes);
+        c.blockDim = s.block;
+        c.dynamicSmemBytes = s.smem;
+        c.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        c.attrs = at;
+        c.numAttrs = 1;
+        const void* arg = d;
+        void* args[1] = {(void*)&arg};
+        cudaError_t e = cudaLaunchKernelExC(&c, s.kern, args);
+        if (e != cudaSuccess) return e;
+        d += (s.packs.size() + 255) & ~(size_t)255;
+    }
+    return cudaSuccess;
+}
+void fy_noise_batch_free(NoiseBatch* b) { delete b; }
+// The statistics pass's parameters for one volume (box pass ZB_NOISE writing the guided
+// (mean, var) pairs too), as noise_sequence forms them.
+fyzb::Params fy_noise_stats_params(const float* in, int nz, int ny, int nx, int win, float* scratch, float* guided_mv) {
+    const NoiseLayout Lay = noise_layout((size_t)nz * ny * nx);
+    fyzb::Params sp{};
+    sp.nz = nz; sp.ny = ny; sp.nx = nx;
+    sp.f0 = in; sp.o0 = scratch + Lay.mean; sp.o1 = scratch + Lay.var; sp.o2 = guided_mv;
+    sp.inv_wc = (float)(1.0 / ((double)win * win * win));
+    sp.wci = win * win * win;
+    return sp;
 }
 
 // Copy the model out of a finished control block (device -> host, async on st).

@@ -9,8 +9,8 @@
 //           copy (TMA) per plane, completing on the slot's mbarrier. Other shapes: cp.async
 //           by all threads.
 //   X phase one item = 4 output columns of one staged row: the row's values, the window
-//           sums of both quantities, two float4 stores; TY x TX/4 = 256 items, one per
-//           thread. The 2R halo rows go as one-column items, spread over all threads.
+//           sums of both quantities, two float4 stores; (TY + 2R) x TX/4 items (the halo
+//           rows included), one or two per thread.
 //   Y phase one thread = one output column x 4 output rows. Its (2R+1)-plane z ring of
 //           XY sums stays in registers and gives the box of plane zi - R to the epilogue.
 // With TMA staging a plane takes one CTA barrier, between the X and Y phases: the X sums
@@ -135,6 +135,13 @@ struct TmaMaps {
     CUtensorMap m1;                    // output passes: the guide I, one TX x TY tile per plane
     int guide;                         // m1 is valid: the guide is staged with the planes
 };
+// The maps a tile's copies use: the kernel parameter's (one volume per launch) or a job's in
+// device memory (the work-queue kernel).
+struct TmaRef {
+    const CUtensorMap* m0;
+    const CUtensorMap* m1;
+    int guide;
+};
 static __device__ int zb_timeout;      // set when a bounded wait expires (never expected)
 constexpr int kWaitSpins = 1 << 20;
 // Polls allowed for each CTA's first wait on its staged plane. Always kWaitSpins, except
@@ -177,12 +184,12 @@ FY_D void tma_load_3d(float* dst, const CUtensorMap* map, int x, int y, int z, u
 // gdst, when not null, receives the guide tile of output plane zi - R (x0 a multiple of TX:
 // 16-byte aligned), completing on the same barrier.
 template <int R, int C>
-FY_D void tma_stage(float* dst, float* gdst, const TmaMaps& tm, unsigned long long* bar, int zi, int x0, int y0) {
+FY_D void tma_stage(float* dst, float* gdst, const TmaRef& tm, unsigned long long* bar, int zi, int x0, int y0) {
     using G = Geo<R, C>;
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // prior generic reads of the slot
     mbar_expect_tx(bar, (unsigned)((G::SY * G::RW + (gdst ? TX * TY : 0)) * sizeof(float)));
-    tma_load_3d(dst, &tm.m0, C * (x0 - 4), y0 - R, zi, bar);
-    if (gdst) tma_load_3d(gdst, &tm.m1, x0, y0, zi - R, bar);
+    tma_load_3d(dst, tm.m0, C * (x0 - 4), y0 - R, zi, bar);
+    if (gdst) tma_load_3d(gdst, tm.m1, x0, y0, zi - R, bar);
 }
 
 // Stage plane zi into dst with cp.async; zero fill outside the volume. VEC: 16-byte copies
@@ -210,14 +217,15 @@ FY_D void stage_plane(float* dst, const Params& p, int zi, int x0, int y0) {
     }
 }
 
+// One CTA's tile (bx, by) and z chunk bz of a box pass. Returns false when a bounded wait gave
+// up (the CTA then raised zb_timeout and drained its copies). With TMA it leaves the slot
+// barriers invalidated, so the CTA can run another tile.
 template <int R, int KIND, bool VEC, bool TMA>
-__global__ void __launch_bounds__(NT, ctas_per_sm(R, KIND)) k_zbox(const __grid_constant__ Params p, const __grid_constant__ TmaMaps tm) {
-    fy_pdl_wait();
+FY_D bool zbox_tile(const Params& p, const TmaRef& tm, int bx, int by, int bz, unsigned long long* bars) {
     constexpr int C = out_kind(KIND) ? 2 : 1;
     using G = Geo<R, C>;
     constexpr int NR = G::NR;
     extern __shared__ float4 zb_smem4[];
-    __shared__ __align__(8) unsigned long long bars[NS];
     float* stage = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(zb_smem4) + 127) & ~(uintptr_t)127);
     float* sguide = stage + NS * G::STAGE;                         // NS guide tiles (output passes)
     float2* xs = reinterpret_cast<float2*>(sguide + NS * G::GUIDE);  // X sums of both quantities, 2 x [SY][TX]
@@ -225,8 +233,8 @@ __global__ void __launch_bounds__(NT, ctas_per_sm(R, KIND)) k_zbox(const __grid_
     float* ry = rx + TX;
     const int t = threadIdx.x;
     const int nz = p.nz, ny = p.ny, nx = p.nx;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int zs = blockIdx.z * p.zchunk, ze = min(nz, zs + p.zchunk);
+    const int x0 = bx * TX, y0 = by * TY;
+    const int zs = bz * p.zchunk, ze = min(nz, zs + p.zchunk);
     const size_t plane = (size_t)ny * nx;
     // per-tile shift: one constant for every window this CTA forms
     const float c = out_kind(KIND) ? 0.f : __ldg(p.f0 + (size_t)zs * plane + (size_t)y0 * nx + x0);
@@ -328,8 +336,11 @@ __global__ void __launch_bounds__(NT, ctas_per_sm(R, KIND)) k_zbox(const __grid_
             }
             const float* sp = stage + slot * G::STAGE;
             const bool zin = zi >= 0 && zi < nz;
-            // X phase, output rows 0 .. TY-1: P[j] = both quantities of staged column x0 - 4 + x4 + j
-            for (int it = t; it < TY * (TX / 4); it += NT) {
+            // X phase, every staged row (the TY output rows and the 2R halo rows): one item = 4
+            // output columns of one row, P[j] = both quantities of staged column x0 - 4 + x4 + j.
+            // (One-column items for the halo rows cost (2R+1) taps' conversions per output
+            // instead of (4+2R)/4; 4-column items keep the same taps in the same order.)
+            for (int it = t; it < G::SY * (TX / 4); it += NT) {
                 const int yy = it >> 4, x4 = (it & 15) << 2;
                 float2 P[12];
                 if (C == 2) {                    // interleaved pairs: float4 = two columns
@@ -381,33 +392,6 @@ __global__ void __launch_bounds__(NT, ctas_per_sm(R, KIND)) k_zbox(const __grid_
                 dst[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
                 dst[1] = make_float4(o[2].x, o[2].y, o[3].x, o[3].y);
             }
-            // X phase, the 2R halo rows: one output column per item, spread over the whole CTA
-            // (one item per thread at R = 2), with the same taps in the same order as above
-            for (int q = t; q < 2 * R * TX; q += NT) {
-                const int yy = TY + (q >> 6), xo = q & (TX - 1);
-                const int gy = y0 - R + yy;
-                const bool rin = zin && gy >= 0 && gy < ny;
-                auto tap = [&](int m) {                  // staged column xo + 4 - R + m
-                    const int col = xo + 4 - R + m;
-                    if (C == 2) {
-                        const float2 v = *reinterpret_cast<const float2*>(sp + yy * G::RW + 2 * col);
-                        return KIND == ZB_GUIDED_OUT_MV ? guided_ab(v, eps) : v;
-                    }
-                    float q1 = sp[yy * G::RW + col];
-                    if (cols_in) {
-                        q1 = q1 - (rin ? c : 0.f);
-                    } else {
-                        const int gxj = x0 - 4 + col;
-                        q1 = (rin && gxj >= 0 && gxj < nx) ? q1 - c : 0.f;
-                    }
-                    return make_float2(q1, q1 * q1);
-                };
-                float2 sm = tap(0);
-#pragma unroll
-                for (int m = 1; m <= 2 * R; ++m) sm = add2(sm, tap(m));
-                if (out_kind(KIND)) sm = mul2(sm, rx[xo]);
-                xcur[yy * TX + xo] = sm;
-            }
             if (TMA) {
                 if (__syncthreads_or(!ok)) {      // plane zi never landed: flag, drain, return
                     if (t == 0) {
@@ -416,7 +400,7 @@ __global__ void __launch_bounds__(NT, ctas_per_sm(R, KIND)) k_zbox(const __grid_
                             mbar_wait_bounded(&bars[(zq - zfirst) & (NS - 1)], (unsigned)(((zq - zfirst) / NS) & 1));
                     }
                     __syncthreads();
-                    return;
+                    return false;
                 }
                 // Refill the slot of plane zi - 1: past this barrier every thread has finished
                 // plane zi - 1, its staged rows and its guide tile alike.
@@ -509,6 +493,70 @@ __global__ void __launch_bounds__(NT, ctas_per_sm(R, KIND)) k_zbox(const __grid_
         }
     }
     if (!TMA) cp_wait<0>();
+    if (TMA) {                 // every copy issued was waited for: the barriers can be retired
+        __syncthreads();
+        if (t == 0)
+            for (int s = 0; s < NS; ++s)
+                asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_u32(&bars[s])) : "memory");
+        __syncthreads();
+    }
+    return true;
+}
+
+template <int R, int KIND, bool VEC, bool TMA>
+__global__ void __launch_bounds__(NT, ctas_per_sm(R, KIND)) k_zbox(const __grid_constant__ Params p, const __grid_constant__ TmaMaps tm) {
+    fy_pdl_wait();
+    __shared__ __align__(8) unsigned long long bars[NS];
+    const TmaRef tr{&tm.m0, &tm.m1, tm.guide};
+    zbox_tile<R, KIND, VEC, TMA>(p, tr, blockIdx.x, blockIdx.y, blockIdx.z, bars);
+}
+
+// A box pass over many volumes: one job per volume (its parameters, its tensor maps in device
+// memory, its tile counts and the index of its first work item; jobs in item order). The
+// work items are (volume, tile, z chunk) in one index space; persistent CTAs (ctas_per_sm per
+// SM) take the next item from *next until none is left, so volumes of any size share one
+// launch with no tail per volume. Each tile's arithmetic is the one-volume kernel's, so the
+// results are bit-identical to it. TMA staging only (every volume's rows 16-byte aligned).
+struct BoxJob {
+    CUtensorMap m0, m1;                // 64-byte aligned
+    Params p;
+    int guide;                         // m1 valid
+    int tx, ty;                        // tiles along x and y
+    long long first;                   // first work item
+};
+template <int R, int KIND>
+__global__ void __launch_bounds__(NT, ctas_per_sm(R, KIND)) k_zbox_queue(const BoxJob* __restrict__ jobs, int njobs,
+                                                                        long long total,
+                                                                        unsigned long long* __restrict__ next) {
+    fy_pdl_wait();
+    __shared__ __align__(8) unsigned long long bars[NS];
+    __shared__ long long s_item;
+    __shared__ __align__(16) Params s_p;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (long long)atomicAdd(next, 1ull);
+        __syncthreads();
+        const long long item = s_item;
+        __syncthreads();                                  // read by every thread before the next ticket
+        if (item >= total) return;
+        int lo = 0, hi = njobs - 1;                       // the last job with first <= item
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].first <= item) lo = mid; else hi = mid - 1;
+        }
+        const BoxJob& J = jobs[lo];
+        const long long local = item - J.first;
+        const int bx = (int)(local % J.tx), by = (int)((local / J.tx) % J.ty), bz = (int)(local / ((long long)J.tx * J.ty));
+        if (threadIdx.x == 0) {          // the maps were written by a copy: acquire them for the tensor proxy
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&J.m0) : "memory");
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&J.m1) : "memory");
+        }
+        static_assert(sizeof(Params) % 4 == 0, "word copy");
+        for (int i = threadIdx.x; i < (int)(sizeof(Params) / 4); i += blockDim.x)   // the job's parameters,
+            reinterpret_cast<int*>(&s_p)[i] = reinterpret_cast<const int*>(&J.p)[i]; // read from shared memory
+        __syncthreads();
+        const TmaRef tr{&J.m0, &J.m1, J.guide};
+        if (!zbox_tile<R, KIND, true, true>(s_p, tr, bx, by, bz, bars)) return;
+    }
 }
 
 // Tiles and z chunks (fy_box_default_chunks, fy_internal.h). The chunk count is fixed by the
@@ -569,6 +617,61 @@ inline cudaError_t launch_r(const Params& p, dim3 grid, cudaStream_t st) {
     auto k = k_zbox<R, KIND, VEC, false>;
     if ((e = fy_smem_optin(k, smem)) != cudaSuccess) return e;
     return fy_launch_pdl(k, grid, dim3(NT), smem, st, p, tm);
+}
+
+// The work-queue pass (k_zbox_queue). make_job fills one volume's job from its parameters
+// (its z chunks as the one-volume launch picks them, so the results match it bit for bit) and
+// returns its number of work items, or -1 when the volume cannot use TMA staging (rows not
+// 16-byte aligned) or the encoder is unavailable.
+template <int KIND, int R>
+inline long long make_job_r(BoxJob& j, const Params& p, int sms, long long first) {
+    constexpr int C = out_kind(KIND) ? 2 : 1;
+    memset(&j, 0, sizeof j);
+    j.p = p;
+    const dim3 grid = grid_for(KIND, p.nz, p.ny, p.nx, R, sms, j.p.zchunk);
+    if (p.nx % 4 || ((uintptr_t)p.f0 & 15)) return -1;
+    if (!make_tma_map(&j.m0, p.f0, p.nz, p.ny, p.nx, C, SXW, Geo<R, C>::SY)) return -1;
+    if (out_kind(KIND) && p.out_mode == 0 && p.guide)
+        j.guide = make_tma_map(&j.m1, p.guide, p.nz, p.ny, p.nx, 1, TX, TY) ? 1 : 0;
+    j.tx = (int)grid.x;
+    j.ty = (int)grid.y;
+    j.first = first;
+    return (long long)grid.x * grid.y * grid.z;
+}
+template <int KIND>
+inline long long make_job(BoxJob& j, const Params& p, int r, int sms, long long first) {
+    switch (r) {
+        case 1: return make_job_r<KIND, 1>(j, p, sms, first);
+        case 2: return make_job_r<KIND, 2>(j, p, sms, first);
+        case 3: return make_job_r<KIND, 3>(j, p, sms, first);
+        case 4: return make_job_r<KIND, 4>(j, p, sms, first);
+        default: return -1;
+    }
+}
+// Launch the queue over njobs jobs in device memory (64-byte aligned) with `total` items;
+// *next must hold 0 (stream order).
+template <int KIND, int R>
+inline cudaError_t launch_queue_r(const BoxJob* jobs, int njobs, long long total, unsigned long long* next, int sms,
+                                  cudaStream_t st) {
+    constexpr int C = out_kind(KIND) ? 2 : 1;
+    const size_t smem = Geo<R, C>::bytes;
+    auto k = k_zbox_queue<R, KIND>;
+    cudaError_t e = fy_smem_optin(k, smem);
+    if (e != cudaSuccess) return e;
+    const long long want = (long long)sms * ctas_per_sm(R, KIND);
+    const unsigned grid = (unsigned)(total < want ? (total > 0 ? total : 1) : want);
+    return fy_launch_pdl(k, dim3(grid), dim3(NT), smem, st, jobs, njobs, total, next);
+}
+template <int KIND>
+inline cudaError_t launch_queue(const BoxJob* jobs, int njobs, long long total, unsigned long long* next, int r,
+                                int sms, cudaStream_t st) {
+    switch (r) {
+        case 1: return launch_queue_r<KIND, 1>(jobs, njobs, total, next, sms, st);
+        case 2: return launch_queue_r<KIND, 2>(jobs, njobs, total, next, sms, st);
+        case 3: return launch_queue_r<KIND, 3>(jobs, njobs, total, next, sms, st);
+        case 4: return launch_queue_r<KIND, 4>(jobs, njobs, total, next, sms, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 // Number of bounded waits that expired in this translation unit's box passes (0 expected).

@@ -458,6 +458,27 @@ int  fy_gpu_restore_u8(const unsigned char *d_u8, float *d_out, int nz, int ny, 
                        double f32_min, double f32_max, const fy_physics *p,
                        const fy_restore_cfg *cfg, void *stream);
 
+/* A batch of device-resident volumes of any sizes through the same chain in one call (no
+ * reference counterpart; the reference runs its tiles in an OpenMP loop, pipeline.c:1008-1020).
+ * Each volume has its own dewindow range and physics; cfg is shared. The deconvolutions
+ * run on several streams, the two box passes (noise statistics, guided output) run as one
+ * work-queue launch each over every volume's (tile, z chunk) items, and the noise model's
+ * selection as one launch per step over all volumes. Each output equals fy_gpu_restore_u8's
+ * for that volume bit for bit. The batched form covers the model's eps with the shared
+ * noise/guided window (noise_win = 2*guided_radius + 1, guided_s <= 1) without rings or a
+ * radial model, for volumes whose x extent is a multiple of 4; other configurations run the
+ * volumes one by one through fy_gpu_restore_u8. Enqueued on `stream` (NULL: legacy
+ * default stream), not synchronised; the thread's batch buffers grow to the batch's need
+ * (about 24 bytes per voxel plus eight half spectra of the largest volume). */
+typedef struct {
+    const unsigned char *u8;    /* device, nz*ny*nx */
+    float *out;                 /* device, nz*ny*nx floats (may not alias u8) */
+    int nz, ny, nx;
+    double f32_min, f32_max;    /* dewindow range (fy_u8_to_phys) */
+    fy_physics phys;
+} fy_batch_cube;
+int  fy_gpu_restore_u8_batch(const fy_batch_cube *cubes, int n, const fy_restore_cfg *cfg, void *stream);
+
 /* fy_process_buffer on device buffers: d_u8 (hz*hy*hx) in, d_out (tz*ty*tx) out, on
  * `stream`. Synchronises the stream twice: after the all-air test (an empty buffer skips
  * the chain, as the reference does) and at the end, so that *all_air and the status are
