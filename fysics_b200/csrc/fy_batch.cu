@@ -8,7 +8,8 @@
 //   2. the noise statistics of every volume in one work-queue launch (k_zbox_queue): the
 //      (volume, tile, z chunk) items of all volumes in one index space, taken by persistent
 //      CTAs, so small volumes leave no tail;
-//   3. the noise model's selection, one launch per step for all volumes (blockIdx.z = volume);
+//   3. the noise model's selection, one launch per step for all volumes (each with the CTAs
+//      it needs, numbered per volume);
 //   4. the guided filter's output pass of every volume in one work-queue launch.
 // Each volume's arithmetic is the single-volume chain's (the same tiles, chunks, kernels and
 // order statistics), so its output equals fy_gpu_restore_u8's bit for bit. The batched form
@@ -18,6 +19,9 @@
 // staging), run one volume after another through fy_gpu_restore_u8.
 #include <string.h>
 
+#include <algorithm>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #include "fy_context.h"
@@ -148,10 +152,23 @@ extern "C" int fy_gpu_restore_u8_batch(const fy_batch_cube* cubes, int n, const 
     fyzb::BoxJob* js = reinterpret_cast<fyzb::BoxJob*>(H + off_jobs_s);
     fyzb::BoxJob* jg = reinterpret_cast<fyzb::BoxJob*>(H + off_jobs_g);
     long long total_s = 0, total_g = 0;
+    {   // the volumes' tables (FP64 weights: ~0.1 ms each) on the host cores, one volume at a time each
+        std::atomic<int> nexti{0};
+        auto fill = [&]() {
+            for (int i = nexti++; i < n; i = nexti++)
+                dl[i].us = fy_deconv_fill_tables(dl[i].g, &cubes[i].phys, params[i], cfg->deconv_kind, fz2ss[i],
+                                                 H + off_tab[i]);
+        };
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int nth = std::min(std::min(n, 16), (int)(hw > 1 ? hw : 1)) - 1;
+        std::vector<std::thread> th;
+        for (int k = 0; k < nth; ++k) th.emplace_back(fill);
+        fill();
+        for (auto& x : th) x.join();
+    }
     for (int i = 0; i < n; ++i) {
         const fy_batch_cube& q = cubes[i];
         DeconvLaunch& d = dl[i];
-        d.us = fy_deconv_fill_tables(d.g, &q.phys, params[i], cfg->deconv_kind, fz2ss[i], H + off_tab[i]);
         unsigned char* tb = D + off_tab[i];
         d.lut = reinterpret_cast<const float*>(tb);
         d.fz2 = reinterpret_cast<const double*>(tb + lut_bytes);

@@ -243,8 +243,9 @@ int fy_gpu_last_status(void) { return fy::ctx().status; }
 const char* fy_gpu_last_error(void) { return fy::ctx().err.c_str(); }
 unsigned long long fy_gpu_kernel_launches(void) { return fy::ctx().launches; }
 int fy_gpu_kernel_timeouts(void) {
-    const int a = fy_guided_wait_timeouts(), b = fy_noise_wait_timeouts(), d = fy_batch_wait_timeouts();
-    return a < 0 || b < 0 || d < 0 ? -1 : a + b + d;
+    const int a = fy_guided_wait_timeouts(), b = fy_noise_wait_timeouts(), d = fy_batch_wait_timeouts(),
+              f = fy_deconv_wait_timeouts();
+    return a < 0 || b < 0 || d < 0 || f < 0 ? -1 : a + b + d + f;
 }
 int fy_gpu_test_box_first_wait(int polls) {
     fy::enter();

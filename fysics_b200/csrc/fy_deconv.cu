@@ -47,3 +47,14 @@ cudaError_t fy_launch_spec_y(float2* spec, const SpecGeom& g, const FftPlan& ply
         return cudaGetLastError();
     });
 }
+
+// Expired bulk waits of the deconvolution's first pass in every unit that instantiates it.
+int fy_deconv_wait_timeouts() {
+    const int v[4] = {dc_timeouts(), fy_deconv_ct_a_timeouts(), fy_deconv_ct_b_timeouts(), fy_deconv_ct_c_timeouts()};
+    int t = 0;
+    for (int x : v) {
+        if (x < 0) return -1;
+        t += x;
+    }
+    return t;
+}

@@ -73,6 +73,45 @@ template <class T> struct VecLoad<T, 1> {
     static FY_D void run(const T* p, float* v) { v[0] = (float)__ldg(p); }
 };
 
+// ---- bulk staging of P1's u8 rows: one thread copies the CTA's rows (one contiguous run,
+// 16-byte aligned) with cp.async.bulk onto an mbarrier; every thread waits on it, bounded. A
+// wait that gives up raises dc_timeout (reported by fy_gpu_kernel_timeouts), waits once more
+// (bounded) for the copy in flight and leaves the CTA's lines unwritten.
+static __device__ int dc_timeout;      // set when a bounded wait expires (never expected)
+constexpr int kDcWaitSpins = 1 << 20;
+FY_D unsigned dc_smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+FY_D bool dc_wait(unsigned long long* bar, unsigned parity) {
+    for (int i = 0; i < kDcWaitSpins; ++i) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(dc_smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+FY_D void dc_bulk_rows(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(dc_smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(dc_smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(dc_smem_u32(dst)), "l"(src), "r"(bytes), "r"(dc_smem_u32(bar))
+                 : "memory");
+}
+// Host: this unit's expired bulk waits (0 expected; -1 when unreadable).
+inline int dc_timeouts() {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, dc_timeout, sizeof v) != cudaSuccess) { cudaGetLastError(); return -1; }
+    return v;
+}
+// Host: whether P1 stages its u8 rows in bulk, and the extra shared memory it then needs.
+inline bool dc_bulk_u8(const DeconvLaunch& d) {
+    return d.src_u8 && d.g.nx % 16 == 0 && ((uintptr_t)d.src & 15) == 0;
+}
+
 template <int N, int E, class T, int VEC>
 __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(const T* __restrict__ src, float lo, float scale, int is_u8,
                                                         float2* __restrict__ spec, SpecGeom g,
@@ -87,8 +126,28 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(const T* __restrict__ sr
     __shared__ long long soff[2 * 16];
     const long Q = (long)g.nz * g.ny;
     const long q0 = (long)blockIdx.x * 2 * W;
+    // u8 rows in bulk (dc_bulk_u8 on the host decides the same and sizes the staging area)
+    const bool bulk = sizeof(T) == 1 && VEC == 4 && is_u8 && (g.nx & 15) == 0 && ((uintptr_t)src & 15) == 0;
+    __shared__ __align__(8) unsigned long long xbar;
+    const unsigned char* su8 =
+        reinterpret_cast<const unsigned char*>((reinterpret_cast<uintptr_t>(stw + pl.n) + 15) & ~(uintptr_t)15);
+    if (bulk && threadIdx.x == 0) {
+        const long nrows = Q - q0 < 2 * W ? Q - q0 : 2 * W;
+        dc_bulk_rows(const_cast<unsigned char*>(su8), src + q0 * g.nx, (unsigned)(nrows * g.nx), &xbar);
+    }
     load_twiddles(stw, tw, pl.n);
     row_offsets(soff, q0, W, Q, g);
+    if (bulk) {
+        __syncthreads();                               // the barrier is initialised
+        if (__syncthreads_or(!dc_wait(&xbar, 0u))) {
+            if (threadIdx.x == 0) {
+                atomicExch(&dc_timeout, 1);
+                dc_wait(&xbar, 0u);                    // the copy in flight, bounded
+            }
+            __syncthreads();
+            return;
+        }
+    }
     const int nch = g.nx / VEC;
     for (int it = threadIdx.x; it < W * nch; it += blockDim.x) {
         const int l = dchunk.div(it), x = (it - l * nch) * VEC;
@@ -96,8 +155,19 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(const T* __restrict__ sr
         float va[VEC], vb[VEC];
 #pragma unroll
         for (int j = 0; j < VEC; ++j) va[j] = vb[j] = 0.f;
-        if (qa < Q) VecLoad<T, VEC>::run(src + qa * g.nx + x, va);
-        if (qb < Q) VecLoad<T, VEC>::run(src + qb * g.nx + x, vb);
+        if (bulk) {                                    // rows 2l and 2l+1 of the staged run
+            if (qa < Q) {
+                const uchar4 u = *reinterpret_cast<const uchar4*>(su8 + (size_t)(2 * l) * g.nx + x);
+                va[0] = u.x; va[1] = u.y; va[2 % VEC] = u.z; va[3 % VEC] = u.w;
+            }
+            if (qb < Q) {
+                const uchar4 u = *reinterpret_cast<const uchar4*>(su8 + (size_t)(2 * l + 1) * g.nx + x);
+                vb[0] = u.x; vb[1] = u.y; vb[2 % VEC] = u.z; vb[3 % VEC] = u.w;
+            }
+        } else {
+            if (qa < Q) VecLoad<T, VEC>::run(src + qa * g.nx + x, va);
+            if (qb < Q) VecLoad<T, VEC>::run(src + qb * g.nx + x, vb);
+        }
         float2* dst = s + l * LPX + x;
 #pragma unroll
         for (int j = 0; j < VEC; ++j) {
@@ -325,7 +395,8 @@ cudaError_t fy_deconv_pass(int pass, const DeconvLaunch& d, cudaStream_t st) {
     switch (pass) {
     case 1: {   // X forward, rows paired two per line (line-major staging)
         const TileShape t = fy_x_tile_shape(1, g.px);
-        const size_t smem = (size_t)t.W * (g.px + 1) * sizeof(float2) + (size_t)g.px * sizeof(float2);
+        const size_t smem = (size_t)t.W * (g.px + 1) * sizeof(float2) + (size_t)g.px * sizeof(float2) +
+                            (dc_bulk_u8(d) ? (size_t)2 * t.W * g.nx + 16 : 0);
         const unsigned grid = (unsigned)((Q + 2 * t.W - 1) / (2 * t.W));
         const int esz = d.src_u8 ? 1 : 4;
         const bool vec = g.nx % 4 == 0 && ((uintptr_t)d.src % (4 * esz)) == 0;

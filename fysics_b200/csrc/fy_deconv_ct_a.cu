@@ -7,3 +7,5 @@ cudaError_t fy_deconv_pass_ct_a(int pass, int n, const DeconvLaunch& d, cudaStre
         default: return cudaErrorNotSupported;
     }
 }
+
+int fy_deconv_ct_a_timeouts() { return dc_timeouts(); }

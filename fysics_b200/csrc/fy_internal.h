@@ -218,6 +218,10 @@ int fy_restore_reserve(int nz, int ny, int nx);
 void fy_tile_release();
 int fy_guided_wait_timeouts();
 int fy_batch_wait_timeouts();
+int fy_deconv_wait_timeouts();
+int fy_deconv_ct_a_timeouts();
+int fy_deconv_ct_b_timeouts();
+int fy_deconv_ct_c_timeouts();
 cudaError_t fy_batch_set_first_wait_polls(int polls);
 int fy_noise_wait_timeouts();
 cudaError_t fy_guided_set_first_wait_polls(int polls);

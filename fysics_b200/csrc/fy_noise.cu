@@ -98,6 +98,13 @@ struct NoiseCtl {
 namespace {
 
 
+// The block index and grid size along x of the CTA's volume, which every selection body uses
+// in place of blockIdx.x / gridDim.x: k_one sets them from its launch, k_many from the step's
+// table of CTAs per volume (a batch launch holds every volume's CTAs along x).
+static __shared__ unsigned s_vbx, s_vgx;
+FY_D unsigned vbx() { return s_vbx; }
+FY_D unsigned vgx() { return s_vgx; }
+
 // ---------------------------------------------------------------- 1. local stats
 // z-sliding box pass (fy_zbox.cuh, ZB_NOISE): 4 B read + 8 B written per voxel.
 
@@ -291,8 +298,9 @@ FY_D void k_sel_hist(const float* __restrict__ mean, const float* __restrict__ v
         wc.v = bv + (threadIdx.x >> 5) * kCompactBuf;
         wc.l = reinterpret_cast<uint8_t*>(bv + (blockDim.x >> 5) * kCompactBuf) + (threadIdx.x >> 5) * kCompactBuf;
     }
-    long long base = (long long)blockIdx.x * chunk;
-    for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
+    long long base = (long long)vbx() * chunk;
+    const long long stride = (long long)vgx() * chunk;        // read once: the loop body has syncs
+    for (; base + chunk <= n4f; base += stride) {
         float4 x[SU];
         uchar4 bb[SU];
         float4 mm[LABEL ? SU : 1];
@@ -388,7 +396,7 @@ FY_D void k_sel_hist(const float* __restrict__ mean, const float* __restrict__ v
     __shared__ int s_last;
     __threadfence();                                     // this CTA's counts before its ticket
     __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(&ctl->done_ctas, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) s_last = atomicAdd(&ctl->done_ctas, 1u) == vgx() - 1;
     __syncthreads();
     if (!s_last) return;
     __threadfence();
@@ -407,7 +415,7 @@ FY_D void k_sel_scan(NoiseCtl* __restrict__ ctl, int db, int want_mode, int last
     __shared__ int s_sel;
     __shared__ unsigned int s_nextb;
     if (ctl->mode != want_mode) return;
-    const int t = blockIdx.x;
+    const int t = vbx();
     if (t >= ctl->ntarget || !ctl->tactive[t]) return;
     const int nbk = 1 << db, per = nbk / 256 > 0 ? nbk / 256 : 1;
     unsigned int* h = ctl->hist + (size_t)t * nbk;
@@ -487,8 +495,9 @@ FY_D void k_sel_next(const float* __restrict__ mean, const float* __restrict__ v
     };
     // SU float4 (and uchar4 labels) per thread before any is used, as the streaming passes
     const long long n4 = (n + 3) / 4, n4f = n / 4, chunk = (long long)SU * blockDim.x;
-    long long base = (long long)blockIdx.x * chunk;
-    for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
+    long long base = (long long)vbx() * chunk;
+    const long long stride = (long long)vgx() * chunk;        // read once: the loop body has syncs
+    for (; base + chunk <= n4f; base += stride) {
         float4 x[SU];
         uchar4 bb[SU];
 #pragma unroll
@@ -613,7 +622,7 @@ FY_D void k_bin_targets(NoiseCtl* ctl) {
     fy_pdl_wait();
     __shared__ unsigned long long part[256];
     if (ctl->mode != 1) return;
-    const int b = blockIdx.x;
+    const int b = vbx();
     unsigned int* h = ctl->hist + (size_t)b * 256;
     part[threadIdx.x] = h[threadIdx.x];
     __syncthreads();
@@ -725,11 +734,11 @@ FY_D void k_win_sample(const float* __restrict__ mean, const NoiseCtl* __restric
     fy_pdl_wait();
     if (ctl->mode != kModeWin0) return;
     const unsigned long long n = (unsigned long long)ctl->n;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+    for (long long i = (long long)vbx() * blockDim.x + threadIdx.x; i < m; i += (long long)vgx() * blockDim.x)
         sm[i] = __ldg(mean + (A * (unsigned long long)i + B) % n);
 }
 
-// One CTA (kBoundThreads threads) per target (blockIdx.x 0/1: 1st/99th percentile) and window
+// One CTA (kBoundThreads threads) per target (block x 0/1: 1st/99th percentile) and window
 // end (blockIdx.y 0: wlo, 1: whi). Dynamic shared memory: kSampleMax keys, then the warps'
 // digit histograms (kBoundThreads/32 x 256 counters).
 FY_D void k_win_bounds(const float* __restrict__ sm,
@@ -740,7 +749,7 @@ FY_D void k_win_bounds(const float* __restrict__ sm,
     __shared__ unsigned long long part[kBoundThreads];
     __shared__ uint32_t s_sel[2];
     if (ctl->mode != kModeWin0) return;
-    const int t = blockIdx.x;
+    const int t = vbx();
     const int c = (int)(m < kSampleMax ? m : kSampleMax);
     for (int i0 = threadIdx.x; i0 < c; i0 += 8 * blockDim.x) {   // eight loads in flight per thread
         float v[8];
@@ -805,8 +814,9 @@ FY_D void k_win_count(const float* __restrict__ mean, NoiseCtl* __restrict__ ctl
     const uint32_t lo0 = ctl->wlo[0], hi0 = ctl->whi[0], lo1 = ctl->wlo[1], hi1 = ctl->whi[1];
     unsigned int bel0 = 0, bel1 = 0;
     const long long chunk = (long long)SU * 256;
-    long long base = (long long)blockIdx.x * chunk;
-    for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
+    long long base = (long long)vbx() * chunk;
+    const long long stride = (long long)vgx() * chunk;        // read once: the loop body has syncs
+    for (; base + chunk <= n4f; base += stride) {
         float4 x[SU];
 #pragma unroll
         for (int u = 0; u < SU; ++u) x[u] = __ldg(reinterpret_cast<const float4*>(mean) + base + t + (long long)u * 256);
@@ -896,7 +906,7 @@ FY_D void k_win_targets(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) {
     fy_pdl_wait();
     __shared__ unsigned long long part[256];
     if (cc->mode != 1) return;
-    const int t = blockIdx.x;
+    const int t = vbx();
     if (t >= cc->ntarget) return;
     unsigned int* h = cc->hist + (size_t)t * 256;
     part[threadIdx.x] = h[threadIdx.x];
@@ -1019,7 +1029,7 @@ FY_D void k_bwin_sample(const float* __restrict__ mean, const float* __restrict_
     __syncthreads();
     const float lo_f = fe[0], fscale = ctl->fscale;
     const unsigned long long n = (unsigned long long)ctl->n;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = (long long)vbx() * blockDim.x + threadIdx.x; i < m; i += (long long)vgx() * blockDim.x) {
         const unsigned long long q = (A * (unsigned long long)i + B) % n;
         const float mv = __ldg(mean + q), vv = __ldg(var + q);
         const int b = bin_of(mv, fe, lo_f, fscale);
@@ -1046,7 +1056,7 @@ FY_D void k_bwin_bounds(const uint32_t* __restrict__ skey,
     __shared__ uint32_t s_sel[2];
     __shared__ int s_wc[NW];
     if (ctl->mode != kModeBinWin) return;
-    const int b = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int b = vbx(), t = threadIdx.x, lane = t & 31, w = t >> 5;
     const unsigned full = 0xffffffffu;
     auto load_labels = [&](long long e0, uint8_t* lab) {
         if (e0 + U <= m) {
@@ -1193,9 +1203,10 @@ FY_D void k_bwin_count(const float* __restrict__ mean, const float* __restrict__
     };
     const long long n = ctl->n, n4 = (n + 3) / 4, n4f = n / 4;
     const long long chunk = (long long)SUB * 256;
-    long long base = (long long)blockIdx.x * chunk;
+    long long base = (long long)vbx() * chunk;
+    const long long stride = (long long)vgx() * chunk;        // read once: the loop body has syncs
     int steps = 0;
-    for (; base + chunk <= n4f; base += (long long)gridDim.x * chunk) {
+    for (; base + chunk <= n4f; base += stride) {
         float4 xm[SUB], xv[SUB];
 #pragma unroll
         for (int u = 0; u < SUB; ++u) {
@@ -1313,7 +1324,7 @@ FY_D void k_bwin_targets(NoiseCtl* __restrict__ ctl, NoiseCtl* __restrict__ cc) 
     fy_pdl_wait();
     __shared__ unsigned long long part[256];
     if (cc->mode != 1 || ctl->mode != kModeBinWin) return;
-    const int b = blockIdx.x;
+    const int b = vbx();
     if (!cc->tactive[b]) return;
     unsigned int* h = cc->hist + (size_t)b * 256;
     part[threadIdx.x] = h[threadIdx.x];
@@ -1549,17 +1560,31 @@ namespace {
 
 // ---------------------------------------------------------------- launching: one cube or a batch
 // Every selection step above is a __device__ body run by one of two wrappers: k_one, one volume,
-// the body's arguments as kernel parameters; k_many, a batch of volumes, blockIdx.z = volume
+// the body's arguments as kernel parameters; k_many, a batch of volumes, the CTA's volume from
+// its block index
 // and each volume's arguments read from a device array. NoiseLaunch either launches k_one at
-// once or, in batch mode, records each volume's arguments for every step of the sequence (the
-// same sequence for every volume) and then replays it: one launch per step for all volumes,
-// with the largest grid any volume asked for (the bodies' loops are grid-stride, and the grids
-// that index targets or bins are the same for every volume).
+// once or, in batch mode, records each volume's arguments and grid for every step of the
+// sequence (the same sequence for every volume) and then replays it: one launch per step for
+// all volumes, each volume with the CTAs it asked for (their blocks are numbered per volume
+// through vbx()/vgx(); the grids that index targets or bins along y are the same for all).
 template <int NTB, int MINB, auto F, class... P>
-__global__ void __launch_bounds__(NTB, MINB) k_one(P... a) { F(a...); }
+__global__ void __launch_bounds__(NTB, MINB) k_one(P... a) {
+    s_vbx = blockIdx.x;                    // every thread stores the same values
+    s_vgx = gridDim.x;
+    F(a...);
+}
+// prefix[v] = the first CTA (along x) of volume v, prefix[nvol] = all of them
 template <int NTB, int MINB, auto F, class... P>
-__global__ void __launch_bounds__(NTB, MINB) k_many(const cuda::std::tuple<P...>* __restrict__ packs) {
-    cuda::std::apply([](auto... x) { F(x...); }, packs[blockIdx.z]);
+__global__ void __launch_bounds__(NTB, MINB) k_many(const cuda::std::tuple<P...>* __restrict__ packs,
+                                                     const unsigned* __restrict__ prefix, int nvol) {
+    int lo = 0, hi = nvol - 1;             // the last volume whose first CTA <= blockIdx.x
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= blockIdx.x) lo = mid; else hi = mid - 1;
+    }
+    s_vbx = blockIdx.x - __ldg(prefix + lo);
+    s_vgx = __ldg(prefix + lo + 1) - __ldg(prefix + lo);
+    cuda::std::apply([](auto... x) { F(x...); }, packs[lo]);
 }
 
 struct NoiseLaunch {
@@ -1570,6 +1595,7 @@ struct NoiseLaunch {
         dim3 grid, block;
         size_t smem, pack;                 // bytes of one volume's arguments
         std::vector<unsigned char> packs;
+        std::vector<unsigned> gx;         // CTAs along x of each volume
     };
     std::vector<Step> steps;
     size_t si = 0;                         // the next step of the volume being recorded
@@ -1593,8 +1619,8 @@ struct NoiseLaunch {
         }
         Step& s = steps[si++];
         if (s.kern != k || s.block.x != block.x || s.smem != smem) return cudaErrorInvalidValue;
-        s.grid.x = s.grid.x > grid.x ? s.grid.x : grid.x;
-        s.grid.y = s.grid.y > grid.y ? s.grid.y : grid.y;
+        if (s.grid.y != grid.y) return cudaErrorInvalidValue;
+        s.gx.push_back(grid.x);
         const T t((P)a...);
         const unsigned char* b = reinterpret_cast<const unsigned char*>(&t);
         s.packs.insert(s.packs.end(), b, b + sizeof(T));
@@ -1660,7 +1686,7 @@ cudaError_t noise_sequence(NoiseLaunch& L, const float* in, int nz, int ny, int 
     // window misses
     RUN(256, 1, k_win_sample, 64, 256, 0, mean, ctl, sm, m, wa, wb);
     RUN(kBoundThreads, 1, k_win_bounds, dim3(2, 2), kBoundThreads, smem_keys, sm, ctl, m);
-    RUN(256, 1, k_win_count, g, 256, 0, mean, ctl, cval, clab, Lay.cap);
+    RUN(256, 4, k_win_count, g, 256, 0, mean, ctl, cval, clab, Lay.cap);
     RUN(32, 1, k_win_arm, 1, 1, 0, ctl, cc, Lay.cap);
     for (int sh = 24; sh >= 0; sh -= 8) {
         // the first digit's histogram sets the ranks (k_win_targets) before its scan; the
@@ -1760,7 +1786,7 @@ cudaError_t fy_launch_estimate_noise(const float* in, int nz, int ny, int nx, in
 
 // ---------------------------------------------------------------- a batch of volumes
 // The selection sequences of many volumes, recorded (no launch) for one replay: each step of
-// the sequence becomes one launch over all volumes (blockIdx.z = volume). The statistics pass
+// the sequence becomes one launch over all volumes' CTAs. The statistics pass
 // is not part of it (the caller runs it for every volume first: fy_noise_stats_params).
 struct NoiseBatch {
     NoiseLaunch L;
@@ -1787,17 +1813,23 @@ NoiseBatch* fy_noise_batch_record(const float* const* in, const int* dims, float
     }
     return b;
 }
-// Bytes of the packed arguments (each step's volumes contiguous, steps 256-byte aligned).
+// Bytes of the packed steps: per step its volumes' arguments, then its table of first CTAs per
+// volume (nvol + 1 entries), each 256-byte aligned.
+static size_t al256n(size_t v) { return (v + 255) & ~(size_t)255; }
 size_t fy_noise_batch_bytes(const NoiseBatch* b) {
     size_t t = 0;
-    for (const auto& s : b->L.steps) t += (s.packs.size() + 255) & ~(size_t)255;
+    for (const auto& s : b->L.steps) t += al256n(s.packs.size()) + al256n((s.gx.size() + 1) * sizeof(unsigned));
     return t;
 }
 void fy_noise_batch_pack(const NoiseBatch* b, void* host) {
     unsigned char* h = (unsigned char*)host;
     for (const auto& s : b->L.steps) {
         memcpy(h, s.packs.data(), s.packs.size());
-        h += (s.packs.size() + 255) & ~(size_t)255;
+        h += al256n(s.packs.size());
+        unsigned* pre = reinterpret_cast<unsigned*>(h);
+        pre[0] = 0;
+        for (size_t v = 0; v < s.gx.size(); ++v) pre[v + 1] = pre[v] + s.gx[v];
+        h += al256n((s.gx.size() + 1) * sizeof(unsigned));
     }
 }
 int fy_noise_batch_steps(const NoiseBatch* b) { return (int)b->L.steps.size(); }
@@ -1806,8 +1838,15 @@ int fy_noise_batch_steps(const NoiseBatch* b) { return (int)b->L.steps.size(); }
 cudaError_t fy_noise_batch_launch(const NoiseBatch* b, const void* dev, cudaStream_t st) {
     const unsigned char* d = (const unsigned char*)dev;
     for (const auto& s : b->L.steps) {
+        unsigned total = 0;
+        for (unsigned g : s.gx) total += g;
+        const void* packs = d;
+        d += al256n(s.packs.size());
+        const void* prefix = d;
+        d += al256n((s.gx.size() + 1) * sizeof(unsigned));
+        int nvol = b->L.cubes;
         cudaLaunchConfig_t c = {};
-        c.gridDim = dim3(s.grid.x, s.grid.y, (unsigned)b->L.cubes);
+        c.gridDim = dim3(total, s.grid.y, 1);
         c.blockDim = s.block;
         c.dynamicSmemBytes = s.smem;
         c.stream = st;
@@ -1816,11 +1855,9 @@ cudaError_t fy_noise_batch_launch(const NoiseBatch* b, const void* dev, cudaStre
         at[0].val.programmaticStreamSerializationAllowed = 1;
         c.attrs = at;
         c.numAttrs = 1;
-        const void* arg = d;
-        void* args[1] = {(void*)&arg};
+        void* args[3] = {(void*)&packs, (void*)&prefix, (void*)&nvol};
         cudaError_t e = cudaLaunchKernelExC(&c, s.kern, args);
         if (e != cudaSuccess) return e;
-        d += (s.packs.size() + 255) & ~(size_t)255;
     }
     return cudaSuccess;
 }

@@ -244,8 +244,9 @@ const char *fy_gpu_last_error(void);
 void        fy_gpu_release(void);
 /* Launch counter: number of kernels this thread has launched (for measurement). */
 unsigned long long fy_gpu_kernel_launches(void);
-/* Number of bounded in-kernel waits (tensor-copy completions of the box passes) that gave
- * up since the library loaded on this device; the kernel then returned without finishing.
+/* Number of bounded in-kernel waits (tensor-copy completions of the box passes, bulk row
+ * copies of the deconvolution's first pass) that gave up since the library loaded on this
+ * device; the kernel then returned without finishing.
  * 0 in normal operation; -1 without a device. */
 int fy_gpu_kernel_timeouts(void);
 /* Failure-detection hook for tests; no reference counterpart. Sets the polls that each box
