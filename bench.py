@@ -158,12 +158,12 @@ def algorithmic_bytes(name: str, n: int, geo: dict) -> float | None:
 
 
 # DRAM bytes per voxel of each instrumented span: dram__bytes_read.sum + dram__bytes_write.sum
-# per launch from a one-pass ncu capture of this chain, divided by the voxels of the captured
-# cube (the spans' traffic grows with the voxel count).
+# per launch from an ncu capture of this chain on a 384^3 cube (the multi-metric capture runs
+# on the smaller cube; every span's traffic grows with the voxel count), divided by its voxels.
 DRAM_BYTES_PER_VOXEL = {
-    "deconv.x_fwd": 4.653, "deconv.y_fwd": 8.031, "deconv.z_weight": 8.290, "deconv.y_inv": 8.031,
-    "deconv.x_inv": 7.880, "noise.stats": 19.647, "noise.lohi": 4.402, "noise.bin_select": 23.931,
-    "guided": 15.938, "dering.accumulate+vote": 0.507,
+    "deconv.x_fwd": 4.035, "deconv.y_fwd": 7.549, "deconv.z_weight": 7.996, "deconv.y_inv": 7.544,
+    "deconv.x_inv": 7.493, "noise.stats": 19.093, "noise.lohi": 4.457, "noise.bin_select": 10.050,
+    "guided": 15.950,
 }
 
 
@@ -1176,7 +1176,7 @@ def main():
         tpv = DRAM_BYTES_PER_VOXEL.get(dom)
         roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                 "frac": ach / hbm_peak, "traffic": tpv * n if tpv is not None and SHAPE == (512, 512, 512) else None,
-                "traffic_source": "ncu one-pass DRAM capture of the chain, bytes per voxel x voxels",
+                "traffic_source": "ncu DRAM capture of the chain on a 384^3 cube, bytes per voxel x voxels",
                 "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": algorithmic_bytes(dom, n, geo)}
 
