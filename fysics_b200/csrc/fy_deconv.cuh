@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_inv(const float2* __restrict
     const int hi_max = g.px - g.hx;                 // m in [1, px-hx] mirrors to px-m
     // kU rows' elements per thread are loaded before any is stored, so that many loads are in
     // flight per thread while the CTA waits for its tile
-    constexpr int kU = 4;
+    constexpr int kU = 8;
     const int total = W * g.hx, step = blockDim.x;
     for (int base = threadIdx.x; base < total; base += kU * step) {
         float2 A[kU], B[kU];

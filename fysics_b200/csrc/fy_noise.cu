@@ -816,10 +816,22 @@ FY_D void k_win_count(const float* __restrict__ mean, NoiseCtl* __restrict__ ctl
     const long long chunk = (long long)SU * 256;
     long long base = (long long)vbx() * chunk;
     const long long stride = (long long)vgx() * chunk;        // read once: the loop body has syncs
+    // the next chunk's keys are loaded before this chunk's are used, so a warp keeps its loads
+    // in flight while it classifies
+    float4 xn[SU];
+    if (base + chunk <= n4f) {
+#pragma unroll
+        for (int u = 0; u < SU; ++u) xn[u] = __ldg(reinterpret_cast<const float4*>(mean) + base + t + (long long)u * 256);
+    }
     for (; base + chunk <= n4f; base += stride) {
         float4 x[SU];
 #pragma unroll
-        for (int u = 0; u < SU; ++u) x[u] = __ldg(reinterpret_cast<const float4*>(mean) + base + t + (long long)u * 256);
+        for (int u = 0; u < SU; ++u) x[u] = xn[u];
+        if (base + stride + chunk <= n4f) {
+#pragma unroll
+            for (int u = 0; u < SU; ++u)
+                xn[u] = __ldg(reinterpret_cast<const float4*>(mean) + base + stride + t + (long long)u * 256);
+        }
         float mv[4 * SU];
         unsigned m0 = 0, m1 = 0;
 #pragma unroll
@@ -1152,6 +1164,7 @@ FY_D void k_bwin_count(const float* __restrict__ mean, const float* __restrict__
     __shared__ unsigned int lc[256 * kLaneRow];          // per-lane counters
     __shared__ float fe[NB + 1];
     __shared__ uint32_t swl[NB], swh[NB];
+    __shared__ float4 stab[NB];                          // per bin: its edges and its window
     __shared__ unsigned int sc[NB * 3];
     __shared__ int s_bad;
     if (ctl->mode != kModeBinWin) return;
@@ -1159,8 +1172,10 @@ FY_D void k_bwin_count(const float* __restrict__ mean, const float* __restrict__
     const int t = threadIdx.x, lane = t & 31;
     if (t <= NB) fe[t] = ctl->fedge[t];
     if (t < NB) {
-        swl[t] = ctl->bwlo[t];
-        swh[t] = ctl->bwhi[t];
+        const uint32_t wl = ctl->bwlo[t], wh = ctl->bwhi[t];
+        swl[t] = wl;
+        swh[t] = wh;
+        stab[t] = make_float4(ctl->fedge[t], ctl->fedge[t + 1], __uint_as_float(wl), __uint_as_float(wh));
     }
     for (int i = t; i < NB * 3; i += blockDim.x) sc[i] = 0;
     for (int i = t; i < 256 * kLaneRow; i += blockDim.x) lc[i] = 0;
@@ -1172,16 +1187,24 @@ FY_D void k_bwin_count(const float* __restrict__ mean, const float* __restrict__
     wc.v = bufv[t >> 5];
     wc.l = bufl[t >> 5];
     bool bad = false;
-    // bin (or -1 outside every bin) and whether the key is inside the bin's window
+    // bin (or -1 outside every bin) and whether the key is inside the bin's window. One
+    // 16-byte lookup gives the guessed bin's edges and window; when the mean lies outside the
+    // guess (rare: rounding at an edge), one step to the neighbour and the exact-membership
+    // check of the step run as before.
     auto classify = [&](float m, float v, bool valid, int& bo, bool& inside) {
         const bool inr = valid && m >= lo_e && m < hi_e;
         const float mc = inr ? m : lo_e;
         int b = (int)((mc - lo_e) * fscale);
         b = b < 0 ? 0 : (b > NB - 1 ? NB - 1 : b);
-        b = b - (int)(mc < fe[b]) + (int)(mc >= fe[b + 1]);
-        bad |= !(mc >= fe[b] && mc < fe[b + 1]);
+        const float4 e = stab[b];
+        uint32_t wl = __float_as_uint(e.z), wh = __float_as_uint(e.w);
+        if (!(mc >= e.x && mc < e.y)) {
+            b = b - (int)(mc < e.x) + (int)(mc >= e.y);
+            bad |= !(mc >= fe[b] && mc < fe[b + 1]);
+            wl = swl[b];
+            wh = swh[b];
+        }
         const uint32_t k = fkey(v);
-        const uint32_t wl = swl[b], wh = swh[b];
         row[b] += inr ? (k < wl ? 0x10001u : 1u) : 0u;
         inside = inr && k >= wl && k <= wh;
         bo = b;
@@ -1686,7 +1709,7 @@ cudaError_t noise_sequence(NoiseLaunch& L, const float* in, int nz, int ny, int 
     // window misses
     RUN(256, 1, k_win_sample, 64, 256, 0, mean, ctl, sm, m, wa, wb);
     RUN(kBoundThreads, 1, k_win_bounds, dim3(2, 2), kBoundThreads, smem_keys, sm, ctl, m);
-    RUN(256, 4, k_win_count, g, 256, 0, mean, ctl, cval, clab, Lay.cap);
+    RUN(256, 3, k_win_count, g, 256, 0, mean, ctl, cval, clab, Lay.cap);
     RUN(32, 1, k_win_arm, 1, 1, 0, ctl, cc, Lay.cap);
     for (int sh = 24; sh >= 0; sh -= 8) {
         // the first digit's histogram sets the ranks (k_win_targets) before its scan; the
