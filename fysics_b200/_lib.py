@@ -244,6 +244,7 @@ SIGNATURES = {
     "fy_gpu_profile_start": (_i, [_i, _P]),
     "fy_gpu_profile_stop": (_i, []),
     "fy_gpu_profile_read": (_i, [_i, C.POINTER(C.c_char_p), C.POINTER(C.c_float)]),
+    "fy_gpu_profile_select": (_i, [C.c_char_p]),
     "fy_gpu_phase_correlate_batch": (_i, [_P, _P, _i, _i, _i, _i, _i, _P, _PDBL, _PDBL,
                                           C.POINTER(C.c_longlong), C.POINTER(_i), _P]),
 }

@@ -6,6 +6,7 @@
 #include <stdlib.h>
 #include <map>
 #include <mutex>
+#include <string>
 #include <vector>
 
 namespace fy {
@@ -192,6 +193,7 @@ struct Prof {
     int n = 0;
     std::vector<cudaEvent_t> ev;
     std::vector<const char*> names;
+    std::vector<std::string> only;      // marks to record (empty: all)
 };
 static thread_local Prof t_prof;
 
@@ -200,6 +202,11 @@ static thread_local Prof t_prof;
 void fy_prof_mark(cudaStream_t st, const char* name) {
     fy::Prof& P = fy::t_prof;
     if (!P.on || P.n >= (int)P.ev.size()) return;
+    if (P.n > 0 && !P.only.empty()) {              // mark 0 is the origin
+        bool keep = false;
+        for (const std::string& o : P.only) keep = keep || o == name;
+        if (!keep) return;
+    }
     if (cudaEventRecord(P.ev[(size_t)P.n], st) == cudaSuccess) P.names[(size_t)P.n++] = name;
 }
 
@@ -220,6 +227,22 @@ int fy_gpu_profile_start(int capacity, void* stream) {
     P.n = 0;
     P.on = true;
     fy_prof_mark((cudaStream_t)stream, "start");
+    return FY_OK;
+}
+int fy_gpu_profile_select(const char* names) {
+    fy::Prof& P = fy::t_prof;
+    P.only.clear();
+    if (!names) return FY_OK;
+    std::string cur;
+    for (const char* c = names;; ++c) {
+        if (*c == ',' || *c == 0) {
+            if (!cur.empty()) P.only.push_back(cur);
+            cur.clear();
+            if (*c == 0) break;
+        } else if (*c != ' ') {
+            cur.push_back(*c);
+        }
+    }
     return FY_OK;
 }
 int fy_gpu_profile_stop(void) {

@@ -202,42 +202,69 @@ constexpr int kCompactBuf = 1152;        // per warp: one step's worst case (32 
 // equal to the selected key and, after the last digit, the next non-empty bucket (the
 // smallest key above the selected one within the prefix; k_sel_next scans only when there is
 // none). The histogram is read through L2 (other CTAs' atomics) and cleared.
-FY_D void warp_scan_target(NoiseCtl* ctl, int t, int db, bool last) {
+// With at most 8 buckets per lane (8-bit digits) the lane's buckets stay in registers: one
+// round of loads (with the target's rank and prefix) instead of one per reading.
+template <int DB>
+FY_D void warp_scan_target(NoiseCtl* ctl, int t, bool last) {
+    constexpr int nbk = 1 << DB, per = nbk / 32;
+    constexpr bool REG = per <= 8;
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const int nbk = 1 << db, per = nbk / 32;
     unsigned int* h = ctl->hist + (size_t)t * nbk;
     const int b0 = lane * per;
+    const long long r = ctl->trank[t];
+    const uint32_t pre = ctl->tprefix[t];
+    unsigned int hv[REG ? per : 1];
     unsigned long long mine = 0;
-    for (int b = b0; b < b0 + per; ++b) mine += __ldcg(h + b);
+    if (REG) {
+#pragma unroll
+        for (int i = 0; i < (REG ? per : 1); ++i) hv[i] = __ldcg(h + b0 + i);
+#pragma unroll
+        for (int i = 0; i < (REG ? per : 1); ++i) mine += hv[i];
+    } else {
+        for (int b = b0; b < b0 + per; ++b) mine += __ldcg(h + b);
+    }
     unsigned long long incl = mine;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const unsigned long long y = __shfl_up_sync(full, incl, o);
         if (lane >= o) incl += y;
     }
-    const long long r = ctl->trank[t];
     const unsigned long long before = incl - mine;
     unsigned int sel = (unsigned)nbk;
     if ((unsigned long long)r >= before && (unsigned long long)r < incl) {
         unsigned long long acc = before;
-        for (int b = b0; b < b0 + per; ++b) {
-            const unsigned int hb = __ldcg(h + b);
-            if (acc + hb > (unsigned long long)r) {
-                ctl->trank[t] = r - (long long)acc;
-                ctl->tprefix[t] = (ctl->tprefix[t] << db) | (uint32_t)b;
-                if (last) ctl->teq[t] = hb;
-                sel = (unsigned)b;
-                break;
+        unsigned int hsel = 0;
+        if (REG) {
+#pragma unroll
+            for (int i = 0; i < (REG ? per : 1); ++i) {
+                if (sel == (unsigned)nbk && acc + hv[i] > (unsigned long long)r) { sel = (unsigned)(b0 + i); hsel = hv[i]; }
+                else if (sel == (unsigned)nbk) acc += hv[i];
             }
-            acc += hb;
+        } else {
+            for (int b = b0; b < b0 + per; ++b) {
+                const unsigned int hb = __ldcg(h + b);
+                if (acc + hb > (unsigned long long)r) { sel = (unsigned)b; hsel = hb; break; }
+                acc += hb;
+            }
+        }
+        if (sel != (unsigned)nbk) {
+            ctl->trank[t] = r - (long long)acc;
+            ctl->tprefix[t] = (pre << DB) | sel;
+            if (last) ctl->teq[t] = hsel;
         }
     }
     sel = __reduce_min_sync(full, sel);
     unsigned int nextb = 0xffffffffu;
     if (last) {
-        for (int b = b0 > (int)sel + 1 ? b0 : (int)sel + 1; b < b0 + per; ++b)
-            if (__ldcg(h + b)) { nextb = (unsigned)b; break; }
+        if (REG) {
+#pragma unroll
+            for (int i = (REG ? per : 1) - 1; i >= 0; --i)
+                if (b0 + i > (int)sel && hv[i]) nextb = (unsigned)(b0 + i);
+        } else {
+            for (int b = b0 > (int)sel + 1 ? b0 : (int)sel + 1; b < b0 + per; ++b)
+                if (__ldcg(h + b)) { nextb = (unsigned)b; break; }
+        }
         nextb = __reduce_min_sync(full, nextb);
     }
     __syncwarp();
@@ -245,7 +272,7 @@ FY_D void warp_scan_target(NoiseCtl* ctl, int t, int db, bool last) {
     __syncwarp();
     if (last && lane == 0) {
         ctl->tneed_next[t] = (ctl->trank[t] + 1 >= (long long)ctl->teq[t]) && (ctl->tk[t] + 1 < ctl->tgroup_n[t]);
-        ctl->tnext[t] = nextb != 0xffffffffu ? ((ctl->tprefix[t] >> db) << db) | nextb : 0xffffffffu;
+        ctl->tnext[t] = nextb != 0xffffffffu ? ((ctl->tprefix[t] >> DB) << DB) | nextb : 0xffffffffu;
     }
 }
 template <int DB, int MODE, bool LABEL = false, bool COMPACT = false>
@@ -401,7 +428,7 @@ FY_D void k_sel_hist(const float* __restrict__ mean, const float* __restrict__ v
     if (!s_last) return;
     __threadfence();
     for (int t = threadIdx.x >> 5; t < nt; t += blockDim.x >> 5)
-        if (ctl->tactive[t]) warp_scan_target(ctl, t, DB, scan == 1);
+        if (ctl->tactive[t]) warp_scan_target<DB>(ctl, t, scan == 1);
     if (threadIdx.x == 0) ctl->done_ctas = 0;
 }
 

@@ -558,6 +558,10 @@ void fy_server_destroy(fy_server *s);
 int fy_gpu_profile_start(int capacity, void *stream);
 int fy_gpu_profile_stop(void);
 int fy_gpu_profile_read(int i, const char **name, float *ms);
+/* Record only the marks named in `names` (comma-separated, e.g. "noise,guided"; each mark's
+ * span then runs from the previous recorded mark); NULL or "" records every mark. Each event
+ * between two launches costs the pair its overlap, so a timed loop records few. */
+int fy_gpu_profile_select(const char *names);
 
 #ifdef __cplusplus
 }
