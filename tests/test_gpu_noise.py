@@ -153,8 +153,23 @@ def test_noise_windows_equal_radix_paths(gpu, shape, win, pct):
     sample-guided windows (one pass over the means, one over mean and variance) or the radix
     passes over the whole field find the 1st/99th mean percentiles and the per-bin variance
     percentiles; and on such volumes the windows are the path that normally runs."""
+    _windows_vs_radix(gpu, _paths_volume(shape, sum(shape) + win), win, pct)
+
+
+def test_noise_window_across_zero(gpu):
+    """Means whose 1st percentile lies at 0: that window holds keys of both signs, a range of
+    ~2^31 keys, so its candidates take all four offset digit passes (a narrow window takes
+    two). The windows must still hold and equal the radix paths bit for bit."""
+    rng = np.random.default_rng(23)
+    vol = (1.0 + 0.1 * rng.standard_normal((96, 96, 96))).astype(np.float32)
+    # a zero-mean slab: the means of its two middle planes (2.1% of the voxels, all of their
+    # windows inside it) are the lowest, so the 1st percentile is about their median, 0
+    vol[40:46] = rng.standard_normal((6, 96, 96)).astype(np.float32)
+    _windows_vs_radix(gpu, vol, 5, 10.0)
+
+
+def _windows_vs_radix(gpu, vol, win, pct):
     lib = gpu.load()
-    vol = _paths_volume(shape, sum(shape) + win)
     used = C.c_int(-1)
     try:
         assert lib.fy_gpu_test_noise_paths(0, C.byref(used)) == 0
