@@ -247,19 +247,16 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_z_weight(float2* __restrict__ 
     float2* s = reinterpret_cast<float2*>(smem4);
     float2* stw = s + pl.n * W;
     double* sfz = reinterpret_cast<double*>(stw + pl.n);
-    float* slut = reinterpret_cast<float*>(sfz + pl.n);
+    double2* syx = reinterpret_cast<double2*>(sfz + pl.n);    // per column (fy^2, fx^2)
     const Lane ln(wlog);
     const int c0 = blockIdx.x * W;
     const size_t zstride = (size_t)g.py * g.hxp;
     float2* col = spec + (size_t)blockIdx.y * g.hxp + c0 + ln.l;
     load_twiddles(stw, tw, pl.n);
     for (int i = threadIdx.x; i < pl.n; i += blockDim.x) sfz[i] = fz2[i];
-    // the table as 16-byte loads (the device table holds FY_LUT_N + 4 floats)
-    if ((reinterpret_cast<uintptr_t>(slut) & 15) == 0) {
-        for (int i = threadIdx.x; i < (FY_LUT_N + 4) / 4; i += blockDim.x)
-            reinterpret_cast<float4*>(slut)[i] = __ldg(reinterpret_cast<const float4*>(lut) + i);
-    } else {
-        for (int i = threadIdx.x; i <= FY_LUT_N; i += blockDim.x) slut[i] = lut[i];
+    for (int i = threadIdx.x; i < W; i += blockDim.x) {
+        const bool in = c0 + i < g.hx;
+        syx[i] = make_double2(in ? fy2[blockIdx.y] : 0.0, in ? __ldg(fx2 + c0 + i) : 0.0);
     }
     __syncthreads();
     fft_line<N, E, ct_pitch(N), -1>(s + ln.l, W, ln.tl, pl, stw,
@@ -269,22 +266,20 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_z_weight(float2* __restrict__ 
                 },
                 [&](int z, float2 v) { s[z * W + ln.l] = v; });
     __syncthreads();
-    {   // weight: the same W-column slot for every element this thread touches
-        const int k = c0 + ln.l;
-        const double fyx = k < g.hx ? fy2[blockIdx.y] : 0.0;
-        const double fxx = k < g.hx ? __ldg(fx2 + k) : 0.0;
-        for (int z = ln.tl; z < pl.n; z += blockDim.x >> wlog) {
-            const double t = ((sfz[z] + fyx) + fxx) * us;    // paganin.c:234-236
-            int ti = (int)t;
-            if (ti >= FY_LUT_N) ti = FY_LUT_N - 1;
-            const float w = slut[ti] + (slut[ti + 1] - slut[ti]) * (float)(t - ti);
-            const float2 v = s[z * W + ln.l];
-            s[z * W + ln.l] = make_float2(v.x * w, v.y * w);
-        }
-    }
-    __syncthreads();
+    // the weight of each point is applied as the inverse transform's first pass reads it (the
+    // thread's own column, every point once), so the weighted tile needs no separate pass
     fft_line<N, E, ct_pitch(N), +1>(s + ln.l, W, ln.tl, pl, stw,
-                [&](int i) { return s[i * W + ln.l]; },
+                [&](int i) {
+                    const float2 v = s[i * W + ln.l];
+                    const double2 yx = syx[ln.l];
+                    const double t = ((sfz[i] + yx.x) + yx.y) * us;  // paganin.c:234-236
+                    int ti = (int)t;
+                    if (ti >= FY_LUT_N) ti = FY_LUT_N - 1;
+                    // the table (16 KB, read-only) through L1 rather than copied per tile
+                    const float l0 = __ldg(lut + ti), l1 = __ldg(lut + ti + 1);
+                    const float w = l0 + (l1 - l0) * (float)(t - ti);
+                    return make_float2(v.x * w, v.y * w);
+                },
                 [&](int z, float2 v) { if (z < g.nz) col[(size_t)z * zstride] = v; });
 }
 
@@ -444,7 +439,7 @@ cudaError_t fy_deconv_pass(int pass, const DeconvLaunch& d, cudaStream_t st) {
     case 3: {   // Z forward, weight, Z inverse
         const TileShape t = fy_tile_shape(g.pz);
         const size_t smem = (size_t)g.pz * t.W * sizeof(float2) + (size_t)g.pz * sizeof(float2) +
-                            (size_t)g.pz * sizeof(double) + (FY_LUT_N + 4) * sizeof(float);
+                            (size_t)g.pz * sizeof(double) + (size_t)t.W * sizeof(double2);
         dim3 grid(ceil_div_i(g.hx, t.W), g.py);
         return with_e(g.pz, [&](auto ec) -> cudaError_t {
             constexpr int E = decltype(ec)::value;
