@@ -32,6 +32,29 @@ FY_D void fft_line(float2* __restrict__ sline, int ps, int tl, const FftPlan& pl
 }
 // Threads per CTA never exceed W*n/E: 512 for 2^k lines (E=16), 256 for 3*2^k (E=24).
 template <int E> struct KB { static constexpr int nt = (E % 3 == 0) ? 256 : 512; };
+// Lines per tile of a column pass with a compile-time length N: the FFT core's tile
+// (ct_tile_lines; N = 0: the runtime plan's, fy_tile_shape), or with NARROW 8 lines of 512
+// points (256 threads, four CTAs per SM), so one CTA's loads overlap three others' transforms.
+// Measured at 512^3: the forward Y pass 266 -> 253 us narrow; the inverse Y pass unchanged;
+// the Z pass 426 -> 466 us (its transform pair per tile keeps the SM busy either way).
+template <int N, int E, bool NARROW> struct YZ {
+    static constexpr bool on = NARROW && N == 512;
+    static constexpr int lines = on ? 8 : ct_pitch(N);
+    static constexpr int nt = on ? 256 : KB<E>::nt;
+    static constexpr int minb = on ? 4 : 2;
+};
+template <int N, bool NARROW> TileShape yz_tile_shape(int n) {
+    if constexpr (YZ<N, 16, NARROW>::on) {
+        TileShape t;
+        t.W = YZ<N, 16, NARROW>::lines;
+        t.wlog = fy_log2i(t.W);
+        t.E = 16;
+        t.NT = t.W * N / t.E;
+        return t;
+    } else {
+        return fy_tile_shape(n);
+    }
+}
 
 
 // Thread -> (line l, thread-in-line tl) with the line index fastest.
@@ -211,7 +234,7 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_x_fwd(const T* __restrict__ sr
 // straight from global memory (W consecutive columns = one 8W-byte run per point);
 // rows >= ny are the reflected (or zero) rows.
 template <int N, int E>
-__global__ void __launch_bounds__(KB<E>::nt, 2) k_y_fwd(float2* __restrict__ spec, SpecGeom g, const __grid_constant__ FftPlan pl,
+__global__ void __launch_bounds__(YZ<N, E, true>::nt, YZ<N, E, true>::minb) k_y_fwd(float2* __restrict__ spec, SpecGeom g, const __grid_constant__ FftPlan pl,
                                                  const float2* __restrict__ tw, int wlog) {
     fy_pdl_wait();
     extern __shared__ float4 smem4[];
@@ -222,7 +245,7 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_y_fwd(float2* __restrict__ spe
     float2* col = spec + (size_t)blockIdx.y * g.py * g.hxp + blockIdx.x * W + ln.l;
     load_twiddles(stw, tw, pl.n);
     __syncthreads();
-    fft_line<N, E, ct_pitch(N), -1>(s + ln.l, W, ln.tl, pl, stw,
+    fft_line<N, E, YZ<N, E, true>::lines, -1>(s + ln.l, W, ln.tl, pl, stw,
                 [&](int i) {
                     const int ys = i < g.ny ? i : (g.zero_pad ? -1 : reflect_idx(i, g.ny));
                     return ys < 0 ? make_float2(0.f, 0.f) : col[(size_t)ys * g.hxp];
@@ -414,7 +437,7 @@ cudaError_t fy_deconv_pass(int pass, const DeconvLaunch& d, cudaStream_t st) {
     }
     case 2:     // Y forward over the stored planes
     case 4: {   // Y inverse, keep rows < ny
-        const TileShape t = fy_tile_shape(g.py);
+        const TileShape t = pass == 2 ? yz_tile_shape<N, true>(g.py) : yz_tile_shape<N, false>(g.py);
         const size_t smem = (size_t)g.py * t.W * sizeof(float2) + (size_t)g.py * sizeof(float2);
         dim3 grid(ceil_div_i(g.hx, t.W), g.nz);
         return with_e(g.py, [&](auto ec) -> cudaError_t {
