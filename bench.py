@@ -157,17 +157,19 @@ def algorithmic_bytes(name: str, n: int, geo: dict) -> float | None:
     return table.get(name)
 
 
-# DRAM bytes per voxel of each instrumented span: dram__bytes_read.sum + dram__bytes_write.sum
-# per launch from an ncu capture of this chain on a 384^3 cube (the multi-metric capture runs
-# on the smaller cube; every span's traffic grows with the voxel count), divided by its voxels.
 # marks recorded inside the timed loop: "noise" closes the span before the guided output pass,
 # "guided" closes the pass itself (the dominant kernel of the chain)
 TIMED_MARKS = "noise,guided"
 
+# DRAM bytes per voxel of each instrumented span: dram__bytes_read.sum + dram__bytes_write.sum
+# of its kernel's launch in an ncu capture of this chain on a 384^3 cube (one kernel per
+# capture, on the smaller cube; every span's traffic grows with the voxel count), divided by
+# its voxels. The two selection spans give their counting pass only: their other launches
+# run over candidate lists of a few percent of the voxels.
 DRAM_BYTES_PER_VOXEL = {
-    "deconv.x_fwd": 4.035, "deconv.y_fwd": 7.549, "deconv.z_weight": 7.996, "deconv.y_inv": 7.544,
-    "deconv.x_inv": 7.493, "noise.stats": 19.093, "noise.lohi": 4.457, "noise.bin_select": 10.050,
-    "guided": 15.950,
+    "deconv.x_fwd": 4.087, "deconv.y_fwd": 7.599, "deconv.z_weight": 8.198, "deconv.y_inv": 7.602,
+    "deconv.x_inv": 7.539, "noise.stats": 19.142, "noise.lohi": 4.108, "noise.bin_select": 8.227,
+    "guided": 15.954,
 }
 
 
