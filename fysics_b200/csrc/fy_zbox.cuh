@@ -47,6 +47,7 @@
 #pragma once
 #include <cuda.h>
 #include <mutex>
+#include <type_traits>
 #include "fy_internal.h"
 
 namespace fyzb {
@@ -336,61 +337,79 @@ FY_D bool zbox_tile(const Params& p, const TmaRef& tm, int bx, int by, int bz, u
             }
             const float* sp = stage + slot * G::STAGE;
             const bool zin = zi >= 0 && zi < nz;
-            // X phase, every staged row (the TY output rows and the 2R halo rows): one item = 4
-            // output columns of one row, P[j] = both quantities of staged column x0 - 4 + x4 + j.
+            // X phase, every staged row (the TY output rows and the 2R halo rows): an item is IW
+            // output columns of one row starting at xs, P[j] = both quantities of staged column
+            // x0 - 4 + xs + j. Each thread takes one 4-column item; the 2R halo rows' 4-column
+            // items left over are split into 2-column halves spread over the first threads, so
+            // the phase that gates the plane's barrier costs 1.5 item times instead of 2.
             // (One-column items for the halo rows cost (2R+1) taps' conversions per output
-            // instead of (4+2R)/4; 4-column items keep the same taps in the same order.)
-            for (int it = t; it < G::SY * (TX / 4); it += NT) {
-                const int yy = it >> 4, x4 = (it & 15) << 2;
+            // instead of (4+2R)/4; every split keeps the same taps in the same order.)
+            auto xitem = [&](auto wc, int yy, int xs) {
+                constexpr int IW = decltype(wc)::value;
                 float2 P[12];
                 if (C == 2) {                    // interleaved pairs: float4 = two columns
-                    const float* row = sp + yy * G::RW + 2 * x4;
+                    const float* row = sp + yy * G::RW + 2 * xs;
 #pragma unroll
-                    for (int j2 = (4 - R) / 2; j2 <= (7 + R) / 2; ++j2) {
+                    for (int j2 = (4 - R) / 2; j2 <= (IW + 3 + R) / 2; ++j2) {
                         const float4 v = *reinterpret_cast<const float4*>(row + 4 * j2);
                         P[2 * j2] = make_float2(v.x, v.y);
                         P[2 * j2 + 1] = make_float2(v.z, v.w);
                     }
                     if (KIND == ZB_GUIDED_OUT_MV) {          // (mean, var) -> (a, b)
 #pragma unroll
-                        for (int j = 4 - R; j < 8 + R; ++j) P[j] = guided_ab(P[j], eps);
+                        for (int j = 4 - R; j < IW + 4 + R; ++j) P[j] = guided_ab(P[j], eps);
                     }
                 } else {
-                    const float* row = sp + yy * G::RW + x4;
+                    const float* row = sp + yy * G::RW + xs;
                     float q1[12];
+                    if (IW == 4) {                   // xs a multiple of 4: 16-byte loads
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        const float4 v = *reinterpret_cast<const float4*>(row + 4 * j);
-                        q1[4 * j] = v.x; q1[4 * j + 1] = v.y; q1[4 * j + 2] = v.z; q1[4 * j + 3] = v.w;
+                        for (int j = 0; j < 3; ++j) {
+                            const float4 v = *reinterpret_cast<const float4*>(row + 4 * j);
+                            q1[4 * j] = v.x; q1[4 * j + 1] = v.y; q1[4 * j + 2] = v.z; q1[4 * j + 3] = v.w;
+                        }
+                    } else {                         // xs even: 8-byte loads
+#pragma unroll
+                        for (int j = (4 - R) & ~1; j < IW + 4 + R; j += 2) {
+                            const float2 v = *reinterpret_cast<const float2*>(row + j);
+                            q1[j] = v.x; q1[j + 1] = v.y;
+                        }
                     }
                     const int gy = y0 - R + yy;
                     const bool rin = zin && gy >= 0 && gy < ny;
                     if (cols_in) {
                         const float cs = rin ? c : 0.f;           // outside rows were staged as 0
 #pragma unroll
-                        for (int j = 4 - R; j < 8 + R; ++j) q1[j] = q1[j] - cs;
+                        for (int j = 4 - R; j < IW + 4 + R; ++j) q1[j] = q1[j] - cs;
                     } else {
 #pragma unroll
-                        for (int j = 4 - R; j < 8 + R; ++j) {
-                            const int gxj = x0 - 4 + x4 + j;
+                        for (int j = 4 - R; j < IW + 4 + R; ++j) {
+                            const int gxj = x0 - 4 + xs + j;
                             q1[j] = (rin && gxj >= 0 && gxj < nx) ? q1[j] - c : 0.f;
                         }
                     }
 #pragma unroll
-                    for (int j = 4 - R; j < 8 + R; ++j) P[j] = make_float2(q1[j], q1[j] * q1[j]);
+                    for (int j = 4 - R; j < IW + 4 + R; ++j) P[j] = make_float2(q1[j], q1[j] * q1[j]);
                 }
-                float2 o[4];
+                float2 o[IW];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < IW; ++k) {
                     float2 sm = P[4 + k - R];
 #pragma unroll
                     for (int j = 5 + k - R; j <= 4 + k + R; ++j) sm = add2(sm, P[j]);
-                    if (out_kind(KIND)) sm = mul2(sm, rx[x4 + k]);
+                    if (out_kind(KIND)) sm = mul2(sm, rx[xs + k]);
                     o[k] = sm;
                 }
-                float4* dst = reinterpret_cast<float4*>(xcur + yy * TX + x4);
-                dst[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
-                dst[1] = make_float4(o[2].x, o[2].y, o[3].x, o[3].y);
+                float4* dst = reinterpret_cast<float4*>(xcur + yy * TX + xs);
+#pragma unroll
+                for (int k2 = 0; k2 < IW / 2; ++k2) dst[k2] = make_float4(o[2 * k2].x, o[2 * k2].y, o[2 * k2 + 1].x, o[2 * k2 + 1].y);
+            };
+            constexpr int NITEM = G::SY * (TX / 4), NHALF = 2 * (NITEM - NT);
+            static_assert(NITEM >= NT && NHALF <= NT, "one full and at most one half item per thread");
+            xitem(std::integral_constant<int, 4>{}, t >> 4, (t & 15) << 2);
+            if (t < NHALF) {
+                const int it = NT + (t >> 1);
+                xitem(std::integral_constant<int, 2>{}, it >> 4, ((it & 15) << 2) + 2 * (t & 1));
             }
             if (TMA) {
                 if (__syncthreads_or(!ok)) {      // plane zi never landed: flag, drain, return
