@@ -30,6 +30,25 @@ FY_D void fft_line(float2* __restrict__ sline, int ps, int tl, const FftPlan& pl
     if constexpr (N > 0) line_fft_ct<N, E, PS, SIGN>(sline, tl, tw, ld, st);
     else line_fft<E>(sline, ps, tl, pl, tw, (float)SIGN, ld, st);
 }
+// A column pass's transform whose first pass reads global memory: with a compile-time plan
+// the first pass's loads are issued before `prologue` fills the tile's shared tables, so the
+// two latencies overlap and one barrier covers both (the runtime plan: prologue, barrier,
+// transform, as before).
+template <int N, int E, int PS, int SIGN, class LD, class PRO, class ST>
+FY_D void fft_line_pre(float2* __restrict__ sline, int ps, int tl, const FftPlan& pl, const float2* __restrict__ tw,
+                       LD ld, PRO prologue, ST st) {
+    if constexpr (N > 0) {
+        float2 v[E];
+        ct_load<N, E, ct_radix(N, 0), PS>(v, tl, ld);
+        prologue();
+        __syncthreads();
+        ct_passes<N, E, PS, SIGN, 0>(v, sline, tl, tw, st);
+    } else {
+        prologue();
+        __syncthreads();
+        line_fft<E>(sline, ps, tl, pl, tw, (float)SIGN, ld, st);
+    }
+}
 // Threads per CTA never exceed W*n/E: 512 for 2^k lines (E=16), 256 for 3*2^k (E=24).
 template <int E> struct KB { static constexpr int nt = (E % 3 == 0) ? 256 : 512; };
 // Lines per tile of a column pass with a compile-time length N: the FFT core's tile
@@ -243,13 +262,12 @@ __global__ void __launch_bounds__(YZ<N, E, true>::nt, YZ<N, E, true>::minb) k_y_
     float2* stw = s + pl.n * W;
     const Lane ln(wlog);
     float2* col = spec + (size_t)blockIdx.y * g.py * g.hxp + blockIdx.x * W + ln.l;
-    load_twiddles(stw, tw, pl.n);
-    __syncthreads();
-    fft_line<N, E, YZ<N, E, true>::lines, -1>(s + ln.l, W, ln.tl, pl, stw,
+    fft_line_pre<N, E, YZ<N, E, true>::lines, -1>(s + ln.l, W, ln.tl, pl, stw,
                 [&](int i) {
                     const int ys = i < g.ny ? i : (g.zero_pad ? -1 : reflect_idx(i, g.ny));
                     return ys < 0 ? make_float2(0.f, 0.f) : col[(size_t)ys * g.hxp];
                 },
+                [&]() { load_twiddles(stw, tw, pl.n); },
                 [&](int i, float2 v) { col[(size_t)i * g.hxp] = v; });
 }
 
@@ -275,6 +293,7 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_z_weight(float2* __restrict__ 
     const int c0 = blockIdx.x * W;
     const size_t zstride = (size_t)g.py * g.hxp;
     float2* col = spec + (size_t)blockIdx.y * g.hxp + c0 + ln.l;
+    // (issuing the first loads before these tables, as the Y passes do, measured 424 -> 434 us)
     load_twiddles(stw, tw, pl.n);
     for (int i = threadIdx.x; i < pl.n; i += blockDim.x) sfz[i] = fz2[i];
     for (int i = threadIdx.x; i < W; i += blockDim.x) {
@@ -317,10 +336,9 @@ __global__ void __launch_bounds__(KB<E>::nt, 2) k_y_inv(float2* __restrict__ spe
     float2* stw = s + pl.n * W;
     const Lane ln(wlog);
     float2* col = spec + (size_t)blockIdx.y * g.py * g.hxp + blockIdx.x * W + ln.l;
-    load_twiddles(stw, tw, pl.n);
-    __syncthreads();
-    fft_line<N, E, ct_pitch(N), +1>(s + ln.l, W, ln.tl, pl, stw,
+    fft_line_pre<N, E, ct_pitch(N), +1>(s + ln.l, W, ln.tl, pl, stw,
                 [&](int i) { return col[(size_t)i * g.hxp]; },
+                [&]() { load_twiddles(stw, tw, pl.n); },
                 [&](int i, float2 v) { if (i < keep_rows) col[(size_t)i * g.hxp] = v; });
 }
 
